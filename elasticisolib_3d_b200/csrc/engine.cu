@@ -1,0 +1,952 @@
+// Engine: device memory, time loops and checkpointing of the elastic 3D
+// propagation path.  Per-shot loops restate the reference drivers
+//   propElasticFwdGpu_3D / propElasticAdjGpu_3D (nonlinearPropElasticGpuFunctions_3D.cu:876-975, :1298-1395)
+//   BornElasticFwdGpu_3D / BornElasticAdjGpu_3D (BornElasticGpuFunctions_3D.cu:1226-1461, :2103-2336)
+// with three B200 changes: the sponge is fused into the stepper, all signals
+// live on the device time-major for coalesced injection/recording, and the
+// Born source-side velocity is never sent to host memory (the forward Born
+// runs the source propagation two coarse blocks ahead of the scattered one;
+// the adjoint Born recomputes it per segment from on-device checkpoints).
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
+#include "engine.h"
+#include "kernels.cuh"
+
+namespace e3d {
+
+static thread_local std::string g_err;
+void setLastError(const char* msg, const char* file, int line) {
+  char buf[512];
+  snprintf(buf, sizeof(buf), "%s (%s:%d)", msg, file, line);
+  g_err = buf;
+}
+const char* lastError() { return g_err.c_str(); }
+
+#define E3D_ARG(cond, msg)                        \
+  do {                                            \
+    if (!(cond)) {                                \
+      setLastError(msg, __FILE__, __LINE__);      \
+      return E3D_ERR_ARG;                         \
+    }                                             \
+  } while (0)
+
+#define E3D_RET(expr)               \
+  do {                              \
+    int _s = (expr);                \
+    if (_s != E3D_OK) return _s;    \
+  } while (0)
+
+#define E3D_LAUNCH_CHECK() E3D_CUDA_TRY(cudaGetLastError())
+
+// ---------------------------------------------------------------------------
+struct Fields9 {
+  float* p[NCOMP] = {};
+};
+
+struct Context {
+  ContextDesc d;
+  cudaStream_t st = nullptr;     // stream all work is queued on
+  cudaStream_t own = nullptr;    // the context's own stream
+  GridConst g{};
+  float* taper = nullptr;
+  int hfilt = 0;
+  std::vector<float> filt;  // 2*(sub+1)
+  float dtsInv = 0.f;
+  float* med[NMED] = {};
+  bool haveMedium = false;
+  int tx = 16;
+  std::vector<void*> owned;  // every device allocation of this context
+  // working wavefields (primary propagation)
+  Fields9 w0, w1;
+  // Born / FWI buffers, allocated on first use
+  Fields9 s0, s1;            // source-side state
+  std::vector<float*> vSlots;  // decimated source velocity slots (3 fields each)
+  Fields9 ss[2];             // secondary sources (forward) / decimated adjoint field (adjoint)
+  float* pertDev[NMED] = {};
+  // checkpoints
+  int ckptType = CKPT_F32;
+  int segment = 0;           // coarse blocks per segment (0 = automatic)
+  double budget = 0;         // bytes available for checkpoints + velocity slots (0 = automatic)
+  std::vector<void*> ckpt;   // one per segment (index = segment id), packed 18-field states
+  std::vector<float*> ckptScale;
+  int ckptSegLen = 0;
+  bool ckptValid = false;
+  // scratch for transposes / signal staging
+  void* scratch = nullptr;
+  size_t scratchBytes = 0;
+};
+
+static int devAlloc(Context* c, void** p, size_t bytes) {
+  if (bytes == 0) bytes = 16;
+  cudaError_t e = cudaMallocAsync(p, bytes, c->st);
+  if (e != cudaSuccess) {
+    setLastError(cudaGetErrorString(e), __FILE__, __LINE__);
+    return e == cudaErrorMemoryAllocation ? E3D_ERR_OOM : E3D_ERR_CUDA;
+  }
+  c->owned.push_back(*p);
+  return E3D_OK;
+}
+
+static void devFree(Context* c, void* p) {
+  if (!p) return;
+  auto it = std::find(c->owned.begin(), c->owned.end(), p);
+  if (it != c->owned.end()) c->owned.erase(it);
+  cudaFreeAsync(p, c->st);
+}
+
+static int allocFields(Context* c, Fields9& f, bool zero) {
+  const size_t bytes = (size_t)c->g.n * sizeof(float);
+  for (int k = 0; k < NCOMP; k++) {
+    if (!f.p[k]) E3D_RET(devAlloc(c, (void**)&f.p[k], bytes));
+    if (zero) E3D_CUDA_TRY(cudaMemsetAsync(f.p[k], 0, bytes, c->st));
+  }
+  return E3D_OK;
+}
+
+static int zeroFields(Context* c, Fields9& f, int ncomp = NCOMP) {
+  for (int k = 0; k < ncomp; k++) E3D_CUDA_TRY(cudaMemsetAsync(f.p[k], 0, (size_t)c->g.n * sizeof(float), c->st));
+  return E3D_OK;
+}
+
+static int scratchAtLeast(Context* c, size_t bytes) {
+  if (c->scratchBytes >= bytes) return E3D_OK;
+  devFree(c, c->scratch);
+  c->scratch = nullptr;
+  c->scratchBytes = 0;
+  E3D_RET(devAlloc(c, &c->scratch, bytes));
+  c->scratchBytes = bytes;
+  return E3D_OK;
+}
+
+// ---------------------------------------------------------------------------
+int createContext(const ContextDesc& d, Context** out) {
+  E3D_ARG(out != nullptr, "null output handle");
+  E3D_ARG(d.nz > 2 * FAT && d.nx > 2 * FAT && d.ny > 2 * FAT, "grid must exceed 2*FAT on every axis");
+  E3D_ARG(d.nts >= 3, "nts must be at least 3");
+  E3D_ARG(d.sub >= 1 && d.sub < SUB_MAX, "sub must be in [1, SUB_MAX)");
+  E3D_ARG(d.minPad >= 0 && d.minPad < PAD_MAX, "minPad must be in [0, PAD_MAX)");
+  E3D_ARG(d.dz > 0 && d.dx > 0 && d.dy > 0 && d.dts > 0, "sampling must be positive");
+  E3D_ARG((long long)d.nz * d.nx * d.ny < (1LL << 40), "grid too large");
+  Context* c = new Context();
+  c->d = d;
+  cudaError_t e = cudaSetDevice(d.device);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->own, cudaStreamNonBlocking);
+  c->st = c->own;
+  if (e != cudaSuccess) {
+    setLastError(cudaGetErrorString(e), __FILE__, __LINE__);
+    delete c;
+    return E3D_ERR_CUDA;
+  }
+  GridConst& g = c->g;
+  g.nz = d.nz; g.nx = d.nx; g.ny = d.ny; g.minPad = d.minPad;
+  g.yStride = (long long)d.nz * d.nx;
+  g.n = g.yStride * d.ny;
+  // FD coefficients (nonlinearPropElasticGpuFunctions_3D.cu:207-220): double
+  // quotients stored as float; y uses dx unless fixQ1 (quirk Q1).
+  const double k[4] = {1.196289062541883, -0.079752604188901, 0.009570312506634, -6.975446437140719e-04};
+  for (int i = 0; i < 4; i++) {
+    g.cz[i] = (float)(k[i] / d.dz);
+    g.cx[i] = (float)(k[i] / d.dx);
+    g.cy[i] = (float)(k[i] / (d.fixQ1 ? d.dy : d.dx));
+  }
+  // time-interpolation filter (nonlinearPropElasticGpuFunctions_3D.cu:223-241)
+  const int ntw = (d.nts - 1) * d.sub + 1;
+  c->hfilt = d.sub + 1;
+  c->filt.assign(2 * c->hfilt, 0.f);
+  const double scale = 1.0 / std::sqrt((float)ntw / (float)d.nts);
+  for (int i = 0; i < c->hfilt; i++) {
+    float left = (float)(1.0 - 1.0 * i / d.sub);
+    float right = (float)(1.0 - left);
+    c->filt[i] = (float)(left * scale);
+    c->filt[i + c->hfilt] = (float)(right * scale);
+  }
+  // cosine taper (nonlinearPropElasticGpuFunctions_3D.cu:243-255)
+  std::vector<float> taper(std::max(d.minPad, 1), 1.f);
+  for (int i = 0; i < d.minPad; i++) {
+    float arg = (float)(M_PI / (1.0 * d.minPad) * 1.0 * (d.minPad - i));
+    taper[i] = (float)(d.alphaCos + (1.0 - d.alphaCos) * std::cos(arg));
+  }
+  c->dtsInv = (float)(1.0 / (2.0 * d.dts));
+  int s = devAlloc(c, (void**)&c->taper, taper.size() * sizeof(float));
+  if (s == E3D_OK) {
+    e = cudaMemcpyAsync(c->taper, taper.data(), taper.size() * sizeof(float), cudaMemcpyHostToDevice, c->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->st);
+    if (e != cudaSuccess) {
+      setLastError(cudaGetErrorString(e), __FILE__, __LINE__);
+      s = E3D_ERR_CUDA;
+    }
+  }
+  if (s != E3D_OK) {
+    destroyContext(c);
+    return s;
+  }
+  g.taper = c->taper;
+  *out = c;
+  return E3D_OK;
+}
+
+void destroyContext(Context* c) {
+  if (!c) return;
+  cudaSetDevice(c->d.device);
+  for (void* p : c->owned) cudaFreeAsync(p, c->st);
+  c->owned.clear();
+  if (c->st) cudaStreamSynchronize(c->st);
+  if (c->own) cudaStreamDestroy(c->own);
+  delete c;
+}
+
+cudaStream_t stream(Context* c) { return c->st; }
+int setStream(Context* c, cudaStream_t s) {
+  E3D_ARG(c != nullptr, "null context");
+  E3D_CUDA_TRY(cudaStreamSynchronize(c->st));
+  c->st = s ? s : c->own;
+  return E3D_OK;
+}
+long long cellsPerStep(const Context* c) {
+  return (long long)(c->d.nz - 2 * FAT) * (c->d.nx - 2 * FAT) * (c->d.ny - 2 * FAT);
+}
+double deviceBytesInUse(const Context* c) {
+  size_t free = 0, total = 0;
+  cudaMemGetInfo(&free, &total);
+  return (double)(total - free);
+}
+
+int setMedium(Context* c, const float* const* planes, bool onDevice) {
+  E3D_ARG(c && planes, "null argument");
+  E3D_CUDA_TRY(cudaSetDevice(c->d.device));
+  const size_t bytes = (size_t)c->g.n * sizeof(float);
+  for (int k = 0; k < NMED; k++) {
+    E3D_ARG(planes[k] != nullptr, "null medium plane");
+    if (!c->med[k]) E3D_RET(devAlloc(c, (void**)&c->med[k], bytes));
+    E3D_CUDA_TRY(cudaMemcpyAsync(c->med[k], planes[k], bytes, onDevice ? cudaMemcpyDeviceToDevice
+                                                                        : cudaMemcpyHostToDevice, c->st));
+  }
+  E3D_CUDA_TRY(cudaStreamSynchronize(c->st));
+  c->haveMedium = true;
+  c->ckptValid = false;
+  return E3D_OK;
+}
+
+int setTileWidth(Context* c, int tx) {
+  E3D_ARG(c && (tx == 8 || tx == 16), "tile width must be 8 or 16");
+  c->tx = tx;
+  return E3D_OK;
+}
+
+int setCheckpointPolicy(Context* c, int type, int segment, double budget) {
+  E3D_ARG(c && type >= CKPT_F32 && type <= CKPT_BF16, "bad checkpoint type");
+  E3D_ARG(segment >= 0, "segment length must be >= 0");
+  c->ckptType = type;
+  c->segment = segment;
+  c->budget = budget;
+  c->ckptValid = false;
+  return E3D_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Launch helpers
+// ---------------------------------------------------------------------------
+static StepPtrs makeStep(Context* c, Fields9& o, const Fields9& cur) {
+  StepPtrs p{};
+  for (int k = 0; k < NCOMP; k++) {
+    p.o[k] = o.p[k];
+    p.c[k] = cur.p[k];
+  }
+  for (int k = 0; k < NMED; k++) p.m[k] = c->med[k];
+  return p;
+}
+
+static int launchStep(Context* c, int mode, const StepPtrs& p) {
+  const GridConst& g = c->g;
+  const int tiz = (g.nz - 2 * FAT + TZ - 1) / TZ;
+  const int tix = (g.nx - 2 * FAT + c->tx - 1) / c->tx;
+  const int nyi = g.ny - 2 * FAT;
+  // enough CTAs for several waves over 148 SMs, chunks of at least 32 planes
+  const long long tiles = (long long)tiz * tix;
+  int chunks = (int)std::min<long long>((4LL * 148 + tiles - 1) / tiles, std::max(1, nyi / 32));
+  chunks = std::max(chunks, 1);
+  const int yChunk = (nyi + chunks - 1) / chunks;
+  chunks = (nyi + yChunk - 1) / yChunk;
+  dim3 grid(tiz, tix, chunks);
+  if (c->tx == 16) {
+    dim3 block(TZ, 16);
+    if (mode == STEP_FWD) kStep<STEP_FWD, 16><<<grid, block, 0, c->st>>>(p, g, yChunk);
+    else if (mode == STEP_ADJ_REVERSED) kStep<STEP_ADJ_REVERSED, 16><<<grid, block, 0, c->st>>>(p, g, yChunk);
+    else kStep<STEP_ADJ_EXACT, 16><<<grid, block, 0, c->st>>>(p, g, yChunk);
+  } else {
+    dim3 block(TZ, 8);
+    if (mode == STEP_FWD) kStep<STEP_FWD, 8><<<grid, block, 0, c->st>>>(p, g, yChunk);
+    else if (mode == STEP_ADJ_REVERSED) kStep<STEP_ADJ_REVERSED, 8><<<grid, block, 0, c->st>>>(p, g, yChunk);
+    else kStep<STEP_ADJ_EXACT, 8><<<grid, block, 0, c->st>>>(p, g, yChunk);
+  }
+  E3D_LAUNCH_CHECK();
+  return E3D_OK;
+}
+
+static int launchInject(Context* c, const StepPtrs& p, const DevSignals& s, const float* sig, int its, int k) {
+  SparseSet ss;
+  ss.pos = s.pos;
+  for (int i = 0; i <= NCOMP; i++) ss.off[i] = s.off[i];
+  const int n = s.off[NCOMP];
+  if (n == 0) return E3D_OK;
+  kInject<<<(n + 127) / 128, 128, 0, c->st>>>(p, c->g, ss, sig, its, c->filt[k], c->filt[c->hfilt + k]);
+  E3D_LAUNCH_CHECK();
+  return E3D_OK;
+}
+
+static int launchRecord(Context* c, const StepPtrs& p, const DevSignals& s, float* out, int its, int k) {
+  SparseSet ss;
+  ss.pos = s.pos;
+  for (int i = 0; i <= NCOMP; i++) ss.off[i] = s.off[i];
+  const int n = s.off[NCOMP];
+  if (n == 0) return E3D_OK;
+  kRecord<<<(n + 127) / 128, 128, 0, c->st>>>(p, ss, out, its, c->filt[k], c->filt[c->hfilt + k]);
+  E3D_LAUNCH_CHECK();
+  return E3D_OK;
+}
+
+static void swapF(Fields9& a, Fields9& b) {
+  for (int k = 0; k < NCOMP; k++) std::swap(a.p[k], b.p[k]);
+}
+
+// transpose a (rows x cols) row-major matrix; one 32x32 tile per CTA over a 1D grid
+__global__ void kTranspose(const float* in, float* out, long long rows, long long cols) {
+  __shared__ float t[32][33];
+  const long long tilesC = (cols + 31) / 32;
+  const long long r0 = (long long)(blockIdx.x / tilesC) * 32, c0 = (long long)(blockIdx.x % tilesC) * 32;
+  for (int j = threadIdx.y; j < 32; j += blockDim.y) {
+    const long long r = r0 + j, cc = c0 + threadIdx.x;
+    if (r < rows && cc < cols) t[j][threadIdx.x] = in[r * cols + cc];
+  }
+  __syncthreads();
+  for (int j = threadIdx.y; j < 32; j += blockDim.y) {
+    const long long cc = c0 + j, r = r0 + threadIdx.x;
+    if (r < rows && cc < cols) out[cc * rows + r] = t[threadIdx.x][j];
+  }
+}
+
+static int transpose(Context* c, const float* in, float* out, long long rows, long long cols) {
+  if (rows == 0 || cols == 0) return E3D_OK;
+  const long long tiles = ((rows + 31) / 32) * ((cols + 31) / 32);
+  E3D_ARG(tiles < (1LL << 31), "transpose too large");
+  kTranspose<<<(unsigned)tiles, dim3(32, 8), 0, c->st>>>(in, out, rows, cols);
+  E3D_LAUNCH_CHECK();
+  return E3D_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Host (reference-layout) <-> device (time-major) signal staging
+// ---------------------------------------------------------------------------
+struct Staged {
+  DevSignals set{};
+  long long* pos = nullptr;
+  float* sig = nullptr;  // time-major [nts][ntot]
+  int ntot = 0;
+};
+
+// Component k uses the positions of grid gridOf(k); with q2 the sxz receiver
+// table is the z-grid table (nonlinearPropElasticGpuFunctions_3D.cu:416).
+static int stageGeom(Context* c, const HostGeom& g, bool receivers, Staged& s) {
+  long long tot = 0;
+  for (int k = 0; k < NCOMP; k++) {
+    const int gi = gridOfComp(k);
+    E3D_ARG(g.n[gi] >= 0 && g.n[gi] < (1LL << 30), "bad device count");
+    s.set.off[k] = (int)tot;
+    tot += g.n[gi];
+  }
+  E3D_ARG(tot < (1LL << 31), "too many acquisition points");
+  s.set.off[NCOMP] = (int)tot;
+  s.ntot = (int)tot;
+  std::vector<long long> h(std::max<long long>(tot, 1));
+  for (int k = 0; k < NCOMP; k++) {
+    int gi = gridOfComp(k);
+    const long long* src = g.pos[gi];
+    if (receivers && k == SXZ && c->d.q2compat) {
+      // reference copies nReceiversRegXZGrid entries of the z-grid table
+      E3D_ARG(g.n[GXZ] <= g.n[GZ], "sxz receivers read past the z-grid table (reference quirk Q2)");
+      src = g.pos[GZ];
+    }
+    const long long n = g.n[gi];
+    E3D_ARG(n == 0 || src != nullptr, "null position table");
+    for (long long i = 0; i < n; i++) {
+      const long long p = src[i];
+      E3D_ARG(p >= 0 && p < c->g.n, "acquisition point outside the grid");
+      const long long iz = p % c->d.nz, ix = (p / c->d.nz) % c->d.nx, iy = p / c->g.yStride;
+      if (iz < FAT || iz >= c->d.nz - FAT || ix < FAT || ix >= c->d.nx - FAT || iy < FAT || iy >= c->d.ny - FAT) {
+        setLastError("acquisition point inside the FAT ring", __FILE__, __LINE__);
+        return E3D_ERR_BOUNDS;
+      }
+      h[s.set.off[k] + i] = p;
+    }
+  }
+  E3D_RET(devAlloc(c, (void**)&s.pos, h.size() * sizeof(long long)));
+  E3D_CUDA_TRY(cudaMemcpyAsync(s.pos, h.data(), h.size() * sizeof(long long), cudaMemcpyHostToDevice, c->st));
+  s.set.pos = s.pos;
+  return E3D_OK;
+}
+
+// Copy 9 reference-layout host blocks ([n_k][nts]) to a time-major device array.
+static int stageSignalsIn(Context* c, Staged& s, const float* const* host) {
+  const int nts = c->d.nts;
+  const size_t bytes = (size_t)std::max(s.ntot, 1) * nts * sizeof(float);
+  E3D_RET(devAlloc(c, (void**)&s.sig, bytes));
+  E3D_RET(scratchAtLeast(c, bytes));
+  float* tmp = (float*)c->scratch;
+  for (int k = 0; k < NCOMP; k++) {
+    const long long n = s.set.off[k + 1] - s.set.off[k];
+    if (n == 0) continue;
+    E3D_ARG(host[k] != nullptr, "null signal block");
+    E3D_CUDA_TRY(cudaMemcpyAsync(tmp + (size_t)s.set.off[k] * nts, host[k], (size_t)n * nts * sizeof(float),
+                                 cudaMemcpyHostToDevice, c->st));
+  }
+  return transpose(c, tmp, s.sig, s.ntot, nts);
+}
+
+static int stageSignalsZero(Context* c, Staged& s) {
+  const size_t bytes = (size_t)std::max(s.ntot, 1) * c->d.nts * sizeof(float);
+  E3D_RET(devAlloc(c, (void**)&s.sig, bytes));
+  E3D_CUDA_TRY(cudaMemsetAsync(s.sig, 0, bytes, c->st));
+  return E3D_OK;
+}
+
+static int stageSignalsOut(Context* c, Staged& s, float* const* host) {
+  const int nts = c->d.nts;
+  const size_t bytes = (size_t)std::max(s.ntot, 1) * nts * sizeof(float);
+  E3D_RET(scratchAtLeast(c, bytes));
+  float* tmp = (float*)c->scratch;
+  E3D_RET(transpose(c, s.sig, tmp, nts, s.ntot));
+  for (int k = 0; k < NCOMP; k++) {
+    const long long n = s.set.off[k + 1] - s.set.off[k];
+    if (n == 0) continue;
+    E3D_ARG(host[k] != nullptr, "null output block");
+    E3D_CUDA_TRY(cudaMemcpyAsync(host[k], tmp + (size_t)s.set.off[k] * nts, (size_t)n * nts * sizeof(float),
+                                 cudaMemcpyDeviceToHost, c->st));
+  }
+  return E3D_OK;
+}
+
+static void releaseStaged(Context* c, Staged& s) {
+  devFree(c, s.pos);
+  devFree(c, s.sig);
+  s.pos = nullptr;
+  s.sig = nullptr;
+}
+
+// ---------------------------------------------------------------------------
+// Nonlinear propagation
+// ---------------------------------------------------------------------------
+// Forward (propElasticFwdGpu_3D): per fine step  step -> inject (k=it2-1) ->
+// [damp fused] -> record (k=it2) -> swap.
+// Adjoint (propElasticAdjGpu_3D, time-reversed stepper, quirk Q7): per fine
+// step step -> inject data (k=it2+1) -> record source (k=it2) -> swap.
+int nlPropagateDevice(Context* c, bool adjoint, const DevSignals& srcSet, const DevSignals& recSet, float* srcSig,
+                      float* recSig) {
+  E3D_ARG(c && c->haveMedium, "medium not set");
+  E3D_CUDA_TRY(cudaSetDevice(c->d.device));
+  E3D_RET(allocFields(c, c->w0, true));
+  E3D_RET(allocFields(c, c->w1, true));
+  const int nts = c->d.nts, sub = c->d.sub;
+  if (!adjoint) {
+    E3D_CUDA_TRY(cudaMemsetAsync(recSig, 0, (size_t)std::max(recSet.off[NCOMP], 1) * nts * sizeof(float), c->st));
+    for (int its = 0; its < nts - 1; its++) {
+      for (int it2 = 1; it2 <= sub; it2++) {
+        StepPtrs p = makeStep(c, c->w0, c->w1);
+        E3D_RET(launchStep(c, STEP_FWD, p));
+        E3D_RET(launchInject(c, p, srcSet, srcSig, its, it2 - 1));
+        E3D_RET(launchRecord(c, p, recSet, recSig, its, it2));
+        swapF(c->w0, c->w1);
+      }
+    }
+  } else {
+    E3D_CUDA_TRY(cudaMemsetAsync(srcSig, 0, (size_t)std::max(srcSet.off[NCOMP], 1) * nts * sizeof(float), c->st));
+    for (int its = nts - 2; its >= 0; its--) {
+      for (int it2 = sub - 1; it2 >= 0; it2--) {
+        StepPtrs p = makeStep(c, c->w0, c->w1);
+        E3D_RET(launchStep(c, STEP_ADJ_REVERSED, p));
+        E3D_RET(launchInject(c, p, recSet, recSig, its, it2 + 1));
+        E3D_RET(launchRecord(c, p, srcSet, srcSig, its, it2));
+        swapF(c->w0, c->w1);
+      }
+    }
+  }
+  return E3D_OK;
+}
+
+int nlPropagateHost(Context* c, bool adjoint, float* const* model, float* const* data, const HostGeom& src,
+                    const HostGeom& rec) {
+  E3D_ARG(c && model && data, "null argument");
+  E3D_CUDA_TRY(cudaSetDevice(c->d.device));
+  Staged S, R;
+  int st = stageGeom(c, src, false, S);
+  if (st == E3D_OK) st = stageGeom(c, rec, true, R);
+  if (st == E3D_OK) st = adjoint ? stageSignalsZero(c, S) : stageSignalsIn(c, S, model);
+  if (st == E3D_OK) st = adjoint ? stageSignalsIn(c, R, data) : stageSignalsZero(c, R);
+  if (st == E3D_OK) st = nlPropagateDevice(c, adjoint, S.set, R.set, S.sig, R.sig);
+  if (st == E3D_OK) st = adjoint ? stageSignalsOut(c, S, model) : stageSignalsOut(c, R, data);
+  if (st == E3D_OK) {
+    cudaError_t e = cudaStreamSynchronize(c->st);
+    if (e != cudaSuccess) {
+      setLastError(cudaGetErrorString(e), __FILE__, __LINE__);
+      st = E3D_ERR_CUDA;
+    }
+  }
+  releaseStaged(c, S);
+  releaseStaged(c, R);
+  return st;
+}
+
+int stepOnly(Context* c, int mode, int nSteps) {
+  E3D_ARG(c && c->haveMedium, "medium not set");
+  E3D_ARG(mode >= 0 && mode <= 2, "bad mode");
+  E3D_RET(allocFields(c, c->w0, false));
+  E3D_RET(allocFields(c, c->w1, false));
+  for (int i = 0; i < nSteps; i++) {
+    StepPtrs p = makeStep(c, c->w0, c->w1);
+    E3D_RET(launchStep(c, mode, p));
+    swapF(c->w0, c->w1);
+  }
+  return E3D_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Born
+// ---------------------------------------------------------------------------
+static int ensureVSlots(Context* c, int nslots) {
+  while ((int)c->vSlots.size() < nslots) {
+    float* v = nullptr;
+    E3D_RET(devAlloc(c, (void**)&v, (size_t)3 * c->g.n * sizeof(float)));
+    c->vSlots.push_back(v);
+  }
+  return E3D_OK;
+}
+
+static float* vComp(float* slot, int k, long long n) { return slot ? slot + (size_t)k * n : nullptr; }
+
+// One coarse block (its) of the source-side forward propagation on state
+// (s0,s1), injecting srcSig and decimating the damped velocity into vLeft
+// (weight f[it2]) and vRight (weight f[h+it2])
+// (interpWavefieldVxVyVz_3D, kernelsElaGpu_3D.cu:1646-1672).
+static int sourceBlock(Context* c, int its, const DevSignals& srcSet, const float* srcSig, float* vLeft,
+                       float* vRight) {
+  const long long n = c->g.n;
+  for (int it2 = 1; it2 <= c->d.sub; it2++) {
+    StepPtrs p = makeStep(c, c->s0, c->s1);
+    for (int k = 0; k < 3; k++) {
+      p.accL[k] = vComp(vLeft, k, n);
+      p.accR[k] = vComp(vRight, k, n);
+    }
+    if (!vLeft) {  // only the right accumulator is wanted
+      for (int k = 0; k < 3; k++) {
+        p.accL[k] = p.accR[k];
+        p.accR[k] = nullptr;
+      }
+      p.accWl = c->filt[c->hfilt + it2];
+    } else {
+      p.accWl = c->filt[it2];
+      p.accWr = c->filt[c->hfilt + it2];
+    }
+    p.nAcc = 3;
+    E3D_RET(launchStep(c, STEP_FWD, p));
+    E3D_RET(launchInject(c, p, srcSet, srcSig, its, it2 - 1));
+    swapF(c->s0, c->s1);
+  }
+  return E3D_OK;
+}
+
+static int launchImaging(Context* c, bool adjoint, int t, float* vPrev, float* vCur, float* vNext, Fields9& ss) {
+  ImagingPtrs q{};
+  const long long n = c->g.n;
+  for (int k = 0; k < 3; k++) {
+    q.vPrev[k] = vComp(vPrev, k, n);
+    q.vCur[k] = vComp(vCur, k, n);
+    q.vNext[k] = vComp(vNext, k, n);
+  }
+  for (int k = 0; k < NCOMP; k++) q.ss[k] = ss.p[k];
+  for (int k = 0; k < NMED; k++) q.pert[k] = c->pertDev[k];
+  q.dtsInv = c->dtsInv;
+  q.q3compat = c->d.q3compat;
+  dim3 block(32, 8);
+  dim3 grid((c->d.nz - 2 * FAT + 31) / 32, (c->d.nx - 2 * FAT + 7) / 8, c->d.ny - 2 * FAT);
+  if (adjoint) kImaging<true><<<grid, block, 0, c->st>>>(q, c->g);
+  else kImaging<false><<<grid, block, 0, c->st>>>(q, c->g);
+  E3D_LAUNCH_CHECK();
+  (void)t;
+  return E3D_OK;
+}
+
+static int ensurePert(Context* c) {
+  for (int k = 0; k < NMED; k++)
+    if (!c->pertDev[k]) E3D_RET(devAlloc(c, (void**)&c->pertDev[k], (size_t)c->g.n * sizeof(float)));
+  return E3D_OK;
+}
+
+// Born forward: the source propagation runs two coarse blocks ahead of the
+// scattered propagation so that S[t] (needs V[t-1..t+1]) is ready when the
+// scattered block t-1 starts.  Four velocity slots and two secondary-source
+// slots rotate; nothing leaves the device.
+static int bornForwardDevice(Context* c, const DevSignals& srcSet, const DevSignals& recSet, const float* srcSig,
+                             float* recSig) {
+  const int nts = c->d.nts, sub = c->d.sub;
+  E3D_RET(allocFields(c, c->s0, true));
+  E3D_RET(allocFields(c, c->s1, true));
+  E3D_RET(allocFields(c, c->w0, true));
+  E3D_RET(allocFields(c, c->w1, true));
+  E3D_RET(allocFields(c, c->ss[0], true));
+  E3D_RET(allocFields(c, c->ss[1], true));
+  E3D_RET(ensureVSlots(c, 4));
+  for (int i = 0; i < 4; i++)
+    E3D_CUDA_TRY(cudaMemsetAsync(c->vSlots[i], 0, (size_t)3 * c->g.n * sizeof(float), c->st));
+  E3D_CUDA_TRY(cudaMemsetAsync(recSig, 0, (size_t)std::max(recSet.off[NCOMP], 1) * nts * sizeof(float), c->st));
+  auto V = [&](int t) -> float* { return (t < 0 || t >= nts) ? nullptr : c->vSlots[t % 4]; };
+  auto SS = [&](int t) -> Fields9& { return c->ss[t % 2]; };
+  int nextS = 0;        // next secondary source to compute
+  int nextScatter = 0;  // next scattered block
+  auto scatterBlock = [&](int its) -> int {
+    for (int it2 = 1; it2 <= sub; it2++) {
+      StepPtrs p = makeStep(c, c->w0, c->w1);
+      for (int k = 0; k < NCOMP; k++) {
+        p.ssL[k] = SS(its).p[k];
+        p.ssR[k] = SS(its + 1).p[k];
+      }
+      p.ssWl = c->filt[it2 - 1];
+      p.ssWr = c->filt[c->hfilt + it2 - 1];
+      E3D_RET(launchStep(c, STEP_FWD, p));
+      E3D_RET(launchRecord(c, p, recSet, recSig, its, it2));
+      swapF(c->w0, c->w1);
+    }
+    return E3D_OK;
+  };
+  auto computeS = [&](int t) -> int { return launchImaging(c, false, t, V(t - 1), V(t), V(t + 1), SS(t)); };
+  for (int b = 0; b < nts - 1; b++) {
+    // slot of V[b+1] was last used by V[b-3]; clear it before accumulating
+    E3D_CUDA_TRY(cudaMemsetAsync(V(b + 1), 0, (size_t)3 * c->g.n * sizeof(float), c->st));
+    E3D_RET(sourceBlock(c, b, srcSet, srcSig, V(b), V(b + 1)));
+    // V[b] is complete: S[b-1] can be formed
+    while (nextS <= b - 1) E3D_RET(computeS(nextS++));
+    while (nextScatter + 1 < nextS) E3D_RET(scatterBlock(nextScatter++));
+  }
+  // tail: each S[t] overwrites S[t-2], so finish the scattered block that
+  // still needs it before forming the next one
+  while (nextS < nts) {
+    E3D_RET(computeS(nextS++));
+    while (nextScatter + 1 < nextS && nextScatter < nts - 1) E3D_RET(scatterBlock(nextScatter++));
+  }
+  while (nextScatter < nts - 1) E3D_RET(scatterBlock(nextScatter++));
+  return E3D_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Checkpointed source wavefield for the Born adjoint / FWI gradient.
+// A checkpoint for segment s (coarse blocks [s*L, s*L+L)) holds the
+// source-side state at the start of block s*L-1; recomputing from it yields
+// V[s*L] complete (its right-weight part comes from block s*L-1).
+// ---------------------------------------------------------------------------
+static size_t ckptBytesPerState(const Context* c) {
+  const size_t eb = c->ckptType == CKPT_F32 ? 4 : 2;
+  size_t b = (size_t)18 * c->g.n * eb;
+  if (c->ckptType != CKPT_F32) b += (size_t)18 * c->d.ny * sizeof(float) + 256;
+  return b;
+}
+
+static int chooseSegment(Context* c, int& L) {
+  const int blocks = c->d.nts - 1;
+  if (c->segment > 0) {
+    L = std::min(c->segment, blocks);
+    return E3D_OK;
+  }
+  size_t free = 0, total = 0;
+  E3D_CUDA_TRY(cudaMemGetInfo(&free, &total));
+  double budget = c->budget > 0 ? c->budget : 0.85 * (double)free;
+  const double ck = (double)ckptBytesPerState(c);
+  const double vs = 3.0 * c->g.n * sizeof(float);
+  // One extra source block is recomputed per segment, so use the longest
+  // segment whose checkpoints and velocity slots fit in the budget.
+  int bestL = -1;
+  for (int l = blocks; l >= 1; l--) {
+    const int nseg = (blocks + l - 1) / l;
+    const double need = (nseg - 1) * ck + (l + 3) * vs;
+    if (need <= budget) {
+      bestL = l;
+      break;
+    }
+  }
+  if (bestL < 0) {
+    setLastError("wavefield checkpoints do not fit in device memory", __FILE__, __LINE__);
+    return E3D_ERR_OOM;
+  }
+  L = bestL;
+  return E3D_OK;
+}
+
+static int packState(Context* c, int seg) {
+  const long long n = c->g.n, ys = c->g.yStride;
+  const int ny = c->d.ny;
+  Fields9* parts[2] = {&c->s0, &c->s1};
+  if (c->ckptType == CKPT_F32) {
+    float* dst = (float*)c->ckpt[seg];
+    for (int h = 0; h < 2; h++)
+      for (int k = 0; k < NCOMP; k++)
+        E3D_CUDA_TRY(cudaMemcpyAsync(dst + (size_t)(h * NCOMP + k) * n, parts[h]->p[k], n * sizeof(float),
+                                     cudaMemcpyDeviceToDevice, c->st));
+    return E3D_OK;
+  }
+  float* scales = c->ckptScale[seg];
+  float* smax = (float*)c->scratch;
+  for (int h = 0; h < 2; h++)
+    for (int k = 0; k < NCOMP; k++) {
+      const int f = h * NCOMP + k;
+      kSliceMaxAbs<<<ny, 256, 0, c->st>>>(parts[h]->p[k], ys, smax);
+      E3D_LAUNCH_CHECK();
+      const unsigned blocks = (unsigned)((n + 255) / 256);
+      if (c->ckptType == CKPT_F16)
+        kPackSlices<__half><<<blocks, 256, 0, c->st>>>(parts[h]->p[k], ys, n, smax, 16384.f,
+                                                       (__half*)c->ckpt[seg] + (size_t)f * n, scales + (size_t)f * ny);
+      else
+        kPackSlices<__nv_bfloat16><<<blocks, 256, 0, c->st>>>(parts[h]->p[k], ys, n, smax, 1.f,
+                                                              (__nv_bfloat16*)c->ckpt[seg] + (size_t)f * n,
+                                                              scales + (size_t)f * ny);
+      E3D_LAUNCH_CHECK();
+    }
+  return E3D_OK;
+}
+
+static int unpackState(Context* c, int seg) {
+  const long long n = c->g.n, ys = c->g.yStride;
+  const int ny = c->d.ny;
+  Fields9* parts[2] = {&c->s0, &c->s1};
+  for (int h = 0; h < 2; h++)
+    for (int k = 0; k < NCOMP; k++) {
+      const int f = h * NCOMP + k;
+      if (c->ckptType == CKPT_F32) {
+        E3D_CUDA_TRY(cudaMemcpyAsync(parts[h]->p[k], (float*)c->ckpt[seg] + (size_t)f * n, n * sizeof(float),
+                                     cudaMemcpyDeviceToDevice, c->st));
+      } else {
+        const unsigned blocks = (unsigned)((n + 255) / 256);
+        if (c->ckptType == CKPT_F16)
+          kUnpackSlices<__half><<<blocks, 256, 0, c->st>>>((const __half*)c->ckpt[seg] + (size_t)f * n, ys, n,
+                                                           c->ckptScale[seg] + (size_t)f * ny, parts[h]->p[k]);
+        else
+          kUnpackSlices<__nv_bfloat16><<<blocks, 256, 0, c->st>>>(
+              (const __nv_bfloat16*)c->ckpt[seg] + (size_t)f * n, ys, n, c->ckptScale[seg] + (size_t)f * ny,
+              parts[h]->p[k]);
+        E3D_LAUNCH_CHECK();
+      }
+    }
+  return E3D_OK;
+}
+
+static int prepareCheckpoints(Context* c, int& L, int& nseg) {
+  const int blocks = c->d.nts - 1;
+  E3D_RET(chooseSegment(c, L));
+  nseg = (blocks + L - 1) / L;
+  if (c->ckptSegLen != L || (int)c->ckpt.size() != nseg) {
+    for (void* p : c->ckpt) devFree(c, p);
+    for (float* p : c->ckptScale) devFree(c, p);
+    c->ckpt.assign(nseg, nullptr);
+    c->ckptScale.assign(nseg, nullptr);
+    for (int s = 1; s < nseg; s++) {
+      const size_t eb = c->ckptType == CKPT_F32 ? 4 : 2;
+      E3D_RET(devAlloc(c, &c->ckpt[s], (size_t)18 * c->g.n * eb));
+      if (c->ckptType != CKPT_F32)
+        E3D_RET(devAlloc(c, (void**)&c->ckptScale[s], (size_t)18 * c->d.ny * sizeof(float)));
+    }
+    c->ckptSegLen = L;
+  }
+  if (c->ckptType != CKPT_F32) E3D_RET(scratchAtLeast(c, (size_t)c->d.ny * sizeof(float)));
+  return E3D_OK;
+}
+
+// Source-side forward pass over all coarse blocks, saving the state at the
+// start of block s*L-1 for every segment s >= 1.  When recSig is non-null the
+// receivers are recorded too (this is the nonlinear forward of FWI).
+static int sourcePassWithCheckpoints(Context* c, const DevSignals& srcSet, const DevSignals* recSet,
+                                     const float* srcSig, float* recSig) {
+  int L = 0, nseg = 0;
+  E3D_RET(prepareCheckpoints(c, L, nseg));
+  E3D_RET(allocFields(c, c->s0, true));
+  E3D_RET(allocFields(c, c->s1, true));
+  const int nts = c->d.nts, sub = c->d.sub;
+  if (recSig)
+    E3D_CUDA_TRY(cudaMemsetAsync(recSig, 0, (size_t)std::max(recSet->off[NCOMP], 1) * nts * sizeof(float), c->st));
+  for (int b = 0; b < nts - 1; b++) {
+    if ((b + 1) % L == 0 && (b + 1) / L < nseg) E3D_RET(packState(c, (b + 1) / L));
+    for (int it2 = 1; it2 <= sub; it2++) {
+      StepPtrs p = makeStep(c, c->s0, c->s1);
+      E3D_RET(launchStep(c, STEP_FWD, p));
+      E3D_RET(launchInject(c, p, srcSet, srcSig, b, it2 - 1));
+      if (recSig) E3D_RET(launchRecord(c, p, *recSet, recSig, b, it2));
+      swapF(c->s0, c->s1);
+    }
+  }
+  c->ckptValid = true;
+  return E3D_OK;
+}
+
+// Adjoint pass (BornElasticAdjGpu_3D phase B) consuming the checkpoints:
+// segments are processed last to first; each recomputes its velocity slots
+// from its checkpoint, then runs its adjoint blocks and imaging.
+static int adjointPassFromCheckpoints(Context* c, const DevSignals& srcSet, const DevSignals& recSet,
+                                      const float* srcSig, const float* resid) {
+  E3D_ARG(c->ckptValid, "no checkpoints for this shot");
+  const int nts = c->d.nts, sub = c->d.sub, L = c->ckptSegLen;
+  const int blocks = nts - 1;
+  const int nseg = (blocks + L - 1) / L;
+  const long long n = c->g.n;
+  E3D_RET(ensureVSlots(c, L + 3));
+  E3D_RET(allocFields(c, c->w0, true));
+  E3D_RET(allocFields(c, c->w1, true));
+  E3D_RET(allocFields(c, c->ss[0], true));
+  E3D_RET(allocFields(c, c->ss[1], true));
+  // adjoint decimation slots: A[its] (left, fresh per block) and A[its+1] (right)
+  Fields9* aLeft = &c->ss[0];
+  Fields9* aRight = &c->ss[1];
+  // velocity slot of coarse time t within the current segment window [s0, ...]
+  int winStart = 0;
+  auto V = [&](int t) -> float* {
+    if (t < 0 || t >= nts) return nullptr;
+    const int i = t - winStart;
+    return (i >= 0 && i < (int)c->vSlots.size()) ? c->vSlots[i] : nullptr;
+  };
+  for (int s = nseg - 1; s >= 0; s--) {
+    const int bBeg = s * L;
+    const int bEnd = std::min(bBeg + L, blocks);  // adjoint blocks [bBeg, bEnd)
+    // recompute V[bBeg .. min(bEnd+1, nts-1)] from the checkpoint
+    winStart = bBeg;
+    const int lastV = std::min(bEnd + 2, nts - 1);
+    for (int t = bBeg; t <= lastV; t++)
+      E3D_CUDA_TRY(cudaMemsetAsync(c->vSlots[t - bBeg], 0, (size_t)3 * n * sizeof(float), c->st));
+    int firstBlock;
+    if (s == 0) {
+      E3D_RET(zeroFields(c, c->s0));
+      E3D_RET(zeroFields(c, c->s1));
+      firstBlock = 0;
+    } else {
+      E3D_RET(unpackState(c, s));
+      firstBlock = bBeg - 1;
+      // block bBeg-1 only feeds V[bBeg] through its right weights
+      E3D_RET(sourceBlock(c, firstBlock, srcSet, srcSig, nullptr, V(bBeg)));
+      firstBlock = bBeg;
+    }
+    const int lastBlock = std::min(bEnd + 1, blocks - 1);
+    for (int b = firstBlock; b <= lastBlock; b++) E3D_RET(sourceBlock(c, b, srcSet, srcSig, V(b), V(b + 1)));
+    // adjoint blocks, last to first
+    for (int its = bEnd - 1; its >= bBeg; its--) {
+      for (int it2 = sub - 1; it2 >= 0; it2--) {
+        StepPtrs p = makeStep(c, c->w0, c->w1);
+        for (int k = 0; k < NCOMP; k++) {
+          p.accL[k] = aLeft->p[k];
+          p.accR[k] = aRight->p[k];
+        }
+        p.accWl = c->filt[it2];
+        p.accWr = c->filt[c->hfilt + it2];
+        p.nAcc = NCOMP;
+        if (it2 == sub - 1) E3D_RET(zeroFields(c, *aLeft));
+        E3D_RET(launchStep(c, STEP_ADJ_EXACT, p));
+        E3D_RET(launchInject(c, p, recSet, resid, its, it2 + 1));
+        swapF(c->w0, c->w1);
+      }
+      // imaging condition at its+1 (A[its+1] complete)
+      E3D_RET(launchImaging(c, true, its + 1, V(its), V(its + 1), V(its + 2), *aRight));
+      std::swap(aLeft, aRight);  // A[its] becomes the right accumulator of block its-1
+    }
+  }
+  // final imaging at t = 0 (uses V[0], V[1] of the first segment window)
+  E3D_RET(launchImaging(c, true, 0, nullptr, V(0), V(1), *aRight));
+  return E3D_OK;
+}
+
+static int bornAdjointDevice(Context* c, const DevSignals& srcSet, const DevSignals& recSet, const float* srcSig,
+                             const float* resid) {
+  E3D_RET(sourcePassWithCheckpoints(c, srcSet, nullptr, srcSig, nullptr));
+  return adjointPassFromCheckpoints(c, srcSet, recSet, srcSig, resid);
+}
+
+int bornForwardHost(Context* c, const float* const* srcSig, float* const* data, const HostGeom& src,
+                    const HostGeom& rec, const float* const* pert) {
+  E3D_ARG(c && c->haveMedium, "medium not set");
+  E3D_ARG(srcSig && data && pert, "null argument");
+  E3D_CUDA_TRY(cudaSetDevice(c->d.device));
+  E3D_RET(ensurePert(c));
+  for (int k = 0; k < NMED; k++)
+    E3D_CUDA_TRY(cudaMemcpyAsync(c->pertDev[k], pert[k], (size_t)c->g.n * sizeof(float), cudaMemcpyHostToDevice,
+                                 c->st));
+  Staged S, R;
+  int st = stageGeom(c, src, false, S);
+  if (st == E3D_OK) st = stageGeom(c, rec, true, R);
+  if (st == E3D_OK) st = stageSignalsIn(c, S, srcSig);
+  if (st == E3D_OK) st = stageSignalsZero(c, R);
+  if (st == E3D_OK) st = bornForwardDevice(c, S.set, R.set, S.sig, R.sig);
+  if (st == E3D_OK) st = stageSignalsOut(c, R, data);
+  if (st == E3D_OK && cudaStreamSynchronize(c->st) != cudaSuccess) {
+    setLastError("stream failure", __FILE__, __LINE__);
+    st = E3D_ERR_CUDA;
+  }
+  releaseStaged(c, S);
+  releaseStaged(c, R);
+  return st;
+}
+
+int bornAdjointHost(Context* c, const float* const* srcSig, const float* const* data, const HostGeom& src,
+                    const HostGeom& rec, float* const* pert) {
+  E3D_ARG(c && c->haveMedium, "medium not set");
+  E3D_ARG(srcSig && data && pert, "null argument");
+  E3D_CUDA_TRY(cudaSetDevice(c->d.device));
+  E3D_RET(ensurePert(c));
+  // the reference copies the caller's planes to the device and accumulates
+  // the image onto them (BornElasticGpuFunctions_3D.cu:2110-2114)
+  for (int k = 0; k < NMED; k++)
+    E3D_CUDA_TRY(cudaMemcpyAsync(c->pertDev[k], pert[k], (size_t)c->g.n * sizeof(float), cudaMemcpyHostToDevice,
+                                 c->st));
+  Staged S, R;
+  int st = stageGeom(c, src, false, S);
+  if (st == E3D_OK) st = stageGeom(c, rec, true, R);
+  if (st == E3D_OK) st = stageSignalsIn(c, S, srcSig);
+  if (st == E3D_OK) st = stageSignalsIn(c, R, const_cast<float* const*>(data));
+  if (st == E3D_OK) st = bornAdjointDevice(c, S.set, R.set, S.sig, R.sig);
+  if (st == E3D_OK) {
+    for (int k = 0; k < NMED && st == E3D_OK; k++) {
+      cudaError_t e = cudaMemcpyAsync(pert[k], c->pertDev[k], (size_t)c->g.n * sizeof(float),
+                                      cudaMemcpyDeviceToHost, c->st);
+      if (e != cudaSuccess) st = E3D_ERR_CUDA;
+    }
+    if (st == E3D_OK && cudaStreamSynchronize(c->st) != cudaSuccess) st = E3D_ERR_CUDA;
+    if (st != E3D_OK) setLastError("copy-out failure", __FILE__, __LINE__);
+  }
+  releaseStaged(c, S);
+  releaseStaged(c, R);
+  return st;
+}
+
+// ---------------------------------------------------------------------------
+// FWI (device API)
+// ---------------------------------------------------------------------------
+int fwiForwardDevice(Context* c, const DevSignals& srcSet, const DevSignals& recSet, const float* srcSig,
+                     float* recSig) {
+  E3D_ARG(c && c->haveMedium, "medium not set");
+  E3D_CUDA_TRY(cudaSetDevice(c->d.device));
+  return sourcePassWithCheckpoints(c, srcSet, &recSet, srcSig, recSig);
+}
+
+int fwiGradientDevice(Context* c, const DevSignals& srcSet, const DevSignals& recSet, const float* srcSig,
+                      const float* residual, float* const* pert8) {
+  E3D_ARG(c && c->haveMedium, "medium not set");
+  E3D_ARG(pert8 != nullptr, "null gradient planes");
+  E3D_CUDA_TRY(cudaSetDevice(c->d.device));
+  for (int k = 0; k < NMED; k++) {
+    E3D_ARG(pert8[k] != nullptr, "null gradient plane");
+    c->pertDev[k] = pert8[k];  // accumulate straight into the caller's planes
+  }
+  int st = adjointPassFromCheckpoints(c, srcSet, recSet, srcSig, residual);
+  for (int k = 0; k < NMED; k++) c->pertDev[k] = nullptr;
+  return st;
+}
+
+}  // namespace e3d

@@ -1,0 +1,75 @@
+// C++ engine behind the C ABI: one Context per (device, propagation grid,
+// time axis).  A Context owns its device buffers and its CUDA stream; the
+// C ABI maps the reference's process-global, per-iGpu state onto Contexts.
+#pragma once
+#include <cstddef>
+#include <string>
+#include <vector>
+#include "common.cuh"
+
+namespace e3d {
+
+// Regular-grid acquisition points of the seven grids (center, x, y, z, xz, xy, yz).
+struct HostGeom {
+  const long long* pos[NGRID];
+  long long n[NGRID];
+};
+
+// Storage type of saved wavefield states.
+enum CkptType { CKPT_F32 = 0, CKPT_F16 = 1, CKPT_BF16 = 2 };
+
+struct ContextDesc {
+  int device = 0;
+  int nz = 0, nx = 0, ny = 0;
+  int nts = 0;       // coarse samples
+  int sub = 0;       // internal (2x parfile) subsampling
+  int minPad = 0;
+  float dz = 0, dx = 0, dy = 0, dts = 0, alphaCos = 0.99f;
+  int fixQ1 = 0;     // 1: y derivatives use dy (the reference uses dx)
+  int q2compat = 1;  // 1: sxz receivers use the z-grid positions (reference behaviour)
+  int q3compat = 1;  // 1: Born yz shear term uses the xz derivative pair (reference behaviour)
+};
+
+struct Context;
+
+int createContext(const ContextDesc& d, Context** out);
+void destroyContext(Context* c);
+// medium: 8 planes of nz*nx*ny floats; onDevice selects host or device pointers
+int setMedium(Context* c, const float* const* planes, bool onDevice);
+// Which stepper tile width to use (8 or 16), for the autotuner.
+int setTileWidth(Context* c, int tx);
+int setCheckpointPolicy(Context* c, int ckptType, int segment, double budgetBytes);
+
+// Reference-layout host entry points ([nDevice][nts] per component).
+int nlPropagateHost(Context* c, bool adjoint, float* const* model, float* const* data, const HostGeom& src,
+                    const HostGeom& rec);
+int bornForwardHost(Context* c, const float* const* srcSig, float* const* data, const HostGeom& src,
+                    const HostGeom& rec, const float* const* pert);
+int bornAdjointHost(Context* c, const float* const* srcSig, const float* const* data, const HostGeom& src,
+                    const HostGeom& rec, float* const* pert);
+
+// Device entry points: signals are time-major and concatenated over the nine
+// components ([nts][sum of per-component counts]); positions are device
+// arrays concatenated the same way with per-component offsets off[0..9].
+struct DevSignals {
+  const long long* pos;
+  int off[NCOMP + 1];
+};
+int nlPropagateDevice(Context* c, bool adjoint, const DevSignals& srcSet, const DevSignals& recSet,
+                      float* srcSig, float* recSig);
+// FWI: nonlinear forward that saves wavefield checkpoints for a later
+// gradient; the gradient call consumes them (Born adjoint of the residual).
+int fwiForwardDevice(Context* c, const DevSignals& srcSet, const DevSignals& recSet, const float* srcSig,
+                     float* recSig);
+int fwiGradientDevice(Context* c, const DevSignals& srcSet, const DevSignals& recSet, const float* srcSig,
+                      const float* residual, float* const* pert8);
+
+// Timing/inspection helpers
+int stepOnly(Context* c, int mode, int nSteps);  // run nSteps bare steps on the working state
+long long cellsPerStep(const Context* c);
+double deviceBytesInUse(const Context* c);
+cudaStream_t stream(Context* c);
+int setStream(Context* c, cudaStream_t s);
+
+const char* lastError();
+}  // namespace e3d

@@ -1,0 +1,373 @@
+// CUDA kernels of the elastic 3D propagation engine (sm_100a).
+//
+// Stepper: one launch advances all nine components of one shot by one fine
+// time step.  2.5D y-marching: a CTA owns a 32(z) x TX(x) column tile and
+// walks a chunk of y-planes.  Per plane the eight fields that need z/x
+// neighbours are staged in shared memory (tile plus a 4-cell halo, loaded
+// cooperatively with 128-byte z rows); the six fields that need y neighbours
+// keep an 8-deep register window.  The cosine sponge is fused: the reference
+// damps both time levels after every step (dampCosineEdge_3D); here the new
+// level is damped when written and the other level is damped when it is next
+// read as the "old" level, which gives the same recursion without a second
+// pass over 18 arrays.
+#pragma once
+#include "common.cuh"
+
+namespace e3d {
+
+constexpr int TZ = 32;
+constexpr int HALO = 4;
+constexpr int SZ = TZ + 2 * HALO;  // shared tile row length (z)
+
+struct StepPtrs {
+  float* o[NCOMP];        // old level in, new level out (in place)
+  const float* c[NCOMP];  // current level
+  const float* m[NMED];   // medium planes
+  // optional Born secondary source injected inside the step (may be null)
+  const float* ssL[NCOMP];
+  const float* ssR[NCOMP];
+  float ssWl, ssWr;
+  // optional decimation of the new level into coarse accumulators (may be null)
+  float* accL[NCOMP];
+  float* accR[NCOMP];
+  float accWl, accWr;
+  int nAcc;               // number of leading components accumulated (3 or 9)
+};
+
+// Shared tiles: fields needing a z or x halo.
+enum Tile { T_VX = 0, T_VY, T_VZ, T_SXX, T_SZZ, T_SXY, T_SXZ, T_SYZ, NTILE };
+// Register windows: fields needing y neighbours.  Window k holds plane y+base+k
+// with base -4 for backward (minus) and -3 for forward (plus) derivatives.
+enum Queue { Q_VX = 0, Q_VY, Q_VZ, Q_SYY, Q_SXY, Q_SYZ, NQUEUE };
+__device__ constexpr int qBase(int q) { return (q == Q_VY || q == Q_SXY || q == Q_SYZ) ? -3 : -4; }
+
+// Field value entering the derivative: raw (modes 0/1) or medium-premultiplied
+// (mode 2, stepAdjGpuBorn_3D kernelsElaGpu_3D.cu:864-920).
+template <int MODE>
+__device__ __forceinline__ float tileValue(const StepPtrs& p, int t, long long i) {
+  if (MODE != STEP_ADJ_EXACT) {
+    const int comp = (t == T_VX) ? VX : (t == T_VY) ? VY : (t == T_VZ) ? VZ : (t == T_SXX) ? SXX
+                   : (t == T_SZZ) ? SZZ : (t == T_SXY) ? SXY : (t == T_SXZ) ? SXZ : SYZ;
+    return __ldg(p.c[comp] + i);
+  } else {
+    switch (t) {
+      case T_VX: return __ldg(p.c[VX] + i) * __ldg(p.m[RHOX] + i);
+      case T_VY: return __ldg(p.c[VY] + i) * __ldg(p.m[RHOY] + i);
+      case T_VZ: return __ldg(p.c[VZ] + i) * __ldg(p.m[RHOZ] + i);
+      case T_SXX: return __ldg(p.c[SXX] + i) * __ldg(p.m[L2M] + i) +
+                         (__ldg(p.c[SYY] + i) + __ldg(p.c[SZZ] + i)) * __ldg(p.m[LAM] + i);
+      case T_SZZ: return __ldg(p.c[SZZ] + i) * __ldg(p.m[L2M] + i) +
+                         (__ldg(p.c[SXX] + i) + __ldg(p.c[SYY] + i)) * __ldg(p.m[LAM] + i);
+      case T_SXY: return __ldg(p.c[SXY] + i) * __ldg(p.m[MUXY] + i);
+      case T_SXZ: return __ldg(p.c[SXZ] + i) * __ldg(p.m[MUXZ] + i);
+      default: return __ldg(p.c[SYZ] + i) * __ldg(p.m[MUYZ] + i);
+    }
+  }
+}
+
+template <int MODE>
+__device__ __forceinline__ float queueValue(const StepPtrs& p, int q, long long i) {
+  if (MODE != STEP_ADJ_EXACT) {
+    const int comp = (q == Q_VX) ? VX : (q == Q_VY) ? VY : (q == Q_VZ) ? VZ : (q == Q_SYY) ? SYY
+                   : (q == Q_SXY) ? SXY : SYZ;
+    return __ldg(p.c[comp] + i);
+  } else {
+    switch (q) {
+      case Q_VX: return __ldg(p.c[VX] + i) * __ldg(p.m[RHOX] + i);
+      case Q_VY: return __ldg(p.c[VY] + i) * __ldg(p.m[RHOY] + i);
+      case Q_VZ: return __ldg(p.c[VZ] + i) * __ldg(p.m[RHOZ] + i);
+      case Q_SYY: return __ldg(p.c[SYY] + i) * __ldg(p.m[L2M] + i) +
+                         (__ldg(p.c[SXX] + i) + __ldg(p.c[SZZ] + i)) * __ldg(p.m[LAM] + i);
+      case Q_SXY: return __ldg(p.c[SXY] + i) * __ldg(p.m[MUXY] + i);
+      default: return __ldg(p.c[SYZ] + i) * __ldg(p.m[MUYZ] + i);
+    }
+  }
+}
+
+__device__ __forceinline__ float dWin(const float* w, const float* c) {
+  return c[0] * (w[4] - w[3]) + c[1] * (w[5] - w[2]) + c[2] * (w[6] - w[1]) + c[3] * (w[7] - w[0]);
+}
+// forward (+) / backward (-) 8th-order staggered derivatives along a shared-tile axis of stride s
+__device__ __forceinline__ float dPlus(const float* t, int i, int s, const float* c) {
+  return c[0] * (t[i + s] - t[i]) + c[1] * (t[i + 2 * s] - t[i - s]) + c[2] * (t[i + 3 * s] - t[i - 2 * s]) +
+         c[3] * (t[i + 4 * s] - t[i - 3 * s]);
+}
+__device__ __forceinline__ float dMinus(const float* t, int i, int s, const float* c) {
+  return c[0] * (t[i] - t[i - s]) + c[1] * (t[i + s] - t[i - 2 * s]) + c[2] * (t[i + 2 * s] - t[i - 3 * s]) +
+         c[3] * (t[i + 3 * s] - t[i - 4 * s]);
+}
+
+// One fine time step for a y-chunk of one (z,x) tile.
+//   MODE 0: new = G*(G*old + M D(cur))              (stepFwdGpu_3D)
+//   MODE 1: new = G*(G*old - M D(cur))              (stepAdjGpu_3D)
+//   MODE 2: new = G*(G*old - D(M cur))              (stepAdjGpuBorn_3D)
+// G is the sponge taper at the cell.  Optional extras: a Born secondary source
+// added before damping, and decimation of the damped new level.
+template <int MODE, int TX>
+__global__ void __launch_bounds__(TZ * TX) kStep(StepPtrs p, GridConst g, int yChunk) {
+  constexpr int SX = TX + 2 * HALO;
+  constexpr int TILE = SZ * SX;
+  __shared__ float tile[NTILE][TILE];
+
+  const int tz = threadIdx.x, tx = threadIdx.y;
+  const int tid = tx * TZ + tz;
+  const int z0 = FAT + blockIdx.x * TZ, x0 = FAT + blockIdx.y * TX;
+  const int iz = z0 + tz, ix = x0 + tx;
+  const bool active = (iz < g.nz - FAT) && (ix < g.nx - FAT);
+  const int yBeg = FAT + blockIdx.z * yChunk;
+  const int yEnd = min(yBeg + yChunk, g.ny - FAT);
+  const long long ys = g.yStride;
+  const long long col = (long long)ix * g.nz + iz;
+
+  float w[NQUEUE][8];
+  if (active) {
+#pragma unroll
+    for (int q = 0; q < NQUEUE; q++) {
+#pragma unroll
+      for (int k = 0; k < 7; k++) w[q][k] = queueValue<MODE>(p, q, (long long)(yBeg + qBase(q) + k) * ys + col);
+    }
+  }
+
+  const int lc = (tx + HALO) * SZ + (tz + HALO);  // this thread's centre in the tile
+  for (int y = yBeg; y < yEnd; y++) {
+    const long long ic = (long long)y * ys + col;
+    float ov[NCOMP], mv[NMED];
+    if (active) {
+#pragma unroll
+      for (int q = 0; q < NQUEUE; q++) w[q][7] = queueValue<MODE>(p, q, ic + (long long)(qBase(q) + 7) * ys);
+#pragma unroll
+      for (int k = 0; k < NCOMP; k++) ov[k] = p.o[k][ic];
+      if (MODE != STEP_ADJ_EXACT) {
+#pragma unroll
+        for (int k = 0; k < NMED; k++) mv[k] = __ldg(p.m[k] + ic);
+      }
+    }
+    __syncthreads();  // previous plane's tile reads are complete
+    {
+      const long long plane = (long long)y * ys;
+      for (int s = tid; s < TILE; s += TZ * TX) {
+        const int lz = s % SZ, lx = s / SZ;
+        const int gz = z0 - HALO + lz, gx = x0 - HALO + lx;
+        const bool in = (gz < g.nz) && (gx < g.nx);
+        const long long gi = plane + (long long)gx * g.nz + gz;
+#pragma unroll
+        for (int t = 0; t < NTILE; t++) tile[t][s] = in ? tileValue<MODE>(p, t, gi) : 0.0f;
+      }
+    }
+    __syncthreads();
+    if (active) {
+      const float* cz = g.cz;
+      const float* cx = g.cx;
+      const float* cy = g.cy;
+      const float dvx_dx = dPlus(tile[T_VX], lc, SZ, cx);
+      const float dvy_dy = dWin(w[Q_VY], cy);
+      const float dvz_dz = dPlus(tile[T_VZ], lc, 1, cz);
+      const float fvx = dMinus(tile[T_SXX], lc, SZ, cx) + dWin(w[Q_SXY], cy) + dPlus(tile[T_SXZ], lc, 1, cz);
+      const float fvy = dPlus(tile[T_SXY], lc, SZ, cx) + dWin(w[Q_SYY], cy) + dPlus(tile[T_SYZ], lc, 1, cz);
+      const float fvz = dPlus(tile[T_SXZ], lc, SZ, cx) + dWin(w[Q_SYZ], cy) + dMinus(tile[T_SZZ], lc, 1, cz);
+      const float fxy = dWin(w[Q_VX], cy) + dMinus(tile[T_VY], lc, SZ, cx);
+      const float fxz = dMinus(tile[T_VX], lc, 1, cz) + dMinus(tile[T_VZ], lc, SZ, cx);
+      const float fyz = dWin(w[Q_VZ], cy) + dMinus(tile[T_VY], lc, 1, cz);
+
+      float up[NCOMP];
+      if (MODE == STEP_ADJ_EXACT) {
+        up[VX] = -fvx; up[VY] = -fvy; up[VZ] = -fvz;
+        up[SXX] = -dvx_dx; up[SYY] = -dvy_dy; up[SZZ] = -dvz_dz;
+        up[SXZ] = -fxz; up[SXY] = -fxy; up[SYZ] = -fyz;
+      } else {
+        const float sgn = (MODE == STEP_FWD) ? 1.0f : -1.0f;
+        up[VX] = sgn * (mv[RHOX] * fvx);
+        up[VY] = sgn * (mv[RHOY] * fvy);
+        up[VZ] = sgn * (mv[RHOZ] * fvz);
+        up[SXX] = sgn * (mv[L2M] * dvx_dx + mv[LAM] * (dvy_dy + dvz_dz));
+        up[SYY] = sgn * (mv[L2M] * dvy_dy + mv[LAM] * (dvx_dx + dvz_dz));
+        up[SZZ] = sgn * (mv[L2M] * dvz_dz + mv[LAM] * (dvx_dx + dvy_dy));
+        up[SXZ] = sgn * (mv[MUXZ] * fxz);
+        up[SXY] = sgn * (mv[MUXY] * fxy);
+        up[SYZ] = sgn * (mv[MUYZ] * fyz);
+      }
+      const float G = taperAt(g, iz, ix, y);
+      const bool hasSS = p.ssL[0] != nullptr;
+      const bool hasAcc = p.accL[0] != nullptr;
+#pragma unroll
+      for (int k = 0; k < NCOMP; k++) {
+        float v = G * ov[k] + up[k];
+        if (hasSS) v += __ldg(p.ssL[k] + ic) * p.ssWl + __ldg(p.ssR[k] + ic) * p.ssWr;
+        v *= G;
+        p.o[k][ic] = v;
+        if (hasAcc && k < p.nAcc) {
+          p.accL[k][ic] += v * p.accWl;
+          if (p.accR[0] != nullptr) p.accR[k][ic] += v * p.accWr;
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < NQUEUE; q++) {
+#pragma unroll
+        for (int k = 0; k < 7; k++) w[q][k] = w[q][k + 1];
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Sparse signal kernels.  A "device set" concatenates the regular-grid points
+// of the nine components: component k owns entries [off[k], off[k+1]) of pos.
+// Signals are time-major on the device: sig[t*ntot + j].
+// ---------------------------------------------------------------------------
+struct SparseSet {
+  const long long* pos;
+  int off[NCOMP + 1];
+};
+
+// field[pos] += G(pos) * (sig[its]*wl + sig[its+1]*wr)
+// (ker_inject_source_* / ker_inject_data_*, kernelsElaGpu_3D.cu:11-52; the
+// source enters before the sponge, hence the taper at the point.)
+__global__ void kInject(StepPtrs p, GridConst g, SparseSet s, const float* sig, int its, float wl, float wr) {
+  const int ntot = s.off[NCOMP];
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= ntot) return;
+  int k = 0;
+#pragma unroll
+  for (int c = 1; c < NCOMP; c++) k += (j >= s.off[c]);
+  const long long pos = s.pos[j];
+  const float v = sig[(long long)its * ntot + j] * wl + sig[(long long)(its + 1) * ntot + j] * wr;
+  const int iz = (int)(pos % g.nz);
+  const int ix = (int)((pos / g.nz) % g.nx);
+  const int iy = (int)(pos / g.yStride);
+  const float add = taperAt(g, iz, ix, iy) * v;
+  p.o[k][pos] += add;
+  // keep a decimation that the stepper fused in consistent with the injected value
+  if (p.accL[0] != nullptr && k < p.nAcc) {
+    p.accL[k][pos] += add * p.accWl;
+    if (p.accR[0] != nullptr) p.accR[k][pos] += add * p.accWr;
+  }
+}
+
+// out[its] += field[pos]*wl; out[its+1] += field[pos]*wr
+// (ker_record_*, kernelsElaGpu_3D.cu:61-104)
+__global__ void kRecord(StepPtrs p, SparseSet s, float* out, int its, float wl, float wr) {
+  const int ntot = s.off[NCOMP];
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= ntot) return;
+  int k = 0;
+#pragma unroll
+  for (int c = 1; c < NCOMP; c++) k += (j >= s.off[c]);
+  const float v = p.o[k][s.pos[j]];
+  out[(long long)its * ntot + j] += v * wl;
+  out[(long long)(its + 1) * ntot + j] += v * wr;
+}
+
+// ---------------------------------------------------------------------------
+// Born scattering (imagingElaFwdGpu_3D, kernelsElaGpu_3D.cu:1232-1438) and
+// imaging (imagingElaAdjGpu_3D, :1440-1641) at one coarse time t.
+// V* are the decimated source velocities at t-1, t, t+1 (null outside [0,nts)).
+// pert: drhox, drhoy, drhoz, dlame, dmu, dmuxz, dmuxy, dmuyz.
+// ---------------------------------------------------------------------------
+struct ImagingPtrs {
+  const float* vPrev[3];
+  const float* vCur[3];
+  const float* vNext[3];
+  float* ss[NCOMP];        // forward: secondary sources written; adjoint: decimated adjoint field read
+  float* pert[NMED];       // forward: read; adjoint: accumulated
+  float dtsInv;            // 1/(2 dts)
+  int q3compat;
+};
+
+__device__ __forceinline__ float gPlus(const float* a, long long i, long long s, const float* c) {
+  return c[0] * (__ldg(a + i + s) - __ldg(a + i)) + c[1] * (__ldg(a + i + 2 * s) - __ldg(a + i - s)) +
+         c[2] * (__ldg(a + i + 3 * s) - __ldg(a + i - 2 * s)) + c[3] * (__ldg(a + i + 4 * s) - __ldg(a + i - 3 * s));
+}
+__device__ __forceinline__ float gMinus(const float* a, long long i, long long s, const float* c) {
+  return c[0] * (__ldg(a + i) - __ldg(a + i - s)) + c[1] * (__ldg(a + i + s) - __ldg(a + i - 2 * s)) +
+         c[2] * (__ldg(a + i + 2 * s) - __ldg(a + i - 3 * s)) + c[3] * (__ldg(a + i + 3 * s) - __ldg(a + i - 4 * s));
+}
+
+template <bool ADJ>
+__global__ void kImaging(ImagingPtrs q, GridConst g) {
+  const int iz = FAT + blockIdx.x * blockDim.x + threadIdx.x;
+  const int ix = FAT + blockIdx.y * blockDim.y + threadIdx.y;
+  const int iy = FAT + blockIdx.z;
+  if (iz >= g.nz - FAT || ix >= g.nx - FAT) return;
+  const long long i = (long long)iy * g.yStride + (long long)ix * g.nz + iz;
+  const long long xs = g.nz, ys = g.yStride;
+  const float* vx = q.vCur[0];
+  const float* vy = q.vCur[1];
+  const float* vz = q.vCur[2];
+  const float dvx_dx = gPlus(vx, i, xs, g.cx);
+  const float dvy_dy = gPlus(vy, i, ys, g.cy);
+  const float dvz_dz = gPlus(vz, i, 1, g.cz);
+  const float exz = gMinus(vx, i, 1, g.cz) + gMinus(vz, i, xs, g.cx);
+  const float exy = gMinus(vx, i, ys, g.cy) + gMinus(vy, i, xs, g.cx);
+  const float eyz = q.q3compat ? exz : (gMinus(vz, i, ys, g.cy) + gMinus(vy, i, 1, g.cz));
+  float tder[3];
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    const float a = q.vPrev[k] ? __ldg(q.vPrev[k] + i) : 0.0f;
+    const float b = q.vNext[k] ? __ldg(q.vNext[k] + i) : 0.0f;
+    tder[k] = (a - b) * q.dtsInv;
+  }
+  const float div = dvx_dx + dvy_dy + dvz_dz;
+  if (!ADJ) {
+    q.ss[VX][i] = __ldg(q.pert[0] + i) * tder[0];
+    q.ss[VY][i] = __ldg(q.pert[1] + i) * tder[1];
+    q.ss[VZ][i] = __ldg(q.pert[2] + i) * tder[2];
+    const float dl = __ldg(q.pert[3] + i), dm = __ldg(q.pert[4] + i);
+    q.ss[SXX][i] = dl * div + 2.0f * dm * dvx_dx;
+    q.ss[SYY][i] = dl * div + 2.0f * dm * dvy_dy;
+    q.ss[SZZ][i] = dl * div + 2.0f * dm * dvz_dz;
+    q.ss[SXZ][i] = __ldg(q.pert[5] + i) * exz;
+    q.ss[SXY][i] = __ldg(q.pert[6] + i) * exy;
+    q.ss[SYZ][i] = __ldg(q.pert[7] + i) * eyz;
+  } else {
+    const float axx = q.ss[SXX][i], ayy = q.ss[SYY][i], azz = q.ss[SZZ][i];
+    q.pert[0][i] += q.ss[VX][i] * tder[0];
+    q.pert[1][i] += q.ss[VY][i] * tder[1];
+    q.pert[2][i] += q.ss[VZ][i] * tder[2];
+    q.pert[3][i] += (axx + ayy + azz) * div;
+    q.pert[4][i] += 2.0f * (dvx_dx * axx + dvy_dy * ayy + dvz_dz * azz);
+    q.pert[5][i] += q.ss[SXZ][i] * exz;
+    q.pert[6][i] += q.ss[SXY][i] * exy;
+    q.pert[7][i] += q.ss[SYZ][i] * eyz;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Checkpoint compression: a field plane (one y slice) is stored as fp16 or
+// bf16 with one fp32 scale per (field, y) slice (max-abs / 2^14 for fp16,
+// max-abs for bf16), or copied raw in fp32.
+// ---------------------------------------------------------------------------
+__global__ void kSliceMaxAbs(const float* a, long long ys, float* out) {
+  const long long base = (long long)blockIdx.x * ys;
+  float m = 0.0f;
+  for (long long i = threadIdx.x; i < ys; i += blockDim.x) m = fmaxf(m, fabsf(a[base + i]));
+  for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+  __shared__ float red[32];
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    m = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0f;
+    for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if (threadIdx.x == 0) out[blockIdx.x] = m;
+  }
+}
+
+template <typename H>
+__global__ void kPackSlices(const float* a, long long ys, long long n, const float* smax, float target, H* out,
+                            float* scales) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const long long y = i / ys;
+  const float m = smax[y];
+  const float s = m > 0.0f ? target / m : 0.0f;
+  if (i % ys == 0) scales[y] = s > 0.0f ? 1.0f / s : 0.0f;
+  out[i] = H(a[i] * s);
+}
+
+template <typename H>
+__global__ void kUnpackSlices(const H* in, long long ys, long long n, const float* scales, float* a) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  a[i] = float(in[i]) * scales[i / ys];
+}
+
+}  // namespace e3d

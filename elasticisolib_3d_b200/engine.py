@@ -1,0 +1,142 @@
+"""Python handle on one propagation context of the native engine.
+
+A ``Propagator`` owns an ``e3d_context`` (device buffers, stream) for one grid
+and time axis.  Host-array methods mirror the reference drivers
+(propElasticFwdGpu_3D, propElasticAdjGpu_3D, BornElasticFwdGpu_3D,
+BornElasticAdjGpu_3D) with signal blocks in the reference layout: a list of
+nine float32 arrays, component k shaped (nDevice_k, nts).
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _native as N
+
+# grid of each wavefield component: vx->x, vy->y, vz->z, sxx/syy/szz->center, sxz->xz, sxy->xy, syz->yz
+COMP_GRID = (1, 2, 3, 0, 0, 0, 4, 5, 6)
+CKPT_TYPES = {"fp32": 0, "fp16": 1, "bf16": 2}
+
+
+def _geom(pos7):
+    pos = [N.as_i64(p) for p in pos7]
+    P = N.ptr_array(pos)
+    C = (ctypes.c_longlong * 7)(*[int(p.shape[0]) for p in pos])
+    return P, C, pos
+
+
+class Propagator:
+    def __init__(self, nz, nx, ny, nts, sub, minPad, dz, dx, dy, dts, alphaCos=0.99, device=0, fix_q1=0,
+                 q2compat=1, q3compat=1):
+        self.nz, self.nx, self.ny, self.nts, self.sub = int(nz), int(nx), int(ny), int(nts), int(sub)
+        self.shape = (self.ny, self.nx, self.nz)
+        d = N.E3DDesc(int(device), self.nz, self.nx, self.ny, self.nts, self.sub, int(minPad), float(dz), float(dx),
+                      float(dy), float(dts), float(alphaCos), int(fix_q1), int(q2compat), int(q3compat))
+        self._h = ctypes.c_void_p()
+        N.call("e3d_context_create", ctypes.byref(d), ctypes.byref(self._h))
+        self.device = int(device)
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            N.lib().e3d_context_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    def set_medium(self, planes8):
+        """Eight scaled medium planes: numpy (8, ny, nx, nz) float32, or a device tensor of that shape."""
+        if hasattr(planes8, "data_ptr"):
+            assert planes8.is_cuda and planes8.dtype.is_floating_point and planes8.is_contiguous()
+            ptrs = N.ptr_array([planes8[k] for k in range(8)])
+            N.call("e3d_set_medium", self._h, ptrs, 1)
+        else:
+            planes = [N.as_f32(planes8[k]) for k in range(8)]
+            N.call("e3d_set_medium", self._h, N.ptr_array(planes), 0)
+
+    def set_tile_width(self, tx):
+        N.call("e3d_set_tile_width", self._h, int(tx))
+
+    def set_checkpoint_policy(self, ckpt="fp32", segment=0, budget_bytes=0.0):
+        N.call("e3d_set_checkpoint_policy", self._h, CKPT_TYPES[ckpt], int(segment), float(budget_bytes))
+
+    def set_stream(self, stream):
+        """Queue work on an existing CUDA stream (a torch.cuda.Stream or a raw handle); None resets."""
+        h = None if stream is None else int(getattr(stream, "cuda_stream", stream))
+        N.call("e3d_set_stream", self._h, h)
+
+    def synchronize(self):
+        N.call("e3d_synchronize", self._h)
+
+    @property
+    def cells_per_step(self):
+        return int(N.lib().e3d_cells_per_step(self._h))
+
+    def _alloc_signals(self, pos7):
+        return [np.zeros((len(pos7[COMP_GRID[k]]), self.nts), dtype=np.float32) for k in range(9)]
+
+    def nl_forward(self, model9, src_pos7, rec_pos7):
+        model = [N.as_f32(m) for m in model9]
+        data = self._alloc_signals(rec_pos7)
+        SP, SN, k1 = _geom(src_pos7)
+        RP, RN, k2 = _geom(rec_pos7)
+        N.call("e3d_nl_forward", self._h, N.ptr_array(model), N.ptr_array(data), SP, SN, RP, RN)
+        return data
+
+    def nl_adjoint(self, data9, src_pos7, rec_pos7):
+        data = [N.as_f32(d) for d in data9]
+        model = self._alloc_signals(src_pos7)
+        SP, SN, k1 = _geom(src_pos7)
+        RP, RN, k2 = _geom(rec_pos7)
+        N.call("e3d_nl_adjoint", self._h, N.ptr_array(model), N.ptr_array(data), SP, SN, RP, RN)
+        return model
+
+    def born_forward(self, src9, pert8, src_pos7, rec_pos7):
+        src = [N.as_f32(s) for s in src9]
+        pert = [N.as_f32(p) for p in pert8]
+        data = self._alloc_signals(rec_pos7)
+        SP, SN, k1 = _geom(src_pos7)
+        RP, RN, k2 = _geom(rec_pos7)
+        N.call("e3d_born_forward", self._h, N.ptr_array(src), N.ptr_array(data), SP, SN, RP, RN, N.ptr_array(pert))
+        return data
+
+    def born_adjoint(self, src9, data9, src_pos7, rec_pos7, pert8_init=None):
+        src = [N.as_f32(s) for s in src9]
+        data = [N.as_f32(d) for d in data9]
+        pert = [np.zeros(self.shape, dtype=np.float32) if pert8_init is None else np.array(pert8_init[k],
+                                                                                             dtype=np.float32)
+                for k in range(8)]
+        SP, SN, k1 = _geom(src_pos7)
+        RP, RN, k2 = _geom(rec_pos7)
+        N.call("e3d_born_adjoint", self._h, N.ptr_array(src), N.ptr_array(data), SP, SN, RP, RN, N.ptr_array(pert))
+        return pert
+
+    def step_only(self, mode, n_steps):
+        N.call("e3d_step_only", self._h, int(mode), int(n_steps))
+
+    # ---- device API (torch tensors) -------------------------------------------------
+    def nl_propagate_device(self, adjoint, src_pos, src_off, rec_pos, rec_off, src_sig, rec_sig):
+        so = (ctypes.c_int * 10)(*[int(v) for v in src_off])
+        ro = (ctypes.c_int * 10)(*[int(v) for v in rec_off])
+        N.call("e3d_nl_propagate_device", self._h, int(adjoint), src_pos.data_ptr(), so, rec_pos.data_ptr(), ro,
+               src_sig.data_ptr(), rec_sig.data_ptr())
+
+    def fwi_forward_device(self, src_pos, src_off, rec_pos, rec_off, src_sig, rec_sig):
+        so = (ctypes.c_int * 10)(*[int(v) for v in src_off])
+        ro = (ctypes.c_int * 10)(*[int(v) for v in rec_off])
+        N.call("e3d_fwi_forward_device", self._h, src_pos.data_ptr(), so, rec_pos.data_ptr(), ro,
+               src_sig.data_ptr(), rec_sig.data_ptr())
+
+    def fwi_gradient_device(self, src_pos, src_off, rec_pos, rec_off, src_sig, residual, grad8):
+        so = (ctypes.c_int * 10)(*[int(v) for v in src_off])
+        ro = (ctypes.c_int * 10)(*[int(v) for v in rec_off])
+        N.call("e3d_fwi_gradient_device", self._h, src_pos.data_ptr(), so, rec_pos.data_ptr(), ro,
+               src_sig.data_ptr(), residual.data_ptr(), N.ptr_array([grad8[k] for k in range(8)]))

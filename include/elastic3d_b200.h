@@ -1,0 +1,295 @@
+/* elastic3d_b200.h -- C ABI of the B200 elastic 3D propagation library.
+ *
+ * Two layers, both plain C (pointers and sizes, no C++ or torch types):
+ *
+ * 1. The drop-in seam.  Same names and argument meaning as the reference's
+ *    raw-pointer driver functions, which its C++ operator classes call:
+ *      elastic_iso_float/include/nonlinearPropElasticGpuFunctions_3D.h:9-18
+ *      elastic_iso_float/include/BornElasticGpuFunctions_3D.h:9-21
+ *    Every function returns an int status (0 = success) instead of void;
+ *    the reference printed and called exit(-1) on CUDA errors
+ *    (elastic_iso_float/src/cudaErrors_3D.cu:4-27).  Host arrays are owned
+ *    by the caller; outputs are overwritten, as in the reference.  The two
+ *    functions that took std::vector take a pointer and a count.
+ *
+ * 2. An explicit-context API (e3d_*) for new callers: several grids per
+ *    process, device-resident signals, checkpointed FWI gradients.
+ *
+ * Conventions: a field has nz*nx*ny floats, z fastest
+ * (index = iy*nz*nx + ix*nz + iz).  Acquisition positions are int64 indices
+ * into that layout, one table per grid in the order
+ * center, x, y, z, xz, xy, yz.  Signal blocks follow the reference:
+ * one block per wavefield component vx, vy, vz, sxx, syy, szz, sxz, sxy, syz,
+ * each [nDevice][nts] with time fastest.  `sub` is always the internal value
+ * (twice the parameter-file value), as the reference drivers receive it.
+ */
+#ifndef ELASTIC3D_B200_H
+#define ELASTIC3D_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes */
+#define E3D_OK 0
+#define E3D_ERR_ARG 1
+#define E3D_ERR_CUDA 2
+#define E3D_ERR_STATE 3
+#define E3D_ERR_OOM 4
+#define E3D_ERR_BOUNDS 5
+
+/* Human-readable description of the last error on the calling thread. */
+const char* e3d_last_error(void);
+/* Library version string. */
+const char* e3d_version(void);
+
+/* ------------------------------------------------------------------------
+ * 1. Drop-in seam -- nonlinear propagator
+ * ---------------------------------------------------------------------- */
+
+/* Replaces bool getGpuInfo_3D(std::vector<int> gpuList, int info, int deviceNumber)
+ * (nonlinearPropElasticGpuFunctions_3D.h:8).  Returns 0 when every listed
+ * device exists, E3D_ERR_ARG otherwise. */
+int getGpuInfo_3D(const int* gpuList, int nGpuList, int info, int deviceNumberInfo);
+
+/* Replaces void setGpuP2P(int nGpu, int info, std::vector<int> gpuList)
+ * (nonlinearPropElasticGpuFunctions_3D.h:9).  Enables peer access between
+ * the listed devices where the hardware allows it. */
+int setGpuP2P(int nGpu, int info, const int* gpuList);
+
+/* Replaces initNonlinearElasticGpu_3D (nonlinearPropElasticGpuFunctions_3D.h:10).
+ * Records grid, time axis, taper and filter constants for slot iGpu. */
+int initNonlinearElasticGpu_3D(float dz, float dx, float dy, int nz, int nx, int ny, int nts, float dts, int sub,
+                               int minPad, int blockSize, float alphaCos, int nGpu, int iGpuId, int iGpuAlloc);
+
+/* Replaces allocateNonlinearElasticGpu_3D (nonlinearPropElasticGpuFunctions_3D.h:11).
+ * Copies the eight scaled medium planes (host) to device iGpuId. */
+int allocateNonlinearElasticGpu_3D(float* rhoxDtw, float* rhoyDtw, float* rhozDtw, float* lamb2MuDtw,
+                                   float* lambDtw, float* muxzDtw, float* muxyDtw, float* muyzDtw, int nx, int ny,
+                                   int nz, int iGpu, int iGpuId);
+
+/* Replaces deallocateNonlinearElasticGpu_3D (nonlinearPropElasticGpuFunctions_3D.h:12). */
+int deallocateNonlinearElasticGpu_3D(int iGpu, int iGpuId);
+
+/* Replaces propElasticFwdGpu_3D (nonlinearPropElasticGpuFunctions_3D.h:15).
+ * model*: nine source blocks (in); data*: nine receiver blocks (out, overwritten). */
+int propElasticFwdGpu_3D(float* modelRegDts_vx, float* modelRegDts_vy, float* modelRegDts_vz,
+                         float* modelRegDts_sigmaxx, float* modelRegDts_sigmayy, float* modelRegDts_sigmazz,
+                         float* modelRegDts_sigmaxz, float* modelRegDts_sigmaxy, float* modelRegDts_sigmayz,
+                         float* dataRegDts_vx, float* dataRegDts_vy, float* dataRegDts_vz,
+                         float* dataRegDts_sigmaxx, float* dataRegDts_sigmayy, float* dataRegDts_sigmazz,
+                         float* dataRegDts_sigmaxz, float* dataRegDts_sigmaxy, float* dataRegDts_sigmayz,
+                         long long* sourcesPositionRegCenterGrid, long long nSourcesRegCenterGrid,
+                         long long* sourcesPositionRegXGrid, long long nSourcesRegXGrid,
+                         long long* sourcesPositionRegYGrid, long long nSourcesRegYGrid,
+                         long long* sourcesPositionRegZGrid, long long nSourcesRegZGrid,
+                         long long* sourcesPositionRegXZGrid, long long nSourcesRegXZGrid,
+                         long long* sourcesPositionRegXYGrid, long long nSourcesRegXYGrid,
+                         long long* sourcesPositionRegYZGrid, long long nSourcesRegYZGrid,
+                         long long* receiversPositionRegCenterGrid, long long nReceiversRegCenterGrid,
+                         long long* receiversPositionRegXGrid, long long nReceiversRegXGrid,
+                         long long* receiversPositionRegYGrid, long long nReceiversRegYGrid,
+                         long long* receiversPositionRegZGrid, long long nReceiversRegZGrid,
+                         long long* receiversPositionRegXZGrid, long long nReceiversRegXZGrid,
+                         long long* receiversPositionRegXYGrid, long long nReceiversRegXYGrid,
+                         long long* receiversPositionRegYZGrid, long long nReceiversRegYZGrid, int nx, int ny,
+                         int nz, int iGpu, int iGpuId);
+
+/* Replaces propElasticAdjGpu_3D (nonlinearPropElasticGpuFunctions_3D.h:19).
+ * data*: nine receiver blocks (in); model*: nine source blocks (out, overwritten).
+ * Uses the reference's time-reversed stepper (not an exact transpose). */
+int propElasticAdjGpu_3D(float* modelRegDts_vx, float* modelRegDts_vy, float* modelRegDts_vz,
+                         float* modelRegDts_sigmaxx, float* modelRegDts_sigmayy, float* modelRegDts_sigmazz,
+                         float* modelRegDts_sigmaxz, float* modelRegDts_sigmaxy, float* modelRegDts_sigmayz,
+                         float* dataRegDts_vx, float* dataRegDts_vy, float* dataRegDts_vz,
+                         float* dataRegDts_sigmaxx, float* dataRegDts_sigmayy, float* dataRegDts_sigmazz,
+                         float* dataRegDts_sigmaxz, float* dataRegDts_sigmaxy, float* dataRegDts_sigmayz,
+                         long long* sourcesPositionRegCenterGrid, long long nSourcesRegCenterGrid,
+                         long long* sourcesPositionRegXGrid, long long nSourcesRegXGrid,
+                         long long* sourcesPositionRegYGrid, long long nSourcesRegYGrid,
+                         long long* sourcesPositionRegZGrid, long long nSourcesRegZGrid,
+                         long long* sourcesPositionRegXZGrid, long long nSourcesRegXZGrid,
+                         long long* sourcesPositionRegXYGrid, long long nSourcesRegXYGrid,
+                         long long* sourcesPositionRegYZGrid, long long nSourcesRegYZGrid,
+                         long long* receiversPositionRegCenterGrid, long long nReceiversRegCenterGrid,
+                         long long* receiversPositionRegXGrid, long long nReceiversRegXGrid,
+                         long long* receiversPositionRegYGrid, long long nReceiversRegYGrid,
+                         long long* receiversPositionRegZGrid, long long nReceiversRegZGrid,
+                         long long* receiversPositionRegXZGrid, long long nReceiversRegXZGrid,
+                         long long* receiversPositionRegXYGrid, long long nReceiversRegXYGrid,
+                         long long* receiversPositionRegYZGrid, long long nReceiversRegYZGrid, int nx, int ny,
+                         int nz, int iGpu, int iGpuId);
+
+/* ------------------------------------------------------------------------
+ * 1b. Drop-in seam -- Born propagator
+ * ---------------------------------------------------------------------- */
+
+/* Replaces initBornElasticGpu_3D (BornElasticGpuFunctions_3D.h:10). */
+int initBornElasticGpu_3D(float dz, float dx, float dy, int nz, int nx, int ny, int nts, float dts, int sub,
+                          int minPad, int blockSize, float alphaCos, int nGpu, int iGpuId, int iGpuAlloc);
+/* Replaces allocateBornElasticGpu_3D (BornElasticGpuFunctions_3D.h:11). */
+int allocateBornElasticGpu_3D(float* rhoxDtw, float* rhoyDtw, float* rhozDtw, float* lamb2MuDtw, float* lambDtw,
+                              float* muxzDtw, float* muxyDtw, float* muyzDtw, int nx, int ny, int nz, int iGpu,
+                              int iGpuId);
+/* Replaces deallocateBornElasticGpu_3D (BornElasticGpuFunctions_3D.h:12). */
+int deallocateBornElasticGpu_3D(int iGpu, int iGpuId);
+/* Replaces allocatePinBornElasticGpu_3D (BornElasticGpuFunctions_3D.h:14).  The
+ * source wavefield stays on the device (checkpoints), so no pinned host
+ * memory is taken; the call only validates its arguments. */
+int allocatePinBornElasticGpu_3D(int nx, int ny, int nz, int nts, int nGpu, int iGpuId, int iGpu, int iGpuAlloc);
+/* Replaces deallocatePinBornElasticGpu_3D (BornElasticGpuFunctions_3D.h:15). */
+int deallocatePinBornElasticGpu_3D(int iGpu, int iGpuId);
+
+/* Replaces BornElasticFwdGpu_3D (BornElasticGpuFunctions_3D.h:18).  source*:
+ * nine source blocks; data*: nine receiver blocks (out); drho*..dmuyz: the
+ * eight staggered, scaled perturbation planes (in). */
+int BornElasticFwdGpu_3D(float* sourceRegDts_vx, float* sourceRegDts_vy, float* sourceRegDts_vz,
+                         float* sourceRegDts_sigmaxx, float* sourceRegDts_sigmayy, float* sourceRegDts_sigmazz,
+                         float* sourceRegDts_sigmaxz, float* sourceRegDts_sigmaxy, float* sourceRegDts_sigmayz,
+                         float* dataRegDts_vx, float* dataRegDts_vy, float* dataRegDts_vz,
+                         float* dataRegDts_sigmaxx, float* dataRegDts_sigmayy, float* dataRegDts_sigmazz,
+                         float* dataRegDts_sigmaxz, float* dataRegDts_sigmaxy, float* dataRegDts_sigmayz,
+                         long long* sourcesPositionRegCenterGrid, long long nSourcesRegCenterGrid,
+                         long long* sourcesPositionRegXGrid, long long nSourcesRegXGrid,
+                         long long* sourcesPositionRegYGrid, long long nSourcesRegYGrid,
+                         long long* sourcesPositionRegZGrid, long long nSourcesRegZGrid,
+                         long long* sourcesPositionRegXZGrid, long long nSourcesRegXZGrid,
+                         long long* sourcesPositionRegXYGrid, long long nSourcesRegXYGrid,
+                         long long* sourcesPositionRegYZGrid, long long nSourcesRegYZGrid,
+                         long long* receiversPositionRegCenterGrid, long long nReceiversRegCenterGrid,
+                         long long* receiversPositionRegXGrid, long long nReceiversRegXGrid,
+                         long long* receiversPositionRegYGrid, long long nReceiversRegYGrid,
+                         long long* receiversPositionRegZGrid, long long nReceiversRegZGrid,
+                         long long* receiversPositionRegXZGrid, long long nReceiversRegXZGrid,
+                         long long* receiversPositionRegXYGrid, long long nReceiversRegXYGrid,
+                         long long* receiversPositionRegYZGrid, long long nReceiversRegYZGrid, float* drhox,
+                         float* drhoy, float* drhoz, float* dlame, float* dmu, float* dmuxz, float* dmuxy,
+                         float* dmuyz, int nx, int ny, int nz, int iGpu, int iGpuId);
+
+/* Replaces BornElasticAdjGpu_3D (BornElasticGpuFunctions_3D.h:21).  The image
+ * is accumulated onto the caller's eight planes (the reference copies them
+ * to the device first and copies the sum back). */
+int BornElasticAdjGpu_3D(float* sourceRegDts_vx, float* sourceRegDts_vy, float* sourceRegDts_vz,
+                         float* sourceRegDts_sigmaxx, float* sourceRegDts_sigmayy, float* sourceRegDts_sigmazz,
+                         float* sourceRegDts_sigmaxz, float* sourceRegDts_sigmaxy, float* sourceRegDts_sigmayz,
+                         float* dataRegDts_vx, float* dataRegDts_vy, float* dataRegDts_vz,
+                         float* dataRegDts_sigmaxx, float* dataRegDts_sigmayy, float* dataRegDts_sigmazz,
+                         float* dataRegDts_sigmaxz, float* dataRegDts_sigmaxy, float* dataRegDts_sigmayz,
+                         long long* sourcesPositionRegCenterGrid, long long nSourcesRegCenterGrid,
+                         long long* sourcesPositionRegXGrid, long long nSourcesRegXGrid,
+                         long long* sourcesPositionRegYGrid, long long nSourcesRegYGrid,
+                         long long* sourcesPositionRegZGrid, long long nSourcesRegZGrid,
+                         long long* sourcesPositionRegXZGrid, long long nSourcesRegXZGrid,
+                         long long* sourcesPositionRegXYGrid, long long nSourcesRegXYGrid,
+                         long long* sourcesPositionRegYZGrid, long long nSourcesRegYZGrid,
+                         long long* receiversPositionRegCenterGrid, long long nReceiversRegCenterGrid,
+                         long long* receiversPositionRegXGrid, long long nReceiversRegXGrid,
+                         long long* receiversPositionRegYGrid, long long nReceiversRegYGrid,
+                         long long* receiversPositionRegZGrid, long long nReceiversRegZGrid,
+                         long long* receiversPositionRegXZGrid, long long nReceiversRegXZGrid,
+                         long long* receiversPositionRegXYGrid, long long nReceiversRegXYGrid,
+                         long long* receiversPositionRegYZGrid, long long nReceiversRegYZGrid, float* drhox,
+                         float* drhoy, float* drhoz, float* dlame, float* dmu, float* dmuxz, float* dmuxy,
+                         float* dmuyz, int nx, int ny, int nz, int iGpu, int iGpuId);
+
+/* ------------------------------------------------------------------------
+ * 2. Explicit-context API
+ * ---------------------------------------------------------------------- */
+typedef struct e3d_context e3d_context;
+
+typedef struct e3d_desc {
+  int device;
+  int nz, nx, ny;
+  int nts;        /* coarse samples */
+  int sub;        /* internal subsampling (2x the parameter-file value) */
+  int minPad;
+  float dz, dx, dy, dts, alphaCos;
+  int fix_q1;     /* 1: y derivatives divide by dy (the reference divides by dx) */
+  int q2compat;   /* 1: sxz receivers read the z-grid table (reference behaviour) */
+  int q3compat;   /* 1: Born yz shear term uses the xz derivative pair (reference behaviour) */
+} e3d_desc;
+
+/* Counterpart of initNonlinearElasticGpu_3D + allocateNonlinearElasticGpu_3D
+ * with an explicit handle instead of process-global slots. */
+int e3d_context_create(const e3d_desc* desc, e3d_context** out);
+int e3d_context_destroy(e3d_context* ctx);
+/* Eight medium planes (see allocateNonlinearElasticGpu_3D); on_device != 0 for device pointers. */
+int e3d_set_medium(e3d_context* ctx, const float* const* planes8, int on_device);
+/* Stepper tile width along x: 8 or 16 (autotuner hook). */
+int e3d_set_tile_width(e3d_context* ctx, int tx);
+/* Checkpoint storage: type 0 = fp32, 1 = fp16, 2 = bf16 (per-slice scaled);
+ * segment = coarse blocks per segment (0 = largest that fits);
+ * budget_bytes = device bytes for checkpoints and velocity slots (0 = 85% of free). */
+int e3d_set_checkpoint_policy(e3d_context* ctx, int type, int segment, double budget_bytes);
+/* Wait for all work queued on the context's stream. */
+int e3d_synchronize(e3d_context* ctx);
+/* cudaStream_t of the context, as void*. */
+void* e3d_stream(e3d_context* ctx);
+/* Queue the context's work on an existing cudaStream_t (passed as void*), e.g. the
+ * caller's framework stream; NULL restores the context's own stream. */
+int e3d_set_stream(e3d_context* ctx, void* stream);
+/* Updated cells per fine step ((nz-8)(nx-8)(ny-8)). */
+long long e3d_cells_per_step(const e3d_context* ctx);
+
+/* Host-buffer propagations.  src_pos/rec_pos: 7 tables; n_src/n_rec: 7 counts. */
+int e3d_nl_forward(e3d_context* ctx, const float* const* model9, float* const* data9,
+                   const long long* const* src_pos, const long long* n_src, const long long* const* rec_pos,
+                   const long long* n_rec);
+int e3d_nl_adjoint(e3d_context* ctx, float* const* model9, const float* const* data9,
+                   const long long* const* src_pos, const long long* n_src, const long long* const* rec_pos,
+                   const long long* n_rec);
+int e3d_born_forward(e3d_context* ctx, const float* const* src9, float* const* data9,
+                     const long long* const* src_pos, const long long* n_src, const long long* const* rec_pos,
+                     const long long* n_rec, const float* const* pert8);
+int e3d_born_adjoint(e3d_context* ctx, const float* const* src9, const float* const* data9,
+                     const long long* const* src_pos, const long long* n_src, const long long* const* rec_pos,
+                     const long long* n_rec, float* const* pert8);
+
+/* Device-buffer propagations.  Signals are time-major [nts][ntot] with the
+ * nine components concatenated; pos_dev is the matching int64 table and
+ * off10[k]..off10[k+1] is component k's range.  Work is queued on the
+ * context's stream; call e3d_synchronize before reading outputs. */
+int e3d_nl_propagate_device(e3d_context* ctx, int adjoint, const long long* src_pos_dev, const int* src_off10,
+                            const long long* rec_pos_dev, const int* rec_off10, float* src_sig_dev,
+                            float* rec_sig_dev);
+/* FWI: nonlinear forward that also saves on-device wavefield checkpoints. */
+int e3d_fwi_forward_device(e3d_context* ctx, const long long* src_pos_dev, const int* src_off10,
+                           const long long* rec_pos_dev, const int* rec_off10, const float* src_sig_dev,
+                           float* rec_sig_dev);
+/* FWI: Born adjoint of the residual, accumulated into eight device planes;
+ * consumes the checkpoints of the preceding e3d_fwi_forward_device. */
+int e3d_fwi_gradient_device(e3d_context* ctx, const long long* src_pos_dev, const int* src_off10,
+                            const long long* rec_pos_dev, const int* rec_off10, const float* src_sig_dev,
+                            const float* residual_dev, float* const* grad8_dev);
+
+/* Bare stepper (mode 0 forward, 1 time-reversed, 2 exact transpose) applied
+ * n_steps times to the context's working wavefields; for benchmarking. */
+int e3d_step_only(e3d_context* ctx, int mode, int n_steps);
+
+/* ------------------------------------------------------------------------
+ * Host preparation (native counterparts of the reference's C++ host code)
+ * ---------------------------------------------------------------------- */
+/* fdParamElastic_3D medium preparation (fdParamElastic_3D.cpp:130-193):
+ * elastic = [rho; lambda; mu] (3*nz*nx*ny, z fastest) -> eight scaled planes. */
+int e3d_medium_planes(int nz, int nx, int ny, float dtw, const float* elastic, float* const* out8);
+
+/* staggerX/Y/Z forward (adjoint=0) or adjoint (adjoint=1), axis 0=z 1=x 2=y,
+ * out = (add ? out : 0) + op(in)   (stagger_3D.cpp:23-208). */
+int e3d_stagger(int nz, int nx, int ny, int axis, int adjoint, int add, const float* in, float* out);
+
+/* spaceInterpGpu_3D linear weights and unique regular-grid points
+ * (spaceInterpGpu_3D.cpp:113-138, 178-348) for one grid.
+ * grid: nz,nx,ny; origins/samplings as float; pads[6] = fat, zPadMinus,
+ * zPadPlus, xPadMinus, xPadPlus, yPad.  Outputs (caller-sized):
+ *   index[nDev*nFilter], weight[nDev*nFilter], unique[<= nDev*nFilter], slot[nDev*nFilter];
+ *   *n_unique receives the unique count.  nFilter = 8, or 16 with dipole. */
+int e3d_space_interp_linear(const float* z, const float* x, const float* y, long long n_dev, int nz, int nx, int ny,
+                            float oz, float ox, float oy, float dz, float dx, float dy, const int* pads6,
+                            float error_tolerance, int dipole, float zshift, float xshift, float yshift,
+                            long long* index, float* weight, long long* unique, long long* slot,
+                            long long* n_unique);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ELASTIC3D_B200_H */

@@ -1,0 +1,98 @@
+"""GPU parity: the CUDA path (through the C ABI) against the oracle on the same inputs.
+
+Tolerances: relative L2 over all traces.  FP32 CUDA vs FP32 oracle differ
+only by summation order/FMA contraction (1e-5); FP32 vs the FP64 oracle is
+the north-star accuracy bound (1e-5 for forward traces, 1e-4 for the Born
+image, whose imaging condition multiplies two propagated fields).
+"""
+import numpy as np
+import pytest
+
+from cases import prepared, random_signals, rel_l2
+from elasticisolib_3d_b200.engine import Propagator
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def _prop(p, **kw):
+    pr = Propagator(p.nz, p.nx, p.ny, p.nts, p.sub, p.minPad, p.dz, p.dx, p.dy, p.dts, p.alphaCos, **kw)
+    return pr
+
+
+@pytest.mark.parametrize("tx", [8, 16])
+def test_nl_forward_matches_oracle(tx):
+    sv, p, med, src, rec, dtw = prepared(seed=1)
+    rng = np.random.default_rng(5)
+    spos = [d.unique for d in src]
+    rpos = [d.unique for d in rec]
+    sig = random_signals(spos, p.nts, rng)
+    pr = _prop(p)
+    pr.set_tile_width(tx)
+    pr.set_medium(med)
+    got = pr.nl_forward(sig, spos, rpos)
+    ref32 = O.nl_forward_reg(p, med, sig, spos, rpos, np.float32)
+    ref64 = O.nl_forward_reg(p, med.astype(np.float64), [s.astype(np.float64) for s in sig], spos, rpos, np.float64)
+    assert rel_l2(got, ref32) < 1e-5
+    assert rel_l2(got, ref64) < 1e-5
+
+
+def test_nl_adjoint_matches_oracle():
+    sv, p, med, src, rec, dtw = prepared(seed=2)
+    rng = np.random.default_rng(6)
+    spos = [d.unique for d in src]
+    rpos = [d.unique for d in rec]
+    dat = random_signals(rpos, p.nts, rng)
+    pr = _prop(p)
+    pr.set_medium(med)
+    got = pr.nl_adjoint(dat, spos, rpos)
+    ref = O.nl_adjoint_reg(p, med, dat, spos, rpos, np.float32)
+    assert rel_l2(got, ref) < 1e-5
+
+
+def test_born_forward_matches_oracle():
+    sv, p, med, src, rec, dtw = prepared(seed=3)
+    rng = np.random.default_rng(7)
+    spos = [d.unique for d in src]
+    rpos = [d.unique for d in rec]
+    sig = random_signals(spos, p.nts, rng)
+    pert = (rng.standard_normal((8,) + med.shape[1:]) * 1e-2).astype(np.float32)
+    pr = _prop(p)
+    pr.set_medium(med)
+    got = pr.born_forward(sig, pert, spos, rpos)
+    ref = O.born_forward_reg(p, med, sig, pert, spos, rpos, np.float32)
+    assert rel_l2(got, ref) < 1e-5
+
+
+@pytest.mark.parametrize("segment", [0, 1, 3])
+def test_born_adjoint_matches_oracle(segment):
+    sv, p, med, src, rec, dtw = prepared(seed=4)
+    rng = np.random.default_rng(8)
+    spos = [d.unique for d in src]
+    rpos = [d.unique for d in rec]
+    sig = random_signals(spos, p.nts, rng)
+    dat = random_signals(rpos, p.nts, rng)
+    pr = _prop(p)
+    pr.set_medium(med)
+    pr.set_checkpoint_policy("fp32", segment)
+    got = pr.born_adjoint(sig, dat, spos, rpos)
+    ref = O.born_adjoint_reg(p, med, sig, dat, spos, rpos, None, np.float32)
+    assert rel_l2(got, ref) < 1e-5
+
+
+def test_born_dot_product():
+    """<B m, d> = <m, B^T d> for the CUDA Born pair (reference tolerance 1e-5, operator.h:50)."""
+    sv, p, med, src, rec, dtw = prepared(seed=5)
+    rng = np.random.default_rng(9)
+    spos = [d.unique for d in src]
+    rpos = [d.unique for d in rec]
+    sig = random_signals(spos, p.nts, rng)
+    dat = random_signals(rpos, p.nts, rng)
+    pert = (rng.standard_normal((8,) + med.shape[1:])).astype(np.float32)
+    pr = _prop(p)
+    pr.set_medium(med)
+    Bm = pr.born_forward(sig, pert, spos, rpos)
+    Btd = pr.born_adjoint(sig, dat, spos, rpos)
+    lhs = sum(float(np.sum(a.astype(np.float64) * b)) for a, b in zip(Bm, dat))
+    rhs = sum(float(np.sum(a.astype(np.float64) * b)) for a, b in zip(pert, Btd))
+    assert abs(lhs - rhs) / abs(rhs) < 1e-5
