@@ -46,7 +46,7 @@ SIGNATURES = {
     "e3d_context_create": ([P, P], I),
     "e3d_context_destroy": ([P], I),
     "e3d_set_medium": ([P, P, I], I),
-    "e3d_set_tile_width": ([P, I], I),
+    "e3d_set_stepper_variant": ([P, I, I, I], I),
     "e3d_set_checkpoint_policy": ([P, I, I, D], I),
     "e3d_synchronize": ([P], I),
     "e3d_stream": ([P], P),

@@ -281,9 +281,9 @@ int e3d_set_medium(e3d_context* ctx, const float* const* planes8, int on_device)
   return setMedium(ctx->c, planes8, on_device != 0);
 }
 
-int e3d_set_tile_width(e3d_context* ctx, int tx) {
+int e3d_set_stepper_variant(e3d_context* ctx, int tx, int stages, int loader) {
   CTX_OR_FAIL(ctx);
-  return setTileWidth(ctx->c, tx);
+  return setStepperVariant(ctx->c, tx, stages, loader);
 }
 
 int e3d_set_checkpoint_policy(e3d_context* ctx, int type, int segment, double budget_bytes) {
@@ -295,7 +295,7 @@ int e3d_synchronize(e3d_context* ctx) {
   CTX_OR_FAIL(ctx);
   cudaError_t e = cudaStreamSynchronize(stream(ctx->c));
   if (e != cudaSuccess) return fail(E3D_ERR_CUDA, cudaGetErrorString(e));
-  return E3D_OK;
+  return checkPipeError(ctx->c);
 }
 
 void* e3d_stream(e3d_context* ctx) { return (ctx && ctx->c) ? (void*)stream(ctx->c) : nullptr; }

@@ -16,6 +16,8 @@
 
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
+#include <cudaTypedefs.h>
+#include <unordered_map>
 
 #include "engine.h"
 #include "kernels.cuh"
@@ -62,7 +64,10 @@ struct Context {
   float dtsInv = 0.f;
   float* med[NMED] = {};
   bool haveMedium = false;
-  int tx = 16;
+  int tx = 8;
+  int stages = 2;            // shared-memory pipeline depth of the stepper
+  int loader = 2;            // 0: plain loads, 1: cp.async, 2: TMA bulk tensor copies
+  std::unordered_map<unsigned long long, CUtensorMap> tmaps;  // (pointer, box) -> tensor map
   std::vector<void*> owned;  // every device allocation of this context
   // working wavefields (primary propagation)
   Fields9 w0, w1;
@@ -235,9 +240,28 @@ int setMedium(Context* c, const float* const* planes, bool onDevice) {
   return E3D_OK;
 }
 
-int setTileWidth(Context* c, int tx) {
+int setStepperVariant(Context* c, int tx, int stages, int loader) {
   E3D_ARG(c && (tx == 8 || tx == 16), "tile width must be 8 or 16");
+  E3D_ARG(stages == 2 || stages == 3, "pipeline depth must be 2 or 3");
+  E3D_ARG(loader >= 0 && loader <= 2, "loader must be 0 (plain), 1 (cp.async) or 2 (TMA)");
+  E3D_ARG(!(tx == 16 && stages == 3), "16-wide tiles fit two stages at most");
   c->tx = tx;
+  c->stages = stages;
+  c->loader = loader;
+  return E3D_OK;
+}
+
+int checkPipeError(Context* c) {
+  unsigned flag = 0;
+  E3D_CUDA_TRY(cudaMemcpyFromSymbolAsync(&flag, g_e3dPipeError, sizeof(flag), 0, cudaMemcpyDeviceToHost, c->st));
+  E3D_CUDA_TRY(cudaStreamSynchronize(c->st));
+  if (flag) {
+    const unsigned zero = 0;
+    cudaMemcpyToSymbolAsync(g_e3dPipeError, &zero, sizeof(zero), 0, cudaMemcpyHostToDevice, c->st);
+    cudaStreamSynchronize(c->st);
+    setLastError("stepper pipeline wait expired (bulk copies did not complete)", __FILE__, __LINE__);
+    return E3D_ERR_CUDA;
+  }
   return E3D_OK;
 }
 
@@ -264,6 +288,116 @@ static StepPtrs makeStep(Context* c, Fields9& o, const Fields9& cur) {
   return p;
 }
 
+template <int MODE, int TX, int STAGES>
+static int launchPipe(Context* c, const StepPtrs& p, dim3 grid, int yChunk) {
+  constexpr size_t smem = (size_t)STAGES * PipeLayout<TX>::STAGE_F * sizeof(float);
+  static bool configured = false;
+  if (!configured) {
+    E3D_CUDA_TRY(cudaFuncSetAttribute(kStepPipe<MODE, TX, STAGES>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)smem));
+    configured = true;
+  }
+  kStepPipe<MODE, TX, STAGES><<<grid, dim3(TZ, TX), smem, c->st>>>(p, c->g, yChunk);
+  return E3D_OK;
+}
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no libcuda link dependency)
+static PFN_cuTensorMapEncodeTiled_v12000 tmaEncoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  if (!fn) {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (PFN_cuTensorMapEncodeTiled_v12000)f;
+  }
+  return fn;
+}
+
+// 3D map over a (nz, nx, ny) float field with a boxZ x boxX x 1 box, zero fill outside
+static int tensorMap(Context* c, const float* ptr, int boxZ, int boxX, const CUtensorMap** out) {
+  const unsigned long long key = (reinterpret_cast<unsigned long long>(ptr) << 8) ^ (unsigned long long)(boxZ * 64 + boxX);
+  auto it = c->tmaps.find(key);
+  if (it != c->tmaps.end()) {
+    *out = &it->second;
+    return E3D_OK;
+  }
+  auto enc = tmaEncoder();
+  E3D_ARG(enc != nullptr, "cuTensorMapEncodeTiled unavailable");
+  E3D_ARG((reinterpret_cast<unsigned long long>(ptr) & 15) == 0, "field not 16-byte aligned");
+  CUtensorMap m;
+  cuuint64_t dims[3] = {(cuuint64_t)c->d.nz, (cuuint64_t)c->d.nx, (cuuint64_t)c->d.ny};
+  cuuint64_t strides[2] = {(cuuint64_t)c->d.nz * 4, (cuuint64_t)c->g.yStride * 4};
+  cuuint32_t box[3] = {(cuuint32_t)boxZ, (cuuint32_t)boxX, 1};
+  cuuint32_t es[3] = {1, 1, 1};
+  CUresult r = enc(&m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float*>(ptr), dims, strides, box, es,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    setLastError("cuTensorMapEncodeTiled failed", __FILE__, __LINE__);
+    return E3D_ERR_CUDA;
+  }
+  auto ins = c->tmaps.emplace(key, m);
+  *out = &ins.first->second;
+  return E3D_OK;
+}
+
+template <int TX>
+static int buildMaps(Context* c, const StepPtrs& p, TmaMaps& mp) {
+  const CUtensorMap* m = nullptr;
+  const float* tileSrc[NTILE] = {p.c[VX], p.c[VY], p.c[VZ], p.c[SXX], p.c[SZZ], p.c[SXY], p.c[SXZ], p.c[SYZ]};
+  const float* leadSrc[NQUEUE] = {p.c[VX], p.c[VY], p.c[VZ], p.c[SYY], p.c[SXY], p.c[SYZ]};
+  for (int t = 0; t < NTILE; t++) {
+    E3D_RET(tensorMap(c, tileSrc[t], SZ, TX + 2 * HALO, &m));
+    mp.halo[t] = *m;
+  }
+  for (int q = 0; q < NQUEUE; q++) {
+    E3D_RET(tensorMap(c, leadSrc[q], TZ, TX, &m));
+    mp.lead[q] = *m;
+  }
+  for (int k = 0; k < NCOMP; k++) {
+    E3D_RET(tensorMap(c, p.o[k], TZ, TX, &m));
+    mp.old[k] = *m;
+  }
+  for (int k = 0; k < NMED; k++) {
+    E3D_RET(tensorMap(c, p.m[k], TZ, TX, &m));
+    mp.med[k] = *m;
+  }
+  return E3D_OK;
+}
+
+template <int MODE, int TX, int STAGES>
+static int launchTma(Context* c, const StepPtrs& p, dim3 grid, int yChunk) {
+  constexpr size_t smem = (size_t)STAGES * PipeLayout<TX>::STAGE_F * sizeof(float);
+  static bool configured = false;
+  if (!configured) {
+    E3D_CUDA_TRY(cudaFuncSetAttribute(kStepTma<MODE, TX, STAGES>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)smem));
+    configured = true;
+  }
+  TmaMaps mp;
+  E3D_RET(buildMaps<TX>(c, p, mp));
+  kStepTma<MODE, TX, STAGES><<<grid, dim3(TZ, TX), smem, c->st>>>(mp, p, c->g, yChunk);
+  return E3D_OK;
+}
+
+template <int MODE>
+static int launchVariant(Context* c, const StepPtrs& p, dim3 grid, int yChunk) {
+  const int key = c->tx * 10 + c->stages;
+  if (c->loader == 2) {
+    switch (key) {
+      case 82: return launchTma<MODE, 8, 2>(c, p, grid, yChunk);
+      case 83: return launchTma<MODE, 8, 3>(c, p, grid, yChunk);
+      default: return launchTma<MODE, 16, 2>(c, p, grid, yChunk);
+    }
+  }
+  switch (key) {
+    case 82: return launchPipe<MODE, 8, 2>(c, p, grid, yChunk);
+    case 83: return launchPipe<MODE, 8, 3>(c, p, grid, yChunk);
+    default: return launchPipe<MODE, 16, 2>(c, p, grid, yChunk);
+  }
+}
+
 static int launchStep(Context* c, int mode, const StepPtrs& p) {
   const GridConst& g = c->g;
   const int tiz = (g.nz - 2 * FAT + TZ - 1) / TZ;
@@ -276,7 +410,11 @@ static int launchStep(Context* c, int mode, const StepPtrs& p) {
   const int yChunk = (nyi + chunks - 1) / chunks;
   chunks = (nyi + yChunk - 1) / yChunk;
   dim3 grid(tiz, tix, chunks);
-  if (c->tx == 16) {
+  const bool pipe = (g.nz % 4 == 0) && mode != STEP_ADJ_EXACT && c->loader > 0;
+  if (pipe) {
+    if (mode == STEP_FWD) E3D_RET(launchVariant<STEP_FWD>(c, p, grid, yChunk));
+    else E3D_RET(launchVariant<STEP_ADJ_REVERSED>(c, p, grid, yChunk));
+  } else if (c->tx == 16) {
     dim3 block(TZ, 16);
     if (mode == STEP_FWD) kStep<STEP_FWD, 16><<<grid, block, 0, c->st>>>(p, g, yChunk);
     else if (mode == STEP_ADJ_REVERSED) kStep<STEP_ADJ_REVERSED, 16><<<grid, block, 0, c->st>>>(p, g, yChunk);
@@ -491,6 +629,7 @@ int nlPropagateHost(Context* c, bool adjoint, float* const* model, float* const*
   if (st == E3D_OK) st = adjoint ? stageSignalsIn(c, R, data) : stageSignalsZero(c, R);
   if (st == E3D_OK) st = nlPropagateDevice(c, adjoint, S.set, R.set, S.sig, R.sig);
   if (st == E3D_OK) st = adjoint ? stageSignalsOut(c, S, model) : stageSignalsOut(c, R, data);
+  if (st == E3D_OK) st = checkPipeError(c);
   if (st == E3D_OK) {
     cudaError_t e = cudaStreamSynchronize(c->st);
     if (e != cudaSuccess) {
@@ -885,6 +1024,7 @@ int bornForwardHost(Context* c, const float* const* srcSig, float* const* data, 
   if (st == E3D_OK) st = stageSignalsZero(c, R);
   if (st == E3D_OK) st = bornForwardDevice(c, S.set, R.set, S.sig, R.sig);
   if (st == E3D_OK) st = stageSignalsOut(c, R, data);
+  if (st == E3D_OK) st = checkPipeError(c);
   if (st == E3D_OK && cudaStreamSynchronize(c->st) != cudaSuccess) {
     setLastError("stream failure", __FILE__, __LINE__);
     st = E3D_ERR_CUDA;
@@ -911,6 +1051,7 @@ int bornAdjointHost(Context* c, const float* const* srcSig, const float* const* 
   if (st == E3D_OK) st = stageSignalsIn(c, S, srcSig);
   if (st == E3D_OK) st = stageSignalsIn(c, R, const_cast<float* const*>(data));
   if (st == E3D_OK) st = bornAdjointDevice(c, S.set, R.set, S.sig, R.sig);
+  if (st == E3D_OK) st = checkPipeError(c);
   if (st == E3D_OK) {
     for (int k = 0; k < NMED && st == E3D_OK; k++) {
       cudaError_t e = cudaMemcpyAsync(pert[k], c->pertDev[k], (size_t)c->g.n * sizeof(float),

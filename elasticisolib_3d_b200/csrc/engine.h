@@ -36,8 +36,12 @@ int createContext(const ContextDesc& d, Context** out);
 void destroyContext(Context* c);
 // medium: 8 planes of nz*nx*ny floats; onDevice selects host or device pointers
 int setMedium(Context* c, const float* const* planes, bool onDevice);
-// Which stepper tile width to use (8 or 16), for the autotuner.
-int setTileWidth(Context* c, int tx);
+// Stepper variant for the autotuner: tile width along x (8 or 16), shared
+// memory pipeline depth (2 or 3) and plane loader (0 plain loads, 1 cp.async,
+// 2 TMA bulk tensor copies).
+int setStepperVariant(Context* c, int tx, int stages, int loader);
+// Reads and clears the device flag set when a bounded pipeline wait expired.
+int checkPipeError(Context* c);
 int setCheckpointPolicy(Context* c, int ckptType, int segment, double budgetBytes);
 
 // Reference-layout host entry points ([nDevice][nts] per component).

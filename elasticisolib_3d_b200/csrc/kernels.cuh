@@ -11,6 +11,7 @@
 // read as the "old" level, which gives the same recursion without a second
 // pass over 18 arrays.
 #pragma once
+#include <cuda.h>
 #include "common.cuh"
 
 namespace e3d {
@@ -206,6 +207,375 @@ __global__ void __launch_bounds__(TZ * TX) kStep(StepPtrs p, GridConst g, int yC
         for (int k = 0; k < 7; k++) w[q][k] = w[q][k + 1];
       }
     }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Pipelined stepper (modes 0/1).  Same arithmetic as kStep; every per-plane
+// global read (the eight halo tiles, the six y-window leads, the old level and
+// the medium) is issued as 16-byte cp.async copies into a STAGES-deep ring of
+// shared-memory stages, so plane y+1.. are in flight while plane y computes,
+// with one barrier per plane.  Requires nz % 4 == 0 (16-byte rows), which the
+// reference's block-size rule guarantees.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void cpAsync16(float* smem, const float* gmem, bool valid) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  const int sz = valid ? 16 : 0;
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(sz) : "memory");
+}
+__device__ __forceinline__ void cpAsyncCommit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cpAsyncWait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+template <int TX>
+struct PipeLayout {
+  static constexpr int SX = TX + 2 * HALO;
+  static constexpr int HALO_F = SZ * SX;       // floats per halo tile
+  static constexpr int INT_F = TZ * TX;        // floats per interior tile
+  static constexpr int HALO_CH = HALO_F / 4;   // 16-byte chunks per halo tile
+  static constexpr int INT_CH = INT_F / 4;
+  static constexpr int N_INT = NQUEUE + NCOMP + NMED;  // leads, old level, medium
+  static constexpr int STAGE_F = NTILE * HALO_F + N_INT * INT_F;
+  static constexpr int LEAD_OFF = NTILE * HALO_F;
+  static constexpr int OLD_OFF = LEAD_OFF + NQUEUE * INT_F;
+  static constexpr int MED_OFF = OLD_OFF + NCOMP * INT_F;
+};
+
+__device__ __forceinline__ int tileComp(int t) {
+  return t == T_VX ? VX : t == T_VY ? VY : t == T_VZ ? VZ : t == T_SXX ? SXX : t == T_SZZ ? SZZ
+         : t == T_SXY ? SXY : t == T_SXZ ? SXZ : SYZ;
+}
+__device__ __forceinline__ int queueComp(int q) {
+  return q == Q_VX ? VX : q == Q_VY ? VY : q == Q_VZ ? VZ : q == Q_SYY ? SYY : q == Q_SXY ? SXY : SYZ;
+}
+
+template <int TX>
+__device__ __forceinline__ void issuePlane(const StepPtrs& p, const GridConst& g, float* st, int y, int z0, int x0,
+                                           int tid) {
+  using L = PipeLayout<TX>;
+  constexpr int NT = TZ * TX;
+  const long long ys = g.yStride;
+  const long long plane = (long long)y * ys;
+  // halo tiles: rows of 40 floats starting at z0-4 (16-byte aligned when nz % 4 == 0)
+  for (int c = tid; c < NTILE * L::HALO_CH; c += NT) {
+    const int t = c / L::HALO_CH;
+    const int r = c - t * L::HALO_CH;
+    const int lx = r / (SZ / 4), q = r - lx * (SZ / 4);
+    const int gz = z0 - HALO + 4 * q, gx = x0 - HALO + lx;
+    const bool ok = (gz < g.nz) && (gx < g.nx);
+    const float* src = p.c[tileComp(t)];
+    cpAsync16(st + t * L::HALO_F + lx * SZ + 4 * q, ok ? src + plane + (long long)gx * g.nz + gz : src, ok);
+  }
+  // interior tiles: y-window leads, old level, medium
+  for (int c = tid; c < L::N_INT * L::INT_CH; c += NT) {
+    const int f = c / L::INT_CH;
+    const int r = c - f * L::INT_CH;
+    const int lx = r / (TZ / 4), q = r - lx * (TZ / 4);
+    const int gz = z0 + 4 * q, gx = x0 + lx;
+    const bool ok = (gz < g.nz) && (gx < g.nx);
+    const float* src;
+    long long off = (long long)gx * g.nz + gz;
+    if (f < NQUEUE) {
+      src = p.c[queueComp(f)];
+      off += (long long)(y + qBase(f) + 7) * ys;
+    } else if (f < NQUEUE + NCOMP) {
+      src = p.o[f - NQUEUE];
+      off += plane;
+    } else {
+      src = p.m[f - NQUEUE - NCOMP];
+      off += plane;
+    }
+    cpAsync16(st + L::LEAD_OFF + f * L::INT_F + lx * TZ + 4 * q, ok ? src + off : src, ok);
+  }
+}
+
+template <int MODE, int TX, int STAGES>
+__global__ void __launch_bounds__(TZ * TX) kStepPipe(StepPtrs p, GridConst g, int yChunk) {
+  using L = PipeLayout<TX>;
+  extern __shared__ __align__(16) float smem[];
+  const int tz = threadIdx.x, tx = threadIdx.y;
+  const int tid = tx * TZ + tz;
+  const int z0 = FAT + blockIdx.x * TZ, x0 = FAT + blockIdx.y * TX;
+  const int iz = z0 + tz, ix = x0 + tx;
+  const bool active = (iz < g.nz - FAT) && (ix < g.nx - FAT);
+  const int yBeg = FAT + blockIdx.z * yChunk;
+  const int yEnd = min(yBeg + yChunk, g.ny - FAT);
+  const long long ys = g.yStride;
+  const long long col = (long long)ix * g.nz + iz;
+
+  // prologue: planes yBeg .. yBeg+STAGES-2 in flight
+#pragma unroll
+  for (int s = 0; s < STAGES - 1; s++) {
+    if (yBeg + s < yEnd) issuePlane<TX>(p, g, smem + s * L::STAGE_F, yBeg + s, z0, x0, tid);
+    cpAsyncCommit();
+  }
+  float w[NQUEUE][8];
+  if (active) {
+#pragma unroll
+    for (int q = 0; q < NQUEUE; q++) {
+#pragma unroll
+      for (int k = 0; k < 7; k++) w[q][k] = __ldg(p.c[queueComp(q)] + (long long)(yBeg + qBase(q) + k) * ys + col);
+    }
+  }
+  const int lc = (tx + HALO) * SZ + (tz + HALO);
+  const int li = tx * TZ + tz;
+  int slot = 0;
+  for (int y = yBeg; y < yEnd; y++) {
+    cpAsyncWait<STAGES - 2>();
+    __syncthreads();  // plane y visible to all; the stage read at y-1 is free again
+    {
+      const int yn = y + STAGES - 1;
+      int ns = slot + STAGES - 1;
+      if (ns >= STAGES) ns -= STAGES;
+      if (yn < yEnd) issuePlane<TX>(p, g, smem + ns * L::STAGE_F, yn, z0, x0, tid);
+      cpAsyncCommit();
+    }
+    const float* st = smem + slot * L::STAGE_F;
+    if (active) {
+#pragma unroll
+      for (int q = 0; q < NQUEUE; q++) w[q][7] = st[L::LEAD_OFF + q * L::INT_F + li];
+      const float* tl[NTILE];
+#pragma unroll
+      for (int t = 0; t < NTILE; t++) tl[t] = st + t * L::HALO_F;
+      const float* cz = g.cz;
+      const float* cx = g.cx;
+      const float* cy = g.cy;
+      const float dvx_dx = dPlus(tl[T_VX], lc, SZ, cx);
+      const float dvy_dy = dWin(w[Q_VY], cy);
+      const float dvz_dz = dPlus(tl[T_VZ], lc, 1, cz);
+      const float fvx = dMinus(tl[T_SXX], lc, SZ, cx) + dWin(w[Q_SXY], cy) + dPlus(tl[T_SXZ], lc, 1, cz);
+      const float fvy = dPlus(tl[T_SXY], lc, SZ, cx) + dWin(w[Q_SYY], cy) + dPlus(tl[T_SYZ], lc, 1, cz);
+      const float fvz = dPlus(tl[T_SXZ], lc, SZ, cx) + dWin(w[Q_SYZ], cy) + dMinus(tl[T_SZZ], lc, 1, cz);
+      const float fxy = dWin(w[Q_VX], cy) + dMinus(tl[T_VY], lc, SZ, cx);
+      const float fxz = dMinus(tl[T_VX], lc, 1, cz) + dMinus(tl[T_VZ], lc, SZ, cx);
+      const float fyz = dWin(w[Q_VZ], cy) + dMinus(tl[T_VY], lc, 1, cz);
+      const float* mv = st + L::MED_OFF + li;
+      const float* ov = st + L::OLD_OFF + li;
+      const float sgn = (MODE == STEP_FWD) ? 1.0f : -1.0f;
+      float up[NCOMP];
+      up[VX] = sgn * (mv[RHOX * L::INT_F] * fvx);
+      up[VY] = sgn * (mv[RHOY * L::INT_F] * fvy);
+      up[VZ] = sgn * (mv[RHOZ * L::INT_F] * fvz);
+      const float l2m = mv[L2M * L::INT_F], lam = mv[LAM * L::INT_F];
+      up[SXX] = sgn * (l2m * dvx_dx + lam * (dvy_dy + dvz_dz));
+      up[SYY] = sgn * (l2m * dvy_dy + lam * (dvx_dx + dvz_dz));
+      up[SZZ] = sgn * (l2m * dvz_dz + lam * (dvx_dx + dvy_dy));
+      up[SXZ] = sgn * (mv[MUXZ * L::INT_F] * fxz);
+      up[SXY] = sgn * (mv[MUXY * L::INT_F] * fxy);
+      up[SYZ] = sgn * (mv[MUYZ * L::INT_F] * fyz);
+      const float G = taperAt(g, iz, ix, y);
+      const long long ic = (long long)y * ys + col;
+      const bool hasSS = p.ssL[0] != nullptr;
+      const bool hasAcc = p.accL[0] != nullptr;
+#pragma unroll
+      for (int k = 0; k < NCOMP; k++) {
+        float v = G * ov[k * L::INT_F] + up[k];
+        if (hasSS) v += __ldg(p.ssL[k] + ic) * p.ssWl + __ldg(p.ssR[k] + ic) * p.ssWr;
+        v *= G;
+        p.o[k][ic] = v;
+        if (hasAcc && k < p.nAcc) {
+          p.accL[k][ic] += v * p.accWl;
+          if (p.accR[0] != nullptr) p.accR[k][ic] += v * p.accWr;
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < NQUEUE; q++) {
+#pragma unroll
+        for (int k = 0; k < 7; k++) w[q][k] = w[q][k + 1];
+      }
+    }
+    slot = (slot + 1 == STAGES) ? 0 : slot + 1;
+  }
+  cpAsyncWait<0>();
+}
+
+// ---------------------------------------------------------------------------
+// TMA stepper.  One elected thread per CTA issues, for every plane, the 31
+// tile copies of that plane (eight halo boxes 40 x (TX+8), six y-window lead
+// boxes, nine old-level and eight medium boxes 32 x TX) as
+// cp.async.bulk.tensor loads completing on one mbarrier per stage; the other
+// threads only compute.  Boxes start at z0-4 or z0, multiples of 4 floats, so
+// the innermost TMA coordinate is 16-byte aligned; boxes reaching past nz/nx
+// are zero-filled by the hardware.  Every mbarrier wait is bounded: on
+// expiry the CTA records the failure in g_e3dPipeError, waits (bounded) for
+// its own copies in flight and returns.
+// ---------------------------------------------------------------------------
+struct TmaMaps {
+  CUtensorMap halo[NTILE];   // current level, halo box
+  CUtensorMap lead[NQUEUE];  // current level, interior box (y-window leads)
+  CUtensorMap old[NCOMP];    // old level, interior box
+  CUtensorMap med[NMED];     // medium, interior box
+};
+
+__device__ unsigned int g_e3dPipeError;
+
+__device__ __forceinline__ unsigned smemAddr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbarInit(unsigned long long* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smemAddr(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbarExpectTx(unsigned long long* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smemAddr(bar)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbarTryWait(unsigned long long* bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smemAddr(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// bounded wait: false when the iteration budget is exhausted
+__device__ __forceinline__ bool mbarWaitBounded(unsigned long long* bar, unsigned parity) {
+  for (int i = 0; i < (1 << 22); i++)
+    if (mbarTryWait(bar, parity)) return true;
+  return false;
+}
+__device__ __forceinline__ void tmaLoad3d(float* dst, const CUtensorMap* map, int c0, int c1, int c2,
+                                          unsigned long long* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+      "[%5];\n" ::"r"(smemAddr(dst)),
+      "l"(reinterpret_cast<unsigned long long>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(smemAddr(bar))
+      : "memory");
+}
+
+template <int TX>
+__device__ __forceinline__ void tmaIssuePlane(const TmaMaps& mp, float* st, unsigned long long* bar, int y, int z0,
+                                              int x0) {
+  using L = PipeLayout<TX>;
+  constexpr unsigned bytes = (unsigned)L::STAGE_F * 4u;
+  mbarExpectTx(bar, bytes);
+#pragma unroll
+  for (int t = 0; t < NTILE; t++) tmaLoad3d(st + t * L::HALO_F, &mp.halo[t], z0 - HALO, x0 - HALO, y, bar);
+#pragma unroll
+  for (int q = 0; q < NQUEUE; q++)
+    tmaLoad3d(st + L::LEAD_OFF + q * L::INT_F, &mp.lead[q], z0, x0, y + qBase(q) + 7, bar);
+#pragma unroll
+  for (int k = 0; k < NCOMP; k++) tmaLoad3d(st + L::OLD_OFF + k * L::INT_F, &mp.old[k], z0, x0, y, bar);
+#pragma unroll
+  for (int k = 0; k < NMED; k++) tmaLoad3d(st + L::MED_OFF + k * L::INT_F, &mp.med[k], z0, x0, y, bar);
+}
+
+template <int MODE, int TX, int STAGES>
+__global__ void __launch_bounds__(TZ * TX) kStepTma(const __grid_constant__ TmaMaps mp, StepPtrs p, GridConst g,
+                                                     int yChunk) {
+  using L = PipeLayout<TX>;
+  extern __shared__ __align__(1024) float smem[];
+  __shared__ __align__(8) unsigned long long bars[STAGES];
+  const int tz = threadIdx.x, tx = threadIdx.y;
+  const int tid = tx * TZ + tz;
+  const int z0 = FAT + blockIdx.x * TZ, x0 = FAT + blockIdx.y * TX;
+  const int iz = z0 + tz, ix = x0 + tx;
+  const bool active = (iz < g.nz - FAT) && (ix < g.nx - FAT);
+  const int yBeg = FAT + blockIdx.z * yChunk;
+  const int yEnd = min(yBeg + yChunk, g.ny - FAT);
+  const long long ys = g.yStride;
+  const long long col = (long long)ix * g.nz + iz;
+
+  if (tid == 0) {
+    for (int s = 0; s < STAGES; s++) mbarInit(&bars[s], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  __syncthreads();
+  if (tid == 0) {
+    for (int s = 0; s < STAGES - 1; s++)
+      if (yBeg + s < yEnd) tmaIssuePlane<TX>(mp, smem + s * L::STAGE_F, &bars[s], yBeg + s, z0, x0);
+  }
+  float w[NQUEUE][8];
+  if (active) {
+#pragma unroll
+    for (int q = 0; q < NQUEUE; q++) {
+#pragma unroll
+      for (int k = 0; k < 7; k++) w[q][k] = __ldg(p.c[queueComp(q)] + (long long)(yBeg + qBase(q) + k) * ys + col);
+    }
+  }
+  // sponge distance: the z/x part is fixed for this thread
+  const int dzx = min(min(iz - FAT, ix - FAT), min(g.nz - iz - 1 - FAT, g.nx - ix - 1 - FAT));
+  const int lc = (tx + HALO) * SZ + (tz + HALO);
+  const int li = tx * TZ + tz;
+  int slot = 0;
+  unsigned parity = 0;  // bit s: parity of the next completion of stage s
+  for (int y = yBeg; y < yEnd; y++) {
+    const bool ok = mbarWaitBounded(&bars[slot], (parity >> slot) & 1u);
+    // barrier: every thread is past plane y-1, so its stage can be refilled;
+    // the OR makes an expired wait a CTA-wide decision
+    if (__syncthreads_or(!ok)) {
+      if (tid == 0) {
+        atomicExch(&g_e3dPipeError, 1u);
+        // drain the copies this CTA still has in flight (bounded), then leave
+        for (int s = 0; s < STAGES; s++) mbarWaitBounded(&bars[s], (parity >> s) & 1u);
+      }
+      __syncthreads();
+      return;
+    }
+    parity ^= 1u << slot;
+    if (tid == 0) {
+      const int yn = y + STAGES - 1;
+      int ns = slot + STAGES - 1;
+      if (ns >= STAGES) ns -= STAGES;
+      if (yn < yEnd) tmaIssuePlane<TX>(mp, smem + ns * L::STAGE_F, &bars[ns], yn, z0, x0);
+    }
+    const float* st = smem + slot * L::STAGE_F;
+    if (active) {
+#pragma unroll
+      for (int q = 0; q < NQUEUE; q++) w[q][7] = st[L::LEAD_OFF + q * L::INT_F + li];
+      const float* tl[NTILE];
+#pragma unroll
+      for (int t = 0; t < NTILE; t++) tl[t] = st + t * L::HALO_F;
+      const float* cz = g.cz;
+      const float* cx = g.cx;
+      const float* cy = g.cy;
+      const float dvx_dx = dPlus(tl[T_VX], lc, SZ, cx);
+      const float dvy_dy = dWin(w[Q_VY], cy);
+      const float dvz_dz = dPlus(tl[T_VZ], lc, 1, cz);
+      const float fvx = dMinus(tl[T_SXX], lc, SZ, cx) + dWin(w[Q_SXY], cy) + dPlus(tl[T_SXZ], lc, 1, cz);
+      const float fvy = dPlus(tl[T_SXY], lc, SZ, cx) + dWin(w[Q_SYY], cy) + dPlus(tl[T_SYZ], lc, 1, cz);
+      const float fvz = dPlus(tl[T_SXZ], lc, SZ, cx) + dWin(w[Q_SYZ], cy) + dMinus(tl[T_SZZ], lc, 1, cz);
+      const float fxy = dWin(w[Q_VX], cy) + dMinus(tl[T_VY], lc, SZ, cx);
+      const float fxz = dMinus(tl[T_VX], lc, 1, cz) + dMinus(tl[T_VZ], lc, SZ, cx);
+      const float fyz = dWin(w[Q_VZ], cy) + dMinus(tl[T_VY], lc, 1, cz);
+      const float* mv = st + L::MED_OFF + li;
+      const float* ov = st + L::OLD_OFF + li;
+      const float sgn = (MODE == STEP_FWD) ? 1.0f : -1.0f;
+      float up[NCOMP];
+      up[VX] = sgn * (mv[RHOX * L::INT_F] * fvx);
+      up[VY] = sgn * (mv[RHOY * L::INT_F] * fvy);
+      up[VZ] = sgn * (mv[RHOZ * L::INT_F] * fvz);
+      const float l2m = mv[L2M * L::INT_F], lam = mv[LAM * L::INT_F];
+      up[SXX] = sgn * (l2m * dvx_dx + lam * (dvy_dy + dvz_dz));
+      up[SYY] = sgn * (l2m * dvy_dy + lam * (dvx_dx + dvz_dz));
+      up[SZZ] = sgn * (l2m * dvz_dz + lam * (dvx_dx + dvy_dy));
+      up[SXZ] = sgn * (mv[MUXZ * L::INT_F] * fxz);
+      up[SXY] = sgn * (mv[MUXY * L::INT_F] * fxy);
+      up[SYZ] = sgn * (mv[MUYZ * L::INT_F] * fyz);
+      const int d = min(dzx, min(y - FAT, g.ny - y - 1 - FAT));
+      const float G = d < g.minPad ? __ldg(g.taper + d) : 1.0f;
+      const long long ic = (long long)y * ys + col;
+      const bool hasSS = p.ssL[0] != nullptr;
+      const bool hasAcc = p.accL[0] != nullptr;
+#pragma unroll
+      for (int k = 0; k < NCOMP; k++) {
+        float v = G * ov[k * L::INT_F] + up[k];
+        if (hasSS) v += __ldg(p.ssL[k] + ic) * p.ssWl + __ldg(p.ssR[k] + ic) * p.ssWr;
+        v *= G;
+        p.o[k][ic] = v;
+        if (hasAcc && k < p.nAcc) {
+          p.accL[k][ic] += v * p.accWl;
+          if (p.accR[0] != nullptr) p.accR[k][ic] += v * p.accWr;
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < NQUEUE; q++) {
+#pragma unroll
+        for (int k = 0; k < 7; k++) w[q][k] = w[q][k + 1];
+      }
+    }
+    slot = (slot + 1 == STAGES) ? 0 : slot + 1;
   }
 }
 

@@ -62,8 +62,11 @@ class Propagator:
             planes = [N.as_f32(planes8[k]) for k in range(8)]
             N.call("e3d_set_medium", self._h, N.ptr_array(planes), 0)
 
-    def set_tile_width(self, tx):
-        N.call("e3d_set_tile_width", self._h, int(tx))
+    LOADERS = {"plain": 0, "cpasync": 1, "tma": 2}
+
+    def set_stepper_variant(self, tx=8, stages=2, loader="tma"):
+        """Stepper variant: x tile width (8/16), shared-memory stages (2/3) and plane loader."""
+        N.call("e3d_set_stepper_variant", self._h, int(tx), int(stages), self.LOADERS[loader])
 
     def set_checkpoint_policy(self, ckpt="fp32", segment=0, budget_bytes=0.0):
         N.call("e3d_set_checkpoint_policy", self._h, CKPT_TYPES[ckpt], int(segment), float(budget_bytes))

@@ -215,13 +215,16 @@ int e3d_context_create(const e3d_desc* desc, e3d_context** out);
 int e3d_context_destroy(e3d_context* ctx);
 /* Eight medium planes (see allocateNonlinearElasticGpu_3D); on_device != 0 for device pointers. */
 int e3d_set_medium(e3d_context* ctx, const float* const* planes8, int on_device);
-/* Stepper tile width along x: 8 or 16 (autotuner hook). */
-int e3d_set_tile_width(e3d_context* ctx, int tx);
+/* Stepper variant (autotuner hook): tile width along x (8 or 16), shared-memory
+ * pipeline depth (2 or 3 stages) and plane loader (0 plain loads, 1 cp.async,
+ * 2 TMA bulk tensor copies; 1 and 2 need nz % 4 == 0). */
+int e3d_set_stepper_variant(e3d_context* ctx, int tx, int stages, int loader);
 /* Checkpoint storage: type 0 = fp32, 1 = fp16, 2 = bf16 (per-slice scaled);
  * segment = coarse blocks per segment (0 = largest that fits);
  * budget_bytes = device bytes for checkpoints and velocity slots (0 = 85% of free). */
 int e3d_set_checkpoint_policy(e3d_context* ctx, int type, int segment, double budget_bytes);
-/* Wait for all work queued on the context's stream. */
+/* Wait for all work queued on the context's stream; reports an expired
+ * bounded pipeline wait inside the stepper as E3D_ERR_CUDA. */
 int e3d_synchronize(e3d_context* ctx);
 /* cudaStream_t of the context, as void*. */
 void* e3d_stream(e3d_context* ctx);

@@ -20,15 +20,19 @@ def _prop(p, **kw):
     return pr
 
 
-@pytest.mark.parametrize("tx", [8, 16])
-def test_nl_forward_matches_oracle(tx):
+VARIANTS = [(8, 2, "plain"), (16, 2, "plain"), (8, 2, "cpasync"), (8, 3, "cpasync"), (16, 2, "cpasync"),
+            (8, 2, "tma"), (8, 3, "tma"), (16, 2, "tma")]
+
+
+@pytest.mark.parametrize("tx,stages,loader", VARIANTS)
+def test_nl_forward_matches_oracle(tx, stages, loader):
     sv, p, med, src, rec, dtw = prepared(seed=1)
     rng = np.random.default_rng(5)
     spos = [d.unique for d in src]
     rpos = [d.unique for d in rec]
     sig = random_signals(spos, p.nts, rng)
     pr = _prop(p)
-    pr.set_tile_width(tx)
+    pr.set_stepper_variant(tx, stages, loader)
     pr.set_medium(med)
     got = pr.nl_forward(sig, spos, rpos)
     ref32 = O.nl_forward_reg(p, med, sig, spos, rpos, np.float32)
@@ -37,13 +41,15 @@ def test_nl_forward_matches_oracle(tx):
     assert rel_l2(got, ref64) < 1e-5
 
 
-def test_nl_adjoint_matches_oracle():
+@pytest.mark.parametrize("loader", ["plain", "tma"])
+def test_nl_adjoint_matches_oracle(loader):
     sv, p, med, src, rec, dtw = prepared(seed=2)
     rng = np.random.default_rng(6)
     spos = [d.unique for d in src]
     rpos = [d.unique for d in rec]
     dat = random_signals(rpos, p.nts, rng)
     pr = _prop(p)
+    pr.set_stepper_variant(8, 2, loader)
     pr.set_medium(med)
     got = pr.nl_adjoint(dat, spos, rpos)
     ref = O.nl_adjoint_reg(p, med, dat, spos, rpos, np.float32)
