@@ -1,0 +1,347 @@
+#!/usr/bin/env python
+"""Benchmark: elastic FWI gradient shots/s on B200.
+
+Workload (the FWI-gradient configuration): 300^3 interior + 40-cell sponge
+(392 x 392 x 388 cells with the FAT ring), dx = 10 m, 2500 coarse samples at
+2 ms (9996 fine steps), explosive Ricker 10 Hz source, 150 x 150 receivers
+(all nine components), L2 misfit.  True model = smooth background + two
+Gaussian anomalies; the gradient is taken at the background model.  Inputs are
+seeded synthetic data (no dataset is involved).
+
+One step = one shot's FWI gradient: nonlinear forward with on-device
+checkpoints, residual at the receivers, Born adjoint of the residual with the
+source wavefield recomputed from the checkpoints, and the Born model
+post-processing, through ``ElasticFwiMisfit`` (autograd forward+backward).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Multi-GPU (torchrun): shots shard across ranks with no data-path collective
+(weak scaling: every rank takes K shots); the time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "FWI gradient shots/s (Born-adjoint gradient, 300^3+40 sponge, 2500 samples)"
+UNIT = "shots/s"
+STEPPER_BYTES_PER_CELL = 140.0          # forward stepper: read old 9 + cur 9 + medium 8, write new 9 (fp32)
+ADJ_BYTES_PER_CELL = 176.0 + 144.0       # dual-state exact adjoint + decimation of 9 fields into 2 accumulators
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--nts", type=int, default=2500)
+    ap.add_argument("--interior", type=int, default=300)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+class ClockSampler:
+    """nvidia-smi clock and throttle-reason samples during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu):
+        self.gpu = gpu
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["clock sampling unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def build_problem(args, device):
+    import torch
+    from elasticisolib_3d_b200 import fwi as F
+    from elasticisolib_3d_b200 import hostprep as H
+    from elasticisolib_3d_b200 import synthetic as S
+    n = args.interior
+    sv = S.config_fwi(nzi=n, nxi=n, nyi=n, nts=args.nts, true_model=False)
+    svt = S.config_fwi(nzi=n, nxi=n, nyi=n, nts=args.nts, true_model=True)
+    fd = H.FdParam(sv.elastic, sv.axes, sv.par)
+    ax7 = H.grid_axes(*(a.n for a in sv.axes), *(a.o for a in sv.axes), *(a.d for a in sv.axes))
+    prob = F.FwiProblem(fd, device=device)
+    rank = int(os.environ.get("RANK", "0"))
+    shot_id = rank % len(sv.src_xyz)
+    src = H.build_devices(*sv.src_xyz[shot_id], ax7, fd.nts, sv.par)
+    rec = H.build_devices(*sv.rec_xyz, ax7, fd.nts, sv.par)
+    irr = [np.zeros((1, fd.nts), dtype=np.float32) for _ in range(9)]
+    for k in (3, 4, 5):
+        irr[k][0] = sv.wavelet
+    shot = F.make_shot(src, rec, irr, None, device)
+    # observed data: nonlinear forward on the true model
+    mt = [torch.tensor(svt.elastic[k], device=device) for k in range(3)]
+    planes = prob.set_model(*mt)
+    rec_t, _ = prob.forward_data(shot, planes)
+    shot.d_obs = shot.rec.to_irregular(rec_t)
+    del rec_t, planes, mt
+    prob.shots.append(shot)
+    torch.cuda.synchronize()
+    return sv, fd, prob
+
+
+def cpu_baseline(fd, n_sample_fwd=2, n_sample_adj=1):
+    """Oracle (C++/OpenMP restatement) stepper timed on the host cores over a bounded sample of the
+    same grid, extrapolated to one gradient (2 forward-type passes + 1 adjoint pass)."""
+    import ctypes
+    from oracle import oracle as O
+    L = O.lib()
+    threads = L.oracle_num_threads(os.cpu_count() or 1)
+    p = O.PropParams(fd.nz, fd.nx, fd.ny, fd.nts, fd.sub, fd.minPad, float(fd.dz), float(fd.dx), float(fd.dy),
+                     float(fd.dts))
+    shape = (fd.ny, fd.nx, fd.nz)
+    rng = np.random.default_rng(0)
+    med = [np.asarray(fd.planes[k]) for k in range(8)]
+    p0 = [np.zeros(shape, np.float32) for _ in range(9)]
+    p1 = [rng.standard_normal(shape, dtype=np.float32) * 1e-3 for _ in range(9)]
+    a, k1 = O._ptrs(p0)
+    b, k2 = O._ptrs(p1)
+    m, k3 = O._ptrs(med)
+    prm = p.c()
+    t0 = time.perf_counter()
+    for _ in range(n_sample_fwd):
+        L.oracle_step_f32(ctypes.byref(prm), a, b, m, 0, 1)
+    t_fwd = (time.perf_counter() - t0) / n_sample_fwd
+    t0 = time.perf_counter()
+    for _ in range(n_sample_adj):
+        L.oracle_step_f32(ctypes.byref(prm), a, b, m, 2, 1)
+    t_adj = (time.perf_counter() - t0) / n_sample_adj
+    steps = (fd.nts - 1) * fd.sub
+    t_shot = 2 * steps * t_fwd + steps * t_adj
+    return {"value": 1.0 / t_shot, "unit": UNIT, "cores": int(threads), "kind": "port",
+            "sample": f"{n_sample_fwd} forward + {n_sample_adj} exact-adjoint fine steps of the oracle stepper "
+                      f"(FP32, fused sponge) on the full {fd.nz}x{fd.nx}x{fd.ny} grid, extrapolated to "
+                      f"2x{steps} forward + {steps} adjoint steps per gradient"}
+
+
+def run_reference(args):
+    """Reference arm: the reference's path has no CPU implementation, so the oracle port runs on the
+    host cores (rank 0 only)."""
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    from elasticisolib_3d_b200 import hostprep as H
+    from elasticisolib_3d_b200 import synthetic as S
+    n = args.interior
+    sv = S.config_fwi(nzi=n, nxi=n, nyi=n, nts=args.nts)
+    fd = H.FdParam(sv.elastic, sv.axes, sv.par)
+    vals = []
+    for i in range(args.warmup + args.steps):
+        cb = cpu_baseline(fd, 1, 1)
+        if i >= args.warmup:
+            vals.append(cb["value"])
+    v = float(np.mean(vals))
+    cb["value"] = v
+    out = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": 1e3 / v, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)", "impl": "reference",
+           "config": {"workload": "fwi-gradient 300^3+40 sponge (392x392x388), 2500 samples, 150x150 receivers",
+                      "l2_flush": "inputs larger than L2"},
+           "cpu_baseline": cb, "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    from elasticisolib_3d_b200 import fwi as F
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=1800), device_id=device)
+
+    sv, fd, prob = build_problem(args, device)
+    m = [torch.tensor(sv.elastic[k], device=device, requires_grad=True) for k in range(3)]
+
+    def step():
+        loss = F.ElasticFwiMisfit.apply(m[0], m[1], m[2], prob)
+        loss.backward()
+        for x in m:
+            x.grad = None
+        return loss
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+
+    stream = torch.cuda.current_stream(device)
+    prob.prop.kernel_timing(16)
+    prob.prop.kernel_timing_read(0)
+    prob.prop.kernel_timing_read(2)
+    launches0 = prob.prop.launch_count
+    clocks = ClockSampler(local)
+    clocks.start()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clk = clocks.stop()
+    launches = prob.prop.launch_count - launches0
+    ms = e0.elapsed_time(e1)
+    fwd_ms, fwd_n = prob.prop.kernel_timing_read(0)
+    adj_ms, adj_n = prob.prop.kernel_timing_read(2)
+    prob.prop.kernel_timing(0)
+    t = torch.tensor([ms], device=device, dtype=torch.float64)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    value = world * args.steps / (ms_max / 1e3)
+
+    # end to end through the public API: model and observed data from pinned host memory,
+    # gradient back to pinned host memory, every step
+    e2e = None
+    if not args.no_e2e:
+        host_model = [torch.from_numpy(np.ascontiguousarray(sv.elastic[k])).pin_memory() for k in range(3)]
+        shot = prob.shots[0]
+        host_obs = shot.d_obs.cpu().pin_memory()
+        host_grad = [torch.empty_like(h).pin_memory() for h in host_model]
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a0.record(stream)
+        for _ in range(args.steps):
+            md = [h.to(device, non_blocking=True).requires_grad_(True) for h in host_model]
+            shot.d_obs = host_obs.to(device, non_blocking=True)
+            loss = F.ElasticFwiMisfit.apply(md[0], md[1], md[2], prob)
+            loss.backward()
+            for hg, x in zip(host_grad, md):
+                hg.copy_(x.grad, non_blocking=True)
+            lv = loss.item()
+        a1.record(stream)
+        torch.cuda.synchronize()
+        t2 = torch.tensor([a0.elapsed_time(a1)], device=device, dtype=torch.float64)
+        if world > 1:
+            dist.all_reduce(t2, op=dist.ReduceOp.MAX)
+        h2d = sum(h.numel() * 4 for h in host_model) + host_obs.numel() * 4
+        d2h = sum(h.numel() * 4 for h in host_grad) + 8
+        e2e = {"value": world * args.steps / (float(t2.item()) / 1e3), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+               "d2h_bytes_per_step": int(d2h), "loss": lv}
+
+    if rank == 0:
+        cells = prob.prop.cells_per_step
+        peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+        if os.path.exists(peaks_path):
+            with open(peaks_path) as f:
+                peak = float(json.load(f)["hbm_gbs"])
+            peak_src = "measured"
+        else:
+            peak, peak_src = 6650.0, "fallback"
+        achieved = STEPPER_BYTES_PER_CELL * cells / (fwd_ms / 1e3) / 1e9 if fwd_ms > 0 else None
+        traffic_per_cell = None
+        prof = os.path.join(ROOT, "profiles", "stepper_fwd_tma_384x384x96.txt")
+        if os.path.exists(prof):
+            for line in open(prof):
+                if line.startswith("dram_bytes_per_cell:"):
+                    traffic_per_cell = float(line.split(":")[1])
+        steps_per_pass = (fd.nts - 1) * fd.sub
+        seg = prob.prop.checkpoint_segment
+        nseg = -(-(fd.nts - 1) // seg) if seg else 1
+        # forward + recompute (one extra block per segment and up to two past its end) + adjoint
+        recompute_blocks = (fd.nts - 1) + 3 * (nseg - 1)
+        cell_updates = cells * (steps_per_pass + recompute_blocks * fd.sub + steps_per_pass)
+        out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+               "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+               "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+               "config": {"workload": f"fwi-gradient {args.interior}^3+40 sponge ({fd.nz}x{fd.nx}x{fd.ny}), "
+                                      f"{fd.nts} samples ({steps_per_pass} fine steps), 150x150 receivers x 9 "
+                                      f"components, Ricker 10 Hz, one shot per step per GPU",
+                          "parallelism": f"shots sharded over {world} GPU(s)",
+                          "l2_flush": "inputs larger than L2 (each field 238 MB, working set > 14 GB)",
+                          "checkpoint_segment_blocks": seg},
+               "gcell_updates_per_s": world * args.steps * cell_updates / (ms_max / 1e3) / 1e9,
+               "roofline": {"kernel": "forward stepper (kStepTma)", "bound": "hbm",
+                            "achieved": achieved, "peak": peak, "peak_source": peak_src, "unit": "GB/s",
+                            "frac": (achieved / peak) if achieved else None,
+                            "traffic": traffic_per_cell * cells if traffic_per_cell else None,
+                            "algorithmic_bytes_per_cell": STEPPER_BYTES_PER_CELL,
+                            "avg_launch_ms": fwd_ms, "sampled_launches": fwd_n,
+                            "adjoint_stepper": {"avg_launch_ms": adj_ms, "sampled_launches": adj_n,
+                                                "algorithmic_bytes_per_cell": ADJ_BYTES_PER_CELL,
+                                                "achieved_gbs": ADJ_BYTES_PER_CELL * cells / (adj_ms / 1e3) / 1e9
+                                                if adj_ms > 0 else None}},
+               "gpu_launches": int(launches), "clocks": clk, "e2e": e2e}
+        if world == 1 and not args.no_cpu:
+            out["cpu_baseline"] = cpu_baseline(fd)
+        print(json.dumps(out), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -50,8 +50,9 @@ SIGNATURES = {
     "e3d_set_checkpoint_policy": ([P, I, I, D], I),
     "e3d_synchronize": ([P], I),
     "e3d_stream": ([P], P),
-    "e3d_set_stream": ([P, P], I),
+    "e3d_set_stream": ([P, P, I], I),
     "e3d_cells_per_step": ([P], LL),
+    "e3d_checkpoint_segment": ([P], I),
     "e3d_nl_forward": ([P] * 7, I),
     "e3d_nl_adjoint": ([P] * 7, I),
     "e3d_born_forward": ([P] * 8, I),
@@ -60,6 +61,9 @@ SIGNATURES = {
     "e3d_fwi_forward_device": ([P] * 7, I),
     "e3d_fwi_gradient_device": ([P] * 8, I),
     "e3d_step_only": ([P, I, I], I),
+    "e3d_kernel_timing": ([P, I], I),
+    "e3d_kernel_timing_read": ([P, I, P, P], I),
+    "e3d_launch_count": ([P], LL),
     "e3d_medium_planes": ([I, I, I, F, P, P], I),
     "e3d_stagger": ([I, I, I, I, I, I, P, P], I),
     "e3d_space_interp_linear": ([P, P, P, LL, I, I, I, F, F, F, F, F, F, P, F, I, F, F, F, P, P, P, P, P], I),

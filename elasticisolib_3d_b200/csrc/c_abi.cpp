@@ -300,12 +300,14 @@ int e3d_synchronize(e3d_context* ctx) {
 
 void* e3d_stream(e3d_context* ctx) { return (ctx && ctx->c) ? (void*)stream(ctx->c) : nullptr; }
 
-int e3d_set_stream(e3d_context* ctx, void* s) {
+int e3d_set_stream(e3d_context* ctx, void* s, int use_own) {
   CTX_OR_FAIL(ctx);
-  return setStream(ctx->c, (cudaStream_t)s);
+  return setStream(ctx->c, (cudaStream_t)s, use_own != 0);
 }
 
 long long e3d_cells_per_step(const e3d_context* ctx) { return (ctx && ctx->c) ? cellsPerStep(ctx->c) : 0; }
+
+int e3d_checkpoint_segment(const e3d_context* ctx) { return (ctx && ctx->c) ? checkpointSegment(ctx->c) : 0; }
 
 int e3d_nl_forward(e3d_context* ctx, const float* const* model9, float* const* data9, const long long* const* src_pos,
                    const long long* n_src, const long long* const* rec_pos, const long long* n_rec) {
@@ -383,6 +385,18 @@ int e3d_fwi_gradient_device(e3d_context* ctx, const long long* src_pos_dev, cons
   if (st != E3D_OK) return st;
   return fwiGradientDevice(ctx->c, S, R, src_sig_dev, residual_dev, grad8_dev);
 }
+
+int e3d_kernel_timing(e3d_context* ctx, int every) {
+  CTX_OR_FAIL(ctx);
+  return setKernelTiming(ctx->c, every);
+}
+
+int e3d_kernel_timing_read(e3d_context* ctx, int mode, double* avg_ms, long long* count) {
+  CTX_OR_FAIL(ctx);
+  return readKernelTiming(ctx->c, mode, avg_ms, count);
+}
+
+long long e3d_launch_count(const e3d_context* ctx) { return (ctx && ctx->c) ? launchCount(ctx->c) : 0; }
 
 int e3d_step_only(e3d_context* ctx, int mode, int n_steps) {
   CTX_OR_FAIL(ctx);

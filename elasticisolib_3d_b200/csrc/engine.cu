@@ -75,18 +75,29 @@ struct Context {
   Fields9 s0, s1;            // source-side state
   std::vector<float*> vSlots;  // decimated source velocity slots (3 fields each)
   Fields9 ss[2];             // secondary sources (forward) / decimated adjoint field (adjoint)
+  Fields9 q0, q1;            // premultiplied adjoint levels (dual-state exact adjoint)
   float* pertDev[NMED] = {};
   // checkpoints
-  int ckptType = CKPT_F32;
+  int ckptType = CKPT_AUTO;
+  int ckptUsed = CKPT_F32;     // storage type of the current checkpoints
+  double ckptHeld = 0;         // bytes of checkpoints + velocity slots currently allocated
   int segment = 0;           // coarse blocks per segment (0 = automatic)
   double budget = 0;         // bytes available for checkpoints + velocity slots (0 = automatic)
   std::vector<void*> ckpt;   // one per segment (index = segment id), packed 18-field states
   std::vector<float*> ckptScale;
   int ckptSegLen = 0;
+  int ckptAllocType = -1;
   bool ckptValid = false;
   // scratch for transposes / signal staging
   void* scratch = nullptr;
   size_t scratchBytes = 0;
+  // launch accounting and sampled stepper timing
+  long long launches = 0;
+  int timingEvery = 0;       // 0: off; n: time every n-th stepper launch
+  long long stepCounter = 0;
+  std::vector<cudaEvent_t> evPool;
+  struct Timed { int mode; cudaEvent_t a, b; };
+  std::vector<Timed> timed;
 };
 
 static int devAlloc(Context* c, void** p, size_t bytes) {
@@ -201,6 +212,11 @@ int createContext(const ContextDesc& d, Context** out) {
 void destroyContext(Context* c) {
   if (!c) return;
   cudaSetDevice(c->d.device);
+  for (auto& t : c->timed) {
+    c->evPool.push_back(t.a);
+    c->evPool.push_back(t.b);
+  }
+  for (cudaEvent_t e : c->evPool) cudaEventDestroy(e);
   for (void* p : c->owned) cudaFreeAsync(p, c->st);
   c->owned.clear();
   if (c->st) cudaStreamSynchronize(c->st);
@@ -209,10 +225,11 @@ void destroyContext(Context* c) {
 }
 
 cudaStream_t stream(Context* c) { return c->st; }
-int setStream(Context* c, cudaStream_t s) {
+int setStream(Context* c, cudaStream_t s, bool useOwn) {
   E3D_ARG(c != nullptr, "null context");
+  if (c->st == (useOwn ? c->own : s)) return E3D_OK;
   E3D_CUDA_TRY(cudaStreamSynchronize(c->st));
-  c->st = s ? s : c->own;
+  c->st = useOwn ? c->own : s;
   return E3D_OK;
 }
 long long cellsPerStep(const Context* c) {
@@ -243,7 +260,7 @@ int setMedium(Context* c, const float* const* planes, bool onDevice) {
 int setStepperVariant(Context* c, int tx, int stages, int loader) {
   E3D_ARG(c && (tx == 8 || tx == 16), "tile width must be 8 or 16");
   E3D_ARG(stages == 2 || stages == 3, "pipeline depth must be 2 or 3");
-  E3D_ARG(loader >= 0 && loader <= 2, "loader must be 0 (plain), 1 (cp.async) or 2 (TMA)");
+  E3D_ARG(loader >= 0 && loader <= 5, "loader must be 0 (plain), 1 (cp.async), 2-5 (TMA forms)");
   E3D_ARG(!(tx == 16 && stages == 3), "16-wide tiles fit two stages at most");
   c->tx = tx;
   c->stages = stages;
@@ -266,7 +283,7 @@ int checkPipeError(Context* c) {
 }
 
 int setCheckpointPolicy(Context* c, int type, int segment, double budget) {
-  E3D_ARG(c && type >= CKPT_F32 && type <= CKPT_BF16, "bad checkpoint type");
+  E3D_ARG(c && type >= CKPT_AUTO && type <= CKPT_BF16, "bad checkpoint type");
   E3D_ARG(segment >= 0, "segment length must be >= 0");
   c->ckptType = type;
   c->segment = segment;
@@ -381,9 +398,44 @@ static int launchTma(Context* c, const StepPtrs& p, dim3 grid, int yChunk) {
   return E3D_OK;
 }
 
+template <int MODE, int TX, int STAGES, bool OM_SMEM, int MINB>
+static int launchTma2(Context* c, const StepPtrs& p, dim3 grid, int yChunk) {
+  constexpr size_t smem = (size_t)STAGES * Tma2Layout<TX, OM_SMEM>::STAGE_F * sizeof(float);
+  static bool configured = false;
+  if (!configured) {
+    E3D_CUDA_TRY(cudaFuncSetAttribute(kStepTma2<MODE, TX, STAGES, OM_SMEM, MINB>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    configured = true;
+  }
+  TmaMaps mp;
+  E3D_RET(buildMaps<TX>(c, p, mp));
+  kStepTma2<MODE, TX, STAGES, OM_SMEM, MINB><<<grid, dim3(TZ, TX), smem, c->st>>>(mp, p, c->g, yChunk);
+  return E3D_OK;
+}
+
 template <int MODE>
 static int launchVariant(Context* c, const StepPtrs& p, dim3 grid, int yChunk) {
   const int key = c->tx * 10 + c->stages;
+  if (c->loader == 3) {  // rotating window, old level and medium in shared memory
+    switch (key) {
+      case 82: return launchTma2<MODE, 8, 2, true, 2>(c, p, grid, yChunk);
+      case 83: return launchTma2<MODE, 8, 3, true, 1>(c, p, grid, yChunk);
+      default: return launchTma2<MODE, 16, 2, true, 1>(c, p, grid, yChunk);
+    }
+  }
+  if (c->loader == 4) {  // rotating window, old level and medium by plain loads, 3 CTAs/SM
+    switch (key) {
+      case 82: return launchTma2<MODE, 8, 2, false, 3>(c, p, grid, yChunk);
+      case 83: return launchTma2<MODE, 8, 3, false, 3>(c, p, grid, yChunk);
+      default: return launchTma2<MODE, 16, 2, false, 1>(c, p, grid, yChunk);
+    }
+  }
+  if (c->loader == 5) {  // as 4 with the register budget of 2 CTAs/SM
+    switch (key) {
+      case 82: return launchTma2<MODE, 8, 2, false, 2>(c, p, grid, yChunk);
+      default: return launchTma2<MODE, 8, 3, false, 2>(c, p, grid, yChunk);
+    }
+  }
   if (c->loader == 2) {
     switch (key) {
       case 82: return launchTma<MODE, 8, 2>(c, p, grid, yChunk);
@@ -398,7 +450,72 @@ static int launchVariant(Context* c, const StepPtrs& p, dim3 grid, int yChunk) {
   }
 }
 
+static int launchStepRaw(Context* c, int mode, const StepPtrs& p);
+
+static cudaEvent_t takeEvent(Context* c) {
+  if (c->evPool.empty()) {
+    cudaEvent_t e;
+    if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
+    return e;
+  }
+  cudaEvent_t e = c->evPool.back();
+  c->evPool.pop_back();
+  return e;
+}
+
+// Every stepper launch goes through here: counts it and, when sampling is
+// on, brackets every n-th one with CUDA events on the launching stream.
 static int launchStep(Context* c, int mode, const StepPtrs& p) {
+  c->launches++;
+  const bool sample = c->timingEvery > 0 && (c->stepCounter++ % c->timingEvery) == 0;
+  cudaEvent_t a = nullptr, b = nullptr;
+  if (sample) {
+    a = takeEvent(c);
+    b = takeEvent(c);
+    if (a && b) cudaEventRecord(a, c->st);
+  }
+  const int st = launchStepRaw(c, mode, p);
+  if (sample && a && b) {
+    cudaEventRecord(b, c->st);
+    c->timed.push_back({mode, a, b});
+  }
+  return st;
+}
+
+int setKernelTiming(Context* c, int every) {
+  E3D_ARG(c && every >= 0, "bad timing interval");
+  c->timingEvery = every;
+  c->stepCounter = 0;
+  return E3D_OK;
+}
+
+int readKernelTiming(Context* c, int mode, double* avgMs, long long* count) {
+  E3D_ARG(c && avgMs && count, "null argument");
+  double sum = 0;
+  long long n = 0;
+  std::vector<Context::Timed> keep;
+  for (auto& t : c->timed) {
+    if (t.mode != mode) {
+      keep.push_back(t);
+      continue;
+    }
+    float ms = 0;
+    E3D_CUDA_TRY(cudaEventSynchronize(t.b));
+    E3D_CUDA_TRY(cudaEventElapsedTime(&ms, t.a, t.b));
+    sum += ms;
+    n++;
+    c->evPool.push_back(t.a);
+    c->evPool.push_back(t.b);
+  }
+  c->timed.swap(keep);
+  *avgMs = n ? sum / n : 0.0;
+  *count = n;
+  return E3D_OK;
+}
+
+long long launchCount(const Context* c) { return c->launches; }
+
+static int launchStepRaw(Context* c, int mode, const StepPtrs& p) {
   const GridConst& g = c->g;
   const int tiz = (g.nz - 2 * FAT + TZ - 1) / TZ;
   const int tix = (g.nx - 2 * FAT + c->tx - 1) / c->tx;
@@ -410,8 +527,14 @@ static int launchStep(Context* c, int mode, const StepPtrs& p) {
   const int yChunk = (nyi + chunks - 1) / chunks;
   chunks = (nyi + yChunk - 1) / yChunk;
   dim3 grid(tiz, tix, chunks);
+  const bool dual = mode == STEP_ADJ_EXACT && p.oP[0] != nullptr;
   const bool pipe = (g.nz % 4 == 0) && mode != STEP_ADJ_EXACT && c->loader > 0;
-  if (pipe) {
+  if (dual) {
+    E3D_ARG(g.nz % 4 == 0, "dual-state adjoint needs nz % 4 == 0");
+    if (c->tx == 16) E3D_RET((launchTma<STEP_ADJ_EXACT, 16, 2>(c, p, grid, yChunk)));
+    else if (c->stages == 3) E3D_RET((launchTma<STEP_ADJ_EXACT, 8, 3>(c, p, grid, yChunk)));
+    else E3D_RET((launchTma<STEP_ADJ_EXACT, 8, 2>(c, p, grid, yChunk)));
+  } else if (pipe) {
     if (mode == STEP_FWD) E3D_RET(launchVariant<STEP_FWD>(c, p, grid, yChunk));
     else E3D_RET(launchVariant<STEP_ADJ_REVERSED>(c, p, grid, yChunk));
   } else if (c->tx == 16) {
@@ -435,6 +558,7 @@ static int launchInject(Context* c, const StepPtrs& p, const DevSignals& s, cons
   for (int i = 0; i <= NCOMP; i++) ss.off[i] = s.off[i];
   const int n = s.off[NCOMP];
   if (n == 0) return E3D_OK;
+  c->launches++;
   kInject<<<(n + 127) / 128, 128, 0, c->st>>>(p, c->g, ss, sig, its, c->filt[k], c->filt[c->hfilt + k]);
   E3D_LAUNCH_CHECK();
   return E3D_OK;
@@ -446,7 +570,20 @@ static int launchRecord(Context* c, const StepPtrs& p, const DevSignals& s, floa
   for (int i = 0; i <= NCOMP; i++) ss.off[i] = s.off[i];
   const int n = s.off[NCOMP];
   if (n == 0) return E3D_OK;
+  c->launches++;
   kRecord<<<(n + 127) / 128, 128, 0, c->st>>>(p, ss, out, its, c->filt[k], c->filt[c->hfilt + k]);
+  E3D_LAUNCH_CHECK();
+  return E3D_OK;
+}
+
+static int launchRefresh(Context* c, const StepPtrs& p, const DevSignals& s) {
+  SparseSet ss;
+  ss.pos = s.pos;
+  for (int i = 0; i <= NCOMP; i++) ss.off[i] = s.off[i];
+  const int n = s.off[NCOMP];
+  if (n == 0) return E3D_OK;
+  c->launches++;
+  kRefreshPremultiplied<<<(n + 127) / 128, 128, 0, c->st>>>(p, ss);
   E3D_LAUNCH_CHECK();
   return E3D_OK;
 }
@@ -475,6 +612,7 @@ static int transpose(Context* c, const float* in, float* out, long long rows, lo
   if (rows == 0 || cols == 0) return E3D_OK;
   const long long tiles = ((rows + 31) / 32) * ((cols + 31) / 32);
   E3D_ARG(tiles < (1LL << 31), "transpose too large");
+  c->launches++;
   kTranspose<<<(unsigned)tiles, dim3(32, 8), 0, c->st>>>(in, out, rows, cols);
   E3D_LAUNCH_CHECK();
   return E3D_OK;
@@ -647,13 +785,27 @@ int stepOnly(Context* c, int mode, int nSteps) {
   E3D_ARG(mode >= 0 && mode <= 2, "bad mode");
   E3D_RET(allocFields(c, c->w0, false));
   E3D_RET(allocFields(c, c->w1, false));
+  // the exact adjoint runs on the dual state, as in the adjoint pass, with the TMA loader
+  const bool dual = mode == STEP_ADJ_EXACT && c->loader >= 2 && c->d.nz % 4 == 0;
+  if (dual) {
+    E3D_RET(allocFields(c, c->q0, false));
+    E3D_RET(allocFields(c, c->q1, false));
+  }
   for (int i = 0; i < nSteps; i++) {
     StepPtrs p = makeStep(c, c->w0, c->w1);
+    if (dual)
+      for (int k = 0; k < NCOMP; k++) {
+        p.c[k] = c->q1.p[k];
+        p.oP[k] = c->q0.p[k];
+      }
     E3D_RET(launchStep(c, mode, p));
     swapF(c->w0, c->w1);
+    if (dual) swapF(c->q0, c->q1);
   }
   return E3D_OK;
 }
+
+int checkpointSegment(const Context* c) { return c->ckptSegLen; }
 
 // ---------------------------------------------------------------------------
 // Born
@@ -714,6 +866,7 @@ static int launchImaging(Context* c, bool adjoint, int t, float* vPrev, float* v
   q.q3compat = c->d.q3compat;
   dim3 block(32, 8);
   dim3 grid((c->d.nz - 2 * FAT + 31) / 32, (c->d.nx - 2 * FAT + 7) / 8, c->d.ny - 2 * FAT);
+  c->launches++;
   if (adjoint) kImaging<true><<<grid, block, 0, c->st>>>(q, c->g);
   else kImaging<false><<<grid, block, 0, c->st>>>(q, c->g);
   E3D_LAUNCH_CHECK();
@@ -788,23 +941,60 @@ static int bornForwardDevice(Context* c, const DevSignals& srcSet, const DevSign
 // source-side state at the start of block s*L-1; recomputing from it yields
 // V[s*L] complete (its right-weight part comes from block s*L-1).
 // ---------------------------------------------------------------------------
-static size_t ckptBytesPerState(const Context* c) {
-  const size_t eb = c->ckptType == CKPT_F32 ? 4 : 2;
+static size_t ckptBytesPerState(const Context* c, int type) {
+  const size_t eb = type == CKPT_F32 ? 4 : 2;
   size_t b = (size_t)18 * c->g.n * eb;
-  if (c->ckptType != CKPT_F32) b += (size_t)18 * c->d.ny * sizeof(float) + 256;
+  if (type != CKPT_F32) b += (size_t)18 * c->d.ny * sizeof(float) + 256;
   return b;
+}
+
+// Device bytes the adjoint pass will still allocate (adjoint levels, decimation
+// slots, premultiplied levels).
+static double pendingAdjointBytes(const Context* c) {
+  const double f = (double)c->g.n * sizeof(float);
+  double b = 0;
+  if (!c->w0.p[0]) b += 18 * f;
+  if (!c->ss[0].p[0]) b += 18 * f;
+  if (!c->q0.p[0] && c->loader >= 2) b += 18 * f;
+  return b;
+}
+
+// Bytes available for checkpoints and velocity slots: the explicit budget, or
+// 85% of the free memory left after the caller's reserve (negative budget)
+// and the adjoint pass's pending allocations.
+static double autoBudget(const Context* c, size_t free) {
+  if (c->budget > 0) return c->budget;
+  const double reserve = c->budget < 0 ? -c->budget : 0.0;
+  return 0.85 * ((double)free - reserve) - pendingAdjointBytes(c);
 }
 
 static int chooseSegment(Context* c, int& L) {
   const int blocks = c->d.nts - 1;
+  if (c->ckptType == CKPT_AUTO) {
+    // FP32 states when they fit, else FP16 with per-slice scales
+    c->ckptUsed = CKPT_F32;
+    if (c->segment == 0) {
+      size_t free = 0, total = 0;
+      E3D_CUDA_TRY(cudaMemGetInfo(&free, &total));
+      const double budget = autoBudget(c, free) + c->ckptHeld;
+      const double ck = (double)ckptBytesPerState(c, CKPT_F32), vs = 3.0 * c->g.n * sizeof(float);
+      bool fits = false;
+      for (int l = 1; l <= blocks && !fits; l++) fits = (((blocks + l - 1) / l) - 1) * ck + (l + 3) * vs <= budget;
+      if (!fits) c->ckptUsed = CKPT_F16;
+    }
+  } else {
+    c->ckptUsed = c->ckptType;
+  }
   if (c->segment > 0) {
     L = std::min(c->segment, blocks);
     return E3D_OK;
   }
   size_t free = 0, total = 0;
   E3D_CUDA_TRY(cudaMemGetInfo(&free, &total));
-  double budget = c->budget > 0 ? c->budget : 0.85 * (double)free;
-  const double ck = (double)ckptBytesPerState(c);
+  // memory this context already holds for checkpoints and velocity slots counts as
+  // available; the adjoint pass's own wavefields, if not yet allocated, do not
+  double budget = autoBudget(c, free) + c->ckptHeld;
+  const double ck = (double)ckptBytesPerState(c, c->ckptUsed);
   const double vs = 3.0 * c->g.n * sizeof(float);
   // One extra source block is recomputed per segment, so use the longest
   // segment whose checkpoints and velocity slots fit in the budget.
@@ -829,7 +1019,7 @@ static int packState(Context* c, int seg) {
   const long long n = c->g.n, ys = c->g.yStride;
   const int ny = c->d.ny;
   Fields9* parts[2] = {&c->s0, &c->s1};
-  if (c->ckptType == CKPT_F32) {
+  if (c->ckptUsed == CKPT_F32) {
     float* dst = (float*)c->ckpt[seg];
     for (int h = 0; h < 2; h++)
       for (int k = 0; k < NCOMP; k++)
@@ -842,10 +1032,11 @@ static int packState(Context* c, int seg) {
   for (int h = 0; h < 2; h++)
     for (int k = 0; k < NCOMP; k++) {
       const int f = h * NCOMP + k;
+      c->launches += 2;
       kSliceMaxAbs<<<ny, 256, 0, c->st>>>(parts[h]->p[k], ys, smax);
       E3D_LAUNCH_CHECK();
       const unsigned blocks = (unsigned)((n + 255) / 256);
-      if (c->ckptType == CKPT_F16)
+      if (c->ckptUsed == CKPT_F16)
         kPackSlices<__half><<<blocks, 256, 0, c->st>>>(parts[h]->p[k], ys, n, smax, 16384.f,
                                                        (__half*)c->ckpt[seg] + (size_t)f * n, scales + (size_t)f * ny);
       else
@@ -864,12 +1055,13 @@ static int unpackState(Context* c, int seg) {
   for (int h = 0; h < 2; h++)
     for (int k = 0; k < NCOMP; k++) {
       const int f = h * NCOMP + k;
-      if (c->ckptType == CKPT_F32) {
+      if (c->ckptUsed == CKPT_F32) {
         E3D_CUDA_TRY(cudaMemcpyAsync(parts[h]->p[k], (float*)c->ckpt[seg] + (size_t)f * n, n * sizeof(float),
                                      cudaMemcpyDeviceToDevice, c->st));
       } else {
         const unsigned blocks = (unsigned)((n + 255) / 256);
-        if (c->ckptType == CKPT_F16)
+        c->launches++;
+        if (c->ckptUsed == CKPT_F16)
           kUnpackSlices<__half><<<blocks, 256, 0, c->st>>>((const __half*)c->ckpt[seg] + (size_t)f * n, ys, n,
                                                            c->ckptScale[seg] + (size_t)f * ny, parts[h]->p[k]);
         else
@@ -886,20 +1078,22 @@ static int prepareCheckpoints(Context* c, int& L, int& nseg) {
   const int blocks = c->d.nts - 1;
   E3D_RET(chooseSegment(c, L));
   nseg = (blocks + L - 1) / L;
-  if (c->ckptSegLen != L || (int)c->ckpt.size() != nseg) {
+  if (c->ckptSegLen != L || (int)c->ckpt.size() != nseg || c->ckptAllocType != c->ckptUsed) {
     for (void* p : c->ckpt) devFree(c, p);
     for (float* p : c->ckptScale) devFree(c, p);
     c->ckpt.assign(nseg, nullptr);
     c->ckptScale.assign(nseg, nullptr);
     for (int s = 1; s < nseg; s++) {
-      const size_t eb = c->ckptType == CKPT_F32 ? 4 : 2;
+      const size_t eb = c->ckptUsed == CKPT_F32 ? 4 : 2;
       E3D_RET(devAlloc(c, &c->ckpt[s], (size_t)18 * c->g.n * eb));
-      if (c->ckptType != CKPT_F32)
+      if (c->ckptUsed != CKPT_F32)
         E3D_RET(devAlloc(c, (void**)&c->ckptScale[s], (size_t)18 * c->d.ny * sizeof(float)));
     }
     c->ckptSegLen = L;
+    c->ckptAllocType = c->ckptUsed;
+    c->ckptHeld = (double)(nseg - 1) * ckptBytesPerState(c, c->ckptUsed) + (double)c->vSlots.size() * 3.0 * c->g.n * 4;
   }
-  if (c->ckptType != CKPT_F32) E3D_RET(scratchAtLeast(c, (size_t)c->d.ny * sizeof(float)));
+  if (c->ckptUsed != CKPT_F32) E3D_RET(scratchAtLeast(c, (size_t)c->d.ny * sizeof(float)));
   return E3D_OK;
 }
 
@@ -944,6 +1138,12 @@ static int adjointPassFromCheckpoints(Context* c, const DevSignals& srcSet, cons
   E3D_RET(allocFields(c, c->w1, true));
   E3D_RET(allocFields(c, c->ss[0], true));
   E3D_RET(allocFields(c, c->ss[1], true));
+  // the TMA stepper runs the exact adjoint on a dual state (raw + premultiplied)
+  const bool dual = c->loader >= 2 && c->d.nz % 4 == 0;
+  if (dual) {
+    E3D_RET(allocFields(c, c->q0, true));
+    E3D_RET(allocFields(c, c->q1, true));
+  }
   // adjoint decimation slots: A[its] (left, fresh per block) and A[its+1] (right)
   Fields9* aLeft = &c->ss[0];
   Fields9* aRight = &c->ss[1];
@@ -987,10 +1187,18 @@ static int adjointPassFromCheckpoints(Context* c, const DevSignals& srcSet, cons
         p.accWl = c->filt[it2];
         p.accWr = c->filt[c->hfilt + it2];
         p.nAcc = NCOMP;
+        if (dual) {
+          for (int k = 0; k < NCOMP; k++) {
+            p.c[k] = c->q1.p[k];
+            p.oP[k] = c->q0.p[k];
+          }
+        }
         if (it2 == sub - 1) E3D_RET(zeroFields(c, *aLeft));
         E3D_RET(launchStep(c, STEP_ADJ_EXACT, p));
         E3D_RET(launchInject(c, p, recSet, resid, its, it2 + 1));
+        if (dual) E3D_RET(launchRefresh(c, p, recSet));
         swapF(c->w0, c->w1);
+        if (dual) swapF(c->q0, c->q1);
       }
       // imaging condition at its+1 (A[its+1] complete)
       E3D_RET(launchImaging(c, true, its + 1, V(its), V(its + 1), V(its + 2), *aRight));

@@ -16,7 +16,7 @@ struct HostGeom {
 };
 
 // Storage type of saved wavefield states.
-enum CkptType { CKPT_F32 = 0, CKPT_F16 = 1, CKPT_BF16 = 2 };
+enum CkptType { CKPT_AUTO = -1, CKPT_F32 = 0, CKPT_F16 = 1, CKPT_BF16 = 2 };
 
 struct ContextDesc {
   int device = 0;
@@ -42,6 +42,12 @@ int setMedium(Context* c, const float* const* planes, bool onDevice);
 int setStepperVariant(Context* c, int tx, int stages, int loader);
 // Reads and clears the device flag set when a bounded pipeline wait expired.
 int checkPipeError(Context* c);
+// Sampled stepper timing: bracket every n-th stepper launch with CUDA events (0 = off).
+int setKernelTiming(Context* c, int every);
+// Average duration (ms) of the sampled stepper launches of one mode since the last read.
+int readKernelTiming(Context* c, int mode, double* avgMs, long long* count);
+// Kernel launches issued by this context so far.
+long long launchCount(const Context* c);
 int setCheckpointPolicy(Context* c, int ckptType, int segment, double budgetBytes);
 
 // Reference-layout host entry points ([nDevice][nts] per component).
@@ -71,9 +77,10 @@ int fwiGradientDevice(Context* c, const DevSignals& srcSet, const DevSignals& re
 // Timing/inspection helpers
 int stepOnly(Context* c, int mode, int nSteps);  // run nSteps bare steps on the working state
 long long cellsPerStep(const Context* c);
+int checkpointSegment(const Context* c);  // coarse blocks per checkpoint segment (0 before first use)
 double deviceBytesInUse(const Context* c);
 cudaStream_t stream(Context* c);
-int setStream(Context* c, cudaStream_t s);
+int setStream(Context* c, cudaStream_t s, bool useOwn);
 
 const char* lastError();
 }  // namespace e3d

@@ -33,7 +33,31 @@ struct StepPtrs {
   float* accR[NCOMP];
   float accWl, accWr;
   int nAcc;               // number of leading components accumulated (3 or 9)
+  // mode 2 with a dual state: c[] holds the medium-premultiplied current level
+  // and the step also writes the premultiplied new level here (may be null)
+  float* oP[NCOMP];
 };
+
+// A "device set" concatenates the regular-grid points of the nine
+// components: component k owns entries [off[k], off[k+1]) of pos.
+struct SparseSet {
+  const long long* pos;
+  int off[NCOMP + 1];
+};
+
+// Medium-premultiplied wavefield at one cell (stepAdjGpuBorn_3D, kernelsElaGpu_3D.cu:864-920).
+__device__ __forceinline__ void premultiply(const float* v, float rhox, float rhoy, float rhoz, float l2m, float lam,
+                                            float muxz, float muxy, float muyz, float* q) {
+  q[VX] = v[VX] * rhox;
+  q[VY] = v[VY] * rhoy;
+  q[VZ] = v[VZ] * rhoz;
+  q[SXX] = v[SXX] * l2m + (v[SYY] + v[SZZ]) * lam;
+  q[SYY] = v[SYY] * l2m + (v[SXX] + v[SZZ]) * lam;
+  q[SZZ] = v[SZZ] * l2m + (v[SXX] + v[SYY]) * lam;
+  q[SXZ] = v[SXZ] * muxz;
+  q[SXY] = v[SXY] * muxy;
+  q[SYZ] = v[SYZ] * muyz;
+}
 
 // Shared tiles: fields needing a z or x halo.
 enum Tile { T_VX = 0, T_VY, T_VZ, T_SXX, T_SZZ, T_SXY, T_SXZ, T_SYZ, NTILE };
@@ -541,33 +565,50 @@ __global__ void __launch_bounds__(TZ * TX) kStepTma(const __grid_constant__ TmaM
       const float fyz = dWin(w[Q_VZ], cy) + dMinus(tl[T_VY], lc, 1, cz);
       const float* mv = st + L::MED_OFF + li;
       const float* ov = st + L::OLD_OFF + li;
-      const float sgn = (MODE == STEP_FWD) ? 1.0f : -1.0f;
-      float up[NCOMP];
-      up[VX] = sgn * (mv[RHOX * L::INT_F] * fvx);
-      up[VY] = sgn * (mv[RHOY * L::INT_F] * fvy);
-      up[VZ] = sgn * (mv[RHOZ * L::INT_F] * fvz);
+      const float rhox = mv[RHOX * L::INT_F], rhoy = mv[RHOY * L::INT_F], rhoz = mv[RHOZ * L::INT_F];
       const float l2m = mv[L2M * L::INT_F], lam = mv[LAM * L::INT_F];
-      up[SXX] = sgn * (l2m * dvx_dx + lam * (dvy_dy + dvz_dz));
-      up[SYY] = sgn * (l2m * dvy_dy + lam * (dvx_dx + dvz_dz));
-      up[SZZ] = sgn * (l2m * dvz_dz + lam * (dvx_dx + dvy_dy));
-      up[SXZ] = sgn * (mv[MUXZ * L::INT_F] * fxz);
-      up[SXY] = sgn * (mv[MUXY * L::INT_F] * fxy);
-      up[SYZ] = sgn * (mv[MUYZ * L::INT_F] * fyz);
+      const float muxz = mv[MUXZ * L::INT_F], muxy = mv[MUXY * L::INT_F], muyz = mv[MUYZ * L::INT_F];
+      float up[NCOMP];
+      if (MODE == STEP_ADJ_EXACT) {
+        // tiles and window hold the premultiplied current level
+        up[VX] = -fvx; up[VY] = -fvy; up[VZ] = -fvz;
+        up[SXX] = -dvx_dx; up[SYY] = -dvy_dy; up[SZZ] = -dvz_dz;
+        up[SXZ] = -fxz; up[SXY] = -fxy; up[SYZ] = -fyz;
+      } else {
+        const float sgn = (MODE == STEP_FWD) ? 1.0f : -1.0f;
+        up[VX] = sgn * (rhox * fvx);
+        up[VY] = sgn * (rhoy * fvy);
+        up[VZ] = sgn * (rhoz * fvz);
+        up[SXX] = sgn * (l2m * dvx_dx + lam * (dvy_dy + dvz_dz));
+        up[SYY] = sgn * (l2m * dvy_dy + lam * (dvx_dx + dvz_dz));
+        up[SZZ] = sgn * (l2m * dvz_dz + lam * (dvx_dx + dvy_dy));
+        up[SXZ] = sgn * (muxz * fxz);
+        up[SXY] = sgn * (muxy * fxy);
+        up[SYZ] = sgn * (muyz * fyz);
+      }
       const int d = min(dzx, min(y - FAT, g.ny - y - 1 - FAT));
       const float G = d < g.minPad ? __ldg(g.taper + d) : 1.0f;
       const long long ic = (long long)y * ys + col;
       const bool hasSS = p.ssL[0] != nullptr;
       const bool hasAcc = p.accL[0] != nullptr;
+      float nv[NCOMP];
 #pragma unroll
       for (int k = 0; k < NCOMP; k++) {
         float v = G * ov[k * L::INT_F] + up[k];
         if (hasSS) v += __ldg(p.ssL[k] + ic) * p.ssWl + __ldg(p.ssR[k] + ic) * p.ssWr;
         v *= G;
+        nv[k] = v;
         p.o[k][ic] = v;
         if (hasAcc && k < p.nAcc) {
           p.accL[k][ic] += v * p.accWl;
           if (p.accR[0] != nullptr) p.accR[k][ic] += v * p.accWr;
         }
+      }
+      if (MODE == STEP_ADJ_EXACT) {
+        float q[NCOMP];
+        premultiply(nv, rhox, rhoy, rhoz, l2m, lam, muxz, muxy, muyz, q);
+#pragma unroll
+        for (int k = 0; k < NCOMP; k++) p.oP[k][ic] = q[k];
       }
 #pragma unroll
       for (int q = 0; q < NQUEUE; q++) {
@@ -579,15 +620,251 @@ __global__ void __launch_bounds__(TZ * TX) kStepTma(const __grid_constant__ TmaM
   }
 }
 
+// Recompute the premultiplied level at injected points (dual-state mode 2):
+// after kInject changed raw values there.  The three normal stresses share
+// the center-grid positions and are refreshed together by the sxx entries.
+__global__ void kRefreshPremultiplied(StepPtrs p, SparseSet s) {
+  const int ntot = s.off[NCOMP];
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= ntot) return;
+  int k = 0;
+#pragma unroll
+  for (int c = 1; c < NCOMP; c++) k += (j >= s.off[c]);
+  if (k == SYY || k == SZZ) return;
+  const long long i = s.pos[j];
+  switch (k) {
+    case VX: p.oP[VX][i] = p.o[VX][i] * __ldg(p.m[RHOX] + i); break;
+    case VY: p.oP[VY][i] = p.o[VY][i] * __ldg(p.m[RHOY] + i); break;
+    case VZ: p.oP[VZ][i] = p.o[VZ][i] * __ldg(p.m[RHOZ] + i); break;
+    case SXZ: p.oP[SXZ][i] = p.o[SXZ][i] * __ldg(p.m[MUXZ] + i); break;
+    case SXY: p.oP[SXY][i] = p.o[SXY][i] * __ldg(p.m[MUXY] + i); break;
+    case SYZ: p.oP[SYZ][i] = p.o[SYZ][i] * __ldg(p.m[MUYZ] + i); break;
+    default: {
+      const float sxx = p.o[SXX][i], syy = p.o[SYY][i], szz = p.o[SZZ][i];
+      const float l2m = __ldg(p.m[L2M] + i), lam = __ldg(p.m[LAM] + i);
+      p.oP[SXX][i] = sxx * l2m + (syy + szz) * lam;
+      p.oP[SYY][i] = syy * l2m + (sxx + szz) * lam;
+      p.oP[SZZ][i] = szz * l2m + (sxx + syy) * lam;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// TMA stepper, second form.  Differences from kStepTma:
+//  * the y-window is a ring of 8 registers addressed by (k + R) & 7 with the
+//    plane loop unrolled by 8, so no register moves per plane;
+//  * OM_SMEM = false: the old level and the medium are read with plain
+//    coalesced loads (issued right after the barrier), which shrinks a stage
+//    to the eight halo boxes and six lead boxes so more CTAs fit per SM.
+// ---------------------------------------------------------------------------
+template <int TX, bool OM_SMEM>
+struct Tma2Layout {
+  using B = PipeLayout<TX>;
+  static constexpr int HALO_F = B::HALO_F;
+  static constexpr int INT_F = B::INT_F;
+  static constexpr int LEAD_OFF = NTILE * HALO_F;
+  static constexpr int OLD_OFF = LEAD_OFF + NQUEUE * INT_F;
+  static constexpr int MED_OFF = OLD_OFF + NCOMP * INT_F;
+  static constexpr int STAGE_F = OM_SMEM ? B::STAGE_F : LEAD_OFF + NQUEUE * INT_F;
+};
+
+template <int TX, bool OM_SMEM>
+__device__ __forceinline__ void tma2IssuePlane(const TmaMaps& mp, float* st, unsigned long long* bar, int y, int z0,
+                                               int x0) {
+  using L = Tma2Layout<TX, OM_SMEM>;
+  constexpr unsigned bytes = (unsigned)L::STAGE_F * 4u;
+  mbarExpectTx(bar, bytes);
+#pragma unroll
+  for (int t = 0; t < NTILE; t++) tmaLoad3d(st + t * L::HALO_F, &mp.halo[t], z0 - HALO, x0 - HALO, y, bar);
+#pragma unroll
+  for (int q = 0; q < NQUEUE; q++)
+    tmaLoad3d(st + L::LEAD_OFF + q * L::INT_F, &mp.lead[q], z0, x0, y + qBase(q) + 7, bar);
+  if (OM_SMEM) {
+#pragma unroll
+    for (int k = 0; k < NCOMP; k++) tmaLoad3d(st + L::OLD_OFF + k * L::INT_F, &mp.old[k], z0, x0, y, bar);
+#pragma unroll
+    for (int k = 0; k < NMED; k++) tmaLoad3d(st + L::MED_OFF + k * L::INT_F, &mp.med[k], z0, x0, y, bar);
+  }
+}
+
+template <int R>
+__device__ __forceinline__ float dRing(const float* w, const float* c) {
+  return c[0] * (w[(4 + R) & 7] - w[(3 + R) & 7]) + c[1] * (w[(5 + R) & 7] - w[(2 + R) & 7]) +
+         c[2] * (w[(6 + R) & 7] - w[(1 + R) & 7]) + c[3] * (w[(7 + R) & 7] - w[(0 + R) & 7]);
+}
+
+template <int MODE, int TX, int STAGES, bool OM_SMEM>
+struct Tma2State {
+  const TmaMaps* mp;
+  const StepPtrs* p;
+  const GridConst* g;
+  float* smem;
+  unsigned long long* bars;
+  int tid, z0, x0, iz, ix, yEnd, dzx, lc, li;
+  bool active;
+  long long col;
+  int slot;
+  unsigned parity;
+  float w[NQUEUE][8];
+};
+
+// One plane with window rotation R.  Returns false if the CTA must stop.
+template <int MODE, int TX, int STAGES, bool OM_SMEM, int R>
+__device__ __forceinline__ bool tma2Plane(Tma2State<MODE, TX, STAGES, OM_SMEM>& S, int y) {
+  using L = Tma2Layout<TX, OM_SMEM>;
+  const StepPtrs& p = *S.p;
+  const GridConst& g = *S.g;
+  const bool ok = mbarWaitBounded(&S.bars[S.slot], (S.parity >> S.slot) & 1u);
+  if (__syncthreads_or(!ok)) {
+    if (S.tid == 0) {
+      atomicExch(&g_e3dPipeError, 1u);
+      for (int s = 0; s < STAGES; s++) mbarWaitBounded(&S.bars[s], (S.parity >> s) & 1u);
+    }
+    __syncthreads();
+    return false;
+  }
+  S.parity ^= 1u << S.slot;
+  if (S.tid == 0) {
+    const int yn = y + STAGES - 1;
+    int ns = S.slot + STAGES - 1;
+    if (ns >= STAGES) ns -= STAGES;
+    if (yn < S.yEnd) tma2IssuePlane<TX, OM_SMEM>(*S.mp, S.smem + ns * L::STAGE_F, &S.bars[ns], yn, S.z0, S.x0);
+  }
+  const float* st = S.smem + S.slot * L::STAGE_F;
+  if (S.active) {
+    const long long ic = (long long)y * g.yStride + S.col;
+    float ovr[NCOMP], mvr[NMED];
+    if (!OM_SMEM) {
+#pragma unroll
+      for (int k = 0; k < NCOMP; k++) ovr[k] = p.o[k][ic];
+#pragma unroll
+      for (int k = 0; k < NMED; k++) mvr[k] = __ldg(p.m[k] + ic);
+    } else {
+#pragma unroll
+      for (int k = 0; k < NCOMP; k++) ovr[k] = st[L::OLD_OFF + k * L::INT_F + S.li];
+#pragma unroll
+      for (int k = 0; k < NMED; k++) mvr[k] = st[L::MED_OFF + k * L::INT_F + S.li];
+    }
+#pragma unroll
+    for (int q = 0; q < NQUEUE; q++) S.w[q][(7 + R) & 7] = st[L::LEAD_OFF + q * L::INT_F + S.li];
+    const float* tl[NTILE];
+#pragma unroll
+    for (int t = 0; t < NTILE; t++) tl[t] = st + t * L::HALO_F;
+    const int lc = S.lc;
+    const float* cz = g.cz;
+    const float* cx = g.cx;
+    const float* cy = g.cy;
+    const float dvx_dx = dPlus(tl[T_VX], lc, SZ, cx);
+    const float dvy_dy = dRing<R>(S.w[Q_VY], cy);
+    const float dvz_dz = dPlus(tl[T_VZ], lc, 1, cz);
+    const float fvx = dMinus(tl[T_SXX], lc, SZ, cx) + dRing<R>(S.w[Q_SXY], cy) + dPlus(tl[T_SXZ], lc, 1, cz);
+    const float fvy = dPlus(tl[T_SXY], lc, SZ, cx) + dRing<R>(S.w[Q_SYY], cy) + dPlus(tl[T_SYZ], lc, 1, cz);
+    const float fvz = dPlus(tl[T_SXZ], lc, SZ, cx) + dRing<R>(S.w[Q_SYZ], cy) + dMinus(tl[T_SZZ], lc, 1, cz);
+    const float fxy = dRing<R>(S.w[Q_VX], cy) + dMinus(tl[T_VY], lc, SZ, cx);
+    const float fxz = dMinus(tl[T_VX], lc, 1, cz) + dMinus(tl[T_VZ], lc, SZ, cx);
+    const float fyz = dRing<R>(S.w[Q_VZ], cy) + dMinus(tl[T_VY], lc, 1, cz);
+    const float sgn = (MODE == STEP_FWD) ? 1.0f : -1.0f;
+    float up[NCOMP];
+    up[VX] = sgn * (mvr[RHOX] * fvx);
+    up[VY] = sgn * (mvr[RHOY] * fvy);
+    up[VZ] = sgn * (mvr[RHOZ] * fvz);
+    up[SXX] = sgn * (mvr[L2M] * dvx_dx + mvr[LAM] * (dvy_dy + dvz_dz));
+    up[SYY] = sgn * (mvr[L2M] * dvy_dy + mvr[LAM] * (dvx_dx + dvz_dz));
+    up[SZZ] = sgn * (mvr[L2M] * dvz_dz + mvr[LAM] * (dvx_dx + dvy_dy));
+    up[SXZ] = sgn * (mvr[MUXZ] * fxz);
+    up[SXY] = sgn * (mvr[MUXY] * fxy);
+    up[SYZ] = sgn * (mvr[MUYZ] * fyz);
+    const int d = min(S.dzx, min(y - FAT, g.ny - y - 1 - FAT));
+    const float G = d < g.minPad ? __ldg(g.taper + d) : 1.0f;
+    const bool hasSS = p.ssL[0] != nullptr;
+    const bool hasAcc = p.accL[0] != nullptr;
+#pragma unroll
+    for (int k = 0; k < NCOMP; k++) {
+      float v = G * ovr[k] + up[k];
+      if (hasSS) v += __ldg(p.ssL[k] + ic) * p.ssWl + __ldg(p.ssR[k] + ic) * p.ssWr;
+      v *= G;
+      p.o[k][ic] = v;
+      if (hasAcc && k < p.nAcc) {
+        p.accL[k][ic] += v * p.accWl;
+        if (p.accR[0] != nullptr) p.accR[k][ic] += v * p.accWr;
+      }
+    }
+  }
+  S.slot = (S.slot + 1 == STAGES) ? 0 : S.slot + 1;
+  return true;
+}
+
+template <int MODE, int TX, int STAGES, bool OM_SMEM, int MINB>
+__global__ void __launch_bounds__(TZ * TX, MINB) kStepTma2(const __grid_constant__ TmaMaps mp, StepPtrs p,
+                                                            GridConst g, int yChunk) {
+  using L = Tma2Layout<TX, OM_SMEM>;
+  extern __shared__ __align__(1024) float smem[];
+  __shared__ __align__(8) unsigned long long bars[STAGES];
+  Tma2State<MODE, TX, STAGES, OM_SMEM> S;
+  S.mp = &mp;
+  S.p = &p;
+  S.g = &g;
+  S.smem = smem;
+  S.bars = bars;
+  const int tz = threadIdx.x, tx = threadIdx.y;
+  S.tid = tx * TZ + tz;
+  S.z0 = FAT + blockIdx.x * TZ;
+  S.x0 = FAT + blockIdx.y * TX;
+  S.iz = S.z0 + tz;
+  S.ix = S.x0 + tx;
+  S.active = (S.iz < g.nz - FAT) && (S.ix < g.nx - FAT);
+  const int yBeg = FAT + blockIdx.z * yChunk;
+  S.yEnd = min(yBeg + yChunk, g.ny - FAT);
+  S.col = (long long)S.ix * g.nz + S.iz;
+  S.dzx = min(min(S.iz - FAT, S.ix - FAT), min(g.nz - S.iz - 1 - FAT, g.nx - S.ix - 1 - FAT));
+  S.lc = (tx + HALO) * SZ + (tz + HALO);
+  S.li = tx * TZ + tz;
+  S.slot = 0;
+  S.parity = 0;
+  if (S.tid == 0) {
+    for (int s = 0; s < STAGES; s++) mbarInit(&bars[s], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  __syncthreads();
+  if (S.tid == 0) {
+    for (int s = 0; s < STAGES - 1; s++)
+      if (yBeg + s < S.yEnd) tma2IssuePlane<TX, OM_SMEM>(mp, smem + s * L::STAGE_F, &bars[s], yBeg + s, S.z0, S.x0);
+  }
+  if (S.active) {
+#pragma unroll
+    for (int q = 0; q < NQUEUE; q++) {
+#pragma unroll
+      for (int k = 0; k < 7; k++)
+        S.w[q][k] = __ldg(p.c[queueComp(q)] + (long long)(yBeg + qBase(q) + k) * g.yStride + S.col);
+    }
+  }
+  int y = yBeg;
+  for (; y + 8 <= S.yEnd; y += 8) {
+    if (!tma2Plane<MODE, TX, STAGES, OM_SMEM, 0>(S, y)) return;
+    if (!tma2Plane<MODE, TX, STAGES, OM_SMEM, 1>(S, y + 1)) return;
+    if (!tma2Plane<MODE, TX, STAGES, OM_SMEM, 2>(S, y + 2)) return;
+    if (!tma2Plane<MODE, TX, STAGES, OM_SMEM, 3>(S, y + 3)) return;
+    if (!tma2Plane<MODE, TX, STAGES, OM_SMEM, 4>(S, y + 4)) return;
+    if (!tma2Plane<MODE, TX, STAGES, OM_SMEM, 5>(S, y + 5)) return;
+    if (!tma2Plane<MODE, TX, STAGES, OM_SMEM, 6>(S, y + 6)) return;
+    if (!tma2Plane<MODE, TX, STAGES, OM_SMEM, 7>(S, y + 7)) return;
+  }
+  // tail: fewer than 8 planes; rotation continues from 0
+  const int r = S.yEnd - y;
+  if (r > 0 && !tma2Plane<MODE, TX, STAGES, OM_SMEM, 0>(S, y)) return;
+  if (r > 1 && !tma2Plane<MODE, TX, STAGES, OM_SMEM, 1>(S, y + 1)) return;
+  if (r > 2 && !tma2Plane<MODE, TX, STAGES, OM_SMEM, 2>(S, y + 2)) return;
+  if (r > 3 && !tma2Plane<MODE, TX, STAGES, OM_SMEM, 3>(S, y + 3)) return;
+  if (r > 4 && !tma2Plane<MODE, TX, STAGES, OM_SMEM, 4>(S, y + 4)) return;
+  if (r > 5 && !tma2Plane<MODE, TX, STAGES, OM_SMEM, 5>(S, y + 5)) return;
+  if (r > 6 && !tma2Plane<MODE, TX, STAGES, OM_SMEM, 6>(S, y + 6)) return;
+}
+
 // ---------------------------------------------------------------------------
 // Sparse signal kernels.  A "device set" concatenates the regular-grid points
 // of the nine components: component k owns entries [off[k], off[k+1]) of pos.
 // Signals are time-major on the device: sig[t*ntot + j].
 // ---------------------------------------------------------------------------
-struct SparseSet {
-  const long long* pos;
-  int off[NCOMP + 1];
-};
 
 // field[pos] += G(pos) * (sig[its]*wl + sig[its+1]*wr)
 // (ker_inject_source_* / ker_inject_data_*, kernelsElaGpu_3D.cu:11-52; the

@@ -16,7 +16,7 @@ from . import _native as N
 
 # grid of each wavefield component: vx->x, vy->y, vz->z, sxx/syy/szz->center, sxz->xz, sxy->xy, syz->yz
 COMP_GRID = (1, 2, 3, 0, 0, 0, 4, 5, 6)
-CKPT_TYPES = {"fp32": 0, "fp16": 1, "bf16": 2}
+CKPT_TYPES = {"auto": -1, "fp32": 0, "fp16": 1, "bf16": 2}
 
 
 def _geom(pos7):
@@ -62,22 +62,29 @@ class Propagator:
             planes = [N.as_f32(planes8[k]) for k in range(8)]
             N.call("e3d_set_medium", self._h, N.ptr_array(planes), 0)
 
-    LOADERS = {"plain": 0, "cpasync": 1, "tma": 2}
+    LOADERS = {"plain": 0, "cpasync": 1, "tma": 2, "tma-ring": 3, "tma-ring-ldg": 4, "tma-ring-ldg2": 5}
 
     def set_stepper_variant(self, tx=8, stages=2, loader="tma"):
         """Stepper variant: x tile width (8/16), shared-memory stages (2/3) and plane loader."""
         N.call("e3d_set_stepper_variant", self._h, int(tx), int(stages), self.LOADERS[loader])
 
-    def set_checkpoint_policy(self, ckpt="fp32", segment=0, budget_bytes=0.0):
+    def set_checkpoint_policy(self, ckpt="auto", segment=0, budget_bytes=0.0):
         N.call("e3d_set_checkpoint_policy", self._h, CKPT_TYPES[ckpt], int(segment), float(budget_bytes))
 
     def set_stream(self, stream):
-        """Queue work on an existing CUDA stream (a torch.cuda.Stream or a raw handle); None resets."""
-        h = None if stream is None else int(getattr(stream, "cuda_stream", stream))
-        N.call("e3d_set_stream", self._h, h)
+        """Queue work on an existing CUDA stream (a torch.cuda.Stream or a raw handle; handle 0 is
+        the legacy default stream); None returns to the context's own stream."""
+        if stream is None:
+            N.call("e3d_set_stream", self._h, None, 1)
+        else:
+            N.call("e3d_set_stream", self._h, int(getattr(stream, "cuda_stream", stream)) or None, 0)
 
     def synchronize(self):
         N.call("e3d_synchronize", self._h)
+
+    @property
+    def checkpoint_segment(self):
+        return int(N.lib().e3d_checkpoint_segment(self._h))
 
     @property
     def cells_per_step(self):
@@ -121,6 +128,21 @@ class Propagator:
         RP, RN, k2 = _geom(rec_pos7)
         N.call("e3d_born_adjoint", self._h, N.ptr_array(src), N.ptr_array(data), SP, SN, RP, RN, N.ptr_array(pert))
         return pert
+
+    def kernel_timing(self, every):
+        """Sample every n-th stepper launch with CUDA events (0 = off)."""
+        N.call("e3d_kernel_timing", self._h, int(every))
+
+    def kernel_timing_read(self, mode):
+        """(mean ms, count) of the sampled stepper launches of one mode since the last read."""
+        avg = ctypes.c_double(0)
+        cnt = ctypes.c_longlong(0)
+        N.call("e3d_kernel_timing_read", self._h, int(mode), ctypes.byref(avg), ctypes.byref(cnt))
+        return avg.value, cnt.value
+
+    @property
+    def launch_count(self):
+        return int(N.lib().e3d_launch_count(self._h))
 
     def step_only(self, mode, n_steps):
         N.call("e3d_step_only", self._h, int(mode), int(n_steps))

@@ -1,0 +1,272 @@
+"""FWI misfit and gradient over (rho, lambda, mu) as a torch.autograd.Function.
+
+Per shot the device runs, through the engine's C ABI:
+  1. the nonlinear forward of the scaled sources (propElasticFwdGpu_3D
+     semantics), saving on-device wavefield checkpoints;
+  2. the L2 residual at the irregular receivers (spaceInterpGpu_3D forward);
+  3. the Born adjoint of the residual (BornElasticAdjGpu_3D semantics: exact
+     transpose stepper, decimated adjoint field, imaging condition), with the
+     source-side velocity recomputed per segment from the checkpoints instead
+     of the reference's pinned-host snapshot storage;
+  4. the post-processing of BornElasticShotsGpu_3D::adjoint
+     (BornElasticShotsGpu_3D.cpp:528-605): scaling by the density planes and
+     2*dtw, unstaggering, giving (d rho, d lambda, d mu).
+The gradient is therefore the reference's Born-adjoint gradient (the one its
+EFWI driver uses, efwiMain_3D.py:195-196) of 0.5*||d_pred - d_obs||^2.
+
+Medium preparation (fdParamElastic_3D.cpp:130-193), source scaling
+(nonlinearPropElasticGpu_3D.cpp:200-277) and receiver interpolation run as
+torch operations on the device.  Fields are (ny, nx, nz) tensors.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import numpy as np
+import torch
+
+from . import hostprep as H
+from .engine import COMP_GRID, Propagator
+
+# ----------------------------------------------------------------------------
+# staggering (stagger_3D.cpp) on (ny, nx, nz) tensors; axis 'z' -> dim 2, 'x' -> 1, 'y' -> 0
+# ----------------------------------------------------------------------------
+_DIM = {"z": 2, "x": 1, "y": 0}
+
+
+def stagger_adjoint(d, axis):
+    """m[i] = 0.5(d[i]+d[i-1]); m[0] = 0.5 d[0]; m[n-1] = d[n-1] + 0.5 d[n-2]."""
+    d = d.movedim(_DIM[axis], -1)
+    m = torch.empty_like(d)
+    m[..., 1:-1] = 0.5 * (d[..., 1:-1] + d[..., :-2])
+    m[..., 0] = 0.5 * d[..., 0]
+    m[..., -1] = d[..., -1] + 0.5 * d[..., -2]
+    return m.movedim(-1, _DIM[axis]).contiguous()
+
+
+def stagger_forward(m, axis):
+    """d[i] = 0.5(m[i]+m[i+1]) (i < n-1); d[n-1] = m[n-1]."""
+    m = m.movedim(_DIM[axis], -1)
+    d = torch.empty_like(m)
+    d[..., :-1] = 0.5 * (m[..., :-1] + m[..., 1:])
+    d[..., -1] = m[..., -1]
+    return d.movedim(-1, _DIM[axis]).contiguous()
+
+
+def medium_planes(rho, lam, mu, dtw):
+    """Eight scaled planes (rhoxDtw ... muyzDtw) from float32 (rho, lambda, mu) tensors."""
+    two = 2.0 * float(dtw)
+    rhox = stagger_adjoint(rho, "x")
+    rhoy = stagger_adjoint(rho, "y")
+    rhoz = stagger_adjoint(rho, "z")
+    t1 = stagger_adjoint(mu, "x")
+    muxz = stagger_adjoint(t1, "z")
+    muxy = stagger_adjoint(t1, "y")
+    muyz = stagger_adjoint(stagger_adjoint(mu, "y"), "z")
+    out = torch.empty((8,) + tuple(rho.shape), dtype=torch.float32, device=rho.device)
+    out[0] = (two / rhox.double()).float()
+    out[1] = (two / rhoy.double()).float()
+    out[2] = (two / rhoz.double()).float()
+    out[3] = (two * (lam.double() + 2.0 * mu.double())).float()
+    out[4] = (two * lam.double()).float()
+    out[5] = (two * muxz.double()).float()
+    out[6] = (two * muxy.double()).float()
+    out[7] = (two * muyz.double()).float()
+    return out
+
+
+def planes_to_model(grad8, planes, dtw):
+    """Adjoint of the Born model preparation: 8 staggered planes -> (d rho, d lambda, d mu)
+    (BornElasticShotsGpu_3D.cpp:542-605)."""
+    two = 2.0 * float(dtw)
+    g = [grad8[k] * planes[k] for k in range(3)] + [(grad8[k].double() * two).float() for k in range(3, 8)]
+    drho = stagger_forward(g[0], "x") + stagger_forward(g[1], "y")
+    drho = drho + stagger_forward(g[2], "z")
+    t2 = stagger_forward(stagger_forward(g[5], "z"), "x")
+    t2 = t2 + stagger_forward(stagger_forward(g[6], "y"), "x")
+    t2 = t2 + stagger_forward(stagger_forward(g[7], "z"), "y")
+    return drho, g[3].clone(), g[4] + t2
+
+
+# ----------------------------------------------------------------------------
+# acquisition on the device
+# ----------------------------------------------------------------------------
+@dataclass
+class DeviceSet:
+    """Nine-component concatenated regular-grid points of one device set."""
+    pos: torch.Tensor        # (ntot,) int64
+    off: list                # 10 offsets
+    slot: list               # per grid: (nIrreg, 8) int64 into that grid's unique list
+    weight: list             # per grid: (nIrreg, 8) float32
+    n_irreg: int
+
+    @staticmethod
+    def from_devices(devices7, device, q2_receivers=False):
+        pos, off = [], [0]
+        for k in range(9):
+            g = COMP_GRID[k]
+            if q2_receivers and k == 6:  # sxz receivers read the z-grid table (reference quirk Q2)
+                u = devices7[3].getRegPosUnique()[:devices7[4].getNDeviceReg()]
+            else:
+                u = devices7[g].getRegPosUnique()
+            pos.append(np.asarray(u, dtype=np.int64))
+            off.append(off[-1] + len(u))
+        return DeviceSet(pos=torch.from_numpy(np.concatenate(pos)).to(device), off=off,
+                         slot=[torch.from_numpy(d.slot).to(device) for d in devices7],
+                         weight=[torch.from_numpy(d.weight).to(device) for d in devices7],
+                         n_irreg=devices7[0].getNDeviceIrreg())
+
+    def comp(self, k):
+        return slice(self.off[k], self.off[k + 1])
+
+    def to_irregular(self, reg):
+        """(nts, ntot) regular-grid traces -> (9, nIrreg, nts) (spaceInterpGpu_3D::forward)."""
+        out = []
+        for k in range(9):
+            g = COMP_GRID[k]
+            rk = reg[:, self.comp(k)]
+            acc = torch.zeros((reg.shape[0], self.n_irreg), dtype=reg.dtype, device=reg.device)
+            for f in range(self.slot[g].shape[1]):
+                acc = acc + self.weight[g][:, f] * rk[:, self.slot[g][:, f]]
+            out.append(acc.t())
+        return torch.stack(out)
+
+    def to_regular(self, irreg):
+        """(9, nIrreg, nts) -> (nts, ntot) (spaceInterpGpu_3D::adjoint)."""
+        nts = irreg.shape[2]
+        reg = torch.zeros((nts, self.off[9]), dtype=irreg.dtype, device=irreg.device)
+        for k in range(9):
+            g = COMP_GRID[k]
+            d = irreg[k].t()  # (nts, nIrreg)
+            blk = torch.zeros((nts, self.off[k + 1] - self.off[k]), dtype=irreg.dtype, device=irreg.device)
+            for f in range(self.slot[g].shape[1]):
+                blk.index_add_(1, self.slot[g][:, f], d * self.weight[g][:, f])
+            reg[:, self.comp(k)] = blk
+        return reg
+
+
+def scale_sources(sig_reg, src: DeviceSet, planes, dx, dy, dz):
+    """Medium scaling of regular-grid source signals (nonlinearPropElasticGpu_3D.cpp:200-277).
+    sig_reg: (nts, ntot) time-major; returns a new tensor."""
+    flat = planes.reshape(8, -1)
+    out = sig_reg.clone()
+    for k, m in ((0, 0), (1, 1), (2, 2), (6, 5), (7, 6), (8, 7)):
+        sl = src.comp(k)
+        out[:, sl] = sig_reg[:, sl] * flat[m][src.pos[sl]]
+    c = src.comp(3)
+    pc = src.pos[c]
+    l2m, lam = flat[3][pc], flat[4][pc]
+    sxx, syy, szz = sig_reg[:, src.comp(3)], sig_reg[:, src.comp(4)], sig_reg[:, src.comp(5)]
+    out[:, src.comp(3)] = sxx * l2m + (syy + szz) * lam
+    out[:, src.comp(4)] = syy * l2m + (sxx + szz) * lam
+    out[:, src.comp(5)] = szz * l2m + (sxx + syy) * lam
+    area = np.float32(1.0 / float(np.float32(np.float32(dx) * np.float32(dy)) * np.float32(dz)))
+    return out * float(area)
+
+
+@dataclass
+class Shot:
+    src: DeviceSet
+    rec: DeviceSet
+    sig_reg: torch.Tensor      # (nts, ntot_src) unscaled regular-grid source signals
+    d_obs: torch.Tensor        # (9, nRec, nts) observed data (irregular receivers)
+
+
+def make_shot(src_devices7, rec_devices7, model_irreg9, d_obs, device, q2compat=True):
+    """Spread the irregular source signals to the regular grid (spaceInterpGpu_3D::adjoint) and
+    move everything to the device.  model_irreg9: list of 9 (nIrregSrc, nts) arrays."""
+    src = DeviceSet.from_devices(src_devices7, device)
+    rec = DeviceSet.from_devices(rec_devices7, device, q2_receivers=q2compat)
+    nts = model_irreg9[0].shape[1]
+    blocks = []
+    for k in range(9):
+        g = COMP_GRID[k]
+        blocks.append(src_devices7[g].adjoint(False, None, np.asarray(model_irreg9[k], dtype=np.float32)))
+    sig = torch.from_numpy(np.ascontiguousarray(np.concatenate(blocks, axis=0).T)).to(device)
+    assert sig.shape == (nts, src.off[9])
+    d_obs = torch.as_tensor(np.asarray(d_obs, dtype=np.float32)).to(device) if d_obs is not None else None
+    return Shot(src, rec, sig, d_obs)
+
+
+class FwiProblem:
+    """One propagation grid, its context and shots; shared by forward modelling and gradients."""
+
+    def __init__(self, fd: H.FdParam, device="cuda", ckpt="auto", segment=0, variant=(8, 2, "tma")):
+        self.fd = fd
+        self.device = torch.device(device)
+        self.prop = Propagator(fd.nz, fd.nx, fd.ny, fd.nts, fd.sub, fd.minPad, float(fd.dz), float(fd.dx),
+                               float(fd.dy), float(fd.dts), float(fd.alphaCos),
+                               device=self.device.index or 0)
+        self.prop.set_stepper_variant(*variant)
+        self.prop.set_checkpoint_policy(ckpt, segment)
+        self.ckpt, self.segment = ckpt, segment
+        self.auto_budget = segment == 0
+        self.shots = []
+
+    def _bind_stream(self):
+        self.prop.set_stream(torch.cuda.current_stream(self.device))
+
+    def set_model(self, rho, lam, mu):
+        planes = medium_planes(rho, lam, mu, self.fd.dtw)
+        self._bind_stream()
+        self.prop.set_medium(planes)
+        return planes
+
+    def forward_data(self, shot: Shot, planes, save_checkpoints=False):
+        """Regular-grid predicted data (nts, ntot_rec) of one shot."""
+        fd = self.fd
+        sig = scale_sources(shot.sig_reg, shot.src, planes, fd.dx, fd.dy, fd.dz).contiguous()
+        rec = torch.zeros((fd.nts, shot.rec.off[9]), dtype=torch.float32, device=self.device)
+        self._bind_stream()
+        if save_checkpoints and self.auto_budget:
+            # leave room for what the gradient step allocates after the forward:
+            # irregular prediction and residual, regular residual, gradient planes
+            n = planes[0].numel()
+            reserve = (rec.numel() + 2 * shot.d_obs.numel() + 24 * n) * 4 + (2 << 30)
+            self.prop.set_checkpoint_policy(self.ckpt, self.segment, -float(reserve))
+        if save_checkpoints:
+            self.prop.fwi_forward_device(shot.src.pos, shot.src.off, shot.rec.pos, shot.rec.off, sig, rec)
+        else:
+            self.prop.nl_propagate_device(False, shot.src.pos, shot.src.off, shot.rec.pos, shot.rec.off, sig, rec)
+        return rec, sig
+
+    def shot_misfit_and_gradient(self, shot: Shot, planes):
+        """0.5*||d_pred - d_obs||^2 of one shot and its Born-adjoint gradient planes (8, ny, nx, nz)."""
+        rec, sig = self.forward_data(shot, planes, save_checkpoints=True)
+        d_pred = shot.rec.to_irregular(rec)
+        res = d_pred - shot.d_obs
+        loss = 0.5 * torch.sum(res * res, dtype=torch.float64)
+        res_reg = shot.rec.to_regular(res).contiguous()
+        grad8 = torch.zeros_like(planes)
+        self._bind_stream()
+        self.prop.fwi_gradient_device(shot.src.pos, shot.src.off, shot.rec.pos, shot.rec.off, sig, res_reg, grad8)
+        return loss, grad8
+
+
+class ElasticFwiMisfit(torch.autograd.Function):
+    """L(rho, lambda, mu) = sum over shots of 0.5*||d_pred - d_obs||^2.
+
+    The forward pass computes the misfit and, shot by shot, the Born-adjoint
+    gradient (so at most one shot's checkpoints are alive at a time); the
+    backward pass scales the stored gradient by the incoming gradient.
+    """
+
+    @staticmethod
+    def forward(ctx, rho, lam, mu, problem: FwiProblem, shot_ids=None):
+        planes = problem.set_model(rho.float().contiguous(), lam.float().contiguous(), mu.float().contiguous())
+        ids = range(len(problem.shots)) if shot_ids is None else shot_ids
+        total = torch.zeros((), dtype=torch.float64, device=rho.device)
+        g8 = torch.zeros_like(planes)
+        for i in ids:
+            loss, grad8 = problem.shot_misfit_and_gradient(problem.shots[i], planes)
+            total = total + loss
+            g8 += grad8
+        g = planes_to_model(g8, planes, problem.fd.dtw)
+        ctx.save_for_backward(*g)
+        return total
+
+    @staticmethod
+    def backward(ctx, grad_out):
+        grho, glam, gmu = ctx.saved_tensors
+        s = grad_out.to(grho.dtype)
+        return grho * s, glam * s, gmu * s, None, None

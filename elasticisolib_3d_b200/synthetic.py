@@ -153,8 +153,8 @@ def config_fwi(nzi=300, nxi=300, nyi=300, pad=40, nts=2500, nshots=32, nrec=150,
     dts = 0.002
     par = base_params(axes, pads, nts, dts, 2, 25.0)
     z0 = (axes[0].n - 2 * FAT - pads["zPadMinus"] - pads["zPadPlus"])
-    x_int = (nxi - 1) * d
-    y_int = (nyi - 1) * d
+    x_int = (nxi - 2) * d  # the last interior cell cannot hold a trilinear stencil on every staggered grid
+    y_int = (nyi - 2) * d
     ns = int(np.ceil(np.sqrt(nshots)))
     sx = np.linspace(0.1, 0.9, ns) * x_int
     src = []

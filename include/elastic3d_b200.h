@@ -219,9 +219,11 @@ int e3d_set_medium(e3d_context* ctx, const float* const* planes8, int on_device)
  * pipeline depth (2 or 3 stages) and plane loader (0 plain loads, 1 cp.async,
  * 2 TMA bulk tensor copies; 1 and 2 need nz % 4 == 0). */
 int e3d_set_stepper_variant(e3d_context* ctx, int tx, int stages, int loader);
-/* Checkpoint storage: type 0 = fp32, 1 = fp16, 2 = bf16 (per-slice scaled);
+/* Checkpoint storage: type -1 = fp32 when it fits else fp16 (default), 0 = fp32,
+ * 1 = fp16, 2 = bf16 (16-bit types carry one scale per y-slice and field);
  * segment = coarse blocks per segment (0 = largest that fits);
- * budget_bytes = device bytes for checkpoints and velocity slots (0 = 85% of free). */
+ * budget_bytes > 0: device bytes for checkpoints and velocity slots; 0: 85% of the
+ * free memory; < 0: 85% of the free memory minus |budget_bytes| kept for the caller. */
 int e3d_set_checkpoint_policy(e3d_context* ctx, int type, int segment, double budget_bytes);
 /* Wait for all work queued on the context's stream; reports an expired
  * bounded pipeline wait inside the stepper as E3D_ERR_CUDA. */
@@ -229,10 +231,13 @@ int e3d_synchronize(e3d_context* ctx);
 /* cudaStream_t of the context, as void*. */
 void* e3d_stream(e3d_context* ctx);
 /* Queue the context's work on an existing cudaStream_t (passed as void*), e.g. the
- * caller's framework stream; NULL restores the context's own stream. */
-int e3d_set_stream(e3d_context* ctx, void* stream);
+ * caller's framework stream; a NULL handle is the legacy default stream.
+ * use_own != 0 returns to the context's own stream (stream is then ignored). */
+int e3d_set_stream(e3d_context* ctx, void* stream, int use_own);
 /* Updated cells per fine step ((nz-8)(nx-8)(ny-8)). */
 long long e3d_cells_per_step(const e3d_context* ctx);
+/* Coarse blocks per checkpoint segment chosen by the last checkpointed forward (0 before). */
+int e3d_checkpoint_segment(const e3d_context* ctx);
 
 /* Host-buffer propagations.  src_pos/rec_pos: 7 tables; n_src/n_rec: 7 counts. */
 int e3d_nl_forward(e3d_context* ctx, const float* const* model9, float* const* data9,
@@ -264,6 +269,15 @@ int e3d_fwi_forward_device(e3d_context* ctx, const long long* src_pos_dev, const
 int e3d_fwi_gradient_device(e3d_context* ctx, const long long* src_pos_dev, const int* src_off10,
                             const long long* rec_pos_dev, const int* rec_off10, const float* src_sig_dev,
                             const float* residual_dev, float* const* grad8_dev);
+
+/* Sampled stepper timing for roofline reporting: every n-th stepper launch is
+ * bracketed by CUDA events on the launching stream (n = 0 switches it off). */
+int e3d_kernel_timing(e3d_context* ctx, int every);
+/* Mean duration in ms and number of the sampled launches of one stepper mode
+ * since the previous read (waits for them to finish). */
+int e3d_kernel_timing_read(e3d_context* ctx, int mode, double* avg_ms, long long* count);
+/* Number of kernel launches this context has issued. */
+long long e3d_launch_count(const e3d_context* ctx);
 
 /* Bare stepper (mode 0 forward, 1 time-reversed, 2 exact transpose) applied
  * n_steps times to the context's working wavefields; for benchmarking. */

@@ -21,7 +21,8 @@ def _prop(p, **kw):
 
 
 VARIANTS = [(8, 2, "plain"), (16, 2, "plain"), (8, 2, "cpasync"), (8, 3, "cpasync"), (16, 2, "cpasync"),
-            (8, 2, "tma"), (8, 3, "tma"), (16, 2, "tma")]
+            (8, 2, "tma"), (8, 3, "tma"), (16, 2, "tma"), (8, 2, "tma-ring"), (16, 2, "tma-ring"),
+            (8, 2, "tma-ring-ldg"), (8, 3, "tma-ring-ldg"), (8, 2, "tma-ring-ldg2")]
 
 
 @pytest.mark.parametrize("tx,stages,loader", VARIANTS)
@@ -70,8 +71,8 @@ def test_born_forward_matches_oracle():
     assert rel_l2(got, ref) < 1e-5
 
 
-@pytest.mark.parametrize("segment", [0, 1, 3])
-def test_born_adjoint_matches_oracle(segment):
+@pytest.mark.parametrize("segment,loader", [(0, "plain"), (1, "plain"), (3, "plain"), (0, "tma"), (3, "tma")])
+def test_born_adjoint_matches_oracle(segment, loader):
     sv, p, med, src, rec, dtw = prepared(seed=4)
     rng = np.random.default_rng(8)
     spos = [d.unique for d in src]
@@ -81,6 +82,7 @@ def test_born_adjoint_matches_oracle(segment):
     pr = _prop(p)
     pr.set_medium(med)
     pr.set_checkpoint_policy("fp32", segment)
+    pr.set_stepper_variant(8, 2, loader)
     got = pr.born_adjoint(sig, dat, spos, rpos)
     ref = O.born_adjoint_reg(p, med, sig, dat, spos, rpos, None, np.float32)
     assert rel_l2(got, ref) < 1e-5
