@@ -127,9 +127,8 @@ def build_problem(args, device):
     # observed data: nonlinear forward on the true model
     mt = [torch.tensor(svt.elastic[k], device=device) for k in range(3)]
     planes = prob.set_model(*mt)
-    rec_t, _ = prob.forward_data(shot, planes)
-    shot.d_obs = shot.rec.to_irregular(rec_t)
-    del rec_t, planes, mt
+    shot.d_obs, _ = prob.forward_data(shot, planes)
+    del planes, mt
     prob.shots.append(shot)
     torch.cuda.synchronize()
     return sv, fd, prob

@@ -58,8 +58,10 @@ SIGNATURES = {
     "e3d_born_forward": ([P] * 8, I),
     "e3d_born_adjoint": ([P] * 8, I),
     "e3d_nl_propagate_device": ([P, I, P, P, P, P, P, P], I),
-    "e3d_fwi_forward_device": ([P] * 7, I),
-    "e3d_fwi_gradient_device": ([P] * 8, I),
+    "e3d_fwi_forward_device": ([P] * 8, I),
+    "e3d_fwi_gradient_device": ([P] * 9, I),
+    "e3d_set_velocity_storage": ([P, I], I),
+    "e3d_velocity_storage": ([P], I),
     "e3d_step_only": ([P, I, I], I),
     "e3d_kernel_timing": ([P, I], I),
     "e3d_kernel_timing_read": ([P, I, P, P], I),
@@ -107,6 +109,10 @@ class E3DDesc(ctypes.Structure):
     _fields_ = [("device", I), ("nz", I), ("nx", I), ("ny", I), ("nts", I), ("sub", I), ("minPad", I),
                 ("dz", F), ("dx", F), ("dy", F), ("dts", F), ("alphaCos", F), ("fix_q1", I), ("q2compat", I),
                 ("q3compat", I)]
+
+
+class E3DTraceMap(ctypes.Structure):
+    _fields_ = [("n_irreg", I), ("n_taps", I), ("slot", P), ("weight", P), ("row_ptr", P), ("idx", P), ("w", P)]
 
 
 def ptr_array(arrays, ctype=P):

@@ -50,7 +50,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
             cmd += ["-Xptxas", "-v"] if verbose else []
         else:
             cmd = [nvcc, "-x", "c++", "-c", os.path.join(CSRC, src), "-o", obj, "-O3", "-std=c++17",
-                   "-Xcompiler", "-fPIC,-fopenmp", "-ccbin", ccbin]
+                   "-Xcompiler", "-fPIC,-fopenmp", "-ccbin", ccbin] + ARCH
         if verbose:
             print(" ".join(cmd), file=sys.stderr)
         subprocess.check_call(cmd)

@@ -364,27 +364,58 @@ int e3d_nl_propagate_device(e3d_context* ctx, int adjoint, const long long* src_
   return nlPropagateDevice(ctx->c, adjoint != 0, S, R, src_sig_dev, rec_sig_dev);
 }
 
+static int traceMap(const e3d_trace_map* m, TraceMap& t) {
+  if (!m) return E3D_OK;
+  if (m->n_irreg < 0 || m->n_taps < 1 || m->n_taps > 64) {
+    setLastError("bad trace map sizes", __FILE__, __LINE__);
+    return E3D_ERR_ARG;
+  }
+  if (!m->row_ptr || (m->n_irreg > 0 && (!m->slot || !m->weight || !m->idx || !m->w))) {
+    setLastError("null trace map table", __FILE__, __LINE__);
+    return E3D_ERR_ARG;
+  }
+  t.nIrreg = m->n_irreg;
+  t.nTaps = m->n_taps;
+  t.slot = m->slot;
+  t.weight = m->weight;
+  t.rowPtr = m->row_ptr;
+  t.idx = m->idx;
+  t.w = m->w;
+  return E3D_OK;
+}
+
 int e3d_fwi_forward_device(e3d_context* ctx, const long long* src_pos_dev, const int* src_off10,
                            const long long* rec_pos_dev, const int* rec_off10, const float* src_sig_dev,
-                           float* rec_sig_dev) {
+                           float* rec_sig_dev, const e3d_trace_map* map) {
   CTX_OR_FAIL(ctx);
   DevSignals S, R;
+  TraceMap T;
   int st = devSet(src_pos_dev, src_off10, S);
   if (st == E3D_OK) st = devSet(rec_pos_dev, rec_off10, R);
+  if (st == E3D_OK) st = traceMap(map, T);
   if (st != E3D_OK) return st;
-  return fwiForwardDevice(ctx->c, S, R, src_sig_dev, rec_sig_dev);
+  return fwiForwardDevice(ctx->c, S, R, src_sig_dev, rec_sig_dev, map ? &T : nullptr);
 }
 
 int e3d_fwi_gradient_device(e3d_context* ctx, const long long* src_pos_dev, const int* src_off10,
                             const long long* rec_pos_dev, const int* rec_off10, const float* src_sig_dev,
-                            const float* residual_dev, float* const* grad8_dev) {
+                            const float* residual_dev, float* const* grad8_dev, const e3d_trace_map* map) {
   CTX_OR_FAIL(ctx);
   DevSignals S, R;
+  TraceMap T;
   int st = devSet(src_pos_dev, src_off10, S);
   if (st == E3D_OK) st = devSet(rec_pos_dev, rec_off10, R);
+  if (st == E3D_OK) st = traceMap(map, T);
   if (st != E3D_OK) return st;
-  return fwiGradientDevice(ctx->c, S, R, src_sig_dev, residual_dev, grad8_dev);
+  return fwiGradientDevice(ctx->c, S, R, src_sig_dev, residual_dev, grad8_dev, map ? &T : nullptr);
 }
+
+int e3d_set_velocity_storage(e3d_context* ctx, int type) {
+  CTX_OR_FAIL(ctx);
+  return setVelocityStorage(ctx->c, type);
+}
+
+int e3d_velocity_storage(const e3d_context* ctx) { return (ctx && ctx->c) ? velocityStorage(ctx->c) : -1; }
 
 int e3d_kernel_timing(e3d_context* ctx, int every) {
   CTX_OR_FAIL(ctx);

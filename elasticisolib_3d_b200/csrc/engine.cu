@@ -73,14 +73,19 @@ struct Context {
   Fields9 w0, w1;
   // Born / FWI buffers, allocated on first use
   Fields9 s0, s1;            // source-side state
-  std::vector<float*> vSlots;  // decimated source velocity slots (3 fields each)
+  std::vector<float*> vSlots;  // decimated source velocity slots, FP32 (3 fields each)
+  std::vector<void*> vStore;   // FP16 velocity slots with per-(field, y-slice) scales
+  int vType = -1;              // velocity slot storage requested: -1 auto, 0 FP32, 1 FP16
+  int vUsed = 0;               // storage of the current plan
+  float* traceRing = nullptr;  // two regular-grid receiver slices (irregular trace mode)
+  size_t traceRingFloats = 0;
   Fields9 ss[2];             // secondary sources (forward) / decimated adjoint field (adjoint)
   Fields9 q0, q1;            // premultiplied adjoint levels (dual-state exact adjoint)
   float* pertDev[NMED] = {};
   // checkpoints
   int ckptType = CKPT_AUTO;
   int ckptUsed = CKPT_F32;     // storage type of the current checkpoints
-  double ckptHeld = 0;         // bytes of checkpoints + velocity slots currently allocated
+  int vAllocType = -1;         // velocity slot storage currently allocated
   int segment = 0;           // coarse blocks per segment (0 = automatic)
   double budget = 0;         // bytes available for checkpoints + velocity slots (0 = automatic)
   std::vector<void*> ckpt;   // one per segment (index = segment id), packed 18-field states
@@ -552,28 +557,41 @@ static int launchStepRaw(Context* c, int mode, const StepPtrs& p) {
   return E3D_OK;
 }
 
-static int launchInject(Context* c, const StepPtrs& p, const DevSignals& s, const float* sig, int its, int k) {
+// Injection of time slices sigL (its) and sigR (its+1), filter weights k.
+static int launchInjectSlices(Context* c, const StepPtrs& p, const DevSignals& s, const float* sigL,
+                              const float* sigR, int k) {
   SparseSet ss;
   ss.pos = s.pos;
   for (int i = 0; i <= NCOMP; i++) ss.off[i] = s.off[i];
   const int n = s.off[NCOMP];
   if (n == 0) return E3D_OK;
   c->launches++;
-  kInject<<<(n + 127) / 128, 128, 0, c->st>>>(p, c->g, ss, sig, its, c->filt[k], c->filt[c->hfilt + k]);
+  kInject<<<(n + 127) / 128, 128, 0, c->st>>>(p, c->g, ss, sigL, sigR, c->filt[k], c->filt[c->hfilt + k]);
+  E3D_LAUNCH_CHECK();
+  return E3D_OK;
+}
+
+// Injection from a time-major [nts][ntot] signal array at coarse time its.
+static int launchInject(Context* c, const StepPtrs& p, const DevSignals& s, const float* sig, int its, int k) {
+  const size_t ntot = (size_t)s.off[NCOMP];
+  return launchInjectSlices(c, p, s, sig + (size_t)its * ntot, sig + (size_t)(its + 1) * ntot, k);
+}
+
+static int launchRecordSlices(Context* c, const StepPtrs& p, const DevSignals& s, float* outL, float* outR, int k) {
+  SparseSet ss;
+  ss.pos = s.pos;
+  for (int i = 0; i <= NCOMP; i++) ss.off[i] = s.off[i];
+  const int n = s.off[NCOMP];
+  if (n == 0) return E3D_OK;
+  c->launches++;
+  kRecord<<<(n + 127) / 128, 128, 0, c->st>>>(p, ss, outL, outR, c->filt[k], c->filt[c->hfilt + k]);
   E3D_LAUNCH_CHECK();
   return E3D_OK;
 }
 
 static int launchRecord(Context* c, const StepPtrs& p, const DevSignals& s, float* out, int its, int k) {
-  SparseSet ss;
-  ss.pos = s.pos;
-  for (int i = 0; i <= NCOMP; i++) ss.off[i] = s.off[i];
-  const int n = s.off[NCOMP];
-  if (n == 0) return E3D_OK;
-  c->launches++;
-  kRecord<<<(n + 127) / 128, 128, 0, c->st>>>(p, ss, out, its, c->filt[k], c->filt[c->hfilt + k]);
-  E3D_LAUNCH_CHECK();
-  return E3D_OK;
+  const size_t ntot = (size_t)s.off[NCOMP];
+  return launchRecordSlices(c, p, s, out + (size_t)its * ntot, out + (size_t)(its + 1) * ntot, k);
 }
 
 static int launchRefresh(Context* c, const StepPtrs& p, const DevSignals& s) {
@@ -940,11 +958,46 @@ static int bornForwardDevice(Context* c, const DevSignals& srcSet, const DevSign
 // A checkpoint for segment s (coarse blocks [s*L, s*L+L)) holds the
 // source-side state at the start of block s*L-1; recomputing from it yields
 // V[s*L] complete (its right-weight part comes from block s*L-1).
+// The plan (segment length, checkpoint storage, velocity-slot storage) is
+// the first that fits the memory budget among
+//   FP32 states + FP32 velocity slots, FP16 states + FP32 slots,
+//   FP16 states + FP16 slots (auto); for an explicit state type T:
+//   T + FP32 slots, T + FP16 slots.
 // ---------------------------------------------------------------------------
+enum { V_F32 = 0, V_F16 = 1 };
+
 static size_t ckptBytesPerState(const Context* c, int type) {
   const size_t eb = type == CKPT_F32 ? 4 : 2;
   size_t b = (size_t)18 * c->g.n * eb;
   if (type != CKPT_F32) b += (size_t)18 * c->d.ny * sizeof(float) + 256;
+  return b;
+}
+
+// FP16 velocity slot: three fields of n halves, padded to 256 B, then 3*ny scales.
+static size_t vHalfBytes(const Context* c) { return ((size_t)3 * c->g.n * 2 + 255) / 256 * 256; }
+static size_t vStoreBytes(const Context* c) { return vHalfBytes(c) + (size_t)3 * c->d.ny * sizeof(float); }
+static double vSlotBytes(const Context* c, int vt) {
+  return vt == V_F32 ? 3.0 * (double)c->g.n * sizeof(float) : (double)vStoreBytes(c);
+}
+
+// Checkpoints plus velocity slots of a plan with segment length L.  FP32 slots
+// hold V[s*L .. s*L+L+2]; FP16 slots hold V[s*L .. s*L+L+1] plus three FP32
+// working slots (two accumulators while recomputing, a three-deep ring for
+// the imaging condition).
+static double planBytes(const Context* c, int ck, int vt, int L) {
+  const int blocks = c->d.nts - 1;
+  const int nseg = (blocks + L - 1) / L;
+  double b = (double)(nseg - 1) * ckptBytesPerState(c, ck);
+  if (vt == V_F32) b += (L + 3) * vSlotBytes(c, V_F32);
+  else b += (L + 2) * vSlotBytes(c, V_F16) + 3 * vSlotBytes(c, V_F32);
+  return b;
+}
+
+static double heldBytes(const Context* c) {
+  double b = 0;
+  for (void* p : c->ckpt)
+    if (p) b += ckptBytesPerState(c, c->ckptAllocType);
+  b += (double)c->vSlots.size() * vSlotBytes(c, V_F32) + (double)c->vStore.size() * vSlotBytes(c, V_F16);
   return b;
 }
 
@@ -968,50 +1021,96 @@ static double autoBudget(const Context* c, size_t free) {
   return 0.85 * ((double)free - reserve) - pendingAdjointBytes(c);
 }
 
-static int chooseSegment(Context* c, int& L) {
+static int choosePlan(Context* c, int& L) {
   const int blocks = c->d.nts - 1;
-  if (c->ckptType == CKPT_AUTO) {
-    // FP32 states when they fit, else FP16 with per-slice scales
-    c->ckptUsed = CKPT_F32;
-    if (c->segment == 0) {
-      size_t free = 0, total = 0;
-      E3D_CUDA_TRY(cudaMemGetInfo(&free, &total));
-      const double budget = autoBudget(c, free) + c->ckptHeld;
-      const double ck = (double)ckptBytesPerState(c, CKPT_F32), vs = 3.0 * c->g.n * sizeof(float);
-      bool fits = false;
-      for (int l = 1; l <= blocks && !fits; l++) fits = (((blocks + l - 1) / l) - 1) * ck + (l + 3) * vs <= budget;
-      if (!fits) c->ckptUsed = CKPT_F16;
-    }
-  } else {
-    c->ckptUsed = c->ckptType;
-  }
-  if (c->segment > 0) {
-    L = std::min(c->segment, blocks);
-    return E3D_OK;
-  }
+  struct Cand {
+    int ck, vt;
+  };
+  const Cand autoList[3] = {{CKPT_F32, V_F32}, {CKPT_F16, V_F32}, {CKPT_F16, V_F16}};
+  const Cand typedList[2] = {{c->ckptType, V_F32}, {c->ckptType, V_F16}};
+  const Cand* all = c->ckptType == CKPT_AUTO ? autoList : typedList;
+  const int nAll = c->ckptType == CKPT_AUTO ? 3 : 2;
+  std::vector<Cand> cands;
+  for (int i = 0; i < nAll; i++)
+    if (c->vType < 0 || all[i].vt == c->vType) cands.push_back(all[i]);
   size_t free = 0, total = 0;
   E3D_CUDA_TRY(cudaMemGetInfo(&free, &total));
-  // memory this context already holds for checkpoints and velocity slots counts as
-  // available; the adjoint pass's own wavefields, if not yet allocated, do not
-  double budget = autoBudget(c, free) + c->ckptHeld;
-  const double ck = (double)ckptBytesPerState(c, c->ckptUsed);
-  const double vs = 3.0 * c->g.n * sizeof(float);
-  // One extra source block is recomputed per segment, so use the longest
-  // segment whose checkpoints and velocity slots fit in the budget.
-  int bestL = -1;
-  for (int l = blocks; l >= 1; l--) {
-    const int nseg = (blocks + l - 1) / l;
-    const double need = (nseg - 1) * ck + (l + 3) * vs;
-    if (need <= budget) {
-      bestL = l;
-      break;
+  // memory this context already holds for checkpoints and velocity slots counts as available
+  const double budget = autoBudget(c, free) + heldBytes(c);
+  for (size_t i = 0; i < cands.size(); i++) {
+    const Cand& k = cands[i];
+    if (c->segment > 0) {
+      const int l = std::min(c->segment, blocks);
+      if (planBytes(c, k.ck, k.vt, l) <= budget || i + 1 == cands.size()) {
+        c->ckptUsed = k.ck;
+        c->vUsed = k.vt;
+        L = l;
+        return E3D_OK;
+      }
+      continue;
     }
+    // one extra source block is recomputed per segment: take the longest segment that fits
+    for (int l = blocks; l >= 1; l--)
+      if (planBytes(c, k.ck, k.vt, l) <= budget) {
+        c->ckptUsed = k.ck;
+        c->vUsed = k.vt;
+        L = l;
+        return E3D_OK;
+      }
   }
-  if (bestL < 0) {
-    setLastError("wavefield checkpoints do not fit in device memory", __FILE__, __LINE__);
-    return E3D_ERR_OOM;
+  setLastError("wavefield checkpoints do not fit in device memory", __FILE__, __LINE__);
+  return E3D_ERR_OOM;
+}
+
+static int resizeVStorage(Context* c, int nF32, int nF16) {
+  while ((int)c->vSlots.size() > nF32) {
+    devFree(c, c->vSlots.back());
+    c->vSlots.pop_back();
   }
-  L = bestL;
+  while ((int)c->vStore.size() > nF16) {
+    devFree(c, c->vStore.back());
+    c->vStore.pop_back();
+  }
+  E3D_RET(ensureVSlots(c, nF32));
+  while ((int)c->vStore.size() < nF16) {
+    void* p = nullptr;
+    E3D_RET(devAlloc(c, &p, vStoreBytes(c)));
+    c->vStore.push_back(p);
+  }
+  return E3D_OK;
+}
+
+// Per-(field, y-slice) scaled FP16 copy of the three velocity fields of slot v.
+static int packVelocity(Context* c, const float* v, void* store) {
+  const long long n = c->g.n, ys = c->g.yStride;
+  const int ny = c->d.ny;
+  __half* h = (__half*)store;
+  float* scales = (float*)((char*)store + vHalfBytes(c));
+  float* smax = (float*)c->scratch;
+  const unsigned blocks = (unsigned)((n + 255) / 256);
+  for (int k = 0; k < 3; k++) {
+    c->launches += 2;
+    kSliceMaxAbs<<<ny, 256, 0, c->st>>>(v + (size_t)k * n, ys, smax);
+    E3D_LAUNCH_CHECK();
+    kPackSlices<__half><<<blocks, 256, 0, c->st>>>(v + (size_t)k * n, ys, n, smax, 16384.f, h + (size_t)k * n,
+                                                   scales + (size_t)k * ny);
+    E3D_LAUNCH_CHECK();
+  }
+  return E3D_OK;
+}
+
+static int unpackVelocity(Context* c, const void* store, float* v) {
+  const long long n = c->g.n, ys = c->g.yStride;
+  const int ny = c->d.ny;
+  const __half* h = (const __half*)store;
+  const float* scales = (const float*)((const char*)store + vHalfBytes(c));
+  const unsigned blocks = (unsigned)((n + 255) / 256);
+  for (int k = 0; k < 3; k++) {
+    c->launches++;
+    kUnpackSlices<__half><<<blocks, 256, 0, c->st>>>(h + (size_t)k * n, ys, n, scales + (size_t)k * ny,
+                                                     v + (size_t)k * n);
+    E3D_LAUNCH_CHECK();
+  }
   return E3D_OK;
 }
 
@@ -1076,13 +1175,17 @@ static int unpackState(Context* c, int seg) {
 
 static int prepareCheckpoints(Context* c, int& L, int& nseg) {
   const int blocks = c->d.nts - 1;
-  E3D_RET(chooseSegment(c, L));
+  E3D_RET(choosePlan(c, L));
   nseg = (blocks + L - 1) / L;
-  if (c->ckptSegLen != L || (int)c->ckpt.size() != nseg || c->ckptAllocType != c->ckptUsed) {
+  if (c->ckptSegLen != L || (int)c->ckpt.size() != nseg || c->ckptAllocType != c->ckptUsed ||
+      c->vAllocType != c->vUsed) {
     for (void* p : c->ckpt) devFree(c, p);
     for (float* p : c->ckptScale) devFree(c, p);
     c->ckpt.assign(nseg, nullptr);
     c->ckptScale.assign(nseg, nullptr);
+    c->ckptAllocType = c->ckptUsed;
+    E3D_RET(resizeVStorage(c, c->vUsed == V_F32 ? L + 3 : 3, c->vUsed == V_F32 ? 0 : L + 2));
+    c->vAllocType = c->vUsed;
     for (int s = 1; s < nseg; s++) {
       const size_t eb = c->ckptUsed == CKPT_F32 ? 4 : 2;
       E3D_RET(devAlloc(c, &c->ckpt[s], (size_t)18 * c->g.n * eb));
@@ -1090,50 +1193,98 @@ static int prepareCheckpoints(Context* c, int& L, int& nseg) {
         E3D_RET(devAlloc(c, (void**)&c->ckptScale[s], (size_t)18 * c->d.ny * sizeof(float)));
     }
     c->ckptSegLen = L;
-    c->ckptAllocType = c->ckptUsed;
-    c->ckptHeld = (double)(nseg - 1) * ckptBytesPerState(c, c->ckptUsed) + (double)c->vSlots.size() * 3.0 * c->g.n * 4;
   }
-  if (c->ckptUsed != CKPT_F32) E3D_RET(scratchAtLeast(c, (size_t)c->d.ny * sizeof(float)));
+  E3D_RET(scratchAtLeast(c, (size_t)c->d.ny * sizeof(float)));
+  return E3D_OK;
+}
+
+// Receiver slices between the regular acquisition points and irregular traces.
+static int traceRingAtLeast(Context* c, size_t floats) {
+  if (c->traceRingFloats >= floats) return E3D_OK;
+  devFree(c, c->traceRing);
+  c->traceRing = nullptr;
+  c->traceRingFloats = 0;
+  E3D_RET(devAlloc(c, (void**)&c->traceRing, std::max<size_t>(floats, 1) * sizeof(float)));
+  c->traceRingFloats = floats;
+  return E3D_OK;
+}
+
+static int traceGather(Context* c, const TraceMap& m, int nReg, const float* reg, float* irr) {
+  const int rows = NCOMP * m.nIrreg;
+  if (rows == 0) return E3D_OK;
+  c->launches++;
+  kTraceGather<<<(rows + 127) / 128, 128, 0, c->st>>>(reg, irr, rows, m.nTaps, m.slot, m.weight, nReg);
+  E3D_LAUNCH_CHECK();
+  return E3D_OK;
+}
+
+static int traceSpread(Context* c, const TraceMap& m, int nReg, const float* irr, float* reg) {
+  if (nReg == 0) return E3D_OK;
+  c->launches++;
+  kTraceSpread<<<(nReg + 127) / 128, 128, 0, c->st>>>(irr, reg, nReg, m.rowPtr, m.idx, m.w, NCOMP * m.nIrreg);
+  E3D_LAUNCH_CHECK();
   return E3D_OK;
 }
 
 // Source-side forward pass over all coarse blocks, saving the state at the
 // start of block s*L-1 for every segment s >= 1.  When recSig is non-null the
-// receivers are recorded too (this is the nonlinear forward of FWI).
+// receivers are recorded too (this is the nonlinear forward of FWI): into a
+// time-major regular-grid array, or, with a trace map, through a two-slice
+// ring converted to irregular traces as each coarse slice completes.
 static int sourcePassWithCheckpoints(Context* c, const DevSignals& srcSet, const DevSignals* recSet,
-                                     const float* srcSig, float* recSig) {
+                                     const float* srcSig, float* recSig, const TraceMap* map) {
   int L = 0, nseg = 0;
   E3D_RET(prepareCheckpoints(c, L, nseg));
   E3D_RET(allocFields(c, c->s0, true));
   E3D_RET(allocFields(c, c->s1, true));
   const int nts = c->d.nts, sub = c->d.sub;
-  if (recSig)
-    E3D_CUDA_TRY(cudaMemsetAsync(recSig, 0, (size_t)std::max(recSet->off[NCOMP], 1) * nts * sizeof(float), c->st));
+  const size_t nr = recSet ? (size_t)recSet->off[NCOMP] : 0;
+  const size_t rows = map ? (size_t)NCOMP * map->nIrreg : 0;
+  float* ring = nullptr;
+  if (recSig && map) {
+    E3D_RET(traceRingAtLeast(c, 2 * nr));
+    ring = c->traceRing;
+    E3D_CUDA_TRY(cudaMemsetAsync(ring, 0, std::max<size_t>(2 * nr, 1) * sizeof(float), c->st));
+  } else if (recSig) {
+    E3D_CUDA_TRY(cudaMemsetAsync(recSig, 0, std::max<size_t>(nr, 1) * nts * sizeof(float), c->st));
+  }
   for (int b = 0; b < nts - 1; b++) {
     if ((b + 1) % L == 0 && (b + 1) / L < nseg) E3D_RET(packState(c, (b + 1) / L));
     for (int it2 = 1; it2 <= sub; it2++) {
       StepPtrs p = makeStep(c, c->s0, c->s1);
       E3D_RET(launchStep(c, STEP_FWD, p));
       E3D_RET(launchInject(c, p, srcSet, srcSig, b, it2 - 1));
-      if (recSig) E3D_RET(launchRecord(c, p, *recSet, recSig, b, it2));
+      if (ring) E3D_RET(launchRecordSlices(c, p, *recSet, ring + (b % 2) * nr, ring + ((b + 1) % 2) * nr, it2));
+      else if (recSig) E3D_RET(launchRecord(c, p, *recSet, recSig, b, it2));
       swapF(c->s0, c->s1);
     }
+    if (ring) {
+      // slice b is complete; its ring slot is reused for slice b+2
+      E3D_RET(traceGather(c, *map, (int)nr, ring + (b % 2) * nr, recSig + (size_t)b * rows));
+      if (nr) E3D_CUDA_TRY(cudaMemsetAsync(ring + (b % 2) * nr, 0, nr * sizeof(float), c->st));
+    }
   }
+  if (ring) E3D_RET(traceGather(c, *map, (int)nr, ring + ((nts - 1) % 2) * nr, recSig + (size_t)(nts - 1) * rows));
   c->ckptValid = true;
   return E3D_OK;
 }
 
 // Adjoint pass (BornElasticAdjGpu_3D phase B) consuming the checkpoints:
 // segments are processed last to first; each recomputes its velocity slots
-// from its checkpoint, then runs its adjoint blocks and imaging.
+// from its checkpoint, then runs its adjoint blocks and imaging.  With a
+// trace map the residual is irregular and time-major; each coarse slice is
+// spread to the regular acquisition points just before the block that
+// injects it.
 static int adjointPassFromCheckpoints(Context* c, const DevSignals& srcSet, const DevSignals& recSet,
-                                      const float* srcSig, const float* resid) {
+                                      const float* srcSig, const float* resid, const TraceMap* map) {
   E3D_ARG(c->ckptValid, "no checkpoints for this shot");
   const int nts = c->d.nts, sub = c->d.sub, L = c->ckptSegLen;
   const int blocks = nts - 1;
   const int nseg = (blocks + L - 1) / L;
   const long long n = c->g.n;
-  E3D_RET(ensureVSlots(c, L + 3));
+  const bool vc = c->vUsed == V_F16;
+  E3D_RET(resizeVStorage(c, std::max<int>(vc ? 3 : L + 3, (int)c->vSlots.size()),
+                         std::max<int>(vc ? L + 2 : 0, (int)c->vStore.size())));
   E3D_RET(allocFields(c, c->w0, true));
   E3D_RET(allocFields(c, c->w1, true));
   E3D_RET(allocFields(c, c->ss[0], true));
@@ -1144,40 +1295,68 @@ static int adjointPassFromCheckpoints(Context* c, const DevSignals& srcSet, cons
     E3D_RET(allocFields(c, c->q0, true));
     E3D_RET(allocFields(c, c->q1, true));
   }
+  const size_t nr = (size_t)recSet.off[NCOMP];
+  const size_t rows = map ? (size_t)NCOMP * map->nIrreg : 0;
+  if (map) {
+    E3D_RET(traceRingAtLeast(c, 2 * nr));
+    E3D_RET(traceSpread(c, *map, (int)nr, resid + (size_t)(nts - 1) * rows, c->traceRing + ((nts - 1) % 2) * nr));
+  }
+  auto dataSlice = [&](int t) -> const float* {
+    return map ? c->traceRing + (t % 2) * nr : resid + (size_t)t * nr;
+  };
   // adjoint decimation slots: A[its] (left, fresh per block) and A[its+1] (right)
   Fields9* aLeft = &c->ss[0];
   Fields9* aRight = &c->ss[1];
-  // velocity slot of coarse time t within the current segment window [s0, ...]
   int winStart = 0;
+  // FP32 velocity of coarse time t for the imaging condition
   auto V = [&](int t) -> float* {
     if (t < 0 || t >= nts) return nullptr;
+    if (vc) return c->vSlots[t % 3];
     const int i = t - winStart;
     return (i >= 0 && i < (int)c->vSlots.size()) ? c->vSlots[i] : nullptr;
+  };
+  // accumulation slot of V[t] while the segment is recomputed
+  auto A = [&](int t) -> float* {
+    if (t < 0 || t >= nts) return nullptr;
+    return vc ? c->vSlots[(t - winStart) % 2] : c->vSlots[t - winStart];
   };
   for (int s = nseg - 1; s >= 0; s--) {
     const int bBeg = s * L;
     const int bEnd = std::min(bBeg + L, blocks);  // adjoint blocks [bBeg, bEnd)
-    // recompute V[bBeg .. min(bEnd+1, nts-1)] from the checkpoint
+    const int lastBlock = std::min(bEnd + 1, blocks - 1);
     winStart = bBeg;
-    const int lastV = std::min(bEnd + 2, nts - 1);
-    for (int t = bBeg; t <= lastV; t++)
-      E3D_CUDA_TRY(cudaMemsetAsync(c->vSlots[t - bBeg], 0, (size_t)3 * n * sizeof(float), c->st));
-    int firstBlock;
+    // recompute V[bBeg .. min(bEnd+1, nts-1)] from the checkpoint
+    const int nClear = vc ? 2 : std::min(bEnd + 2, nts - 1) - bBeg + 1;
+    for (int i = 0; i < nClear; i++)
+      E3D_CUDA_TRY(cudaMemsetAsync(c->vSlots[i], 0, (size_t)3 * n * sizeof(float), c->st));
+    int firstBlock = 0;
     if (s == 0) {
       E3D_RET(zeroFields(c, c->s0));
       E3D_RET(zeroFields(c, c->s1));
-      firstBlock = 0;
     } else {
       E3D_RET(unpackState(c, s));
-      firstBlock = bBeg - 1;
       // block bBeg-1 only feeds V[bBeg] through its right weights
-      E3D_RET(sourceBlock(c, firstBlock, srcSet, srcSig, nullptr, V(bBeg)));
+      E3D_RET(sourceBlock(c, bBeg - 1, srcSet, srcSig, nullptr, A(bBeg)));
       firstBlock = bBeg;
     }
-    const int lastBlock = std::min(bEnd + 1, blocks - 1);
-    for (int b = firstBlock; b <= lastBlock; b++) E3D_RET(sourceBlock(c, b, srcSet, srcSig, V(b), V(b + 1)));
+    for (int b = firstBlock; b <= lastBlock; b++) {
+      E3D_RET(sourceBlock(c, b, srcSet, srcSig, A(b), A(b + 1)));
+      if (vc) {
+        // V[b] is complete: store it and reuse its slot for V[b+2]
+        E3D_RET(packVelocity(c, A(b), c->vStore[b - bBeg]));
+        E3D_CUDA_TRY(cudaMemsetAsync(A(b), 0, (size_t)3 * n * sizeof(float), c->st));
+      }
+    }
+    // V[nts-1] has no block of its own: complete after block nts-2
+    if (vc && lastBlock + 1 == nts - 1 && nts - 1 <= bEnd + 1)
+      E3D_RET(packVelocity(c, A(nts - 1), c->vStore[nts - 1 - bBeg]));
+    if (vc)
+      for (int t = bEnd; t <= std::min(bEnd + 1, nts - 1); t++)
+        E3D_RET(unpackVelocity(c, c->vStore[t - bBeg], V(t)));
     // adjoint blocks, last to first
     for (int its = bEnd - 1; its >= bBeg; its--) {
+      if (vc) E3D_RET(unpackVelocity(c, c->vStore[its - bBeg], V(its)));
+      if (map) E3D_RET(traceSpread(c, *map, (int)nr, resid + (size_t)its * rows, c->traceRing + (its % 2) * nr));
       for (int it2 = sub - 1; it2 >= 0; it2--) {
         StepPtrs p = makeStep(c, c->w0, c->w1);
         for (int k = 0; k < NCOMP; k++) {
@@ -1195,7 +1374,7 @@ static int adjointPassFromCheckpoints(Context* c, const DevSignals& srcSet, cons
         }
         if (it2 == sub - 1) E3D_RET(zeroFields(c, *aLeft));
         E3D_RET(launchStep(c, STEP_ADJ_EXACT, p));
-        E3D_RET(launchInject(c, p, recSet, resid, its, it2 + 1));
+        E3D_RET(launchInjectSlices(c, p, recSet, dataSlice(its), dataSlice(its + 1), it2 + 1));
         if (dual) E3D_RET(launchRefresh(c, p, recSet));
         swapF(c->w0, c->w1);
         if (dual) swapF(c->q0, c->q1);
@@ -1212,8 +1391,8 @@ static int adjointPassFromCheckpoints(Context* c, const DevSignals& srcSet, cons
 
 static int bornAdjointDevice(Context* c, const DevSignals& srcSet, const DevSignals& recSet, const float* srcSig,
                              const float* resid) {
-  E3D_RET(sourcePassWithCheckpoints(c, srcSet, nullptr, srcSig, nullptr));
-  return adjointPassFromCheckpoints(c, srcSet, recSet, srcSig, resid);
+  E3D_RET(sourcePassWithCheckpoints(c, srcSet, nullptr, srcSig, nullptr, nullptr));
+  return adjointPassFromCheckpoints(c, srcSet, recSet, srcSig, resid, nullptr);
 }
 
 int bornForwardHost(Context* c, const float* const* srcSig, float* const* data, const HostGeom& src,
@@ -1278,14 +1457,15 @@ int bornAdjointHost(Context* c, const float* const* srcSig, const float* const* 
 // FWI (device API)
 // ---------------------------------------------------------------------------
 int fwiForwardDevice(Context* c, const DevSignals& srcSet, const DevSignals& recSet, const float* srcSig,
-                     float* recSig) {
+                     float* recSig, const TraceMap* map) {
   E3D_ARG(c && c->haveMedium, "medium not set");
+  E3D_ARG(c->d.nts >= 2, "FWI needs at least two coarse samples");
   E3D_CUDA_TRY(cudaSetDevice(c->d.device));
-  return sourcePassWithCheckpoints(c, srcSet, &recSet, srcSig, recSig);
+  return sourcePassWithCheckpoints(c, srcSet, &recSet, srcSig, recSig, map);
 }
 
 int fwiGradientDevice(Context* c, const DevSignals& srcSet, const DevSignals& recSet, const float* srcSig,
-                      const float* residual, float* const* pert8) {
+                      const float* residual, float* const* pert8, const TraceMap* map) {
   E3D_ARG(c && c->haveMedium, "medium not set");
   E3D_ARG(pert8 != nullptr, "null gradient planes");
   E3D_CUDA_TRY(cudaSetDevice(c->d.device));
@@ -1293,9 +1473,18 @@ int fwiGradientDevice(Context* c, const DevSignals& srcSet, const DevSignals& re
     E3D_ARG(pert8[k] != nullptr, "null gradient plane");
     c->pertDev[k] = pert8[k];  // accumulate straight into the caller's planes
   }
-  int st = adjointPassFromCheckpoints(c, srcSet, recSet, srcSig, residual);
+  int st = adjointPassFromCheckpoints(c, srcSet, recSet, srcSig, residual, map);
   for (int k = 0; k < NMED; k++) c->pertDev[k] = nullptr;
   return st;
 }
+
+int setVelocityStorage(Context* c, int type) {
+  E3D_ARG(c && type >= -1 && type <= 1, "bad velocity slot storage type");
+  c->vType = type;
+  c->ckptValid = false;
+  return E3D_OK;
+}
+
+int velocityStorage(const Context* c) { return c->vUsed; }
 
 }  // namespace e3d

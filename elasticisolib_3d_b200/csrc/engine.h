@@ -67,12 +67,32 @@ struct DevSignals {
 };
 int nlPropagateDevice(Context* c, bool adjoint, const DevSignals& srcSet, const DevSignals& recSet,
                       float* srcSig, float* recSig);
+// Irregular receivers as linear combinations of the regular acquisition
+// points (device arrays).  Receiver row r = k*nIrreg + i (component k).
+//   gather (regular -> irregular): irr[r] = sum_f weight[r*nTaps+f] * reg[slot[r*nTaps+f]]
+//   spread (irregular -> regular): reg[j] = sum_{e in [rowPtr[j], rowPtr[j+1])} w[e] * irr[idx[e]]
+// slot and j index the concatenated regular list of the receiver DevSignals.
+struct TraceMap {
+  int nIrreg = 0;
+  int nTaps = 0;
+  const int* slot = nullptr;
+  const float* weight = nullptr;
+  const int* rowPtr = nullptr;
+  const int* idx = nullptr;
+  const float* w = nullptr;
+};
 // FWI: nonlinear forward that saves wavefield checkpoints for a later
 // gradient; the gradient call consumes them (Born adjoint of the residual).
+// Without a trace map recSig/residual are regular-grid and time-major
+// ([nts][recSet.off[9]]); with one they are irregular and time-major
+// ([nts][9*nIrreg]) and no regular-grid trace array is ever allocated.
 int fwiForwardDevice(Context* c, const DevSignals& srcSet, const DevSignals& recSet, const float* srcSig,
-                     float* recSig);
+                     float* recSig, const TraceMap* map);
 int fwiGradientDevice(Context* c, const DevSignals& srcSet, const DevSignals& recSet, const float* srcSig,
-                      const float* residual, float* const* pert8);
+                      const float* residual, float* const* pert8, const TraceMap* map);
+// Source velocity slot storage of the checkpoint plan: -1 auto, 0 FP32, 1 FP16 per-slice scaled.
+int setVelocityStorage(Context* c, int type);
+int velocityStorage(const Context* c);
 
 // Timing/inspection helpers
 int stepOnly(Context* c, int mode, int nSteps);  // run nSteps bare steps on the working state

@@ -318,7 +318,7 @@ __device__ __forceinline__ void issuePlane(const StepPtrs& p, const GridConst& g
 template <int MODE, int TX, int STAGES>
 __global__ void __launch_bounds__(TZ * TX) kStepPipe(StepPtrs p, GridConst g, int yChunk) {
   using L = PipeLayout<TX>;
-  extern __shared__ __align__(16) float smem[];
+  extern __shared__ __align__(1024) float smem[];
   const int tz = threadIdx.x, tx = threadIdx.y;
   const int tid = tx * TZ + tz;
   const int z0 = FAT + blockIdx.x * TZ, x0 = FAT + blockIdx.y * TX;
@@ -869,7 +869,8 @@ __global__ void __launch_bounds__(TZ * TX, MINB) kStepTma2(const __grid_constant
 // field[pos] += G(pos) * (sig[its]*wl + sig[its+1]*wr)
 // (ker_inject_source_* / ker_inject_data_*, kernelsElaGpu_3D.cu:11-52; the
 // source enters before the sponge, hence the taper at the point.)
-__global__ void kInject(StepPtrs p, GridConst g, SparseSet s, const float* sig, int its, float wl, float wr) {
+__global__ void kInject(StepPtrs p, GridConst g, SparseSet s, const float* sigL, const float* sigR, float wl,
+                        float wr) {
   const int ntot = s.off[NCOMP];
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= ntot) return;
@@ -877,7 +878,7 @@ __global__ void kInject(StepPtrs p, GridConst g, SparseSet s, const float* sig, 
 #pragma unroll
   for (int c = 1; c < NCOMP; c++) k += (j >= s.off[c]);
   const long long pos = s.pos[j];
-  const float v = sig[(long long)its * ntot + j] * wl + sig[(long long)(its + 1) * ntot + j] * wr;
+  const float v = sigL[j] * wl + sigR[j] * wr;
   const int iz = (int)(pos % g.nz);
   const int ix = (int)((pos / g.nz) % g.nx);
   const int iy = (int)(pos / g.yStride);
@@ -890,9 +891,9 @@ __global__ void kInject(StepPtrs p, GridConst g, SparseSet s, const float* sig, 
   }
 }
 
-// out[its] += field[pos]*wl; out[its+1] += field[pos]*wr
-// (ker_record_*, kernelsElaGpu_3D.cu:61-104)
-__global__ void kRecord(StepPtrs p, SparseSet s, float* out, int its, float wl, float wr) {
+// outL[j] += field[pos]*wl; outR[j] += field[pos]*wr, with outL/outR the
+// time slices its and its+1 (ker_record_*, kernelsElaGpu_3D.cu:61-104)
+__global__ void kRecord(StepPtrs p, SparseSet s, float* outL, float* outR, float wl, float wr) {
   const int ntot = s.off[NCOMP];
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= ntot) return;
@@ -900,8 +901,45 @@ __global__ void kRecord(StepPtrs p, SparseSet s, float* out, int its, float wl, 
 #pragma unroll
   for (int c = 1; c < NCOMP; c++) k += (j >= s.off[c]);
   const float v = p.o[k][s.pos[j]];
-  out[(long long)its * ntot + j] += v * wl;
-  out[(long long)(its + 1) * ntot + j] += v * wr;
+  outL[j] += v * wl;
+  outR[j] += v * wr;
+}
+
+// ---------------------------------------------------------------------------
+// Receiver traces between the regular acquisition points and the irregular
+// receivers, one coarse time slice at a time (spaceInterpGpu_3D::forward /
+// ::adjoint, spaceInterpGpu_3D.cpp:140-175).
+// Gather: irr[r] = sum_f w[r*nf+f] * reg[slot[r*nf+f]], f ascending from 0,
+//   r = k*nIrreg + i over the nine components.
+// Spread: reg[j] = sum over the entries e of row j (ordered by receiver, then
+//   tap) of w[e] * irr[idx[e]] -- the accumulation order of the reference's
+//   device loop, without atomics.
+// Table entries outside the slice (a slot >= nReg, a receiver row >= nRows)
+// contribute nothing.
+// ---------------------------------------------------------------------------
+__global__ void kTraceGather(const float* __restrict__ reg, float* __restrict__ irr, int nRows, int nf,
+                             const int* __restrict__ slot, const float* __restrict__ w, int nReg) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= nRows) return;
+  float acc = 0.f;
+  for (int f = 0; f < nf; f++) {
+    const int j = __ldg(slot + (long long)r * nf + f);
+    if ((unsigned)j < (unsigned)nReg) acc += __ldg(w + (long long)r * nf + f) * __ldg(reg + j);
+  }
+  irr[r] = acc;
+}
+
+__global__ void kTraceSpread(const float* __restrict__ irr, float* __restrict__ reg, int nReg,
+                             const int* __restrict__ rowPtr, const int* __restrict__ idx,
+                             const float* __restrict__ w, int nRows) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= nReg) return;
+  float acc = 0.f;
+  for (int e = __ldg(rowPtr + j); e < __ldg(rowPtr + j + 1); e++) {
+    const int r = __ldg(idx + e);
+    if ((unsigned)r < (unsigned)nRows) acc += __ldg(w + e) * __ldg(irr + r);
+  }
+  reg[j] = acc;
 }
 
 // ---------------------------------------------------------------------------

@@ -154,14 +154,36 @@ class Propagator:
         N.call("e3d_nl_propagate_device", self._h, int(adjoint), src_pos.data_ptr(), so, rec_pos.data_ptr(), ro,
                src_sig.data_ptr(), rec_sig.data_ptr())
 
-    def fwi_forward_device(self, src_pos, src_off, rec_pos, rec_off, src_sig, rec_sig):
-        so = (ctypes.c_int * 10)(*[int(v) for v in src_off])
-        ro = (ctypes.c_int * 10)(*[int(v) for v in rec_off])
-        N.call("e3d_fwi_forward_device", self._h, src_pos.data_ptr(), so, rec_pos.data_ptr(), ro,
-               src_sig.data_ptr(), rec_sig.data_ptr())
+    @staticmethod
+    def _trace_map(tmap):
+        """ctypes reference to an E3DTraceMap built from a TraceTables-like object (or None)."""
+        if tmap is None:
+            return None
+        m = N.E3DTraceMap(int(tmap.n_irreg), int(tmap.n_taps), tmap.slot.data_ptr(), tmap.weight.data_ptr(),
+                          tmap.row_ptr.data_ptr(), tmap.idx.data_ptr(), tmap.w.data_ptr())
+        return ctypes.byref(m), m
 
-    def fwi_gradient_device(self, src_pos, src_off, rec_pos, rec_off, src_sig, residual, grad8):
+    def fwi_forward_device(self, src_pos, src_off, rec_pos, rec_off, src_sig, rec_sig, tmap=None):
+        """Checkpointed nonlinear forward.  rec_sig: regular time-major (nts, rec_off[9]) without a
+        trace map, irregular time-major (nts, 9*n_irreg) with one."""
         so = (ctypes.c_int * 10)(*[int(v) for v in src_off])
         ro = (ctypes.c_int * 10)(*[int(v) for v in rec_off])
+        ref = self._trace_map(tmap)
+        N.call("e3d_fwi_forward_device", self._h, src_pos.data_ptr(), so, rec_pos.data_ptr(), ro,
+               src_sig.data_ptr(), rec_sig.data_ptr(), ref[0] if ref else None)
+
+    def fwi_gradient_device(self, src_pos, src_off, rec_pos, rec_off, src_sig, residual, grad8, tmap=None):
+        so = (ctypes.c_int * 10)(*[int(v) for v in src_off])
+        ro = (ctypes.c_int * 10)(*[int(v) for v in rec_off])
+        ref = self._trace_map(tmap)
         N.call("e3d_fwi_gradient_device", self._h, src_pos.data_ptr(), so, rec_pos.data_ptr(), ro,
-               src_sig.data_ptr(), residual.data_ptr(), N.ptr_array([grad8[k] for k in range(8)]))
+               src_sig.data_ptr(), residual.data_ptr(), N.ptr_array([grad8[k] for k in range(8)]),
+               ref[0] if ref else None)
+
+    def set_velocity_storage(self, kind="auto"):
+        """Source velocity slots of the checkpoint plan: "auto", "fp32" or "fp16"."""
+        N.call("e3d_set_velocity_storage", self._h, {"auto": -1, "fp32": 0, "fp16": 1}[kind])
+
+    @property
+    def velocity_storage(self):
+        return ("fp32", "fp16")[int(N.lib().e3d_velocity_storage(self._h))]

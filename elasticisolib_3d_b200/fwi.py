@@ -165,16 +165,71 @@ def scale_sources(sig_reg, src: DeviceSet, planes, dx, dy, dz):
 
 
 @dataclass
+class TraceTables:
+    """Device tables of the engine's trace map (e3d_trace_map): the nine components'
+    irregular receivers as linear combinations of the regular receiver points.
+    Receiver row r = k*n_irreg + i; irregular traces are time-major (nts, 9*n_irreg)."""
+    n_irreg: int
+    n_taps: int
+    slot: torch.Tensor       # (9*n_irreg*n_taps,) int32, index into the concatenated regular list
+    weight: torch.Tensor     # (9*n_irreg*n_taps,) float32
+    row_ptr: torch.Tensor    # (n_reg+1,) int32, spread rows
+    idx: torch.Tensor        # (nnz,) int32, receiver row of each spread entry
+    w: torch.Tensor          # (nnz,) float32
+
+    @staticmethod
+    def from_set(rec: DeviceSet, device):
+        """Gather rows follow spaceInterpGpu_3D::forward (device, then tap); each spread row lists
+        its entries in the order spaceInterpGpu_3D::adjoint accumulates them (device, then tap),
+        spaceInterpGpu_3D.cpp:140-175."""
+        n_irreg = rec.n_irreg
+        slots, wts = [], []
+        for k in range(9):
+            g = COMP_GRID[k]
+            slots.append(rec.slot[g].cpu().numpy().astype(np.int64) + rec.off[k])
+            wts.append(rec.weight[g].cpu().numpy().astype(np.float32))
+        slot = np.concatenate(slots).reshape(-1) if n_irreg else np.zeros(0, np.int64)
+        weight = np.concatenate(wts).reshape(-1) if n_irreg else np.zeros(0, np.float32)
+        n_taps = slot.size // (9 * n_irreg) if n_irreg else 8
+        n_reg = rec.off[9]
+        assert slot.size == 0 or (slot.min() >= 0 and slot.max() < n_reg)
+        rows = np.repeat(np.arange(9 * n_irreg, dtype=np.int64), n_taps)
+        order = np.argsort(slot, kind="stable")
+        row_ptr = np.zeros(n_reg + 1, dtype=np.int64)
+        np.cumsum(np.bincount(slot, minlength=n_reg), out=row_ptr[1:])
+        assert row_ptr[-1] < 2 ** 31
+
+        def dev(a, dt):
+            return torch.from_numpy(np.ascontiguousarray(a).astype(dt)).to(device)
+
+        return TraceTables(n_irreg, n_taps, dev(slot, np.int32), dev(weight, np.float32), dev(row_ptr, np.int32),
+                           dev(rows[order], np.int32), dev(weight[order], np.float32))
+
+
+def time_major(d9):
+    """(9, nIrreg, nts) irregular traces -> time-major (nts, 9*nIrreg)."""
+    d9 = torch.as_tensor(d9)
+    return d9.permute(2, 0, 1).reshape(d9.shape[2], -1).contiguous()
+
+
+def component_major(dt, n_irreg):
+    """Time-major (nts, 9*nIrreg) -> (9, nIrreg, nts)."""
+    return dt.reshape(dt.shape[0], 9, n_irreg).permute(1, 2, 0).contiguous()
+
+
+@dataclass
 class Shot:
     src: DeviceSet
     rec: DeviceSet
     sig_reg: torch.Tensor      # (nts, ntot_src) unscaled regular-grid source signals
-    d_obs: torch.Tensor        # (9, nRec, nts) observed data (irregular receivers)
+    d_obs: torch.Tensor        # (nts, 9*nRec) observed data at the irregular receivers, time-major
+    tables: TraceTables = None
 
 
 def make_shot(src_devices7, rec_devices7, model_irreg9, d_obs, device, q2compat=True):
     """Spread the irregular source signals to the regular grid (spaceInterpGpu_3D::adjoint) and
-    move everything to the device.  model_irreg9: list of 9 (nIrregSrc, nts) arrays."""
+    move everything to the device.  model_irreg9: list of 9 (nIrregSrc, nts) arrays; d_obs:
+    (9, nRec, nts) observed traces or None."""
     src = DeviceSet.from_devices(src_devices7, device)
     rec = DeviceSet.from_devices(rec_devices7, device, q2_receivers=q2compat)
     nts = model_irreg9[0].shape[1]
@@ -184,14 +239,25 @@ def make_shot(src_devices7, rec_devices7, model_irreg9, d_obs, device, q2compat=
         blocks.append(src_devices7[g].adjoint(False, None, np.asarray(model_irreg9[k], dtype=np.float32)))
     sig = torch.from_numpy(np.ascontiguousarray(np.concatenate(blocks, axis=0).T)).to(device)
     assert sig.shape == (nts, src.off[9])
-    d_obs = torch.as_tensor(np.asarray(d_obs, dtype=np.float32)).to(device) if d_obs is not None else None
-    return Shot(src, rec, sig, d_obs)
+    if d_obs is not None:
+        d_obs = time_major(torch.as_tensor(np.asarray(d_obs, dtype=np.float32)).to(device))
+    return Shot(src, rec, sig, d_obs, TraceTables.from_set(rec, device))
+
+
+def _half_sum_sq(x, rows_per_chunk=64):
+    """0.5*sum(x^2) accumulated in float64 over chunks of time samples (bounded temporaries)."""
+    tot = torch.zeros((), dtype=torch.float64, device=x.device)
+    for i in range(0, x.shape[0], rows_per_chunk):
+        c = x[i:i + rows_per_chunk]
+        tot += torch.sum(c * c, dtype=torch.float64)
+    return 0.5 * tot
 
 
 class FwiProblem:
     """One propagation grid, its context and shots; shared by forward modelling and gradients."""
 
-    def __init__(self, fd: H.FdParam, device="cuda", ckpt="auto", segment=0, variant=(8, 2, "tma")):
+    def __init__(self, fd: H.FdParam, device="cuda", ckpt="auto", segment=0, variant=(8, 2, "tma"),
+                 velocity="auto"):
         self.fd = fd
         self.device = torch.device(device)
         self.prop = Propagator(fd.nz, fd.nx, fd.ny, fd.nts, fd.sub, fd.minPad, float(fd.dz), float(fd.dx),
@@ -199,6 +265,7 @@ class FwiProblem:
                                device=self.device.index or 0)
         self.prop.set_stepper_variant(*variant)
         self.prop.set_checkpoint_policy(ckpt, segment)
+        self.prop.set_velocity_storage(velocity)
         self.ckpt, self.segment = ckpt, segment
         self.auto_budget = segment == 0
         self.shots = []
@@ -212,34 +279,37 @@ class FwiProblem:
         self.prop.set_medium(planes)
         return planes
 
-    def forward_data(self, shot: Shot, planes, save_checkpoints=False):
-        """Regular-grid predicted data (nts, ntot_rec) of one shot."""
+    def forward_data(self, shot: Shot, planes):
+        """Checkpointed nonlinear forward of one shot: predicted irregular traces, time-major
+        (nts, 9*nRec), and the scaled regular-grid source signals."""
         fd = self.fd
         sig = scale_sources(shot.sig_reg, shot.src, planes, fd.dx, fd.dy, fd.dz).contiguous()
-        rec = torch.zeros((fd.nts, shot.rec.off[9]), dtype=torch.float32, device=self.device)
+        d_pred = torch.empty((fd.nts, 9 * shot.rec.n_irreg), dtype=torch.float32, device=self.device)
         self._bind_stream()
-        if save_checkpoints and self.auto_budget:
-            # leave room for what the gradient step allocates after the forward:
-            # irregular prediction and residual, regular residual, gradient planes
+        if self.auto_budget:
+            # leave room for what the gradient step allocates after the forward: gradient planes
+            # and the model post-processing temporaries
             n = planes[0].numel()
-            reserve = (rec.numel() + 2 * shot.d_obs.numel() + 24 * n) * 4 + (2 << 30)
-            self.prop.set_checkpoint_policy(self.ckpt, self.segment, -float(reserve))
-        if save_checkpoints:
-            self.prop.fwi_forward_device(shot.src.pos, shot.src.off, shot.rec.pos, shot.rec.off, sig, rec)
-        else:
-            self.prop.nl_propagate_device(False, shot.src.pos, shot.src.off, shot.rec.pos, shot.rec.off, sig, rec)
-        return rec, sig
+            torch.cuda.empty_cache()
+            self.prop.set_checkpoint_policy(self.ckpt, self.segment, -float(24 * n * 4 + (2 << 30)))
+        self.prop.fwi_forward_device(shot.src.pos, shot.src.off, shot.rec.pos, shot.rec.off, sig, d_pred,
+                                     shot.tables)
+        return d_pred, sig
+
+    def predict(self, shot: Shot, planes):
+        """Predicted data (9, nRec, nts) of one shot."""
+        d_pred, _ = self.forward_data(shot, planes)
+        return component_major(d_pred, shot.rec.n_irreg)
 
     def shot_misfit_and_gradient(self, shot: Shot, planes):
         """0.5*||d_pred - d_obs||^2 of one shot and its Born-adjoint gradient planes (8, ny, nx, nz)."""
-        rec, sig = self.forward_data(shot, planes, save_checkpoints=True)
-        d_pred = shot.rec.to_irregular(rec)
-        res = d_pred - shot.d_obs
-        loss = 0.5 * torch.sum(res * res, dtype=torch.float64)
-        res_reg = shot.rec.to_regular(res).contiguous()
+        res, sig = self.forward_data(shot, planes)
+        res.sub_(shot.d_obs)  # the residual overwrites the prediction
+        loss = _half_sum_sq(res)
         grad8 = torch.zeros_like(planes)
         self._bind_stream()
-        self.prop.fwi_gradient_device(shot.src.pos, shot.src.off, shot.rec.pos, shot.rec.off, sig, res_reg, grad8)
+        self.prop.fwi_gradient_device(shot.src.pos, shot.src.off, shot.rec.pos, shot.rec.off, sig, res, grad8,
+                                      shot.tables)
         return loss, grad8
 
 

@@ -219,8 +219,10 @@ int e3d_set_medium(e3d_context* ctx, const float* const* planes8, int on_device)
  * pipeline depth (2 or 3 stages) and plane loader (0 plain loads, 1 cp.async,
  * 2 TMA bulk tensor copies; 1 and 2 need nz % 4 == 0). */
 int e3d_set_stepper_variant(e3d_context* ctx, int tx, int stages, int loader);
-/* Checkpoint storage: type -1 = fp32 when it fits else fp16 (default), 0 = fp32,
- * 1 = fp16, 2 = bf16 (16-bit types carry one scale per y-slice and field);
+/* Checkpoint storage: type -1 = the first plan that fits among fp32 states with
+ * fp32 velocity slots, fp16 states with fp32 slots, fp16 states with fp16 slots
+ * (default); 0 = fp32, 1 = fp16, 2 = bf16 (16-bit types carry one scale per
+ * y-slice and field);
  * segment = coarse blocks per segment (0 = largest that fits);
  * budget_bytes > 0: device bytes for checkpoints and velocity slots; 0: 85% of the
  * free memory; < 0: 85% of the free memory minus |budget_bytes| kept for the caller. */
@@ -238,6 +240,12 @@ int e3d_set_stream(e3d_context* ctx, void* stream, int use_own);
 long long e3d_cells_per_step(const e3d_context* ctx);
 /* Coarse blocks per checkpoint segment chosen by the last checkpointed forward (0 before). */
 int e3d_checkpoint_segment(const e3d_context* ctx);
+/* Storage of the decimated source velocity kept per segment for the imaging
+ * condition: -1 = fp32 when the plan fits else fp16 (default), 0 = fp32,
+ * 1 = fp16 with one scale per y-slice and field. */
+int e3d_set_velocity_storage(e3d_context* ctx, int type);
+/* Velocity slot storage of the current plan (0 fp32, 1 fp16). */
+int e3d_velocity_storage(const e3d_context* ctx);
 
 /* Host-buffer propagations.  src_pos/rec_pos: 7 tables; n_src/n_rec: 7 counts. */
 int e3d_nl_forward(e3d_context* ctx, const float* const* model9, float* const* data9,
@@ -260,15 +268,36 @@ int e3d_born_adjoint(e3d_context* ctx, const float* const* src9, const float* co
 int e3d_nl_propagate_device(e3d_context* ctx, int adjoint, const long long* src_pos_dev, const int* src_off10,
                             const long long* rec_pos_dev, const int* rec_off10, float* src_sig_dev,
                             float* rec_sig_dev);
-/* FWI: nonlinear forward that also saves on-device wavefield checkpoints. */
+/* Irregular receivers as linear combinations of the regular receiver points
+ * (spaceInterpGpu_3D::forward/adjoint, spaceInterpGpu_3D.cpp:140-175), all
+ * arrays on the device.  Receiver row r = k*n_irreg + i for component k.
+ *   regular -> irregular: irr[r] = sum_{f<n_taps} weight[r*n_taps+f] * reg[slot[r*n_taps+f]]
+ *   irregular -> regular: reg[j] = sum_{row_ptr[j] <= e < row_ptr[j+1]} w[e] * irr[idx[e]]
+ * slot and j index the concatenated regular receiver list (rec_pos_dev);
+ * entries outside the lists contribute nothing. */
+typedef struct e3d_trace_map {
+  int n_irreg;
+  int n_taps;
+  const int* slot;
+  const float* weight;
+  const int* row_ptr;
+  const int* idx;
+  const float* w;
+} e3d_trace_map;
+
+/* FWI: nonlinear forward that also saves on-device wavefield checkpoints.
+ * map == NULL: rec_sig_dev is regular-grid, time-major [nts][rec_off10[9]].
+ * map != NULL: rec_sig_dev is irregular, time-major [nts][9*n_irreg]; the
+ * regular traces only exist as a two-slice ring on the device. */
 int e3d_fwi_forward_device(e3d_context* ctx, const long long* src_pos_dev, const int* src_off10,
                            const long long* rec_pos_dev, const int* rec_off10, const float* src_sig_dev,
-                           float* rec_sig_dev);
+                           float* rec_sig_dev, const e3d_trace_map* map);
 /* FWI: Born adjoint of the residual, accumulated into eight device planes;
- * consumes the checkpoints of the preceding e3d_fwi_forward_device. */
+ * consumes the checkpoints of the preceding e3d_fwi_forward_device.  The
+ * residual has the layout of rec_sig_dev above for the same map. */
 int e3d_fwi_gradient_device(e3d_context* ctx, const long long* src_pos_dev, const int* src_off10,
                             const long long* rec_pos_dev, const int* rec_off10, const float* src_sig_dev,
-                            const float* residual_dev, float* const* grad8_dev);
+                            const float* residual_dev, float* const* grad8_dev, const e3d_trace_map* map);
 
 /* Sampled stepper timing for roofline reporting: every n-th stepper launch is
  * bracketed by CUDA events on the launching stream (n = 0 switches it off). */

@@ -11,30 +11,53 @@ from elasticisolib_3d_b200 import hostprep as H
 pytestmark = pytest.mark.gpu
 
 
-def _problem(sv, ckpt="fp32", segment=0, variant=(8, 2, "tma")):
+def _problem(sv, ckpt="fp32", segment=0, variant=(8, 2, "tma"), velocity="auto"):
     fd = H.FdParam(sv.elastic, sv.axes, sv.par)
-    prob = F.FwiProblem(fd, ckpt=ckpt, segment=segment, variant=variant)
+    prob = F.FwiProblem(fd, ckpt=ckpt, segment=segment, variant=variant, velocity=velocity)
     ax7 = H.grid_axes(*(a.n for a in sv.axes), *(a.o for a in sv.axes), *(a.d for a in sv.axes))
     src = H.build_devices(*sv.src_xyz[0], ax7, fd.nts, sv.par)
     rec = H.build_devices(*sv.rec_xyz, ax7, fd.nts, sv.par)
     return prob, src, rec
 
 
-@pytest.mark.parametrize("ckpt,segment,variant", [("fp32", 0, (8, 2, "tma")), ("fp32", 3, (8, 2, "plain")),
-                                                   ("fp16", 4, (8, 2, "tma"))])
-def test_fwi_gradient_matches_fp64_oracle(ckpt, segment, variant):
+# BF16 states (8-bit mantissa) measured 1.26e-3 on this case, above the 1e-3 bound that the
+# FP32 and FP16 plans meet; they are checked against 3e-3.
+@pytest.mark.parametrize("ckpt,segment,variant,velocity,tol", [
+    ("fp32", 0, (8, 2, "tma"), "auto", 1e-3),
+    ("fp32", 3, (8, 2, "plain"), "fp32", 1e-3),
+    ("fp16", 4, (8, 2, "tma"), "auto", 1e-3),
+    ("fp16", 5, (8, 2, "tma"), "fp16", 1e-3),
+    ("fp32", 1, (8, 2, "tma"), "fp16", 1e-3),
+    ("bf16", 4, (8, 2, "tma"), "fp16", 3e-3),
+])
+def test_fwi_gradient_matches_fp64_oracle(ckpt, segment, variant, velocity, tol):
     sv, true = survey()
     orc = OracleFwi(sv)
     d_obs, _ = orc.data(true)
     loss_ref, g_ref = orc.misfit_and_gradient(sv.elastic, d_obs)
-    prob, src, rec = _problem(sv, ckpt, segment, variant)
+    prob, src, rec = _problem(sv, ckpt, segment, variant, velocity)
     prob.shots.append(F.make_shot(src, rec, explosive(sv.par.getInt("nts"), sv.wavelet), d_obs.astype(np.float32),
                                   "cuda"))
     m = [torch.tensor(sv.elastic[k], device="cuda", requires_grad=True) for k in range(3)]
     loss = F.ElasticFwiMisfit.apply(m[0], m[1], m[2], prob)
     loss.backward()
+    if velocity != "auto":
+        assert prob.prop.velocity_storage == velocity
     g = np.stack([x.grad.double().cpu().numpy() for x in m])
     assert abs(loss.item() - loss_ref) / loss_ref < 1e-4
     for k in range(3):
         err = np.linalg.norm(g[k] - g_ref[k]) / np.linalg.norm(g_ref[k])
-        assert err < 1e-3, (k, err)
+        assert err < tol, (k, err)
+
+
+def test_predicted_traces_match_fp64_oracle():
+    """Irregular traces from the on-device slice ring + gather (no regular trace array)."""
+    sv, true = survey()
+    orc = OracleFwi(sv)
+    d_ref, _ = orc.data(true)
+    prob, src, rec = _problem(sv)
+    shot = F.make_shot(src, rec, explosive(sv.par.getInt("nts"), sv.wavelet), None, "cuda")
+    planes = prob.set_model(*[torch.tensor(true[k], device="cuda") for k in range(3)])
+    d = prob.predict(shot, planes).double().cpu().numpy()
+    assert d.shape == d_ref.shape
+    assert np.linalg.norm(d - d_ref) / np.linalg.norm(d_ref) < 1e-5
