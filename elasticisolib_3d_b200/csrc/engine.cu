@@ -1092,7 +1092,7 @@ static int packVelocity(Context* c, const float* v, void* store) {
     c->launches += 2;
     kSliceMaxAbs<<<ny, 256, 0, c->st>>>(v + (size_t)k * n, ys, smax);
     E3D_LAUNCH_CHECK();
-    kPackSlices<__half><<<blocks, 256, 0, c->st>>>(v + (size_t)k * n, ys, n, smax, 16384.f, h + (size_t)k * n,
+    kPackSlices<__half><<<blocks, 256, 0, c->st>>>(v + (size_t)k * n, ys, n, smax, 14, h + (size_t)k * n,
                                                    scales + (size_t)k * ny);
     E3D_LAUNCH_CHECK();
   }
@@ -1136,10 +1136,10 @@ static int packState(Context* c, int seg) {
       E3D_LAUNCH_CHECK();
       const unsigned blocks = (unsigned)((n + 255) / 256);
       if (c->ckptUsed == CKPT_F16)
-        kPackSlices<__half><<<blocks, 256, 0, c->st>>>(parts[h]->p[k], ys, n, smax, 16384.f,
+        kPackSlices<__half><<<blocks, 256, 0, c->st>>>(parts[h]->p[k], ys, n, smax, 14,
                                                        (__half*)c->ckpt[seg] + (size_t)f * n, scales + (size_t)f * ny);
       else
-        kPackSlices<__nv_bfloat16><<<blocks, 256, 0, c->st>>>(parts[h]->p[k], ys, n, smax, 1.f,
+        kPackSlices<__nv_bfloat16><<<blocks, 256, 0, c->st>>>(parts[h]->p[k], ys, n, smax, 0,
                                                               (__nv_bfloat16*)c->ckpt[seg] + (size_t)f * n,
                                                               scales + (size_t)f * ny);
       E3D_LAUNCH_CHECK();

@@ -546,6 +546,26 @@ __global__ void __launch_bounds__(TZ * TX) kStepTma(const __grid_constant__ TmaM
     }
     const float* st = smem + slot * L::STAGE_F;
     if (active) {
+      // Secondary sources or decimation accumulators of this cell, loaded before any
+      // store of the step, so that they are issued together instead of one at a
+      // time behind stores that the compiler cannot move them across.
+      const long long ic = (long long)y * ys + col;
+      const bool hasSS = p.ssL[0] != nullptr;
+      const bool hasAcc = p.accL[0] != nullptr;
+      const bool hasR = hasSS || p.accR[0] != nullptr;
+      float preL[NCOMP], preR[NCOMP];
+#pragma unroll
+      for (int k = 0; k < NCOMP; k++) {
+        preL[k] = 0.f;
+        preR[k] = 0.f;
+        if (hasSS) {
+          preL[k] = __ldg(p.ssL[k] + ic);
+          preR[k] = __ldg(p.ssR[k] + ic);
+        } else if (hasAcc && k < p.nAcc) {
+          preL[k] = p.accL[k][ic];
+          if (hasR) preR[k] = p.accR[k][ic];
+        }
+      }
 #pragma unroll
       for (int q = 0; q < NQUEUE; q++) w[q][7] = st[L::LEAD_OFF + q * L::INT_F + li];
       const float* tl[NTILE];
@@ -588,20 +608,20 @@ __global__ void __launch_bounds__(TZ * TX) kStepTma(const __grid_constant__ TmaM
       }
       const int d = min(dzx, min(y - FAT, g.ny - y - 1 - FAT));
       const float G = d < g.minPad ? __ldg(g.taper + d) : 1.0f;
-      const long long ic = (long long)y * ys + col;
-      const bool hasSS = p.ssL[0] != nullptr;
-      const bool hasAcc = p.accL[0] != nullptr;
       float nv[NCOMP];
 #pragma unroll
       for (int k = 0; k < NCOMP; k++) {
         float v = G * ov[k * L::INT_F] + up[k];
-        if (hasSS) v += __ldg(p.ssL[k] + ic) * p.ssWl + __ldg(p.ssR[k] + ic) * p.ssWr;
+        if (hasSS) v += preL[k] * p.ssWl + preR[k] * p.ssWr;
         v *= G;
         nv[k] = v;
-        p.o[k][ic] = v;
+      }
+#pragma unroll
+      for (int k = 0; k < NCOMP; k++) {
+        p.o[k][ic] = nv[k];
         if (hasAcc && k < p.nAcc) {
-          p.accL[k][ic] += v * p.accWl;
-          if (p.accR[0] != nullptr) p.accR[k][ic] += v * p.accWr;
+          p.accL[k][ic] = preL[k] + nv[k] * p.accWl;
+          if (hasR) p.accR[k][ic] = preR[k] + nv[k] * p.accWr;
         }
       }
       if (MODE == STEP_ADJ_EXACT) {
@@ -1036,15 +1056,26 @@ __global__ void kSliceMaxAbs(const float* a, long long ys, float* out) {
   }
 }
 
+// Per-slice scaling by a power of two 2^sh chosen so that the slice maximum m
+// lands in [2^(topExp-1), 2^topExp): scaling and unscaling are exact, and sh is
+// clamped to +-126 so that slices whose maximum is tiny or subnormal (far from
+// the wavefront) keep finite scales.  A zero or non-finite maximum stores zeros.
 template <typename H>
-__global__ void kPackSlices(const float* a, long long ys, long long n, const float* smax, float target, H* out,
+__global__ void kPackSlices(const float* a, long long ys, long long n, const float* smax, int topExp, H* out,
                             float* scales) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const long long y = i / ys;
   const float m = smax[y];
-  const float s = m > 0.0f ? target / m : 0.0f;
-  if (i % ys == 0) scales[y] = s > 0.0f ? 1.0f / s : 0.0f;
+  float s = 0.0f, inv = 0.0f;
+  if (m > 0.0f && isfinite(m)) {
+    int e;
+    frexpf(m, &e);  // m in [2^(e-1), 2^e)
+    const int sh = max(-126, min(126, topExp - e));
+    s = ldexpf(1.0f, sh);
+    inv = ldexpf(1.0f, -sh);
+  }
+  if (i % ys == 0) scales[y] = inv;
   out[i] = H(a[i] * s);
 }
 
