@@ -417,6 +417,26 @@ int e3d_set_velocity_storage(e3d_context* ctx, int type) {
 
 int e3d_velocity_storage(const e3d_context* ctx) { return (ctx && ctx->c) ? velocityStorage(ctx->c) : -1; }
 
+int e3d_nl_propagate_device_noalloc(const e3d_desc* desc, const float* const* planes8_dev, int adjoint,
+                                    const long long* src_pos_dev, const int* src_off10,
+                                    const long long* rec_pos_dev, const int* rec_off10, float* src_sig_dev,
+                                    float* rec_sig_dev, void* stream) {
+  if (!desc) return fail(E3D_ERR_ARG, "null descriptor");
+  ContextDesc d;
+  d.device = desc->device;
+  d.nz = desc->nz; d.nx = desc->nx; d.ny = desc->ny;
+  d.nts = desc->nts; d.sub = desc->sub; d.minPad = desc->minPad;
+  d.dz = desc->dz; d.dx = desc->dx; d.dy = desc->dy; d.dts = desc->dts; d.alphaCos = desc->alphaCos;
+  d.fixQ1 = desc->fix_q1; d.q2compat = desc->q2compat; d.q3compat = desc->q3compat;
+  DevSignals S, R;
+  int st = devSet(src_pos_dev, src_off10, S);
+  if (st == E3D_OK) st = devSet(rec_pos_dev, rec_off10, R);
+  if (st != E3D_OK) return st;
+  return nlPropagateStatic(d, planes8_dev, adjoint != 0, S, R, src_sig_dev, rec_sig_dev, (cudaStream_t)stream);
+}
+
+size_t e3d_noalloc_work_bytes(void) { return staticWorkBytes(); }
+
 int e3d_kernel_timing(e3d_context* ctx, int every) {
   CTX_OR_FAIL(ctx);
   return setKernelTiming(ctx->c, every);

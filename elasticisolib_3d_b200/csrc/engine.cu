@@ -17,6 +17,7 @@
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 #include <cudaTypedefs.h>
+#include <mutex>
 #include <unordered_map>
 
 #include "engine.h"
@@ -1486,5 +1487,181 @@ int setVelocityStorage(Context* c, int type) {
 }
 
 int velocityStorage(const Context* c) { return c->vUsed; }
+
+// ---------------------------------------------------------------------------
+// Allocation-free nonlinear propagation.  Some callers cannot allocate device
+// memory while they propagate: a host framework may already hold nearly all of
+// the device's memory in its own pool, or a caller may not be allowed to make
+// cudaMalloc/cudaFree calls (which can synchronize the whole device) inside its
+// time-critical loop.  For them the two wavefield levels and the sponge taper
+// live in one fixed device array, sized for small grids; the caller passes the
+// medium planes, positions and signals as device pointers.  The array is a
+// module global, so every GPU that loads this library reserves it until the
+// process exits, and every call on a device uses the same array.
+// ---------------------------------------------------------------------------
+constexpr size_t kStaticWorkBytes = (size_t)64 << 20;  // 64 MiB: 18 fields of up to ~0.93 M cells + taper
+constexpr int kStaticMaxDevices = 64;
+static __device__ __align__(256) unsigned char g_e3dStaticWork[kStaticWorkBytes];
+static std::mutex g_staticWorkMutex;
+static void* g_staticWorkAddr[kStaticMaxDevices] = {};
+
+size_t staticWorkBytes() { return kStaticWorkBytes; }
+
+// Device address of the static work array on the current device.  The name
+// g_e3dStaticWork is a host-side stand-in in host code, so its device address
+// is looked up once per device (with that device current) and cached.
+static int staticWorkAddress(int dev, float** out) {
+  if (dev < 0 || dev >= kStaticMaxDevices) {
+    setLastError("device ordinal beyond the static work table", __FILE__, __LINE__);
+    return E3D_ERR_ARG;
+  }
+  std::lock_guard<std::mutex> lock(g_staticWorkMutex);
+  if (!g_staticWorkAddr[dev]) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_e3dStaticWork);
+    if (e != cudaSuccess || !p) {
+      setLastError(e != cudaSuccess ? cudaGetErrorString(e) : "null static work address", __FILE__, __LINE__);
+      return E3D_ERR_CUDA;
+    }
+    g_staticWorkAddr[dev] = p;
+  }
+  *out = (float*)g_staticWorkAddr[dev];
+  return E3D_OK;
+}
+
+int nlPropagateStatic(const ContextDesc& d, const float* const* planes, bool adjoint, const DevSignals& srcSet,
+                      const DevSignals& recSet, float* srcSig, float* recSig, cudaStream_t st) {
+  E3D_ARG(planes != nullptr, "null medium planes");
+  for (int k = 0; k < NMED; k++) E3D_ARG(planes[k] != nullptr, "null medium plane");
+  E3D_ARG(d.nz > 2 * FAT && d.nx > 2 * FAT && d.ny > 2 * FAT, "grid must exceed 2*FAT on every axis");
+  E3D_ARG(d.nts >= 3, "nts must be at least 3");
+  E3D_ARG(d.sub >= 1 && d.sub < SUB_MAX, "sub must be in [1, SUB_MAX)");
+  E3D_ARG(d.minPad >= 0 && d.minPad < PAD_MAX, "minPad must be in [0, PAD_MAX)");
+  E3D_ARG(d.dz > 0 && d.dx > 0 && d.dy > 0 && d.dts > 0, "sampling must be positive");
+  E3D_ARG(srcSet.off[NCOMP] == 0 || srcSig, "null source signals");
+  E3D_ARG(recSet.off[NCOMP] == 0 || recSig, "null receiver signals");
+  const long long n = (long long)d.nz * d.nx * d.ny;
+  const size_t fieldsBytes = ((size_t)2 * NCOMP * n * sizeof(float) + 255) / 256 * 256;
+  const size_t need = fieldsBytes + (size_t)PAD_MAX * sizeof(float);
+  if (n >= (1LL << 34) || need > kStaticWorkBytes) {
+    char msg[256];
+    snprintf(msg, sizeof(msg),
+             "grid of %lld cells needs %zu bytes of static work memory; the allocation-free entry point holds "
+             "%zu bytes (18 fields of at most %zu cells)",
+             n, need, kStaticWorkBytes, (kStaticWorkBytes - (size_t)PAD_MAX * sizeof(float)) / (18 * sizeof(float)));
+    setLastError(msg, __FILE__, __LINE__);
+    return E3D_ERR_ARG;
+  }
+  int dev = 0;
+  E3D_CUDA_TRY(cudaGetDevice(&dev));
+  float* work = nullptr;
+  E3D_RET(staticWorkAddress(dev, &work));
+  // grid constants as in createContext
+  GridConst g{};
+  g.nz = d.nz; g.nx = d.nx; g.ny = d.ny; g.minPad = d.minPad;
+  g.yStride = (long long)d.nz * d.nx;
+  g.n = n;
+  const double kc[4] = {1.196289062541883, -0.079752604188901, 0.009570312506634, -6.975446437140719e-04};
+  for (int i = 0; i < 4; i++) {
+    g.cz[i] = (float)(kc[i] / d.dz);
+    g.cx[i] = (float)(kc[i] / d.dx);
+    g.cy[i] = (float)(kc[i] / (d.fixQ1 ? d.dy : d.dx));
+  }
+  const int ntw = (d.nts - 1) * d.sub + 1;
+  const int hfilt = d.sub + 1;
+  std::vector<float> filt(2 * hfilt, 0.f);
+  const double scale = 1.0 / std::sqrt((float)ntw / (float)d.nts);
+  for (int i = 0; i < hfilt; i++) {
+    float left = (float)(1.0 - 1.0 * i / d.sub);
+    float right = (float)(1.0 - left);
+    filt[i] = (float)(left * scale);
+    filt[i + hfilt] = (float)(right * scale);
+  }
+  float taper[PAD_MAX];
+  for (int i = 0; i < PAD_MAX; i++) taper[i] = 1.f;
+  for (int i = 0; i < d.minPad; i++) {
+    float arg = (float)(M_PI / (1.0 * d.minPad) * 1.0 * (d.minPad - i));
+    taper[i] = (float)(d.alphaCos + (1.0 - d.alphaCos) * std::cos(arg));
+  }
+  float* taperDev = (float*)((char*)work + fieldsBytes);
+  // the array keeps the previous call's contents: both levels start at zero
+  E3D_CUDA_TRY(cudaMemcpyAsync(taperDev, taper, sizeof(taper), cudaMemcpyHostToDevice, st));
+  E3D_CUDA_TRY(cudaMemsetAsync(work, 0, (size_t)2 * NCOMP * n * sizeof(float), st));
+  g.taper = taperDev;
+  Fields9 a, b;
+  for (int k = 0; k < NCOMP; k++) {
+    a.p[k] = work + (size_t)k * n;
+    b.p[k] = work + (size_t)(NCOMP + k) * n;
+  }
+  constexpr int TXS = 8;
+  const int tiz = (g.nz - 2 * FAT + TZ - 1) / TZ;
+  const int tix = (g.nx - 2 * FAT + TXS - 1) / TXS;
+  const int nyi = g.ny - 2 * FAT;
+  const long long tiles = (long long)tiz * tix;
+  int chunks = (int)std::min<long long>((4LL * 148 + tiles - 1) / tiles, std::max(1, nyi / 32));
+  chunks = std::max(chunks, 1);
+  const int yChunk = (nyi + chunks - 1) / chunks;
+  chunks = (nyi + yChunk - 1) / yChunk;
+  const dim3 grid(tiz, tix, chunks), block(TZ, TXS);
+  auto sparse = [](const DevSignals& s) {
+    SparseSet ss;
+    ss.pos = s.pos;
+    for (int i = 0; i <= NCOMP; i++) ss.off[i] = s.off[i];
+    return ss;
+  };
+  const SparseSet S = sparse(srcSet), R = sparse(recSet);
+  const int nS = srcSet.off[NCOMP], nR = recSet.off[NCOMP];
+  const size_t ns = (size_t)nS, nr = (size_t)nR;
+  auto makeP = [&](Fields9& o, const Fields9& cur) {
+    StepPtrs p{};
+    for (int k = 0; k < NCOMP; k++) {
+      p.o[k] = o.p[k];
+      p.c[k] = cur.p[k];
+    }
+    for (int k = 0; k < NMED; k++) p.m[k] = planes[k];
+    return p;
+  };
+  const int nts = d.nts, sub = d.sub;
+  if (!adjoint) {
+    if (nR) E3D_CUDA_TRY(cudaMemsetAsync(recSig, 0, nr * nts * sizeof(float), st));
+    for (int its = 0; its < nts - 1; its++)
+      for (int it2 = 1; it2 <= sub; it2++) {
+        StepPtrs p = makeP(a, b);
+        kStep<STEP_FWD, TXS><<<grid, block, 0, st>>>(p, g, yChunk);
+        E3D_LAUNCH_CHECK();
+        if (nS) {
+          kInject<<<(nS + 127) / 128, 128, 0, st>>>(p, g, S, srcSig + its * ns, srcSig + (its + 1) * ns,
+                                                   filt[it2 - 1], filt[hfilt + it2 - 1]);
+          E3D_LAUNCH_CHECK();
+        }
+        if (nR) {
+          kRecord<<<(nR + 127) / 128, 128, 0, st>>>(p, R, recSig + its * nr, recSig + (its + 1) * nr, filt[it2],
+                                                   filt[hfilt + it2]);
+          E3D_LAUNCH_CHECK();
+        }
+        swapF(a, b);
+      }
+  } else {
+    if (nS) E3D_CUDA_TRY(cudaMemsetAsync(srcSig, 0, ns * nts * sizeof(float), st));
+    for (int its = nts - 2; its >= 0; its--)
+      for (int it2 = sub - 1; it2 >= 0; it2--) {
+        StepPtrs p = makeP(a, b);
+        kStep<STEP_ADJ_REVERSED, TXS><<<grid, block, 0, st>>>(p, g, yChunk);
+        E3D_LAUNCH_CHECK();
+        if (nR) {
+          kInject<<<(nR + 127) / 128, 128, 0, st>>>(p, g, R, recSig + its * nr, recSig + (its + 1) * nr,
+                                                   filt[it2 + 1], filt[hfilt + it2 + 1]);
+          E3D_LAUNCH_CHECK();
+        }
+        if (nS) {
+          kRecord<<<(nS + 127) / 128, 128, 0, st>>>(p, S, srcSig + its * ns, srcSig + (its + 1) * ns, filt[it2],
+                                                   filt[hfilt + it2]);
+          E3D_LAUNCH_CHECK();
+        }
+        swapF(a, b);
+      }
+  }
+  return E3D_OK;
+}
 
 }  // namespace e3d

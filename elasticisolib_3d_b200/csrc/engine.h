@@ -94,6 +94,14 @@ int fwiGradientDevice(Context* c, const DevSignals& srcSet, const DevSignals& re
 int setVelocityStorage(Context* c, int type);
 int velocityStorage(const Context* c);
 
+// Allocation-free nonlinear propagation on the current device: the wavefield
+// levels and the taper live in a fixed 64 MiB device array (staticWorkBytes());
+// planes are the eight medium planes on the device.  Calls on one device share
+// the array, so calls that overlap on the GPU race.
+int nlPropagateStatic(const ContextDesc& d, const float* const* planes, bool adjoint, const DevSignals& srcSet,
+                      const DevSignals& recSet, float* srcSig, float* recSig, cudaStream_t st);
+size_t staticWorkBytes();
+
 // Timing/inspection helpers
 int stepOnly(Context* c, int mode, int nSteps);  // run nSteps bare steps on the working state
 long long cellsPerStep(const Context* c);

@@ -26,6 +26,8 @@
 #ifndef ELASTIC3D_B200_H
 #define ELASTIC3D_B200_H
 
+#include <stddef.h>
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -298,6 +300,34 @@ int e3d_fwi_forward_device(e3d_context* ctx, const long long* src_pos_dev, const
 int e3d_fwi_gradient_device(e3d_context* ctx, const long long* src_pos_dev, const int* src_off10,
                             const long long* rec_pos_dev, const int* rec_off10, const float* src_sig_dev,
                             const float* residual_dev, float* const* grad8_dev, const e3d_trace_map* map);
+
+/* Allocation-free variant of e3d_nl_propagate_device.  It has no counterpart
+ * in the reference (whose drivers allocate and free device buffers on every
+ * call).  It serves callers that cannot allocate device memory while they
+ * propagate: a host framework that already holds most of the device's memory
+ * in its own pool, or a loop that must not make cudaMalloc/cudaFree calls,
+ * which can synchronize the whole device.  Nothing is allocated: the two
+ * wavefield levels and the sponge taper live in one fixed device array of
+ * e3d_noalloc_work_bytes() = 64 MiB, which every GPU that loads this library
+ * holds until the process exits.  That limits the grid to nz*nx*ny of about
+ * 0.93 M cells (18 float fields); larger grids return E3D_ERR_ARG with the
+ * sizes in e3d_last_error().  No context is needed: the propagation runs on
+ * the calling thread's current device, on `stream` (NULL = legacy default
+ * stream), with the stepper of the "plain" variant; desc->device is ignored.
+ * planes8_dev: the eight medium planes on that device; positions, offsets and
+ * time-major signals as for e3d_nl_propagate_device (the output signals are
+ * overwritten).  The first call on a device looks up the device address of
+ * the array (cudaGetSymbolAddress, with the device current) and caches it;
+ * make that first call before any stream capture.  Every call on a device
+ * uses the same array and clears it at the start, so calls that overlap on
+ * the GPU (on different streams, or from different threads) race and give
+ * wrong results; order them on one stream. */
+int e3d_nl_propagate_device_noalloc(const e3d_desc* desc, const float* const* planes8_dev, int adjoint,
+                                    const long long* src_pos_dev, const int* src_off10,
+                                    const long long* rec_pos_dev, const int* rec_off10, float* src_sig_dev,
+                                    float* rec_sig_dev, void* stream);
+/* Size in bytes of the fixed device array used by e3d_nl_propagate_device_noalloc. */
+size_t e3d_noalloc_work_bytes(void);
 
 /* Sampled stepper timing for roofline reporting: every n-th stepper launch is
  * bracketed by CUDA events on the launching stream (n = 0 switches it off). */
