@@ -483,7 +483,9 @@ static int launchStep(Context* c, int mode, const StepPtrs& p) {
   const int st = launchStepRaw(c, mode, p);
   if (sample && a && b) {
     cudaEventRecord(b, c->st);
-    c->timed.push_back({mode, a, b});
+    // launches that also fuse a decimation or a secondary source are kept apart (mode + 3)
+    const bool fused = p.accL[0] != nullptr || p.ssL[0] != nullptr;
+    c->timed.push_back({mode + (fused ? 3 : 0), a, b});
   }
   return st;
 }
@@ -801,11 +803,20 @@ int nlPropagateHost(Context* c, bool adjoint, float* const* model, float* const*
 
 int stepOnly(Context* c, int mode, int nSteps) {
   E3D_ARG(c && c->haveMedium, "medium not set");
-  E3D_ARG(mode >= 0 && mode <= 2, "bad mode");
+  E3D_ARG(mode >= 0 && mode <= 5, "bad mode");
+  // modes 3..5: modes 0..2 with the new level decimated into two coarse
+  // accumulators, as the gradient's passes run them (3 velocity fields for the
+  // source recompute, 9 fields for the adjoint)
+  const bool fused = mode >= 3;
+  const int m = fused ? mode - 3 : mode;
   E3D_RET(allocFields(c, c->w0, false));
   E3D_RET(allocFields(c, c->w1, false));
+  if (fused) {
+    E3D_RET(allocFields(c, c->ss[0], true));
+    E3D_RET(allocFields(c, c->ss[1], true));
+  }
   // the exact adjoint runs on the dual state, as in the adjoint pass, with the TMA loader
-  const bool dual = mode == STEP_ADJ_EXACT && c->loader >= 2 && c->d.nz % 4 == 0;
+  const bool dual = m == STEP_ADJ_EXACT && c->loader >= 2 && c->d.nz % 4 == 0;
   if (dual) {
     E3D_RET(allocFields(c, c->q0, false));
     E3D_RET(allocFields(c, c->q1, false));
@@ -817,7 +828,16 @@ int stepOnly(Context* c, int mode, int nSteps) {
         p.c[k] = c->q1.p[k];
         p.oP[k] = c->q0.p[k];
       }
-    E3D_RET(launchStep(c, mode, p));
+    if (fused) {
+      p.nAcc = m == STEP_ADJ_EXACT ? NCOMP : 3;
+      for (int k = 0; k < p.nAcc; k++) {
+        p.accL[k] = c->ss[0].p[k];
+        p.accR[k] = c->ss[1].p[k];
+      }
+      p.accWl = c->filt[1];
+      p.accWr = c->filt[c->hfilt + 1];
+    }
+    E3D_RET(launchStep(c, m, p));
     swapF(c->w0, c->w1);
     if (dual) swapF(c->q0, c->q1);
   }

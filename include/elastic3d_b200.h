@@ -333,13 +333,18 @@ size_t e3d_noalloc_work_bytes(void);
  * bracketed by CUDA events on the launching stream (n = 0 switches it off). */
 int e3d_kernel_timing(e3d_context* ctx, int every);
 /* Mean duration in ms and number of the sampled launches of one stepper mode
- * since the previous read (waits for them to finish). */
+ * since the previous read (waits for them to finish).  mode 0..2: bare steps
+ * of that mode; 3..5: the same modes with a fused decimation into coarse
+ * accumulators or a fused Born secondary source. */
 int e3d_kernel_timing_read(e3d_context* ctx, int mode, double* avg_ms, long long* count);
 /* Number of kernel launches this context has issued. */
 long long e3d_launch_count(const e3d_context* ctx);
 
 /* Bare stepper (mode 0 forward, 1 time-reversed, 2 exact transpose) applied
- * n_steps times to the context's working wavefields; for benchmarking. */
+ * n_steps times to the context's working wavefields; for benchmarking.
+ * Modes 3..5 run modes 0..2 with the new level decimated into two coarse
+ * accumulators (3 velocity fields for modes 3 and 4, all 9 fields for 5), as
+ * the FWI gradient's source recompute and adjoint passes do. */
 int e3d_step_only(e3d_context* ctx, int mode, int n_steps);
 
 /* ------------------------------------------------------------------------
