@@ -269,6 +269,15 @@ class FwiProblem:
         self.ckpt, self.segment = ckpt, segment
         self.auto_budget = segment == 0
         self.shots = []
+        # multi-GPU: every rank holds all shots, takes its share and all-reduces the result
+        self.distributed = False
+        self.group = None
+
+    def distribute(self, group=None):
+        """Shard the shots over the ranks of `group` (torch.distributed, one rank per GPU)."""
+        self.distributed = True
+        self.group = group
+        return self
 
     def _bind_stream(self):
         self.prop.set_stream(torch.cuda.current_stream(self.device))
@@ -313,6 +322,28 @@ class FwiProblem:
         return loss, grad8
 
 
+def shard_shots(n_shots, rank, world):
+    """Shots of one rank: rank, rank+world, ...  Shots are independent propagations, so they
+    shard with no exchange (the reference deals them to GPUs from one OpenMP loop,
+    nonlinearPropElasticShotsGpu_3D.cpp:178-204)."""
+    return list(range(rank, n_shots, world))
+
+
+def reduce_misfit(total, grads, group=None):
+    """Sum the misfit and the (rho, lambda, mu) gradient over the ranks of `group`: one
+    all-reduce of a flat buffer (NCCL over NVLink between GPUs; the reference sums shot
+    gradients on the host, BornElasticShotsGpu_3D.cpp:528-540)."""
+    if not (torch.distributed.is_available() and torch.distributed.is_initialized()):
+        return total, grads
+    flat = torch.cat([total.reshape(1).to(grads[0].dtype)] + [g.reshape(-1) for g in grads])
+    torch.distributed.all_reduce(flat, group=group)
+    out, off = [], 1
+    for g in grads:
+        out.append(flat[off:off + g.numel()].view_as(g))
+        off += g.numel()
+    return flat[0].to(total.dtype), out
+
+
 class ElasticFwiMisfit(torch.autograd.Function):
     """L(rho, lambda, mu) = sum over shots of 0.5*||d_pred - d_obs||^2.
 
@@ -324,7 +355,13 @@ class ElasticFwiMisfit(torch.autograd.Function):
     @staticmethod
     def forward(ctx, rho, lam, mu, problem: FwiProblem, shot_ids=None):
         planes = problem.set_model(rho.float().contiguous(), lam.float().contiguous(), mu.float().contiguous())
-        ids = range(len(problem.shots)) if shot_ids is None else shot_ids
+        if shot_ids is not None:
+            ids = shot_ids
+        elif problem.distributed:
+            ids = shard_shots(len(problem.shots), torch.distributed.get_rank(problem.group),
+                              torch.distributed.get_world_size(problem.group))
+        else:
+            ids = range(len(problem.shots))
         total = torch.zeros((), dtype=torch.float64, device=rho.device)
         g8 = torch.zeros_like(planes)
         for i in ids:
@@ -332,6 +369,8 @@ class ElasticFwiMisfit(torch.autograd.Function):
             total = total + loss
             g8 += grad8
         g = planes_to_model(g8, planes, problem.fd.dtw)
+        if problem.distributed:
+            total, g = reduce_misfit(total, list(g), problem.group)
         ctx.save_for_backward(*g)
         return total
 
