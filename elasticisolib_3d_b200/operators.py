@@ -32,6 +32,7 @@ Outputs follow the reference's `add` semantics: overwritten unless add.
 """
 from __future__ import annotations
 
+import builtins
 import threading
 from concurrent.futures import ThreadPoolExecutor
 
@@ -125,8 +126,8 @@ class _ShotOperatorBase:
         self.fd = H.FdParam(_nd(elasticParam), self.axes, paramP)
         if len(devices14) != 14:
             raise ValueError("expected 7 source and 7 receiver acquisition lists")
-        self.src = [list(devices14[g]) for g in range(7)]
-        self.rec = [list(devices14[7 + g]) for g in range(7)]
+        self.src = [list(devices14[g]) for g in builtins.range(7)]
+        self.rec = [list(devices14[7 + g]) for g in builtins.range(7)]
         self.nExp = len(self.src[0])
         if any(len(s) != self.nExp for s in self.src):
             raise ValueError("source acquisition lists differ in length")
@@ -140,7 +141,7 @@ class _ShotOperatorBase:
                 raise ValueError("duplicate GPU ids in iGpu")
             self.gpus = sorted(ids)
         else:
-            self.gpus = list(range(paramP.getInt("nGpu", 1)))
+            self.gpus = list(builtins.range(paramP.getInt("nGpu", 1)))
         if len(self.gpus) > self.nExp:
             raise ValueError("more GPUs than shots to model")
         fd = self.fd
