@@ -110,7 +110,7 @@ def call(name, *args):
 class E3DDesc(ctypes.Structure):
     _fields_ = [("device", I), ("nz", I), ("nx", I), ("ny", I), ("nts", I), ("sub", I), ("minPad", I),
                 ("dz", F), ("dx", F), ("dy", F), ("dts", F), ("alphaCos", F), ("fix_q1", I), ("q2compat", I),
-                ("q3compat", I)]
+                ("q3compat", I), ("free_surface", I)]
 
 
 class E3DTraceMap(ctypes.Structure):

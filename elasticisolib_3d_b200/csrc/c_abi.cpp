@@ -258,6 +258,7 @@ int e3d_context_create(const e3d_desc* desc, e3d_context** out) {
   d.nts = desc->nts; d.sub = desc->sub; d.minPad = desc->minPad;
   d.dz = desc->dz; d.dx = desc->dx; d.dy = desc->dy; d.dts = desc->dts; d.alphaCos = desc->alphaCos;
   d.fixQ1 = desc->fix_q1; d.q2compat = desc->q2compat; d.q3compat = desc->q3compat;
+  d.freeSurface = desc->free_surface;
   Context* c = nullptr;
   int st = createContext(d, &c);
   if (st != E3D_OK) return st;
@@ -422,6 +423,7 @@ int e3d_nl_propagate_device_noalloc(const e3d_desc* desc, const float* const* pl
                                     const long long* rec_pos_dev, const int* rec_off10, float* src_sig_dev,
                                     float* rec_sig_dev, void* stream) {
   if (!desc) return fail(E3D_ERR_ARG, "null descriptor");
+  if (desc->free_surface) return fail(E3D_ERR_ARG, "the allocation-free entry point has no free surface");
   ContextDesc d;
   d.device = desc->device;
   d.nz = desc->nz; d.nx = desc->nx; d.ny = desc->ny;

@@ -46,13 +46,18 @@ struct GridConst {
   long long n;        // nz*nx*ny
   float cz[4], cx[4], cy[4];
   const float* taper;  // device, minPad entries
+  int freeSurface;     // 1: free surface at z = FAT, whose face is not tapered (0: the reference's sponge)
 };
 
 #ifdef __CUDACC__
 // Distance to the closest non-FAT edge and the cosine taper there
-// (dampCosineEdge_3D, kernelsElaGpu_3D.cu:1182-1226): one minPad for all six faces.
+// (dampCosineEdge_3D, kernelsElaGpu_3D.cu:1182-1226): one minPad for all six
+// faces, the top face excluded when the free surface is on.
+__device__ __forceinline__ int topDistance(const GridConst& g, int iz) {
+  return g.freeSurface ? (1 << 30) : iz - FAT;
+}
 __device__ __forceinline__ float taperAt(const GridConst& g, int iz, int ix, int iy) {
-  int d = min(min(iz - FAT, ix - FAT), min(g.nz - iz - 1 - FAT, g.nx - ix - 1 - FAT));
+  int d = min(min(topDistance(g, iz), ix - FAT), min(g.nz - iz - 1 - FAT, g.nx - ix - 1 - FAT));
   d = min(d, min(iy - FAT, g.ny - iy - 1 - FAT));
   return d < g.minPad ? __ldg(g.taper + d) : 1.0f;
 }

@@ -157,6 +157,7 @@ int createContext(const ContextDesc& d, Context** out) {
   E3D_ARG(d.minPad >= 0 && d.minPad < PAD_MAX, "minPad must be in [0, PAD_MAX)");
   E3D_ARG(d.dz > 0 && d.dx > 0 && d.dy > 0 && d.dts > 0, "sampling must be positive");
   E3D_ARG((long long)d.nz * d.nx * d.ny < (1LL << 40), "grid too large");
+  E3D_ARG(!d.freeSurface || d.nz >= 3 * FAT + 2, "the free surface needs nz >= 3*FAT+2");
   Context* c = new Context();
   c->d = d;
   cudaError_t e = cudaSetDevice(d.device);
@@ -169,6 +170,7 @@ int createContext(const ContextDesc& d, Context** out) {
   }
   GridConst& g = c->g;
   g.nz = d.nz; g.nx = d.nx; g.ny = d.ny; g.minPad = d.minPad;
+  g.freeSurface = d.freeSurface ? 1 : 0;
   g.yStride = (long long)d.nz * d.nx;
   g.n = g.yStride * d.ny;
   // FD coefficients (nonlinearPropElasticGpuFunctions_3D.cu:207-220): double
@@ -609,6 +611,26 @@ static int launchRefresh(Context* c, const StepPtrs& p, const DevSignals& s) {
   return E3D_OK;
 }
 
+// Free-surface conditions on the new level after a step and its injection
+// (nonlinear propagation only; sgn +1 forward, -1 time-reversed).
+static int launchFreeSurface(Context* c, const StepPtrs& p, float sgn) {
+  if (!c->g.freeSurface) return E3D_OK;
+  const int nxi = c->d.nx - 2 * FAT, nyi = c->d.ny - 2 * FAT;
+  c->launches++;
+  kFreeSurface<<<dim3((nxi + 127) / 128, nyi), 128, 0, c->st>>>(p, c->g, sgn);
+  E3D_LAUNCH_CHECK();
+  return E3D_OK;
+}
+
+static int rejectFreeSurface(const Context* c) {
+  if (c->g.freeSurface) {
+    setLastError("the free surface is implemented for nonlinear propagation only (no exact adjoint of it yet)",
+                 __FILE__, __LINE__);
+    return E3D_ERR_ARG;
+  }
+  return E3D_OK;
+}
+
 static void swapF(Fields9& a, Fields9& b) {
   for (int k = 0; k < NCOMP; k++) std::swap(a.p[k], b.p[k]);
 }
@@ -758,6 +780,7 @@ int nlPropagateDevice(Context* c, bool adjoint, const DevSignals& srcSet, const 
         StepPtrs p = makeStep(c, c->w0, c->w1);
         E3D_RET(launchStep(c, STEP_FWD, p));
         E3D_RET(launchInject(c, p, srcSet, srcSig, its, it2 - 1));
+        E3D_RET(launchFreeSurface(c, p, 1.f));
         E3D_RET(launchRecord(c, p, recSet, recSig, its, it2));
         swapF(c->w0, c->w1);
       }
@@ -769,6 +792,7 @@ int nlPropagateDevice(Context* c, bool adjoint, const DevSignals& srcSet, const 
         StepPtrs p = makeStep(c, c->w0, c->w1);
         E3D_RET(launchStep(c, STEP_ADJ_REVERSED, p));
         E3D_RET(launchInject(c, p, recSet, recSig, its, it2 + 1));
+        E3D_RET(launchFreeSurface(c, p, -1.f));
         E3D_RET(launchRecord(c, p, srcSet, srcSig, its, it2));
         swapF(c->w0, c->w1);
       }
@@ -1419,6 +1443,7 @@ static int bornAdjointDevice(Context* c, const DevSignals& srcSet, const DevSign
 int bornForwardHost(Context* c, const float* const* srcSig, float* const* data, const HostGeom& src,
                     const HostGeom& rec, const float* const* pert) {
   E3D_ARG(c && c->haveMedium, "medium not set");
+  E3D_RET(rejectFreeSurface(c));
   E3D_ARG(srcSig && data && pert, "null argument");
   E3D_CUDA_TRY(cudaSetDevice(c->d.device));
   E3D_RET(ensurePert(c));
@@ -1445,6 +1470,7 @@ int bornForwardHost(Context* c, const float* const* srcSig, float* const* data, 
 int bornAdjointHost(Context* c, const float* const* srcSig, const float* const* data, const HostGeom& src,
                     const HostGeom& rec, float* const* pert) {
   E3D_ARG(c && c->haveMedium, "medium not set");
+  E3D_RET(rejectFreeSurface(c));
   E3D_ARG(srcSig && data && pert, "null argument");
   E3D_CUDA_TRY(cudaSetDevice(c->d.device));
   E3D_RET(ensurePert(c));
@@ -1481,6 +1507,7 @@ int fwiForwardDevice(Context* c, const DevSignals& srcSet, const DevSignals& rec
                      float* recSig, const TraceMap* map) {
   E3D_ARG(c && c->haveMedium, "medium not set");
   E3D_ARG(c->d.nts >= 2, "FWI needs at least two coarse samples");
+  E3D_RET(rejectFreeSurface(c));
   E3D_CUDA_TRY(cudaSetDevice(c->d.device));
   return sourcePassWithCheckpoints(c, srcSet, &recSet, srcSig, recSig, map);
 }
@@ -1489,6 +1516,7 @@ int fwiGradientDevice(Context* c, const DevSignals& srcSet, const DevSignals& re
                       const float* residual, float* const* pert8, const TraceMap* map) {
   E3D_ARG(c && c->haveMedium, "medium not set");
   E3D_ARG(pert8 != nullptr, "null gradient planes");
+  E3D_RET(rejectFreeSurface(c));
   E3D_CUDA_TRY(cudaSetDevice(c->d.device));
   for (int k = 0; k < NMED; k++) {
     E3D_ARG(pert8[k] != nullptr, "null gradient plane");

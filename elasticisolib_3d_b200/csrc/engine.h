@@ -28,6 +28,7 @@ struct ContextDesc {
   int fixQ1 = 0;     // 1: y derivatives use dy (the reference uses dx)
   int q2compat = 1;  // 1: sxz receivers use the z-grid positions (reference behaviour)
   int q3compat = 1;  // 1: Born yz shear term uses the xz derivative pair (reference behaviour)
+  int freeSurface = 0;  // 1: stress-free surface at z = FAT (nonlinear propagation only)
 };
 
 struct Context;

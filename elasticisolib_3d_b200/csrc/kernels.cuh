@@ -519,7 +519,7 @@ __global__ void __launch_bounds__(TZ * TX) kStepTma(const __grid_constant__ TmaM
     }
   }
   // sponge distance: the z/x part is fixed for this thread
-  const int dzx = min(min(iz - FAT, ix - FAT), min(g.nz - iz - 1 - FAT, g.nx - ix - 1 - FAT));
+  const int dzx = min(min(topDistance(g, iz), ix - FAT), min(g.nz - iz - 1 - FAT, g.nx - ix - 1 - FAT));
   const int lc = (tx + HALO) * SZ + (tz + HALO);
   const int li = tx * TZ + tz;
   int slot = 0;
@@ -836,7 +836,7 @@ __global__ void __launch_bounds__(TZ * TX, MINB) kStepTma2(const __grid_constant
   const int yBeg = FAT + blockIdx.z * yChunk;
   S.yEnd = min(yBeg + yChunk, g.ny - FAT);
   S.col = (long long)S.ix * g.nz + S.iz;
-  S.dzx = min(min(S.iz - FAT, S.ix - FAT), min(g.nz - S.iz - 1 - FAT, g.nx - S.ix - 1 - FAT));
+  S.dzx = min(min(topDistance(g, S.iz), S.ix - FAT), min(g.nz - S.iz - 1 - FAT, g.nx - S.ix - 1 - FAT));
   S.lc = (tx + HALO) * SZ + (tz + HALO);
   S.li = tx * TZ + tz;
   S.slot = 0;
@@ -908,6 +908,52 @@ __global__ void kInject(StepPtrs p, GridConst g, SparseSet s, const float* sigL,
   if (p.accL[0] != nullptr && k < p.nAcc) {
     p.accL[k][pos] += add * p.accWl;
     if (p.accR[0] != nullptr) p.accR[k][pos] += add * p.accWr;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Free surface at the first interior row zs = FAT, the row of the normal
+// stresses.  The reference parses freeSurface but applies it nowhere
+// (fdParamElastic_3D.cpp:19, 44-45); this is new physics: stress imaging with
+// the horizontal normal stresses re-derived at the surface.
+//   * sxx, syy at zs: the step's lambda*d(vz)/dz term is replaced by the
+//     stress-free relation d(vz)/dz = -lambda/(lambda+2mu) (d(vx)/dx + d(vy)/dy),
+//     i.e. new += sgn*G*(-lam*dvz - lam^2/l2m*(dvx + dvy)) with the derivatives
+//     of the current level (the ones the step used) and the 2dtw-scaled planes;
+//   * szz = 0 at zs and odd about it: szz[zs-k] = -szz[zs+k], k = 1..FAT;
+//   * sxz, syz (rows r at depth r-1/2) odd about zs: row r = -row 2*FAT+1-r,
+//     r = 0..FAT (row FAT lies half a cell above the surface);
+//   * vz rows 0..FAT (at or above zs-1/2) are ghosts held at zero.
+// One thread per interior (x, y) column; sgn = +1 forward, -1 time-reversed.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float dPlusG(const float* a, long long i, long long s, const float* c) {
+  return c[0] * (__ldg(a + i + s) - __ldg(a + i)) + c[1] * (__ldg(a + i + 2 * s) - __ldg(a + i - s)) +
+         c[2] * (__ldg(a + i + 3 * s) - __ldg(a + i - 2 * s)) + c[3] * (__ldg(a + i + 4 * s) - __ldg(a + i - 3 * s));
+}
+
+__global__ void kFreeSurface(StepPtrs p, GridConst g, float sgn) {
+  const int ix = FAT + blockIdx.x * blockDim.x + threadIdx.x;
+  const int iy = FAT + blockIdx.y;
+  if (ix >= g.nx - FAT || iy >= g.ny - FAT) return;
+  const long long ys = g.yStride;
+  const long long col = (long long)iy * ys + (long long)ix * g.nz;
+  const long long i = col + FAT;
+  const float dvx = dPlusG(p.c[VX], i, g.nz, g.cx);
+  const float dvy = dPlusG(p.c[VY], i, ys, g.cy);
+  const float dvz = dPlusG(p.c[VZ], i, 1, g.cz);
+  const float l2m = __ldg(p.m[L2M] + i), lam = __ldg(p.m[LAM] + i);
+  const float G = taperAt(g, FAT, ix, iy);
+  const float corr = sgn * G * (-lam * dvz - (lam * lam / l2m) * (dvx + dvy));
+  p.o[SXX][i] += corr;
+  p.o[SYY][i] += corr;
+  p.o[SZZ][i] = 0.0f;
+#pragma unroll
+  for (int k = 1; k <= FAT; k++) p.o[SZZ][i - k] = -p.o[SZZ][i + k];
+#pragma unroll
+  for (int r = 0; r <= FAT; r++) {
+    p.o[SXZ][col + r] = -p.o[SXZ][col + 2 * FAT + 1 - r];
+    p.o[SYZ][col + r] = -p.o[SYZ][col + 2 * FAT + 1 - r];
+    p.o[VZ][col + r] = 0.0f;
   }
 }
 

@@ -28,11 +28,12 @@ def _geom(pos7):
 
 class Propagator:
     def __init__(self, nz, nx, ny, nts, sub, minPad, dz, dx, dy, dts, alphaCos=0.99, device=0, fix_q1=0,
-                 q2compat=1, q3compat=1):
+                 q2compat=1, q3compat=1, free_surface=0):
         self.nz, self.nx, self.ny, self.nts, self.sub = int(nz), int(nx), int(ny), int(nts), int(sub)
         self.shape = (self.ny, self.nx, self.nz)
         d = N.E3DDesc(int(device), self.nz, self.nx, self.ny, self.nts, self.sub, int(minPad), float(dz), float(dx),
-                      float(dy), float(dts), float(alphaCos), int(fix_q1), int(q2compat), int(q3compat))
+                      float(dy), float(dts), float(alphaCos), int(fix_q1), int(q2compat), int(q3compat),
+                      int(free_surface))
         self._h = ctypes.c_void_p()
         N.call("e3d_context_create", ctypes.byref(d), ctypes.byref(self._h))
         self.device = int(device)

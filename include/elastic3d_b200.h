@@ -209,6 +209,9 @@ typedef struct e3d_desc {
   int fix_q1;     /* 1: y derivatives divide by dy (the reference divides by dx) */
   int q2compat;   /* 1: sxz receivers read the z-grid table (reference behaviour) */
   int q3compat;   /* 1: Born yz shear term uses the xz derivative pair (reference behaviour) */
+  int free_surface; /* 1: stress-free surface at z = FAT, the top face not tapered; nonlinear
+                       propagation only (the reference parses freeSurface but implements none,
+                       fdParamElastic_3D.cpp:44-45); 0: the reference's sponge on all faces */
 } e3d_desc;
 
 /* Counterpart of initNonlinearElasticGpu_3D + allocateNonlinearElasticGpu_3D
@@ -313,7 +316,8 @@ int e3d_fwi_gradient_device(e3d_context* ctx, const long long* src_pos_dev, cons
  * 0.93 M cells (18 float fields); larger grids return E3D_ERR_ARG with the
  * sizes in e3d_last_error().  No context is needed: the propagation runs on
  * the calling thread's current device, on `stream` (NULL = legacy default
- * stream), with the stepper of the "plain" variant; desc->device is ignored.
+ * stream), with the stepper of the "plain" variant; desc->device is ignored
+ * and desc->free_surface must be 0.
  * planes8_dev: the eight medium planes on that device; positions, offsets and
  * time-major signals as for e3d_nl_propagate_device (the output signals are
  * overwritten).  The first call on a device looks up the device address of

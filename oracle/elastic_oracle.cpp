@@ -38,6 +38,7 @@ struct Ctx {
   std::vector<T> filt;  // 2*(sub+1) time-interpolation weights
   std::vector<T> damp;  // minPad cosine taper
   T dtsInv;             // 1/(2 dts), Born time derivative
+  int freeSurface = 0;  // 1: stress-free surface at z = FAT, top face not tapered
 };
 
 // Constants of initNonlinearElasticGpu_3D (nonlinearPropElasticGpuFunctions_3D.cu:203-255)
@@ -178,7 +179,7 @@ void dampBoth(const Ctx<T>& C, T* const* p0, T* const* p1) {
   for (int iy = FAT; iy < ny - FAT; iy++) {
     for (int ix = FAT; ix < nx - FAT; ix++) {
       for (int iz = FAT; iz < nz - FAT; iz++) {
-        int d = iz - FAT;
+        int d = C.freeSurface ? (1 << 30) : iz - FAT;
         d = std::min(d, ix - FAT);
         d = std::min(d, nz - iz - 1 - FAT);
         d = std::min(d, nx - ix - 1 - FAT);
@@ -192,6 +193,55 @@ void dampBoth(const Ctx<T>& C, T* const* p0, T* const* p1) {
       }
     }
   }
+}
+
+// Free surface at the first interior row zs = FAT (new physics; the reference
+// parses freeSurface but applies it nowhere, fdParamElastic_3D.cpp:19, 44-45).
+// Stress imaging: szz = 0 at zs and odd about it; sxz, syz (row r at depth
+// r-1/2) odd about zs; vz rows 0..zs held at zero; and sxx, syy at zs with the
+// step's lambda*d(vz)/dz replaced through d(vz)/dz = -lambda/(lambda+2mu)
+// (d(vx)/dx + d(vy)/dy).  The correction uses the current level as the step
+// did, so it is formed before the sponge damps that level, and is applied,
+// scaled by the taper, after damping, together with the imaging.
+template <typename T>
+void freeSurfaceDelta(const Ctx<T>& C, const T* const* p1, const T* const* m, T sgn, std::vector<T>& delta) {
+  const long long ys = C.yStride, xs = C.nz;
+  delta.assign((size_t)C.nx * C.ny, T(0));
+#pragma omp parallel for collapse(2)
+  for (int iy = FAT; iy < C.ny - FAT; iy++)
+    for (int ix = FAT; ix < C.nx - FAT; ix++) {
+      const long long i = (long long)iy * ys + (long long)ix * xs + FAT;
+      const T dvx = dPlus(p1[VX], i, xs, C.cx);
+      const T dvy = dPlus(p1[VY], i, ys, C.cy);
+      const T dvz = dPlus(p1[VZ], i, 1, C.cz);
+      const T lam = m[LAM][i], l2m = m[L2M][i];
+      delta[(size_t)iy * C.nx + ix] = sgn * (-lam * dvz - (lam * lam / l2m) * (dvx + dvy));
+    }
+}
+
+template <typename T>
+void freeSurfaceApply(const Ctx<T>& C, T* const* p0, const std::vector<T>& delta) {
+  const long long ys = C.yStride, xs = C.nz;
+#pragma omp parallel for collapse(2)
+  for (int iy = FAT; iy < C.ny - FAT; iy++)
+    for (int ix = FAT; ix < C.nx - FAT; ix++) {
+      const long long col = (long long)iy * ys + (long long)ix * xs;
+      const long long i = col + FAT;
+      int d = std::min(ix - FAT, C.nx - ix - 1 - FAT);
+      d = std::min(d, C.nz - FAT - 1 - FAT);
+      d = std::min(d, std::min(iy - FAT, C.ny - iy - 1 - FAT));
+      const T g = d < C.minPad ? C.damp[d] : T(1);
+      const T corr = g * delta[(size_t)iy * C.nx + ix];
+      p0[SXX][i] += corr;
+      p0[SYY][i] += corr;
+      p0[SZZ][i] = T(0);
+      for (int k = 1; k <= FAT; k++) p0[SZZ][i - k] = -p0[SZZ][i + k];
+      for (int r = 0; r <= FAT; r++) {
+        p0[SXZ][col + r] = -p0[SXZ][col + 2 * FAT + 1 - r];
+        p0[SYZ][col + r] = -p0[SYZ][col + 2 * FAT + 1 - r];
+        p0[VZ][col + r] = T(0);
+      }
+    }
 }
 
 struct Geom {
@@ -283,11 +333,14 @@ void nlFwd(const Ctx<T>& C, const T* const* med, const T* const* model, T* const
     std::fill(data[comp], data[comp] + (size_t)rec.n[gridOf(comp)] * C.nts, T(0));
   const long long* rpos[NCOMP];
   receiverTable(rec, q2compat, rpos);
+  std::vector<T> fs;
   for (int its = 0; its < C.nts - 1; its++) {
     for (int it2 = 1; it2 < C.sub + 1; it2++) {
       step(C, p0.p, p1.p, med, 0);
       injectSignals(C, p0.p, model, src, its, it2 - 1);
+      if (C.freeSurface) freeSurfaceDelta(C, p1.p, med, T(1), fs);
       dampBoth(C, p0.p, p1.p);
+      if (C.freeSurface) freeSurfaceApply(C, p0.p, fs);
       recordSignals(C, p0.p, data, rec, its, it2, rpos);
       swapFields(p0, p1);
     }
@@ -306,11 +359,14 @@ void nlAdj(const Ctx<T>& C, const T* const* med, T* const* model, const T* const
     std::fill(model[comp], model[comp] + (size_t)src.n[gridOf(comp)] * C.nts, T(0));
   const long long* rpos[NCOMP];
   receiverTable(rec, q2compat, rpos);
+  std::vector<T> fs;
   for (int its = C.nts - 2; its > -1; its--) {
     for (int it2 = C.sub - 1; it2 > -1; it2--) {
       step(C, p0.p, p1.p, med, 1);
       injectSignals(C, p0.p, data, rec, its, it2 + 1, rpos);
+      if (C.freeSurface) freeSurfaceDelta(C, p1.p, med, T(-1), fs);
       dampBoth(C, p0.p, p1.p);
+      if (C.freeSurface) freeSurfaceApply(C, p0.p, fs);
       recordSignals(C, p0.p, model, src, its, it2);
       swapFields(p0, p1);
     }
@@ -520,6 +576,7 @@ struct oracle_params {
   int nz, nx, ny, nts, sub, minPad;
   double dz, dx, dy, dts, alphaCos;
   int q2compat, q3compat, fix_q1;
+  int free_surface;  // nonlinear propagation only; the Born entry points reject it
 };
 
 int oracle_num_threads(int n) {
@@ -534,6 +591,7 @@ int oracle_num_threads(int n) {
     Ctx<T> C;                                                                                            \
     makeCtx(C, P->nz, P->nx, P->ny, P->nts, P->dts, P->sub, P->minPad, P->dz, P->dx, P->dy,             \
             P->alphaCos, P->fix_q1);                                                                     \
+    C.freeSurface = P->free_surface;                                                                     \
     nlFwd(C, med, model, data, makeGeom<T>(spos, sn), makeGeom<T>(rpos, rn), P->q2compat);             \
     return 0;                                                                                            \
   }                                                                                                      \
@@ -543,6 +601,7 @@ int oracle_num_threads(int n) {
     Ctx<T> C;                                                                                            \
     makeCtx(C, P->nz, P->nx, P->ny, P->nts, P->dts, P->sub, P->minPad, P->dz, P->dx, P->dy,             \
             P->alphaCos, P->fix_q1);                                                                     \
+    C.freeSurface = P->free_surface;                                                                     \
     nlAdj(C, med, model, data, makeGeom<T>(spos, sn), makeGeom<T>(rpos, rn), P->q2compat);             \
     return 0;                                                                                            \
   }                                                                                                      \
@@ -552,6 +611,7 @@ int oracle_num_threads(int n) {
     Ctx<T> C;                                                                                            \
     makeCtx(C, P->nz, P->nx, P->ny, P->nts, P->dts, P->sub, P->minPad, P->dz, P->dx, P->dy,             \
             P->alphaCos, P->fix_q1);                                                                     \
+    if (P->free_surface) return 1;                                                                       \
     bornFwd(C, med, src, data, makeGeom<T>(spos, sn), makeGeom<T>(rpos, rn), pert, P->q2compat,        \
             P->q3compat);                                                                                \
     return 0;                                                                                            \
@@ -562,6 +622,7 @@ int oracle_num_threads(int n) {
     Ctx<T> C;                                                                                            \
     makeCtx(C, P->nz, P->nx, P->ny, P->nts, P->dts, P->sub, P->minPad, P->dz, P->dx, P->dy,             \
             P->alphaCos, P->fix_q1);                                                                     \
+    if (P->free_surface) return 1;                                                                       \
     bornAdj(C, med, src, data, makeGeom<T>(spos, sn), makeGeom<T>(rpos, rn), pert, P->q2compat,        \
             P->q3compat);                                                                                \
     return 0;                                                                                            \

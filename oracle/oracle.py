@@ -66,7 +66,8 @@ class OracleParams(ctypes.Structure):
                 ("nts", ctypes.c_int), ("sub", ctypes.c_int), ("minPad", ctypes.c_int),
                 ("dz", ctypes.c_double), ("dx", ctypes.c_double), ("dy", ctypes.c_double),
                 ("dts", ctypes.c_double), ("alphaCos", ctypes.c_double),
-                ("q2compat", ctypes.c_int), ("q3compat", ctypes.c_int), ("fix_q1", ctypes.c_int)]
+                ("q2compat", ctypes.c_int), ("q3compat", ctypes.c_int), ("fix_q1", ctypes.c_int),
+                ("free_surface", ctypes.c_int)]
 
 
 # ----------------------------------------------------------------------------
@@ -342,10 +343,12 @@ class PropParams:
     q2compat: int = 1
     q3compat: int = 1
     fix_q1: int = 0
+    free_surface: int = 0
 
     def c(self):
         return OracleParams(self.nz, self.nx, self.ny, self.nts, self.sub, self.minPad, self.dz, self.dx,
-                            self.dy, self.dts, self.alphaCos, self.q2compat, self.q3compat, self.fix_q1)
+                            self.dy, self.dts, self.alphaCos, self.q2compat, self.q3compat, self.fix_q1,
+                            self.free_surface)
 
 
 def _suffix(dtype):
