@@ -1417,7 +1417,12 @@ static int adjointPassFromCheckpoints(Context* c, const DevSignals& srcSet, cons
             p.oP[k] = c->q0.p[k];
           }
         }
-        if (it2 == sub - 1) E3D_RET(zeroFields(c, *aLeft));
+        // A[its] starts with this block: the TMA stepper writes it on the first
+        // fine step instead of accumulating onto a cleared slot
+        if (it2 == sub - 1) {
+          if (dual) p.accInitL = 1;
+          else E3D_RET(zeroFields(c, *aLeft));
+        }
         E3D_RET(launchStep(c, STEP_ADJ_EXACT, p));
         E3D_RET(launchInjectSlices(c, p, recSet, dataSlice(its), dataSlice(its + 1), it2 + 1));
         if (dual) E3D_RET(launchRefresh(c, p, recSet));

@@ -33,6 +33,7 @@ struct StepPtrs {
   float* accR[NCOMP];
   float accWl, accWr;
   int nAcc;               // number of leading components accumulated (3 or 9)
+  int accInitL;           // 1: accL is written (v*accWl) rather than accumulated; TMA stepper only
   // mode 2 with a dual state: c[] holds the medium-premultiplied current level
   // and the step also writes the premultiplied new level here (may be null)
   float* oP[NCOMP];
@@ -520,11 +521,16 @@ __global__ void __launch_bounds__(TZ * TX) kStepTma(const __grid_constant__ TmaM
   }
   // sponge distance: the z/x part is fixed for this thread
   const int dzx = min(min(topDistance(g, iz), ix - FAT), min(g.nz - iz - 1 - FAT, g.nx - ix - 1 - FAT));
+  // the taper of the (z, x) part is fixed for this thread; the y part is uniform
+  // over the CTA and is fetched at the top of each plane, ahead of the wait
+  const float Gzx = (active && dzx < g.minPad) ? __ldg(g.taper + dzx) : 1.0f;
   const int lc = (tx + HALO) * SZ + (tz + HALO);
   const int li = tx * TZ + tz;
   int slot = 0;
   unsigned parity = 0;  // bit s: parity of the next completion of stage s
   for (int y = yBeg; y < yEnd; y++) {
+    const int dyy = min(y - FAT, g.ny - y - 1 - FAT);
+    const float Gy = dyy < g.minPad ? __ldg(g.taper + dyy) : 1.0f;
     const bool ok = mbarWaitBounded(&bars[slot], (parity >> slot) & 1u);
     // barrier: every thread is past plane y-1, so its stage can be refilled;
     // the OR makes an expired wait a CTA-wide decision
@@ -562,7 +568,7 @@ __global__ void __launch_bounds__(TZ * TX) kStepTma(const __grid_constant__ TmaM
           preL[k] = __ldg(p.ssL[k] + ic);
           preR[k] = __ldg(p.ssR[k] + ic);
         } else if (hasAcc && k < p.nAcc) {
-          preL[k] = p.accL[k][ic];
+          if (!p.accInitL) preL[k] = p.accL[k][ic];
           if (hasR) preR[k] = p.accR[k][ic];
         }
       }
@@ -606,8 +612,8 @@ __global__ void __launch_bounds__(TZ * TX) kStepTma(const __grid_constant__ TmaM
         up[SXY] = sgn * (muxy * fxy);
         up[SYZ] = sgn * (muyz * fyz);
       }
-      const int d = min(dzx, min(y - FAT, g.ny - y - 1 - FAT));
-      const float G = d < g.minPad ? __ldg(g.taper + d) : 1.0f;
+      // = taper[min(dzx, dyy)] when that distance is below minPad, else 1
+      const float G = dyy < dzx ? Gy : Gzx;
       float nv[NCOMP];
 #pragma unroll
       for (int k = 0; k < NCOMP; k++) {
