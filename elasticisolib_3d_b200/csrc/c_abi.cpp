@@ -287,6 +287,11 @@ int e3d_set_stepper_variant(e3d_context* ctx, int tx, int stages, int loader) {
   return setStepperVariant(ctx->c, tx, stages, loader);
 }
 
+int e3d_set_stepper_chunks(e3d_context* ctx, int chunks) {
+  CTX_OR_FAIL(ctx);
+  return setStepperChunks(ctx->c, chunks);
+}
+
 int e3d_set_checkpoint_policy(e3d_context* ctx, int type, int segment, double budget_bytes) {
   CTX_OR_FAIL(ctx);
   return setCheckpointPolicy(ctx->c, type, segment, budget_bytes);

@@ -68,6 +68,7 @@ struct Context {
   int tx = 8;
   int stages = 2;            // shared-memory pipeline depth of the stepper
   int loader = 2;            // 0: plain loads, 1: cp.async, 2: TMA bulk tensor copies
+  int yChunks = 0;           // y chunks per (z, x) tile column of the stepper grid (0: automatic)
   std::unordered_map<unsigned long long, CUtensorMap> tmaps;  // (pointer, box) -> tensor map
   std::vector<void*> owned;  // every device allocation of this context
   // working wavefields (primary propagation)
@@ -273,6 +274,12 @@ int setStepperVariant(Context* c, int tx, int stages, int loader) {
   c->tx = tx;
   c->stages = stages;
   c->loader = loader;
+  return E3D_OK;
+}
+
+int setStepperChunks(Context* c, int chunks) {
+  E3D_ARG(c && chunks >= 0, "chunk count must be >= 0");
+  c->yChunks = chunks;
   return E3D_OK;
 }
 
@@ -533,11 +540,17 @@ static int launchStepRaw(Context* c, int mode, const StepPtrs& p) {
   // enough CTAs for several waves over 148 SMs, chunks of at least 32 planes
   const long long tiles = (long long)tiz * tix;
   int chunks = (int)std::min<long long>((4LL * 148 + tiles - 1) / tiles, std::max(1, nyi / 32));
+  const bool dual = mode == STEP_ADJ_EXACT && p.oP[0] != nullptr;
+  // The dual-state adjoint runs faster on short y runs: measured on B200 at
+  // 392x392x388, about 16 planes per CTA with the 9-field decimation fused
+  // (0.64 -> 0.75 of the copy bandwidth) and about 32 without it; the other
+  // steps prefer the long runs above.
+  if (dual) chunks = std::max(chunks, (nyi + (p.accL[0] ? 15 : 31)) / (p.accL[0] ? 16 : 32));
+  if (c->yChunks > 0) chunks = std::min(c->yChunks, nyi);
   chunks = std::max(chunks, 1);
   const int yChunk = (nyi + chunks - 1) / chunks;
   chunks = (nyi + yChunk - 1) / yChunk;
   dim3 grid(tiz, tix, chunks);
-  const bool dual = mode == STEP_ADJ_EXACT && p.oP[0] != nullptr;
   const bool pipe = (g.nz % 4 == 0) && mode != STEP_ADJ_EXACT && c->loader > 0;
   if (dual) {
     E3D_ARG(g.nz % 4 == 0, "dual-state adjoint needs nz % 4 == 0");

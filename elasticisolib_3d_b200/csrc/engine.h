@@ -41,6 +41,8 @@ int setMedium(Context* c, const float* const* planes, bool onDevice);
 // memory pipeline depth (2 or 3) and plane loader (0 plain loads, 1 cp.async,
 // 2 TMA bulk tensor copies).
 int setStepperVariant(Context* c, int tx, int stages, int loader);
+// Number of y chunks the stepper grid splits each (z, x) tile column into (0: automatic).
+int setStepperChunks(Context* c, int chunks);
 // Reads and clears the device flag set when a bounded pipeline wait expired.
 int checkPipeError(Context* c);
 // Sampled stepper timing: bracket every n-th stepper launch with CUDA events (0 = off).

@@ -69,6 +69,10 @@ class Propagator:
         """Stepper variant: x tile width (8/16), shared-memory stages (2/3) and plane loader."""
         N.call("e3d_set_stepper_variant", self._h, int(tx), int(stages), self.LOADERS[loader])
 
+    def set_stepper_chunks(self, chunks=0):
+        """y chunks per (z, x) tile column of the stepper grid (0 = automatic)."""
+        N.call("e3d_set_stepper_chunks", self._h, int(chunks))
+
     def set_checkpoint_policy(self, ckpt="auto", segment=0, budget_bytes=0.0):
         N.call("e3d_set_checkpoint_policy", self._h, CKPT_TYPES[ckpt], int(segment), float(budget_bytes))
 

@@ -41,6 +41,7 @@ def main(argv=None):
     ap.add_argument("--tx", type=int, default=8)
     ap.add_argument("--stages", type=int, default=2)
     ap.add_argument("--loader", default="tma", choices=sorted(Propagator.LOADERS))
+    ap.add_argument("--chunks", type=int, default=0, help="y chunks of the stepper grid (0 = automatic)")
     a = ap.parse_args(argv)
     dev = torch.device("cuda", torch.cuda.current_device())
     shape = (a.ny, a.nx, a.nz)
@@ -51,6 +52,7 @@ def main(argv=None):
     planes = medium_planes(rho, lam, mu, 0.0005)
     pr = Propagator(a.nz, a.nx, a.ny, 10, 4, 30, 10.0, 10.0, 10.0, 0.002, device=dev.index or 0)
     pr.set_stepper_variant(a.tx, a.stages, a.loader)
+    pr.set_stepper_chunks(a.chunks)
     pr.set_stream(torch.cuda.current_stream(dev))
     pr.set_medium(planes)
     pr.step_only(a.mode, a.warmup)
@@ -63,7 +65,7 @@ def main(argv=None):
     ms = e0.elapsed_time(e1) / a.steps
     cells = pr.cells_per_step
     b = BYTES_PER_CELL[a.mode]
-    print(json.dumps({"grid": [a.nz, a.nx, a.ny], "mode": a.mode, "variant": [a.tx, a.stages, a.loader],
+    print(json.dumps({"grid": [a.nz, a.nx, a.ny], "mode": a.mode, "variant": [a.tx, a.stages, a.loader], "chunks": a.chunks,
                       "ms_per_step": ms, "cells_per_step": cells, "gcells_per_s": cells / ms / 1e6,
                       "algorithmic_bytes_per_cell": b, "achieved_gbs": b * cells / ms / 1e6}), flush=True)
     pr.close()

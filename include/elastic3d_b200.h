@@ -224,6 +224,9 @@ int e3d_set_medium(e3d_context* ctx, const float* const* planes8, int on_device)
  * pipeline depth (2 or 3 stages) and plane loader (0 plain loads, 1 cp.async,
  * 2 TMA bulk tensor copies; 1 and 2 need nz % 4 == 0). */
 int e3d_set_stepper_variant(e3d_context* ctx, int tx, int stages, int loader);
+/* Autotuner hook: the number of y chunks each (z, x) tile column of the
+ * stepper grid is split into (CTAs = z tiles * x tiles * chunks); 0 = automatic. */
+int e3d_set_stepper_chunks(e3d_context* ctx, int chunks);
 /* Checkpoint storage: type -1 = the first plan that fits among fp32 states with
  * fp32 velocity slots, fp16 states with fp32 slots, fp16 states with fp16 slots
  * (default); 0 = fp32, 1 = fp16, 2 = bf16 (16-bit types carry one scale per
