@@ -263,7 +263,11 @@ class FwiProblem:
         self.prop = Propagator(fd.nz, fd.nx, fd.ny, fd.nts, fd.sub, fd.minPad, float(fd.dz), float(fd.dx),
                                float(fd.dy), float(fd.dts), float(fd.alphaCos),
                                device=self.device.index or 0)
-        self.prop.set_stepper_variant(*variant)
+        # variant "auto": timed on the grid by the autotuner at the first set_model
+        self.autotune = variant == "auto"
+        self.tuned = None
+        if not self.autotune:
+            self.prop.set_stepper_variant(*variant)
         self.prop.set_checkpoint_policy(ckpt, segment)
         self.prop.set_velocity_storage(velocity)
         self.ckpt, self.segment = ckpt, segment
@@ -286,6 +290,10 @@ class FwiProblem:
         planes = medium_planes(rho, lam, mu, self.fd.dtw)
         self._bind_stream()
         self.prop.set_medium(planes)
+        if self.autotune and self.tuned is None:
+            from .autotune import autotune_gradient
+            self.tuned = autotune_gradient(self.prop)
+            self._bind_stream()
         return planes
 
     def forward_data(self, shot: Shot, planes):
