@@ -276,6 +276,10 @@ class FwiProblem:
         # multi-GPU: every rank holds all shots, takes its share and all-reduces the result
         self.distributed = False
         self.group = None
+        # optional masks (efwiMain_3D.py:158-233): data mask on the residual, time-major
+        # (nts, 9*nRec) or broadcastable to it; gradient mask (3, ny, nx, nz) on (rho, lambda, mu)
+        self.data_mask = None
+        self.grad_mask = None
 
     def distribute(self, group=None):
         """Shard the shots over the ranks of `group` (torch.distributed, one rank per GPU)."""
@@ -322,7 +326,12 @@ class FwiProblem:
         """0.5*||d_pred - d_obs||^2 of one shot and its Born-adjoint gradient planes (8, ny, nx, nz)."""
         res, sig = self.forward_data(shot, planes)
         res.sub_(shot.d_obs)  # the residual overwrites the prediction
+        if self.data_mask is not None:
+            # objective 0.5*||M (d_pred - d_obs)||^2: residual M r, adjoint source M (M r)
+            res.mul_(self.data_mask)
         loss = _half_sum_sq(res)
+        if self.data_mask is not None:
+            res.mul_(self.data_mask)
         grad8 = torch.zeros_like(planes)
         self._bind_stream()
         self.prop.fwi_gradient_device(shot.src.pos, shot.src.off, shot.rec.pos, shot.rec.off, sig, res, grad8,
@@ -377,6 +386,8 @@ class ElasticFwiMisfit(torch.autograd.Function):
             total = total + loss
             g8 += grad8
         g = planes_to_model(g8, planes, problem.fd.dtw)
+        if problem.grad_mask is not None:
+            g = tuple(gk * problem.grad_mask[k] for k, gk in enumerate(g))
         if problem.distributed:
             total, g = reduce_misfit(total, list(g), problem.group)
         ctx.save_for_backward(*g)

@@ -80,3 +80,33 @@ def test_tiny_wavefield_checkpoints_stay_finite(ckpt):
     assert np.isfinite(loss.item())
     for x in m:
         assert torch.isfinite(x.grad).all()
+
+
+def test_masked_fwi_matches_fp64_oracle():
+    """Data mask on the residual and gradient mask on (rho, lambda, mu), as efwiMain_3D.py chains
+    its diagonal masks: objective 0.5*||Md (d_pred - d_obs)||^2, gradient Mg * J^T Md^T Md r."""
+    from oracle import oracle as O
+    sv, true = survey()
+    orc = OracleFwi(sv)
+    d_obs, _ = orc.data(true)
+    rng = np.random.default_rng(21)
+    dmask = (rng.random(d_obs.shape) > 0.25).astype(np.float64)
+    gmask = np.clip(rng.random(sv.elastic.shape), 0.2, 1.0)
+    d, med = orc.data(sv.elastic)
+    res = dmask * (d - d_obs)
+    loss_ref = 0.5 * float(np.sum(res * res))
+    rreg = [orc.rec[O.COMP_GRID[k]].adjoint(dmask[k] * res[k]) for k in range(9)]
+    g8 = O.born_adjoint_reg(orc.p, med, orc.src_reg(med), rreg, orc.spos, orc.rpos, None, np.float64)
+    g_ref = O.born_planes_to_model(g8, med[0:3], orc.dtw, None, np.float64) * gmask
+    prob, src, rec = _problem(sv)
+    prob.shots.append(F.make_shot(src, rec, explosive(sv.par.getInt("nts"), sv.wavelet), d_obs.astype(np.float32),
+                                  "cuda"))
+    prob.data_mask = F.time_major(torch.tensor(dmask, dtype=torch.float32)).cuda()
+    prob.grad_mask = torch.tensor(gmask, dtype=torch.float32, device="cuda")
+    m = [torch.tensor(sv.elastic[k], device="cuda", requires_grad=True) for k in range(3)]
+    loss = F.ElasticFwiMisfit.apply(m[0], m[1], m[2], prob)
+    loss.backward()
+    assert abs(loss.item() - loss_ref) / loss_ref < 1e-4
+    for k in range(3):
+        g = m[k].grad.double().cpu().numpy()
+        assert np.linalg.norm(g - g_ref[k]) / np.linalg.norm(g_ref[k]) < 1e-3, k
