@@ -62,6 +62,7 @@ SIGNATURES = {
     "e3d_fwi_gradient_device": ([P] * 9, I),
     "e3d_set_velocity_storage": ([P, I], I),
     "e3d_set_stepper_chunks": ([P, I], I),
+    "e3d_set_graph_loop": ([P, I], I),
     "e3d_nl_propagate_device_noalloc": ([P, P, I, P, P, P, P, P, P, P], I),
     "e3d_noalloc_work_bytes": ([], ctypes.c_size_t),
     "e3d_velocity_storage": ([P], I),

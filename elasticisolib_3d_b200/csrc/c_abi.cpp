@@ -287,6 +287,11 @@ int e3d_set_stepper_variant(e3d_context* ctx, int tx, int stages, int loader) {
   return setStepperVariant(ctx->c, tx, stages, loader);
 }
 
+int e3d_set_graph_loop(e3d_context* ctx, int on) {
+  CTX_OR_FAIL(ctx);
+  return setGraphLoop(ctx->c, on);
+}
+
 int e3d_set_stepper_chunks(e3d_context* ctx, int chunks) {
   CTX_OR_FAIL(ctx);
   return setStepperChunks(ctx->c, chunks);

@@ -17,6 +17,7 @@
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 #include <cudaTypedefs.h>
+#include <atomic>
 #include <mutex>
 #include <unordered_map>
 
@@ -69,6 +70,9 @@ struct Context {
   int stages = 2;            // shared-memory pipeline depth of the stepper
   int loader = 2;            // 0: plain loads, 1: cp.async, 2: TMA bulk tensor copies
   int yChunks = 0;           // y chunks per (z, x) tile column of the stepper grid (0: automatic)
+  int graphLoop = 1;         // 1: replay coarse blocks of the nonlinear loop as a CUDA graph
+  bool inCapture = false;    // a coarse block is being captured (no timing samples)
+  int* blockIndex = nullptr; // device coarse-time index of replayed blocks
   std::unordered_map<unsigned long long, CUtensorMap> tmaps;  // (pointer, box) -> tensor map
   std::vector<void*> owned;  // every device allocation of this context
   // working wavefields (primary propagation)
@@ -320,15 +324,23 @@ static StepPtrs makeStep(Context* c, Fields9& o, const Fields9& cur) {
   return p;
 }
 
+// Opt a kernel into its dynamic shared memory once per device (function
+// attributes are per device; several GPUs may be driven from one process).
+static int ensureSmemAttr(const void* fn, size_t smem, std::atomic<unsigned long long>& doneMask) {
+  int dev = 0;
+  E3D_CUDA_TRY(cudaGetDevice(&dev));
+  const unsigned long long bit = 1ULL << (dev & 63);
+  if (doneMask.load() & bit) return E3D_OK;
+  E3D_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  doneMask.fetch_or(bit);
+  return E3D_OK;
+}
+
 template <int MODE, int TX, int STAGES>
 static int launchPipe(Context* c, const StepPtrs& p, dim3 grid, int yChunk) {
   constexpr size_t smem = (size_t)STAGES * PipeLayout<TX>::STAGE_F * sizeof(float);
-  static bool configured = false;
-  if (!configured) {
-    E3D_CUDA_TRY(cudaFuncSetAttribute(kStepPipe<MODE, TX, STAGES>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)smem));
-    configured = true;
-  }
+  static std::atomic<unsigned long long> configured{0};
+  E3D_RET(ensureSmemAttr((const void*)kStepPipe<MODE, TX, STAGES>, smem, configured));
   kStepPipe<MODE, TX, STAGES><<<grid, dim3(TZ, TX), smem, c->st>>>(p, c->g, yChunk);
   return E3D_OK;
 }
@@ -401,12 +413,8 @@ static int buildMaps(Context* c, const StepPtrs& p, TmaMaps& mp) {
 template <int MODE, int TX, int STAGES>
 static int launchTma(Context* c, const StepPtrs& p, dim3 grid, int yChunk) {
   constexpr size_t smem = (size_t)STAGES * PipeLayout<TX>::STAGE_F * sizeof(float);
-  static bool configured = false;
-  if (!configured) {
-    E3D_CUDA_TRY(cudaFuncSetAttribute(kStepTma<MODE, TX, STAGES>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)smem));
-    configured = true;
-  }
+  static std::atomic<unsigned long long> configured{0};
+  E3D_RET(ensureSmemAttr((const void*)kStepTma<MODE, TX, STAGES>, smem, configured));
   TmaMaps mp;
   E3D_RET(buildMaps<TX>(c, p, mp));
   kStepTma<MODE, TX, STAGES><<<grid, dim3(TZ, TX), smem, c->st>>>(mp, p, c->g, yChunk);
@@ -416,12 +424,8 @@ static int launchTma(Context* c, const StepPtrs& p, dim3 grid, int yChunk) {
 template <int MODE, int TX, int STAGES, bool OM_SMEM, int MINB>
 static int launchTma2(Context* c, const StepPtrs& p, dim3 grid, int yChunk) {
   constexpr size_t smem = (size_t)STAGES * Tma2Layout<TX, OM_SMEM>::STAGE_F * sizeof(float);
-  static bool configured = false;
-  if (!configured) {
-    E3D_CUDA_TRY(cudaFuncSetAttribute(kStepTma2<MODE, TX, STAGES, OM_SMEM, MINB>,
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    configured = true;
-  }
+  static std::atomic<unsigned long long> configured{0};
+  E3D_RET(ensureSmemAttr((const void*)kStepTma2<MODE, TX, STAGES, OM_SMEM, MINB>, smem, configured));
   TmaMaps mp;
   E3D_RET(buildMaps<TX>(c, p, mp));
   kStepTma2<MODE, TX, STAGES, OM_SMEM, MINB><<<grid, dim3(TZ, TX), smem, c->st>>>(mp, p, c->g, yChunk);
@@ -482,7 +486,7 @@ static cudaEvent_t takeEvent(Context* c) {
 // on, brackets every n-th one with CUDA events on the launching stream.
 static int launchStep(Context* c, int mode, const StepPtrs& p) {
   c->launches++;
-  const bool sample = c->timingEvery > 0 && (c->stepCounter++ % c->timingEvery) == 0;
+  const bool sample = !c->inCapture && c->timingEvery > 0 && (c->stepCounter++ % c->timingEvery) == 0;
   cudaEvent_t a = nullptr, b = nullptr;
   if (sample) {
     a = takeEvent(c);
@@ -779,6 +783,110 @@ static void releaseStaged(Context* c, Staged& s) {
 // [damp fused] -> record (k=it2) -> swap.
 // Adjoint (propElasticAdjGpu_3D, time-reversed stepper, quirk Q7): per fine
 // step step -> inject data (k=it2+1) -> record source (k=it2) -> swap.
+__global__ void kSetIndex(int* its, int v) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) *its = v;
+}
+
+static int launchInjectIdx(Context* c, const StepPtrs& p, const DevSignals& s, const float* sig, const int* idx,
+                           int k) {
+  SparseSet ss;
+  ss.pos = s.pos;
+  for (int i = 0; i <= NCOMP; i++) ss.off[i] = s.off[i];
+  const int n = s.off[NCOMP];
+  if (n == 0) return E3D_OK;
+  c->launches++;
+  kInjectIdx<<<(n + 127) / 128, 128, 0, c->st>>>(p, c->g, ss, sig, idx, c->filt[k], c->filt[c->hfilt + k]);
+  E3D_LAUNCH_CHECK();
+  return E3D_OK;
+}
+
+static int launchRecordIdx(Context* c, const StepPtrs& p, const DevSignals& s, float* out, const int* idx, int k) {
+  SparseSet ss;
+  ss.pos = s.pos;
+  for (int i = 0; i <= NCOMP; i++) ss.off[i] = s.off[i];
+  const int n = s.off[NCOMP];
+  if (n == 0) return E3D_OK;
+  c->launches++;
+  kRecordIdx<<<(n + 127) / 128, 128, 0, c->st>>>(p, ss, out, idx, c->filt[k], c->filt[c->hfilt + k]);
+  E3D_LAUNCH_CHECK();
+  return E3D_OK;
+}
+
+// One coarse block of the nonlinear loops.  Forward (propElasticFwdGpu_3D):
+// per fine step it2 = 1..sub  step -> inject (k=it2-1) -> [free surface] ->
+// record (k=it2) -> swap.  Time-reversed (propElasticAdjGpu_3D, quirk Q7):
+// it2 = sub-1..0  step -> inject data (k=it2+1) -> [free surface] -> record
+// source (k=it2) -> swap.  With idx the coarse index is read on the device.
+static int nlBlock(Context* c, bool adjoint, const DevSignals& srcSet, const DevSignals& recSet, float* srcSig,
+                   float* recSig, int its, const int* idx) {
+  const int sub = c->d.sub;
+  const DevSignals& inSet = adjoint ? recSet : srcSet;
+  const DevSignals& outSet = adjoint ? srcSet : recSet;
+  float* inSig = adjoint ? recSig : srcSig;
+  float* outSig = adjoint ? srcSig : recSig;
+  for (int s = 0; s < sub; s++) {
+    const int it2 = adjoint ? sub - 1 - s : s + 1;
+    const int kIn = adjoint ? it2 + 1 : it2 - 1;
+    StepPtrs p = makeStep(c, c->w0, c->w1);
+    E3D_RET(launchStep(c, adjoint ? STEP_ADJ_REVERSED : STEP_FWD, p));
+    if (idx) E3D_RET(launchInjectIdx(c, p, inSet, inSig, idx, kIn));
+    else E3D_RET(launchInject(c, p, inSet, inSig, its, kIn));
+    E3D_RET(launchFreeSurface(c, p, adjoint ? -1.f : 1.f));
+    if (idx) E3D_RET(launchRecordIdx(c, p, outSet, outSig, idx, it2));
+    else E3D_RET(launchRecord(c, p, outSet, outSig, its, it2));
+    swapF(c->w0, c->w1);
+  }
+  return E3D_OK;
+}
+
+// Capture one coarse block (device-indexed, then the index advanced by `delta`)
+// into an executable graph.  Counted launches of the capture are returned in
+// *perBlock and taken back out of the context's count.
+static int captureBlock(Context* c, bool adjoint, const DevSignals& srcSet, const DevSignals& recSet,
+                        float* srcSig, float* recSig, cudaGraphExec_t* exec, long long* perBlock) {
+  const long long before = c->launches;
+  cudaGraph_t graph = nullptr;
+  E3D_CUDA_TRY(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
+  c->inCapture = true;
+  int st = nlBlock(c, adjoint, srcSet, recSet, srcSig, recSig, 0, c->blockIndex);
+  if (st == E3D_OK) {
+    kAdvanceIndex<<<1, 32, 0, c->st>>>(c->blockIndex, adjoint ? -1 : 1);
+    c->launches++;
+    if (cudaGetLastError() != cudaSuccess) {
+      setLastError("index advance launch failed", __FILE__, __LINE__);
+      st = E3D_ERR_CUDA;
+    }
+  }
+  c->inCapture = false;
+  const cudaError_t e = cudaStreamEndCapture(c->st, &graph);
+  *perBlock = c->launches - before;
+  c->launches = before;
+  if (st == E3D_OK && e != cudaSuccess) {
+    setLastError(cudaGetErrorString(e), __FILE__, __LINE__);
+    st = E3D_ERR_CUDA;
+  }
+  if (st == E3D_OK) {
+    const cudaError_t ei = cudaGraphInstantiate(exec, graph, 0);
+    if (ei != cudaSuccess) {
+      setLastError(cudaGetErrorString(ei), __FILE__, __LINE__);
+      st = E3D_ERR_CUDA;
+    }
+  }
+  if (graph) cudaGraphDestroy(graph);
+  return st;
+}
+
+int setGraphLoop(Context* c, int on) {
+  E3D_ARG(c, "null context");
+  c->graphLoop = on ? 1 : 0;
+  return E3D_OK;
+}
+
+// Nonlinear propagation (propElasticFwdGpu_3D / propElasticAdjGpu_3D).  The
+// first coarse block runs eagerly; with the graph loop on (and a stream other
+// than the legacy default stream) the remaining blocks replay one captured
+// block (two when sub is odd, for the two pointer parities), the coarse index
+// living on the device.
 int nlPropagateDevice(Context* c, bool adjoint, const DevSignals& srcSet, const DevSignals& recSet, float* srcSig,
                       float* recSig) {
   E3D_ARG(c && c->haveMedium, "medium not set");
@@ -786,32 +894,42 @@ int nlPropagateDevice(Context* c, bool adjoint, const DevSignals& srcSet, const 
   E3D_RET(allocFields(c, c->w0, true));
   E3D_RET(allocFields(c, c->w1, true));
   const int nts = c->d.nts, sub = c->d.sub;
-  if (!adjoint) {
-    E3D_CUDA_TRY(cudaMemsetAsync(recSig, 0, (size_t)std::max(recSet.off[NCOMP], 1) * nts * sizeof(float), c->st));
-    for (int its = 0; its < nts - 1; its++) {
-      for (int it2 = 1; it2 <= sub; it2++) {
-        StepPtrs p = makeStep(c, c->w0, c->w1);
-        E3D_RET(launchStep(c, STEP_FWD, p));
-        E3D_RET(launchInject(c, p, srcSet, srcSig, its, it2 - 1));
-        E3D_RET(launchFreeSurface(c, p, 1.f));
-        E3D_RET(launchRecord(c, p, recSet, recSig, its, it2));
-        swapF(c->w0, c->w1);
-      }
-    }
-  } else {
-    E3D_CUDA_TRY(cudaMemsetAsync(srcSig, 0, (size_t)std::max(srcSet.off[NCOMP], 1) * nts * sizeof(float), c->st));
-    for (int its = nts - 2; its >= 0; its--) {
-      for (int it2 = sub - 1; it2 >= 0; it2--) {
-        StepPtrs p = makeStep(c, c->w0, c->w1);
-        E3D_RET(launchStep(c, STEP_ADJ_REVERSED, p));
-        E3D_RET(launchInject(c, p, recSet, recSig, its, it2 + 1));
-        E3D_RET(launchFreeSurface(c, p, -1.f));
-        E3D_RET(launchRecord(c, p, srcSet, srcSig, its, it2));
-        swapF(c->w0, c->w1);
-      }
-    }
+  const int blocks = nts - 1;
+  float* outSig = adjoint ? srcSig : recSig;
+  const DevSignals& outSet = adjoint ? srcSet : recSet;
+  E3D_CUDA_TRY(cudaMemsetAsync(outSig, 0, (size_t)std::max(outSet.off[NCOMP], 1) * nts * sizeof(float), c->st));
+  const int first = adjoint ? nts - 2 : 0;
+  const int dir = adjoint ? -1 : 1;
+  const bool graph = c->graphLoop && c->st != nullptr && c->timingEvery == 0 && blocks >= 4;
+  if (!graph) {
+    for (int b = 0; b < blocks; b++) E3D_RET(nlBlock(c, adjoint, srcSet, recSet, srcSig, recSig, first + dir * b, nullptr));
+    return E3D_OK;
   }
-  return E3D_OK;
+  E3D_RET(nlBlock(c, adjoint, srcSet, recSet, srcSig, recSig, first, nullptr));
+  if (!c->blockIndex) E3D_RET(devAlloc(c, (void**)&c->blockIndex, sizeof(int)));
+  kSetIndex<<<1, 32, 0, c->st>>>(c->blockIndex, first + dir);
+  c->launches++;
+  E3D_LAUNCH_CHECK();
+  const int ng = (sub % 2) ? 2 : 1;
+  cudaGraphExec_t exec[2] = {nullptr, nullptr};
+  long long perBlock[2] = {0, 0};
+  int st = E3D_OK;
+  for (int i = 0; i < ng && st == E3D_OK; i++)
+    st = captureBlock(c, adjoint, srcSet, recSet, srcSig, recSig, &exec[i], &perBlock[i]);
+  for (int b = 1; b < blocks && st == E3D_OK; b++) {
+    const int i = (b - 1) % ng;
+    const cudaError_t e = cudaGraphLaunch(exec[i], c->st);
+    if (e != cudaSuccess) {
+      setLastError(cudaGetErrorString(e), __FILE__, __LINE__);
+      st = E3D_ERR_CUDA;
+    }
+    c->launches += perBlock[i];
+  }
+  // the host-side level pointers follow the replayed blocks
+  if (st == E3D_OK && ((long long)(blocks - 1) * sub) % 2) swapF(c->w0, c->w1);
+  for (int i = 0; i < ng; i++)
+    if (exec[i]) cudaGraphExecDestroy(exec[i]);
+  return st;
 }
 
 int nlPropagateHost(Context* c, bool adjoint, float* const* model, float* const* data, const HostGeom& src,

@@ -70,6 +70,8 @@ struct DevSignals {
 };
 int nlPropagateDevice(Context* c, bool adjoint, const DevSignals& srcSet, const DevSignals& recSet,
                       float* srcSig, float* recSig);
+// 1 (default): nonlinear propagation replays captured coarse blocks as CUDA graphs.
+int setGraphLoop(Context* c, int on);
 // Irregular receivers as linear combinations of the regular acquisition
 // points (device arrays).  Receiver row r = k*nIrreg + i (component k).
 //   gather (regular -> irregular): irr[r] = sum_f weight[r*nTaps+f] * reg[slot[r*nTaps+f]]

@@ -895,8 +895,8 @@ __global__ void __launch_bounds__(TZ * TX, MINB) kStepTma2(const __grid_constant
 // field[pos] += G(pos) * (sig[its]*wl + sig[its+1]*wr)
 // (ker_inject_source_* / ker_inject_data_*, kernelsElaGpu_3D.cu:11-52; the
 // source enters before the sponge, hence the taper at the point.)
-__global__ void kInject(StepPtrs p, GridConst g, SparseSet s, const float* sigL, const float* sigR, float wl,
-                        float wr) {
+__device__ __forceinline__ void injectAt(const StepPtrs& p, const GridConst& g, const SparseSet& s,
+                                         const float* sigL, const float* sigR, float wl, float wr) {
   const int ntot = s.off[NCOMP];
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= ntot) return;
@@ -915,6 +915,24 @@ __global__ void kInject(StepPtrs p, GridConst g, SparseSet s, const float* sigL,
     p.accL[k][pos] += add * p.accWl;
     if (p.accR[0] != nullptr) p.accR[k][pos] += add * p.accWr;
   }
+}
+
+__global__ void kInject(StepPtrs p, GridConst g, SparseSet s, const float* sigL, const float* sigR, float wl,
+                        float wr) {
+  injectAt(p, g, s, sigL, sigR, wl, wr);
+}
+
+// The same with the coarse time index read on the device (time-major signals
+// [nts][ntot], slices its and its+1): the form a replayed CUDA graph uses.
+__global__ void kInjectIdx(StepPtrs p, GridConst g, SparseSet s, const float* sig, const int* its, float wl,
+                           float wr) {
+  const long long t = *its, ntot = s.off[NCOMP];
+  injectAt(p, g, s, sig + t * ntot, sig + (t + 1) * ntot, wl, wr);
+}
+
+// Advance the device-side coarse time index of a replayed coarse block.
+__global__ void kAdvanceIndex(int* its, int delta) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) *its += delta;
 }
 
 // ---------------------------------------------------------------------------
@@ -965,7 +983,8 @@ __global__ void kFreeSurface(StepPtrs p, GridConst g, float sgn) {
 
 // outL[j] += field[pos]*wl; outR[j] += field[pos]*wr, with outL/outR the
 // time slices its and its+1 (ker_record_*, kernelsElaGpu_3D.cu:61-104)
-__global__ void kRecord(StepPtrs p, SparseSet s, float* outL, float* outR, float wl, float wr) {
+__device__ __forceinline__ void recordAt(const StepPtrs& p, const SparseSet& s, float* outL, float* outR, float wl,
+                                         float wr) {
   const int ntot = s.off[NCOMP];
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= ntot) return;
@@ -975,6 +994,15 @@ __global__ void kRecord(StepPtrs p, SparseSet s, float* outL, float* outR, float
   const float v = p.o[k][s.pos[j]];
   outL[j] += v * wl;
   outR[j] += v * wr;
+}
+
+__global__ void kRecord(StepPtrs p, SparseSet s, float* outL, float* outR, float wl, float wr) {
+  recordAt(p, s, outL, outR, wl, wr);
+}
+
+__global__ void kRecordIdx(StepPtrs p, SparseSet s, float* out, const int* its, float wl, float wr) {
+  const long long t = *its, ntot = s.off[NCOMP];
+  recordAt(p, s, out + t * ntot, out + (t + 1) * ntot, wl, wr);
 }
 
 // ---------------------------------------------------------------------------

@@ -69,6 +69,10 @@ class Propagator:
         """Stepper variant: x tile width (8/16), shared-memory stages (2/3) and plane loader."""
         N.call("e3d_set_stepper_variant", self._h, int(tx), int(stages), self.LOADERS[loader])
 
+    def set_graph_loop(self, on=True):
+        """Replay coarse blocks of the nonlinear loop as CUDA graphs (default on)."""
+        N.call("e3d_set_graph_loop", self._h, int(bool(on)))
+
     def set_stepper_chunks(self, chunks=0):
         """y chunks per (z, x) tile column of the stepper grid (0 = automatic)."""
         N.call("e3d_set_stepper_chunks", self._h, int(chunks))

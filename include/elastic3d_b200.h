@@ -224,6 +224,12 @@ int e3d_set_medium(e3d_context* ctx, const float* const* planes8, int on_device)
  * pipeline depth (2 or 3 stages) and plane loader (0 plain loads, 1 cp.async,
  * 2 TMA bulk tensor copies; 1 and 2 need nz % 4 == 0). */
 int e3d_set_stepper_variant(e3d_context* ctx, int tx, int stages, int loader);
+/* Nonlinear propagation (e3d_nl_* and the seam's propElastic*Gpu_3D): on = 1
+ * (default) captures one coarse block as a CUDA graph after running the first
+ * block eagerly and replays it for the others, the coarse time index living on
+ * the device; 0 launches every kernel from the host.  Graphs are not used on
+ * the legacy default stream or while stepper timing samples are being taken. */
+int e3d_set_graph_loop(e3d_context* ctx, int on);
 /* Autotuner hook: the number of y chunks each (z, x) tile column of the
  * stepper grid is split into (CTAs = z tiles * x tiles * chunks); 0 = automatic. */
 int e3d_set_stepper_chunks(e3d_context* ctx, int chunks);
