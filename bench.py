@@ -196,7 +196,9 @@ def run_reference(args):
     out = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
            "warmup": args.warmup, "ms_per_step": 1e3 / v, "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)", "impl": "reference",
-           "config": {"workload": "fwi-gradient 300^3+40 sponge (392x392x388), 2500 samples, 150x150 receivers",
+           "config": {"workload": f"fwi-gradient {args.interior}^3+40 sponge ({fd.nz}x{fd.nx}x{fd.ny}), "
+                                  f"{fd.nts} samples ({(fd.nts - 1) * fd.sub} fine steps), 150x150 receivers x 9 "
+                                  f"components, Ricker 10 Hz, one shot per step",
                       "l2_flush": "inputs larger than L2"},
            "cpu_baseline": cb, "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out), flush=True)
