@@ -257,12 +257,14 @@ class FwiProblem:
     """One propagation grid, its context and shots; shared by forward modelling and gradients."""
 
     def __init__(self, fd: H.FdParam, device="cuda", ckpt="auto", segment=0, variant=(8, 2, "tma"),
-                 velocity="auto"):
+                 velocity="auto", q3compat=1):
+        """q3compat=1 keeps the reference's Born yz shear term (the xz derivative pair, quirk Q3);
+        0 uses the yz pair, the linearisation of the propagator's own yz stress update."""
         self.fd = fd
         self.device = torch.device(device)
         self.prop = Propagator(fd.nz, fd.nx, fd.ny, fd.nts, fd.sub, fd.minPad, float(fd.dz), float(fd.dx),
                                float(fd.dy), float(fd.dts), float(fd.alphaCos),
-                               device=self.device.index or 0)
+                               device=self.device.index or 0, q3compat=q3compat)
         # variant "auto": timed on the grid by the autotuner at the first set_model
         self.autotune = variant == "auto"
         self.tuned = None

@@ -56,6 +56,11 @@ class OracleFwi:
         d = O.nl_forward_reg(self.p, med, self.src_reg(med), self.spos, self.rpos, np.float64)
         return np.stack([self.rec[O.COMP_GRID[k]].forward(d[k]) for k in range(9)]), med
 
+    def misfit(self, ep, d_obs):
+        d, _ = self.data(ep)
+        res = d - np.asarray(d_obs, dtype=np.float64)
+        return 0.5 * float(np.sum(res * res))
+
     def misfit_and_gradient(self, ep, d_obs):
         d, med = self.data(ep)
         res = d - np.asarray(d_obs, dtype=np.float64)

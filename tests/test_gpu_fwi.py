@@ -110,3 +110,50 @@ def test_masked_fwi_matches_fp64_oracle():
     for k in range(3):
         g = m[k].grad.double().cpu().numpy()
         assert np.linalg.norm(g - g_ref[k]) / np.linalg.norm(g_ref[k]) < 1e-3, k
+
+
+def test_gradient_against_finite_differences_of_the_misfit():
+    """20 random directions: <g, dm> from the CUDA gradient against central differences of the
+    nonlinear misfit (FP64 oracle).  The gradient is the reference's Born-adjoint gradient, not the
+    derivative of the discrete nonlinear misfit: its linearisation leaves out the derivative of the
+    medium scaling of the source signals at the source cells, and the reference's yz shear term
+    (quirk Q3) uses the xz derivative pair.  With the yz pair (q3compat=0) and directions that do not
+    touch the source cells, the measured agreement is correlation 0.987 and relative error 0.25
+    (FP64 oracle gradient); the bound is correlation > 0.95, relative error < 0.4, and every
+    sign right where the derivative is not small."""
+    sv, true = survey()
+    orc = OracleFwi(sv)
+    d_obs, _ = orc.data(true)
+    fd_ = H.FdParam(sv.elastic, sv.axes, sv.par)
+    prob = F.FwiProblem(fd_, ckpt="fp32", q3compat=0)
+    ax7 = H.grid_axes(*(a.n for a in sv.axes), *(a.o for a in sv.axes), *(a.d for a in sv.axes))
+    src = H.build_devices(*sv.src_xyz[0], ax7, fd_.nts, sv.par)
+    rec = H.build_devices(*sv.rec_xyz, ax7, fd_.nts, sv.par)
+    prob.shots.append(F.make_shot(src, rec, explosive(sv.par.getInt("nts"), sv.wavelet), d_obs.astype(np.float32),
+                                  "cuda"))
+    m0 = sv.elastic.astype(np.float64)
+    m = [torch.tensor(sv.elastic[k], device="cuda", requires_grad=True) for k in range(3)]
+    F.ElasticFwiMisfit.apply(m[0], m[1], m[2], prob).backward()
+    g = np.stack([x.grad.double().cpu().numpy() for x in m])
+    rng = np.random.default_rng(77)
+    mask = np.zeros((3,) + m0.shape[1:], dtype=bool)
+    mask[:, 4:-4, 4:-4, 4:-4] = True
+    ny, nx, nz = m0.shape[1:]
+    for dset in orc.src:
+        for pnt in dset.unique:
+            iy, ix, iz = pnt // (nz * nx), (pnt // nz) % nx, pnt % nz
+            mask[:, max(iy - 2, 0):iy + 3, max(ix - 2, 0):ix + 3, max(iz - 2, 0):iz + 3] = False
+    gd, fd = [], []
+    for _ in range(20):
+        dm = rng.standard_normal(m0.shape) * mask * (0.002 * np.abs(m0))
+        fd.append((orc.misfit(m0 + dm, d_obs) - orc.misfit(m0 - dm, d_obs)) / 2.0)
+        gd.append(float(np.sum(g * dm)))
+    gd, fd = np.array(gd), np.array(fd)
+    corr = float(np.corrcoef(gd, fd)[0, 1])
+    rel = float(np.linalg.norm(gd - fd) / np.linalg.norm(fd))
+    print(f"gradient vs finite differences over 20 directions: correlation {corr:.4f}, relative L2 {rel:.3f}",
+          flush=True)
+    assert corr > 0.95
+    assert rel < 0.4
+    big = np.abs(fd) > 0.1 * np.abs(fd).max()
+    assert np.all(np.sign(gd[big]) == np.sign(fd[big]))
