@@ -8,15 +8,17 @@ Workload (the FWI-gradient configuration): 300^3 interior + 40-cell sponge
 Gaussian anomalies; the gradient is taken at the background model.  Inputs are
 seeded synthetic data (no dataset is involved).
 
-One step = one shot's FWI gradient: nonlinear forward with on-device
+One step = one shot's FWI gradient per GPU: nonlinear forward with on-device
 checkpoints, residual at the receivers, Born adjoint of the residual with the
 source wavefield recomputed from the checkpoints, and the Born model
-post-processing, through ``ElasticFwiMisfit`` (autograd forward+backward).
+post-processing, through ``ElasticFwiMisfit`` (autograd forward+backward);
+with several GPUs the misfit and gradient are then summed over ranks (one
+NCCL all-reduce of the flat gradient).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-Multi-GPU (torchrun): shots shard across ranks with no data-path collective
-(weak scaling: every rank takes K shots); the time is the max over ranks.
+Multi-GPU (torchrun): every rank takes its own shot each step (weak scaling) and
+the gradients are summed with one all-reduce; the time is the max over ranks.
 """
 from __future__ import annotations
 
@@ -219,10 +221,13 @@ def run_ours(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=1800), device_id=device)
 
     sv, fd, prob = build_problem(args, device)
+    # every rank holds its own shot; under torchrun the misfit and gradient of the step are
+    # summed over ranks with one all-reduce, as an FWI iteration needs
+    prob.distributed = world > 1
     m = [torch.tensor(sv.elastic[k], device=device, requires_grad=True) for k in range(3)]
 
     def step():
-        loss = F.ElasticFwiMisfit.apply(m[0], m[1], m[2], prob)
+        loss = F.ElasticFwiMisfit.apply(m[0], m[1], m[2], prob, [0])
         loss.backward()
         for x in m:
             x.grad = None
@@ -277,7 +282,7 @@ def run_ours(args):
         for _ in range(args.steps):
             md = [h.to(device, non_blocking=True).requires_grad_(True) for h in host_model]
             shot.d_obs = host_obs.to(device, non_blocking=True)
-            loss = F.ElasticFwiMisfit.apply(md[0], md[1], md[2], prob)
+            loss = F.ElasticFwiMisfit.apply(md[0], md[1], md[2], prob, [0])
             loss.backward()
             for hg, x in zip(host_grad, md):
                 hg.copy_(x.grad, non_blocking=True)
