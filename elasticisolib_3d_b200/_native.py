@@ -59,7 +59,7 @@ SIGNATURES = {
     "e3d_born_adjoint": ([P] * 8, I),
     "e3d_nl_propagate_device": ([P, I, P, P, P, P, P, P], I),
     "e3d_fwi_forward_device": ([P] * 8, I),
-    "e3d_fwi_gradient_device": ([P] * 9, I),
+    "e3d_fwi_gradient_device": ([P] * 10, I),
     "e3d_set_velocity_storage": ([P, I], I),
     "e3d_set_stepper_chunks": ([P, I], I),
     "e3d_set_graph_loop": ([P, I], I),

@@ -410,7 +410,8 @@ int e3d_fwi_forward_device(e3d_context* ctx, const long long* src_pos_dev, const
 
 int e3d_fwi_gradient_device(e3d_context* ctx, const long long* src_pos_dev, const int* src_off10,
                             const long long* rec_pos_dev, const int* rec_off10, const float* src_sig_dev,
-                            const float* residual_dev, float* const* grad8_dev, const e3d_trace_map* map) {
+                            const float* residual_dev, float* const* grad8_dev, const e3d_trace_map* map,
+                            float* src_adj_dev) {
   CTX_OR_FAIL(ctx);
   DevSignals S, R;
   TraceMap T;
@@ -418,7 +419,7 @@ int e3d_fwi_gradient_device(e3d_context* ctx, const long long* src_pos_dev, cons
   if (st == E3D_OK) st = devSet(rec_pos_dev, rec_off10, R);
   if (st == E3D_OK) st = traceMap(map, T);
   if (st != E3D_OK) return st;
-  return fwiGradientDevice(ctx->c, S, R, src_sig_dev, residual_dev, grad8_dev, map ? &T : nullptr);
+  return fwiGradientDevice(ctx->c, S, R, src_sig_dev, residual_dev, grad8_dev, map ? &T : nullptr, src_adj_dev);
 }
 
 int e3d_set_velocity_storage(e3d_context* ctx, int type) {

@@ -616,6 +616,21 @@ static int launchRecord(Context* c, const StepPtrs& p, const DevSignals& s, floa
   return launchRecordSlices(c, p, s, out + (size_t)its * ntot, out + (size_t)(its + 1) * ntot, k);
 }
 
+static int launchExtractSource(Context* c, const StepPtrs& p, const DevSignals& s, float* out, int its, int k) {
+  SparseSet ss;
+  ss.pos = s.pos;
+  for (int i = 0; i <= NCOMP; i++) ss.off[i] = s.off[i];
+  const int n = s.off[NCOMP];
+  if (n == 0) return E3D_OK;
+  const size_t ntot = (size_t)n;
+  c->launches++;
+  kExtractSource<<<(n + 127) / 128, 128, 0, c->st>>>(p, c->g, ss, out + (size_t)its * ntot,
+                                                     out + (size_t)(its + 1) * ntot, c->filt[k],
+                                                     c->filt[c->hfilt + k]);
+  E3D_LAUNCH_CHECK();
+  return E3D_OK;
+}
+
 static int launchRefresh(Context* c, const StepPtrs& p, const DevSignals& s) {
   SparseSet ss;
   ss.pos = s.pos;
@@ -1452,7 +1467,8 @@ static int sourcePassWithCheckpoints(Context* c, const DevSignals& srcSet, const
 // spread to the regular acquisition points just before the block that
 // injects it.
 static int adjointPassFromCheckpoints(Context* c, const DevSignals& srcSet, const DevSignals& recSet,
-                                      const float* srcSig, const float* resid, const TraceMap* map) {
+                                      const float* srcSig, const float* resid, const TraceMap* map,
+                                      float* srcAdj = nullptr) {
   E3D_ARG(c->ckptValid, "no checkpoints for this shot");
   const int nts = c->d.nts, sub = c->d.sub, L = c->ckptSegLen;
   const int blocks = nts - 1;
@@ -1473,6 +1489,8 @@ static int adjointPassFromCheckpoints(Context* c, const DevSignals& srcSet, cons
   }
   const size_t nr = (size_t)recSet.off[NCOMP];
   const size_t rows = map ? (size_t)NCOMP * map->nIrreg : 0;
+  if (srcAdj)
+    E3D_CUDA_TRY(cudaMemsetAsync(srcAdj, 0, (size_t)std::max(srcSet.off[NCOMP], 1) * nts * sizeof(float), c->st));
   if (map) {
     E3D_RET(traceRingAtLeast(c, 2 * nr));
     E3D_RET(traceSpread(c, *map, (int)nr, resid + (size_t)(nts - 1) * rows, c->traceRing + ((nts - 1) % 2) * nr));
@@ -1557,6 +1575,9 @@ static int adjointPassFromCheckpoints(Context* c, const DevSignals& srcSet, cons
         E3D_RET(launchStep(c, STEP_ADJ_EXACT, p));
         E3D_RET(launchInjectSlices(c, p, recSet, dataSlice(its), dataSlice(its + 1), it2 + 1));
         if (dual) E3D_RET(launchRefresh(c, p, recSet));
+        // transpose of the source injection of forward step (its, it2+1): the exact
+        // adjoint of the nonlinear propagation with respect to the scaled source signals
+        if (srcAdj) E3D_RET(launchExtractSource(c, p, srcSet, srcAdj, its, it2));
         swapF(c->w0, c->w1);
         if (dual) swapF(c->q0, c->q1);
       }
@@ -1649,7 +1670,7 @@ int fwiForwardDevice(Context* c, const DevSignals& srcSet, const DevSignals& rec
 }
 
 int fwiGradientDevice(Context* c, const DevSignals& srcSet, const DevSignals& recSet, const float* srcSig,
-                      const float* residual, float* const* pert8, const TraceMap* map) {
+                      const float* residual, float* const* pert8, const TraceMap* map, float* srcAdj) {
   E3D_ARG(c && c->haveMedium, "medium not set");
   E3D_ARG(pert8 != nullptr, "null gradient planes");
   E3D_RET(rejectFreeSurface(c));
@@ -1658,7 +1679,7 @@ int fwiGradientDevice(Context* c, const DevSignals& srcSet, const DevSignals& re
     E3D_ARG(pert8[k] != nullptr, "null gradient plane");
     c->pertDev[k] = pert8[k];  // accumulate straight into the caller's planes
   }
-  int st = adjointPassFromCheckpoints(c, srcSet, recSet, srcSig, residual, map);
+  int st = adjointPassFromCheckpoints(c, srcSet, recSet, srcSig, residual, map, srcAdj);
   for (int k = 0; k < NMED; k++) c->pertDev[k] = nullptr;
   return st;
 }

@@ -93,8 +93,10 @@ struct TraceMap {
 // ([nts][9*nIrreg]) and no regular-grid trace array is ever allocated.
 int fwiForwardDevice(Context* c, const DevSignals& srcSet, const DevSignals& recSet, const float* srcSig,
                      float* recSig, const TraceMap* map);
+// srcAdj (optional, time-major [nts][srcSet.off[9]]): the exact adjoint of the nonlinear
+// propagation with respect to the scaled source signals, sampled during the same pass.
 int fwiGradientDevice(Context* c, const DevSignals& srcSet, const DevSignals& recSet, const float* srcSig,
-                      const float* residual, float* const* pert8, const TraceMap* map);
+                      const float* residual, float* const* pert8, const TraceMap* map, float* srcAdj);
 // Source velocity slot storage of the checkpoint plan: -1 auto, 0 FP32, 1 FP16 per-slice scaled.
 int setVelocityStorage(Context* c, int type);
 int velocityStorage(const Context* c);

@@ -1000,6 +1000,24 @@ __global__ void kRecord(StepPtrs p, SparseSet s, float* outL, float* outR, float
   recordAt(p, s, outL, outR, wl, wr);
 }
 
+// Transpose of kInject: outL[j] += G(pos)*field[pos]*wl, outR[j] += G(pos)*field[pos]*wr, the
+// taper G being the factor the injection applied at the point.
+__global__ void kExtractSource(StepPtrs p, GridConst g, SparseSet s, float* outL, float* outR, float wl, float wr) {
+  const int ntot = s.off[NCOMP];
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= ntot) return;
+  int k = 0;
+#pragma unroll
+  for (int c = 1; c < NCOMP; c++) k += (j >= s.off[c]);
+  const long long pos = s.pos[j];
+  const int iz = (int)(pos % g.nz);
+  const int ix = (int)((pos / g.nz) % g.nx);
+  const int iy = (int)(pos / g.yStride);
+  const float v = taperAt(g, iz, ix, iy) * p.o[k][pos];
+  outL[j] += v * wl;
+  outR[j] += v * wr;
+}
+
 __global__ void kRecordIdx(StepPtrs p, SparseSet s, float* out, const int* its, float wl, float wr) {
   const long long t = *its, ntot = s.off[NCOMP];
   recordAt(p, s, out + t * ntot, out + (t + 1) * ntot, wl, wr);

@@ -181,13 +181,16 @@ class Propagator:
         N.call("e3d_fwi_forward_device", self._h, src_pos.data_ptr(), so, rec_pos.data_ptr(), ro,
                src_sig.data_ptr(), rec_sig.data_ptr(), ref[0] if ref else None)
 
-    def fwi_gradient_device(self, src_pos, src_off, rec_pos, rec_off, src_sig, residual, grad8, tmap=None):
+    def fwi_gradient_device(self, src_pos, src_off, rec_pos, rec_off, src_sig, residual, grad8, tmap=None,
+                            src_adj=None):
+        """Born-adjoint gradient planes into grad8; optionally the exact adjoint with respect to the
+        scaled source signals into src_adj (time-major (nts, src_off[9]))."""
         so = (ctypes.c_int * 10)(*[int(v) for v in src_off])
         ro = (ctypes.c_int * 10)(*[int(v) for v in rec_off])
         ref = self._trace_map(tmap)
         N.call("e3d_fwi_gradient_device", self._h, src_pos.data_ptr(), so, rec_pos.data_ptr(), ro,
                src_sig.data_ptr(), residual.data_ptr(), N.ptr_array([grad8[k] for k in range(8)]),
-               ref[0] if ref else None)
+               ref[0] if ref else None, src_adj.data_ptr() if src_adj is not None else None)
 
     def set_velocity_storage(self, kind="auto"):
         """Source velocity slots of the checkpoint plan: "auto", "fp32" or "fp16"."""

@@ -257,9 +257,12 @@ class FwiProblem:
     """One propagation grid, its context and shots; shared by forward modelling and gradients."""
 
     def __init__(self, fd: H.FdParam, device="cuda", ckpt="auto", segment=0, variant=(8, 2, "tma"),
-                 velocity="auto", q3compat=1):
+                 velocity="auto", q3compat=1, source_term=False):
         """q3compat=1 keeps the reference's Born yz shear term (the xz derivative pair, quirk Q3);
-        0 uses the yz pair, the linearisation of the propagator's own yz stress update."""
+        0 uses the yz pair, the linearisation of the propagator's own yz stress update.
+        source_term=True adds the misfit's derivative through the medium scaling of the source
+        signals (the exact adjoint sampled at the source points, chained through medium_planes and
+        scale_sources by autograd), which the reference's Born-adjoint gradient leaves out."""
         self.fd = fd
         self.device = torch.device(device)
         self.prop = Propagator(fd.nz, fd.nx, fd.ny, fd.nts, fd.sub, fd.minPad, float(fd.dz), float(fd.dx),
@@ -273,6 +276,7 @@ class FwiProblem:
         self.prop.set_checkpoint_policy(ckpt, segment)
         self.prop.set_velocity_storage(velocity)
         self.ckpt, self.segment = ckpt, segment
+        self.source_term = source_term
         self.auto_budget = segment == 0
         self.shots = []
         # multi-GPU: every rank holds all shots, takes its share and all-reduces the result
@@ -324,8 +328,9 @@ class FwiProblem:
         d_pred, _ = self.forward_data(shot, planes)
         return component_major(d_pred, shot.rec.n_irreg)
 
-    def shot_misfit_and_gradient(self, shot: Shot, planes):
-        """0.5*||d_pred - d_obs||^2 of one shot and its Born-adjoint gradient planes (8, ny, nx, nz)."""
+    def shot_misfit_and_gradient(self, shot: Shot, planes, src_adj=None):
+        """0.5*||d_pred - d_obs||^2 of one shot and its Born-adjoint gradient planes (8, ny, nx, nz);
+        with src_adj (nts, src.off[9]) the exact adjoint at the source points is written there."""
         res, sig = self.forward_data(shot, planes)
         res.sub_(shot.d_obs)  # the residual overwrites the prediction
         if self.data_mask is not None:
@@ -337,7 +342,7 @@ class FwiProblem:
         grad8 = torch.zeros_like(planes)
         self._bind_stream()
         self.prop.fwi_gradient_device(shot.src.pos, shot.src.off, shot.rec.pos, shot.rec.off, sig, res, grad8,
-                                      shot.tables)
+                                      shot.tables, src_adj)
         return loss, grad8
 
 
@@ -363,6 +368,20 @@ def reduce_misfit(total, grads, group=None):
     return flat[0].to(total.dtype), out
 
 
+def _source_scaling_gradient(rho, lam, mu, problem, src_terms):
+    """d/d(rho, lambda, mu) of sum_shots <src_adj, scale_sources(sig, medium_planes(rho, lambda, mu))>:
+    the misfit's dependence through the medium scaling of the source signals."""
+    fd = problem.fd
+    with torch.enable_grad():
+        m = [x.detach().float().requires_grad_(True) for x in (rho, lam, mu)]
+        planes = medium_planes(m[0], m[1], m[2], fd.dtw)
+        acc = torch.zeros((), dtype=torch.float64, device=rho.device)
+        for shot, adj in src_terms:
+            s = scale_sources(shot.sig_reg, shot.src, planes, fd.dx, fd.dy, fd.dz)
+            acc = acc + torch.sum(s.double() * adj.double())
+        return torch.autograd.grad(acc, m)
+
+
 class ElasticFwiMisfit(torch.autograd.Function):
     """L(rho, lambda, mu) = sum over shots of 0.5*||d_pred - d_obs||^2.
 
@@ -383,11 +402,20 @@ class ElasticFwiMisfit(torch.autograd.Function):
             ids = range(len(problem.shots))
         total = torch.zeros((), dtype=torch.float64, device=rho.device)
         g8 = torch.zeros_like(planes)
+        src_terms = []
         for i in ids:
-            loss, grad8 = problem.shot_misfit_and_gradient(problem.shots[i], planes)
+            shot = problem.shots[i]
+            src_adj = None
+            if problem.source_term:
+                src_adj = torch.empty((problem.fd.nts, shot.src.off[9]), dtype=torch.float32, device=rho.device)
+            loss, grad8 = problem.shot_misfit_and_gradient(shot, planes, src_adj)
             total = total + loss
             g8 += grad8
+            if src_adj is not None:
+                src_terms.append((shot, src_adj))
         g = planes_to_model(g8, planes, problem.fd.dtw)
+        if src_terms:
+            g = tuple(a + b for a, b in zip(g, _source_scaling_gradient(rho, lam, mu, problem, src_terms)))
         if problem.grad_mask is not None:
             g = tuple(gk * problem.grad_mask[k] for k, gk in enumerate(g))
         if problem.distributed:

@@ -308,10 +308,18 @@ int e3d_fwi_forward_device(e3d_context* ctx, const long long* src_pos_dev, const
                            float* rec_sig_dev, const e3d_trace_map* map);
 /* FWI: Born adjoint of the residual, accumulated into eight device planes;
  * consumes the checkpoints of the preceding e3d_fwi_forward_device.  The
- * residual has the layout of rec_sig_dev above for the same map. */
+ * residual has the layout of rec_sig_dev above for the same map.
+ * src_adj_dev (optional, time-major [nts][src_off10[9]], overwritten): the
+ * exact adjoint of the nonlinear propagation with respect to the scaled
+ * source signals -- the residual propagated by the exact-transpose stepper
+ * and sampled at the source points with the transposed injection weights and
+ * taper.  It makes the exact nonlinear adjoint available (the reference's
+ * propElasticAdjGpu_3D runs the time-reversed stepper instead) and gives the
+ * misfit's derivative through the medium scaling of the sources. */
 int e3d_fwi_gradient_device(e3d_context* ctx, const long long* src_pos_dev, const int* src_off10,
                             const long long* rec_pos_dev, const int* rec_off10, const float* src_sig_dev,
-                            const float* residual_dev, float* const* grad8_dev, const e3d_trace_map* map);
+                            const float* residual_dev, float* const* grad8_dev, const e3d_trace_map* map,
+                            float* src_adj_dev);
 
 /* Allocation-free variant of e3d_nl_propagate_device.  It has no counterpart
  * in the reference (whose drivers allocate and free device buffers on every
