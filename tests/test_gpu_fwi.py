@@ -187,7 +187,9 @@ def test_exact_nonlinear_adjoint_dot_test():
 
 def test_source_term_gradient_against_finite_differences():
     """With the source-scaling term the gradient also follows the misfit through the sources:
-    directions that touch the source cells now agree (yz pair, q3compat=0)."""
+    directions that touch the source cells now agree (yz pair, q3compat=0).  Measured on B200:
+    correlation 0.993, relative error 0.13 over all cells (reference-equivalent gradient: 0.74,
+    0.71); bound: correlation > 0.98, relative error < 0.2."""
     sv, true = survey()
     orc = OracleFwi(sv)
     d_obs, _ = orc.data(true)
@@ -215,4 +217,5 @@ def test_source_term_gradient_against_finite_differences():
     rel = float(np.linalg.norm(gd - fd) / np.linalg.norm(fd))
     print(f"gradient with source term vs finite differences (all cells): correlation {corr:.4f}, "
           f"relative L2 {rel:.3f}", flush=True)
-    assert corr > 0.95
+    assert corr > 0.98
+    assert rel < 0.2
