@@ -132,6 +132,31 @@ def gardner_model(shape, seed, vmin=1500.0, vmax=4500.0, sigma=8.0):
     return vp, vs, rho
 
 
+def config1(nts=2000, seed=1, nshots=16, coarse=8):
+    """Batched forward modelling: 400 x 400 (x, y) x 300 (z) interior + 40-cell sponge (392 x 488 x 488
+    cells with FAT), Gardner model family (vp smooth random in [1500, 4500] m/s, vs = vp/sqrt(3),
+    rho = 310 vp^0.25), explosive Ricker 15 Hz sources on a 4 x 4 surface grid (20 m depth), 200 x 200
+    receivers at 10 m spacing (10 m depth), dts 2 ms.  The random field is drawn on a grid `coarse`
+    times coarser and repeated, which keeps the set-up cheap on 93 M cells."""
+    d = 10.0
+    axes, pads = make_grid(300, 400, 400, 40, d)
+    shape = (axes[2].n, axes[1].n, axes[0].n)
+    cshape = tuple(-(-n // coarse) for n in shape)
+    vpc, _, _ = gardner_model(cshape, seed, vmax=4450.0, sigma=2.0)  # Courant 0.45 needs vmax < 4500
+    vp = np.repeat(np.repeat(np.repeat(vpc, coarse, 0), coarse, 1), coarse, 2)[:shape[0], :shape[1], :shape[2]]
+    vs = vp / np.sqrt(3.0)
+    rho = 310.0 * vp ** 0.25
+    el = elastic_from_velocity(vp, vs, rho)
+    dts = 0.002
+    par = base_params(axes, pads, nts, dts, 2, 25.0)
+    g4 = np.linspace(800.0, 3200.0, 4)
+    src = [(np.array([20.0]), np.array([g4[i % 4]]), np.array([g4[(i // 4) % 4]])) for i in range(nshots)]
+    g = 2000.0 + (np.arange(200) - 99.5) * 10.0
+    X, Y = np.meshgrid(g, g, indexing="ij")
+    rec = (np.full(X.size, 10.0), X.reshape(-1), Y.reshape(-1))
+    return Survey(el, axes, par, src, rec, ricker(nts, dts, 15.0, 1.0 / 15.0), "config1-batched-fwd")
+
+
 def config_fwi(nzi=300, nxi=300, nyi=300, pad=40, nts=2500, nshots=32, nrec=150, fdom=10.0, seed=3,
                true_model=False):
     """FWI gradient survey (config 3 family): smooth background (vp 2500, vs vp/1.732, rho 2000 with
