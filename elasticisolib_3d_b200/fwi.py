@@ -263,6 +263,8 @@ class FwiProblem:
         source_term=True adds the misfit's derivative through the medium scaling of the source
         signals (the exact adjoint sampled at the source points, chained through medium_planes and
         scale_sources by autograd), which the reference's Born-adjoint gradient leaves out."""
+        if getattr(fd, "freeSurface", 0):
+            raise ValueError("FWI gradients with a free surface are not supported (no exact adjoint of it)")
         self.fd = fd
         self.device = torch.device(device)
         self.prop = Propagator(fd.nz, fd.nx, fd.ny, fd.nts, fd.sub, fd.minPad, float(fd.dz), float(fd.dx),

@@ -145,8 +145,11 @@ class _ShotOperatorBase:
         if len(self.gpus) > self.nExp:
             raise ValueError("more GPUs than shots to model")
         fd = self.fd
+        # freeSurface=1 in the parameters runs the free surface (nonlinear operators only: the
+        # engine refuses it on the Born path, which has no exact adjoint of it)
         self.props = [Propagator(fd.nz, fd.nx, fd.ny, fd.nts, fd.sub, fd.minPad, float(fd.dz), float(fd.dx),
-                                 float(fd.dy), float(fd.dts), float(fd.alphaCos), device=g) for g in self.gpus]
+                                 float(fd.dy), float(fd.dts), float(fd.alphaCos), device=g,
+                                 free_surface=int(fd.freeSurface)) for g in self.gpus]
         for pr in self.props:
             pr.set_medium(fd.planes)
         self._lock = threading.Lock()
