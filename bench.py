@@ -121,8 +121,8 @@ def build_problem(args, device):
     from elasticisolib_3d_b200 import hostprep as H
     from elasticisolib_3d_b200 import synthetic as S
     n = args.interior
-    sv = S.config_fwi(nzi=n, nxi=n, nyi=n, nts=args.nts, true_model=False)
-    svt = S.config_fwi(nzi=n, nxi=n, nyi=n, nts=args.nts, true_model=True)
+    sv = S.fwi_gradient_survey(nzi=n, nxi=n, nyi=n, nts=args.nts, true_model=False)
+    svt = S.fwi_gradient_survey(nzi=n, nxi=n, nyi=n, nts=args.nts, true_model=True)
     fd = H.FdParam(sv.elastic, sv.axes, sv.par)
     ax7 = H.grid_axes(*(a.n for a in sv.axes), *(a.o for a in sv.axes), *(a.d for a in sv.axes))
     prob = F.FwiProblem(fd, device=device)
@@ -186,7 +186,7 @@ def run_reference(args):
     from elasticisolib_3d_b200 import hostprep as H
     from elasticisolib_3d_b200 import synthetic as S
     n = args.interior
-    sv = S.config_fwi(nzi=n, nxi=n, nyi=n, nts=args.nts)
+    sv = S.fwi_gradient_survey(nzi=n, nxi=n, nyi=n, nts=args.nts)
     fd = H.FdParam(sv.elastic, sv.axes, sv.par)
     vals = []
     for i in range(args.warmup + args.steps):

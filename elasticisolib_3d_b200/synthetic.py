@@ -103,7 +103,7 @@ def gaussian_perturbed_model(shape, vp0, vs0, rho0, amp, sigma, seed):
     return (vp0 * (1 + amp * f), vs0 * (1 + amp * f), rho0 * (1 + amp * f))
 
 
-def config0(nts=1000, seed=0):
+def plain_forward_survey(nts=1000, seed=0):
     """Plain forward, single shot: 120^3 interior + 30 sponge, free surface top, dx=10 m,
     vp=2500, vs=vp/1.732, rho=2000 with smooth +-10% perturbations (sigma 5 cells);
     explosive Ricker 15 Hz at the centre, 200 m depth; 40x40 receivers at 20 m depth (30 m spacing)."""
@@ -119,7 +119,7 @@ def config0(nts=1000, seed=0):
     g = (np.arange(40) - 19.5) * 30.0 + c
     X, Y = np.meshgrid(g, g, indexing="ij")
     rec = (np.full(X.size, 20.0), X.reshape(-1), Y.reshape(-1))
-    return Survey(el, axes, par, src, rec, ricker(nts, dts, 15.0, 1.0 / 15.0), "config0-nl-fwd-120^3")
+    return Survey(el, axes, par, src, rec, ricker(nts, dts, 15.0, 1.0 / 15.0), "plain-forward-120^3+30")
 
 
 def gardner_model(shape, seed, vmin=1500.0, vmax=4500.0, sigma=8.0):
@@ -132,7 +132,7 @@ def gardner_model(shape, seed, vmin=1500.0, vmax=4500.0, sigma=8.0):
     return vp, vs, rho
 
 
-def config1(nts=2000, seed=1, nshots=16, coarse=8):
+def batched_forward_survey(nts=2000, seed=1, nshots=16, coarse=8):
     """Batched forward modelling: 400 x 400 (x, y) x 300 (z) interior + 40-cell sponge (392 x 488 x 488
     cells with FAT), Gardner model family (vp smooth random in [1500, 4500] m/s, vs = vp/sqrt(3),
     rho = 310 vp^0.25), explosive Ricker 15 Hz sources on a 4 x 4 surface grid (20 m depth), 200 x 200
@@ -154,12 +154,12 @@ def config1(nts=2000, seed=1, nshots=16, coarse=8):
     g = 2000.0 + (np.arange(200) - 99.5) * 10.0
     X, Y = np.meshgrid(g, g, indexing="ij")
     rec = (np.full(X.size, 10.0), X.reshape(-1), Y.reshape(-1))
-    return Survey(el, axes, par, src, rec, ricker(nts, dts, 15.0, 1.0 / 15.0), "config1-batched-fwd")
+    return Survey(el, axes, par, src, rec, ricker(nts, dts, 15.0, 1.0 / 15.0), "batched-forward-400x400x300+40")
 
 
-def config_fwi(nzi=300, nxi=300, nyi=300, pad=40, nts=2500, nshots=32, nrec=150, fdom=10.0, seed=3,
+def fwi_gradient_survey(nzi=300, nxi=300, nyi=300, pad=40, nts=2500, nshots=32, nrec=150, fdom=10.0, seed=3,
                true_model=False):
-    """FWI gradient survey (config 3 family): smooth background (vp 2500, vs vp/1.732, rho 2000 with
+    """FWI gradient survey (300^3 interior + 40 sponge by default): smooth background (vp 2500, vs vp/1.732, rho 2000 with
     +-10% smooth perturbations) plus, for the true model, two Gaussian anomalies (+-8% vp/vs, +-3% rho)."""
     d = 10.0
     axes, pads = make_grid(nzi, nxi, nyi, pad, d)

@@ -79,7 +79,7 @@ def test_batched_forward_configuration_two_shots_linear_in_the_source():
     40 samples.  Size-independent checks: the traces are linear in the source signals (scaling by
     -2.5 scales them to 1e-6), finite, non-zero, and differ between the shots."""
     from elasticisolib_3d_b200 import operators as OP
-    sv = S.config1(nts=40, nshots=2)
+    sv = S.batched_forward_survey(nts=40, nshots=2)
     par = sv.par
     za, xa, ya = sv.axes
     ax7 = H.grid_axes(za.n, xa.n, ya.n, za.o, xa.o, ya.o, za.d, xa.d, ya.d)
@@ -105,7 +105,7 @@ def test_plain_forward_configuration_with_free_surface_matches_oracle():
     through the drop-in operator and ElasticDatComp_3D (vx, vy, vz, p), against the oracle's FP32
     pipeline with the same free surface; 60 samples keep the CPU side short."""
     from elasticisolib_3d_b200 import operators as OP
-    sv = S.config0(nts=60)
+    sv = S.plain_forward_survey(nts=60)
     par = sv.par
     assert par.getInt("freeSurface") == 1
     fd = H.FdParam(sv.elastic, sv.axes, par)

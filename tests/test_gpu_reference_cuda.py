@@ -57,7 +57,7 @@ def _ref_nl_forward(lib, dims, reals, med, sig, spos, rpos, nts, dtype):
 @pytest.mark.skipif(not os.path.exists(os.path.join(REF, "libref_nl_f64.so")),
                     reason="the reference's CUDA drivers were not built (make -C oracle ref)")
 def test_plain_forward_matches_reference_cuda_fp64_and_fp32():
-    sv = S.config0(nts=1000)
+    sv = S.plain_forward_survey(nts=1000)
     par = sv.par
     fd = H.FdParam(sv.elastic, sv.axes, par)
     za, xa, ya = sv.axes
