@@ -58,6 +58,10 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--nts", type=int, default=2500)
     ap.add_argument("--interior", type=int, default=300)
+    ap.add_argument("--variant", default="tma", choices=["tma", "plain", "auto"],
+                    help="stepper: tma (8-wide, 2 stages, TMA; default), plain (plain loads, no dual-state "
+                         "adjoint), auto (autotuned)")
+    ap.add_argument("--ckpt", default="auto", choices=["auto", "fp32", "fp16", "bf16"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     return ap.parse_args()
@@ -125,7 +129,8 @@ def build_problem(args, device):
     svt = S.fwi_gradient_survey(nzi=n, nxi=n, nyi=n, nts=args.nts, true_model=True)
     fd = H.FdParam(sv.elastic, sv.axes, sv.par)
     ax7 = H.grid_axes(*(a.n for a in sv.axes), *(a.o for a in sv.axes), *(a.d for a in sv.axes))
-    prob = F.FwiProblem(fd, device=device)
+    variant = {"tma": (8, 2, "tma"), "plain": (8, 2, "plain"), "auto": "auto"}[args.variant]
+    prob = F.FwiProblem(fd, device=device, ckpt=args.ckpt, variant=variant)
     rank = int(os.environ.get("RANK", "0"))
     shot_id = rank % len(sv.src_xyz)
     src = H.build_devices(*sv.src_xyz[shot_id], ax7, fd.nts, sv.par)
@@ -340,7 +345,7 @@ def run_ours(args):
                                       f"components, Ricker 10 Hz, one shot per step per GPU",
                           "parallelism": f"shots sharded over {world} GPU(s)",
                           "l2_flush": "inputs larger than L2 (each field 238 MB, working set > 14 GB)",
-                          "checkpoint_segment_blocks": seg},
+                          "checkpoint_segment_blocks": seg, "stepper": args.variant, "checkpoints": args.ckpt},
                "gcell_updates_per_s": world * args.steps * cell_updates / (ms_max / 1e3) / 1e9,
                "roofline": roofline,
                "gpu_launches": int(launches), "clocks": clk, "e2e": e2e}
