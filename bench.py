@@ -265,6 +265,13 @@ def run_ours(args):
     ms = e0.elapsed_time(e1)
     sampled = {mode: prob.prop.kernel_timing_read(mode) for mode in STEPPER_BYTES}
     prob.prop.kernel_timing(0)
+    stepper_bytes, stepper_names = dict(STEPPER_BYTES), dict(STEPPER_NAMES)
+    if args.variant == "plain":
+        # plain loads: the adjoint runs on the raw state only (medium applied at the halo), no dual level
+        stepper_bytes[5] = 284.0
+        stepper_names = {0: "forward stepper (kStep<0>, plain loads)",
+                         3: "forward stepper + 3-field decimation (kStep<0>, plain loads)",
+                         5: "exact-adjoint stepper + 9-field decimation (kStep<2>, plain loads)"}
     t = torch.tensor([ms], device=device, dtype=torch.float64)
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -321,16 +328,16 @@ def run_ours(args):
         kernels = {}
         for mode, (avg, cnt) in sampled.items():
             traffic_per_cell = None
-            prof = os.path.join(ROOT, PROFILE[mode]) if mode in PROFILE else None
+            prof = os.path.join(ROOT, PROFILE[mode]) if mode in PROFILE and args.variant != "plain" else None
             if prof and os.path.exists(prof):
                 for line in open(prof):
                     if line.startswith("dram_bytes_per_cell:"):
                         traffic_per_cell = float(line.split(":")[1])
-            ach = STEPPER_BYTES[mode] * cells / (avg / 1e3) / 1e9 if avg > 0 else None
-            kernels[mode] = {"kernel": STEPPER_NAMES[mode], "bound": "hbm", "achieved": ach, "peak": peak,
+            ach = stepper_bytes[mode] * cells / (avg / 1e3) / 1e9 if avg > 0 else None
+            kernels[mode] = {"kernel": stepper_names[mode], "bound": "hbm", "achieved": ach, "peak": peak,
                              "peak_source": peak_src, "unit": "GB/s", "frac": (ach / peak) if ach else None,
                              "traffic": traffic_per_cell * cells if traffic_per_cell else None,
-                             "algorithmic_bytes_per_cell": STEPPER_BYTES[mode], "avg_launch_ms": avg,
+                             "algorithmic_bytes_per_cell": stepper_bytes[mode], "avg_launch_ms": avg,
                              "sampled_launches": cnt,
                              "share_of_step_est": avg * launches_per_step[mode] / (ms_max / args.steps)}
         # the dominant kernel: largest estimated share of the step
