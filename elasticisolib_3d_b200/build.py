@@ -15,7 +15,7 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libelastic3d_b200.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 SOURCES = ["engine.cu", "c_abi.cpp", "host_prep.cpp"]
-HEADERS = ["common.cuh", "kernels.cuh", "engine.h"]
+HEADERS = ["common.cuh", "kernels.cuh", "engine.h", "shot_operators.cpp"]
 
 
 def _host_compiler():
@@ -60,7 +60,28 @@ def build(force: bool = False, verbose: bool = False) -> str:
                                                          "-lcudart"]
     subprocess.check_call(cmd)
     os.replace(tmp, LIB)
+    build_operators(ccbin, verbose)
     return LIB
+
+
+def build_operators(cxx=None, verbose=False):
+    """The pybind11 module of the C++ shot operators (csrc/shot_operators.cpp), linked against the
+    library above and loaded from the package directory."""
+    import sysconfig
+
+    import pybind11
+    cxx = cxx or _host_compiler()
+    suffix = sysconfig.get_config_var("EXT_SUFFIX") or ".so"
+    out = os.path.join(HERE, "pyElastic_iso_float_3D" + suffix)
+    cmd = [cxx, "-O3", "-shared", "-fPIC", "-fvisibility=hidden", "-std=c++17", "-I" + pybind11.get_include(),
+           "-I" + sysconfig.get_paths()["include"], "-I" + os.path.join(HERE, "..", "include"),
+           os.path.join(CSRC, "shot_operators.cpp"), "-L" + HERE, "-lelastic3d_b200", "-Wl,-rpath,$ORIGIN",
+           "-o", out + ".tmp"]
+    if verbose:
+        print(" ".join(cmd), file=sys.stderr)
+    subprocess.check_call(cmd)
+    os.replace(out + ".tmp", out)
+    return out
 
 
 if __name__ == "__main__":

@@ -1,0 +1,32 @@
+"""CPU: the C++ operator module loads, and its host parts (parameters, acquisition mapping)
+agree with the Python host preparation bit for bit."""
+import numpy as np
+
+from operator_case import OperatorCase
+from elasticisolib_3d_b200 import hostprep as H
+from elasticisolib_3d_b200 import pyElastic_iso_float_3D as P
+
+
+def _cpp_grids(c):
+    za, xa, ya = c.axes
+    ax7 = H.grid_axes(za.n, xa.n, ya.n, za.o, xa.o, ya.o, za.d, xa.d, ya.d)
+    return [P.hypercube([P.axis(a.n, a.o, a.d) for a in g]) for g in ax7]
+
+
+def test_space_interp_matches_python_host_preparation():
+    c = OperatorCase()
+    par = P.paramObj(dict(c.par))
+    grids = _cpp_grids(c)
+    z, x, y = c.sv.rec_xyz
+    for g in range(7):
+        cpp = P.spaceInterpGpu_3D(z, x, y, grids[g], c.nts, par)
+        np.testing.assert_array_equal(np.asarray(cpp.getRegPosUnique()), c.rec_dev[g].getRegPosUnique())
+        assert cpp.getNDeviceIrreg() == c.rec_dev[g].getNDeviceIrreg()
+
+
+def test_param_object_defaults():
+    par = P.paramObj({"nts": 12, "dts": 0.002})
+    assert par.getInt("nts") == 12
+    assert abs(par.getFloat("dts") - 0.002) < 1e-9
+    assert par.getInt("nGpu", 1) == 1
+    assert par.getString("iGpu", "-1") == "-1"
