@@ -24,8 +24,13 @@ def _host_compiler():
     return "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else shutil.which("g++")
 
 
+def _operators_module():
+    import sysconfig
+    return os.path.join(HERE, "pyElastic_iso_float_3D" + (sysconfig.get_config_var("EXT_SUFFIX") or ".so"))
+
+
 def _stale():
-    if not os.path.exists(LIB):
+    if not os.path.exists(LIB) or not os.path.exists(_operators_module()):
         return True
     t = os.path.getmtime(LIB)
     deps = [os.path.join(CSRC, f) for f in SOURCES + HEADERS]
@@ -71,8 +76,7 @@ def build_operators(cxx=None, verbose=False):
 
     import pybind11
     cxx = cxx or _host_compiler()
-    suffix = sysconfig.get_config_var("EXT_SUFFIX") or ".so"
-    out = os.path.join(HERE, "pyElastic_iso_float_3D" + suffix)
+    out = _operators_module()
     cmd = [cxx, "-O3", "-shared", "-fPIC", "-fvisibility=hidden", "-std=c++17", "-I" + pybind11.get_include(),
            "-I" + sysconfig.get_paths()["include"], "-I" + os.path.join(HERE, "..", "include"),
            os.path.join(CSRC, "shot_operators.cpp"), "-L" + HERE, "-lelastic3d_b200", "-Wl,-rpath,$ORIGIN",
