@@ -44,10 +44,13 @@ def test_fwi_gradient_matches_fp64_oracle(ckpt, segment, variant, velocity, tol)
     if velocity != "auto":
         assert prob.prop.velocity_storage == velocity
     g = np.stack([x.grad.double().cpu().numpy() for x in m])
+    errs = [float(np.linalg.norm(g[k] - g_ref[k]) / np.linalg.norm(g_ref[k])) for k in range(3)]
+    print(f"plan ckpt={ckpt} segment={segment} velocity={prob.prop.velocity_storage}: misfit rel err "
+          f"{abs(loss.item() - loss_ref) / loss_ref:.2e}, gradient rel err rho {errs[0]:.2e} lambda {errs[1]:.2e} "
+          f"mu {errs[2]:.2e}", flush=True)
     assert abs(loss.item() - loss_ref) / loss_ref < 1e-4
     for k in range(3):
-        err = np.linalg.norm(g[k] - g_ref[k]) / np.linalg.norm(g_ref[k])
-        assert err < tol, (k, err)
+        assert errs[k] < tol, (k, errs[k])
 
 
 def test_predicted_traces_match_fp64_oracle():

@@ -107,3 +107,86 @@ def test_plain_forward_matches_reference_cuda_fp64_and_fp32():
                       "rel_l2_vs_ref_fp64": e64, "rel_l2_vs_ref_fp32": e32}), flush=True)
     assert e64 < 1e-5
     assert e32 < 1e-5
+
+
+@pytest.mark.skipif(not os.path.exists(os.path.join(REF, "libref_born_f32.so")),
+                    reason="the reference's CUDA drivers were not built (make -C oracle ref)")
+def test_born_matches_reference_cuda_fp32_and_times_both():
+    """Born forward and adjoint against the reference's FP32 CUDA drivers on an 80^3 interior + 16
+    sponge grid (120^3 cells), 400 samples (1596 fine steps), explosive source, 20 x 20 receivers:
+    data within 1e-5 and image within 1e-4 relative L2 (the image multiplies two propagated fields).
+    The reference stores the source wavefield in pinned host memory (3*N*nts floats, 8.3 GB here)
+    and streams it back for the adjoint; this library recomputes it from on-device checkpoints.
+    With -s the test prints the end-to-end time of each call on both sides."""
+    d = 10.0
+    axes, pads = S.make_grid(80, 80, 80, 16, d)
+    shape = (axes[2].n, axes[1].n, axes[0].n)
+    vp, vs, rho = S.gaussian_perturbed_model(shape, 2500.0, 2500.0 / 1.732, 2000.0, 0.10, 4.0, 5)
+    el = S.elastic_from_velocity(vp, vs, rho)
+    par = S.base_params(axes, pads, 400, 0.002, 2, 40.0)
+    fd = H.FdParam(el, axes, par)
+    za, xa, ya = axes
+    ax7 = H.grid_axes(za.n, xa.n, ya.n, za.o, xa.o, ya.o, za.d, xa.d, ya.d)
+    src = H.build_devices(np.array([300.0]), np.array([400.0]), np.array([400.0]), ax7, fd.nts, par)
+    g = np.linspace(100.0, 700.0, 20)
+    X, Y = np.meshgrid(g, g, indexing="ij")
+    rec = H.build_devices(np.full(X.size, 20.0), X.ravel(), Y.ravel(), ax7, fd.nts, par)
+    spos = [x.getRegPosUnique() for x in src]
+    rpos = [x.getRegPosUnique() for x in rec]
+    irr = [np.zeros((1, fd.nts), np.float32) for _ in range(9)]
+    for k in (3, 4, 5):
+        irr[k][0] = S.ricker(fd.nts, 0.002, 15.0, 1.0 / 15.0)
+    sig = [src[COMP_GRID[k]].adjoint(False, None, irr[k]) for k in range(9)]
+    OP.scale_signals(sig, src, fd.planes, fd.dx, fd.dy, fd.dz)
+    rng = np.random.default_rng(9)
+    mask = rng.random(shape) < 0.01
+    pert = np.zeros((8,) + shape, np.float32)
+    for k in range(8):
+        pert[k][mask] = (0.05 * rng.uniform(-1, 1, mask.sum()) * np.abs(fd.planes[k][mask])).astype(np.float32)
+    dat = [rng.standard_normal((len(rpos[COMP_GRID[k]]), fd.nts)).astype(np.float32) for k in range(9)]
+
+    pr = Propagator(fd.nz, fd.nx, fd.ny, fd.nts, fd.sub, fd.minPad, float(fd.dz), float(fd.dx), float(fd.dy),
+                    float(fd.dts), float(fd.alphaCos))
+    pr.set_medium(fd.planes)
+    pr.born_forward(sig, pert, spos, rpos)  # warm-up
+    t0 = time.perf_counter()
+    ours_d = pr.born_forward(sig, pert, spos, rpos)
+    t_fwd = time.perf_counter() - t0
+    pr.born_adjoint(sig, dat, spos, rpos)  # warm-up
+    t0 = time.perf_counter()
+    ours_g = pr.born_adjoint(sig, dat, spos, rpos)
+    t_adj = time.perf_counter() - t0
+
+    lib = ctypes.CDLL(os.path.join(REF, "libref_born_f32.so"))
+    dims = (ctypes.c_int * 6)(fd.nz, fd.nx, fd.ny, fd.nts, fd.sub, fd.minPad)
+    reals = (ctypes.c_double * 5)(float(fd.dz), float(fd.dx), float(fd.dy), float(fd.dts), float(fd.alphaCos))
+    med = [np.ascontiguousarray(m) for m in fd.planes]
+    sp = [np.ascontiguousarray(x, dtype=np.int64) for x in spos]
+    rp = [np.ascontiguousarray(x, dtype=np.int64) for x in rpos]
+    sn = (ctypes.c_longlong * 7)(*[len(x) for x in sp])
+    rn = (ctypes.c_longlong * 7)(*[len(x) for x in rp])
+    sg = [np.ascontiguousarray(x) for x in sig]
+
+    def ref(adjoint, data, pp):
+        t0 = time.perf_counter()
+        st = lib.ref_born_run(adjoint, dims, reals, _pp(med), _pp(sg), _pp(data), _pp(sp), sn, _pp(rp), rn, _pp(pp))
+        assert st == 0
+        return time.perf_counter() - t0
+
+    ref_d = [np.zeros((len(rpos[COMP_GRID[k]]), fd.nts), np.float32) for k in range(9)]
+    pp_in = [np.ascontiguousarray(pert[k]) for k in range(8)]
+    r_fwd = ref(0, ref_d, pp_in)
+    ref_g = [np.zeros(shape, np.float32) for _ in range(8)]
+    r_adj = ref(1, [np.ascontiguousarray(x) for x in dat], ref_g)
+
+    def rel(a, b):
+        a = np.concatenate([np.asarray(x, np.float64).ravel() for x in a])
+        b = np.concatenate([np.asarray(x, np.float64).ravel() for x in b])
+        return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+    e_d, e_g = rel(ours_d, ref_d), rel(ours_g, ref_g)
+    print(json.dumps({"workload": f"Born {fd.nz}x{fd.nx}x{fd.ny}, {fd.nts} samples", "ours_fwd_s": t_fwd,
+                      "ours_adj_s": t_adj, "reference_fp32_fwd_s": r_fwd, "reference_fp32_adj_s": r_adj,
+                      "rel_l2_data": e_d, "rel_l2_image": e_g}), flush=True)
+    assert e_d < 1e-5
+    assert e_g < 1e-4
