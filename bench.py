@@ -50,6 +50,15 @@ PROFILE = {5: "profiles/kStepTma_adjoint_decimated_392x392x104.txt",
            0: "profiles/kStepTma_forward_392x392x104.txt"}
 
 
+def recomputed_blocks(blocks, seg):
+    """Source blocks the gradient's adjoint pass recomputes: every checkpoint segment but the last
+    (segments of `seg` blocks aligned to the end of the record), each from the block before it
+    (none before the first) to two blocks past its end."""
+    nseg = -(-blocks // seg)
+    start = [max(0, blocks - (nseg - s) * seg) for s in range(nseg + 1)]
+    return sum(min(start[s + 1] + 1, blocks - 1) - (start[s] - 1 if s else 0) + 1 for s in range(nseg - 1))
+
+
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -62,6 +71,9 @@ def parse():
                     help="stepper: tma (8-wide, 2 stages, TMA; default), plain (plain loads, no dual-state "
                          "adjoint), auto (autotuned)")
     ap.add_argument("--ckpt", default="auto", choices=["auto", "fp32", "fp16", "bf16"])
+    ap.add_argument("--velocity", default="auto", choices=["auto", "fp32", "fp16"],
+                    help="storage of the decimated source velocity slots (fp32 with --ckpt fp32: the "
+                         "all-FP32 plan)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     return ap.parse_args()
@@ -130,7 +142,7 @@ def build_problem(args, device):
     fd = H.FdParam(sv.elastic, sv.axes, sv.par)
     ax7 = H.grid_axes(*(a.n for a in sv.axes), *(a.o for a in sv.axes), *(a.d for a in sv.axes))
     variant = {"tma": (8, 2, "tma"), "plain": (8, 2, "plain"), "auto": "auto"}[args.variant]
-    prob = F.FwiProblem(fd, device=device, ckpt=args.ckpt, variant=variant)
+    prob = F.FwiProblem(fd, device=device, ckpt=args.ckpt, variant=variant, velocity=args.velocity)
     rank = int(os.environ.get("RANK", "0"))
     shot_id = rank % len(sv.src_xyz)
     src = H.build_devices(*sv.src_xyz[shot_id], ax7, fd.nts, sv.par)
@@ -319,14 +331,18 @@ def run_ours(args):
         else:
             peak, peak_src = 6650.0, "fallback"
         steps_per_pass = (fd.nts - 1) * fd.sub
-        seg = prob.prop.checkpoint_segment
-        nseg = -(-(fd.nts - 1) // seg) if seg else 1
-        # forward + recompute (one extra block per segment and up to two past its end) + adjoint
-        recompute_blocks = (fd.nts - 1) + 3 * (nseg - 1)
+        blocks = fd.nts - 1
+        seg = prob.prop.checkpoint_segment or blocks
+        recompute_blocks = recomputed_blocks(blocks, seg)
+        # the forward pass decimates from the block before the last segment on
+        plain_fwd = max(blocks - seg - 1, 0) if seg < blocks else 0
         cell_updates = cells * (steps_per_pass + recompute_blocks * fd.sub + steps_per_pass)
-        launches_per_step = {0: steps_per_pass, 3: recompute_blocks * fd.sub, 5: steps_per_pass}
+        launches_per_step = {0: plain_fwd * fd.sub, 3: (blocks - plain_fwd + recompute_blocks) * fd.sub,
+                             5: steps_per_pass}
         kernels = {}
         for mode, (avg, cnt) in sampled.items():
+            if cnt == 0:
+                continue  # e.g. the plain forward stepper when the whole record is decimated in the forward pass
             traffic_per_cell = None
             prof = os.path.join(ROOT, PROFILE[mode]) if mode in PROFILE and args.variant != "plain" else None
             if prof and os.path.exists(prof):
@@ -352,7 +368,8 @@ def run_ours(args):
                                       f"components, Ricker 10 Hz, one shot per step per GPU",
                           "parallelism": f"shots sharded over {world} GPU(s)",
                           "l2_flush": "inputs larger than L2 (each field 238 MB, working set > 14 GB)",
-                          "checkpoint_segment_blocks": seg, "stepper": args.variant, "checkpoints": args.ckpt},
+                          "checkpoint_segment_blocks": seg, "stepper": args.variant, "checkpoints": prob.prop.checkpoint_type,
+                          "velocity_slots": prob.prop.velocity_storage},
                "gcell_updates_per_s": world * args.steps * cell_updates / (ms_max / 1e3) / 1e9,
                "roofline": roofline,
                "gpu_launches": int(launches), "clocks": clk, "e2e": e2e}

@@ -66,6 +66,7 @@ SIGNATURES = {
     "e3d_nl_propagate_device_noalloc": ([P, P, I, P, P, P, P, P, P, P], I),
     "e3d_noalloc_work_bytes": ([], ctypes.c_size_t),
     "e3d_velocity_storage": ([P], I),
+    "e3d_checkpoint_type": ([P], I),
     "e3d_step_only": ([P, I, I], I),
     "e3d_kernel_timing": ([P, I], I),
     "e3d_kernel_timing_read": ([P, I, P, P], I),

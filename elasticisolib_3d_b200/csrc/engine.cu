@@ -100,6 +100,7 @@ struct Context {
   int ckptSegLen = 0;
   int ckptAllocType = -1;
   bool ckptValid = false;
+  bool tailValid = false;    // the last segment's velocity slots were filled by the forward pass
   // scratch for transposes / signal staging
   void* scratch = nullptr;
   size_t scratchBytes = 0;
@@ -273,6 +274,7 @@ int setMedium(Context* c, const float* const* planes, bool onDevice) {
   E3D_CUDA_TRY(cudaStreamSynchronize(c->st));
   c->haveMedium = true;
   c->ckptValid = false;
+  c->tailValid = false;
   return E3D_OK;
 }
 
@@ -314,6 +316,7 @@ int setCheckpointPolicy(Context* c, int type, int segment, double budget) {
   c->segment = segment;
   c->budget = budget;
   c->ckptValid = false;
+  c->tailValid = false;
   return E3D_OK;
 }
 
@@ -1053,30 +1056,35 @@ static int ensureVSlots(Context* c, int nslots) {
 
 static float* vComp(float* slot, int k, long long n) { return slot ? slot + (size_t)k * n : nullptr; }
 
+// Decimation of the damped velocity of fine step it2 of a source block into
+// vLeft (weight f[it2]) and vRight (weight f[h+it2]); with vLeft null only the
+// right slot accumulates (interpWavefieldVxVyVz_3D, kernelsElaGpu_3D.cu:1646-1672).
+static void setSourceAcc(const Context* c, StepPtrs& p, int it2, float* vLeft, float* vRight) {
+  const long long n = c->g.n;
+  for (int k = 0; k < 3; k++) {
+    p.accL[k] = vComp(vLeft, k, n);
+    p.accR[k] = vComp(vRight, k, n);
+  }
+  if (!vLeft) {  // only the right accumulator is wanted
+    for (int k = 0; k < 3; k++) {
+      p.accL[k] = p.accR[k];
+      p.accR[k] = nullptr;
+    }
+    p.accWl = c->filt[c->hfilt + it2];
+  } else {
+    p.accWl = c->filt[it2];
+    p.accWr = c->filt[c->hfilt + it2];
+  }
+  p.nAcc = 3;
+}
+
 // One coarse block (its) of the source-side forward propagation on state
-// (s0,s1), injecting srcSig and decimating the damped velocity into vLeft
-// (weight f[it2]) and vRight (weight f[h+it2])
-// (interpWavefieldVxVyVz_3D, kernelsElaGpu_3D.cu:1646-1672).
+// (s0,s1), injecting srcSig and decimating into vLeft / vRight.
 static int sourceBlock(Context* c, int its, const DevSignals& srcSet, const float* srcSig, float* vLeft,
                        float* vRight) {
-  const long long n = c->g.n;
   for (int it2 = 1; it2 <= c->d.sub; it2++) {
     StepPtrs p = makeStep(c, c->s0, c->s1);
-    for (int k = 0; k < 3; k++) {
-      p.accL[k] = vComp(vLeft, k, n);
-      p.accR[k] = vComp(vRight, k, n);
-    }
-    if (!vLeft) {  // only the right accumulator is wanted
-      for (int k = 0; k < 3; k++) {
-        p.accL[k] = p.accR[k];
-        p.accR[k] = nullptr;
-      }
-      p.accWl = c->filt[c->hfilt + it2];
-    } else {
-      p.accWl = c->filt[it2];
-      p.accWr = c->filt[c->hfilt + it2];
-    }
-    p.nAcc = 3;
+    setSourceAcc(c, p, it2, vLeft, vRight);
     E3D_RET(launchStep(c, STEP_FWD, p));
     E3D_RET(launchInject(c, p, srcSet, srcSig, its, it2 - 1));
     swapF(c->s0, c->s1);
@@ -1126,6 +1134,7 @@ static int bornForwardDevice(Context* c, const DevSignals& srcSet, const DevSign
   E3D_RET(allocFields(c, c->ss[0], true));
   E3D_RET(allocFields(c, c->ss[1], true));
   E3D_RET(ensureVSlots(c, 4));
+  c->tailValid = false;  // the rotating slots overwrite a kept source segment
   for (int i = 0; i < 4; i++)
     E3D_CUDA_TRY(cudaMemsetAsync(c->vSlots[i], 0, (size_t)3 * c->g.n * sizeof(float), c->st));
   E3D_CUDA_TRY(cudaMemsetAsync(recSig, 0, (size_t)std::max(recSet.off[NCOMP], 1) * nts * sizeof(float), c->st));
@@ -1169,16 +1178,39 @@ static int bornForwardDevice(Context* c, const DevSignals& srcSet, const DevSign
 
 // ---------------------------------------------------------------------------
 // Checkpointed source wavefield for the Born adjoint / FWI gradient.
-// A checkpoint for segment s (coarse blocks [s*L, s*L+L)) holds the
-// source-side state at the start of block s*L-1; recomputing from it yields
-// V[s*L] complete (its right-weight part comes from block s*L-1).
+// The blocks are cut into segments of L blocks aligned to the END of the
+// record: segment s covers [segStart(s), segStart(s+1)) and the first segment
+// holds the remainder.  A checkpoint for segment s >= 1 holds the source-side
+// state at the start of block segStart(s)-1; recomputing from it yields
+// V[segStart(s)] complete (its right-weight part comes from that block).
+// The forward pass decimates the last segment's velocity into the slots as it
+// goes, so the adjoint pass recomputes every segment but the last (which is
+// the longest, hence the end alignment).
 // The plan (segment length, checkpoint storage, velocity-slot storage) is
-// the first that fits the memory budget among
+// chosen among
 //   FP32 states + FP32 velocity slots, FP16 states + FP32 slots,
 //   FP16 states + FP16 slots (auto); for an explicit state type T:
-//   T + FP32 slots, T + FP16 slots.
+//   T + FP32 slots, T + FP16 slots;
+// each at the longest segment that fits the memory budget, taking the plan
+// that recomputes the fewest blocks once a lower-precision plan is charged a
+// margin (5% of the blocks for 16-bit states, 15% for 16-bit slots): a
+// 16-bit plan is taken only where it removes that much recomputation.
 // ---------------------------------------------------------------------------
 enum { V_F32 = 0, V_F16 = 1 };
+
+static int segStart(int blocks, int L, int nseg, int s) { return std::max(0, blocks - (nseg - s) * L); }
+
+// Source blocks the adjoint pass recomputes: every segment but the last, each
+// from the block before it (none before the first) to two blocks past its end.
+static int recomputedBlocks(int blocks, int L) {
+  const int nseg = (blocks + L - 1) / L;
+  int r = 0;
+  for (int s = 0; s + 1 < nseg; s++) {
+    const int b0 = s == 0 ? 0 : segStart(blocks, L, nseg, s) - 1;
+    r += std::min(segStart(blocks, L, nseg, s + 1) + 1, blocks - 1) - b0 + 1;
+  }
+  return r;
+}
 
 static size_t ckptBytesPerState(const Context* c, int type) {
   const size_t eb = type == CKPT_F32 ? 4 : 2;
@@ -1251,26 +1283,36 @@ static int choosePlan(Context* c, int& L) {
   E3D_CUDA_TRY(cudaMemGetInfo(&free, &total));
   // memory this context already holds for checkpoints and velocity slots counts as available
   const double budget = autoBudget(c, free) + heldBytes(c);
+  if (c->segment > 0) {
+    // explicit segment length: the first candidate that fits it, else the last
+    const int l = std::min(c->segment, blocks);
+    for (size_t i = 0; i < cands.size(); i++)
+      if (planBytes(c, cands[i].ck, cands[i].vt, l) <= budget || i + 1 == cands.size()) {
+        c->ckptUsed = cands[i].ck;
+        c->vUsed = cands[i].vt;
+        L = l;
+        return E3D_OK;
+      }
+  }
+  int best = -1;
+  double bestCost = 0;
   for (size_t i = 0; i < cands.size(); i++) {
     const Cand& k = cands[i];
-    if (c->segment > 0) {
-      const int l = std::min(c->segment, blocks);
-      if (planBytes(c, k.ck, k.vt, l) <= budget || i + 1 == cands.size()) {
-        c->ckptUsed = k.ck;
-        c->vUsed = k.vt;
-        L = l;
-        return E3D_OK;
-      }
-      continue;
+    int l = blocks;
+    while (l >= 1 && planBytes(c, k.ck, k.vt, l) > budget) l--;
+    if (l < 1) continue;
+    const double cost = recomputedBlocks(blocks, l) + blocks * ((k.ck != CKPT_F32 ? 0.05 : 0.0) +
+                                                                (k.vt == V_F16 ? 0.15 : 0.0));
+    if (best < 0 || cost < bestCost) {
+      best = (int)i;
+      bestCost = cost;
+      L = l;
     }
-    // one extra source block is recomputed per segment: take the longest segment that fits
-    for (int l = blocks; l >= 1; l--)
-      if (planBytes(c, k.ck, k.vt, l) <= budget) {
-        c->ckptUsed = k.ck;
-        c->vUsed = k.vt;
-        L = l;
-        return E3D_OK;
-      }
+  }
+  if (best >= 0) {
+    c->ckptUsed = cands[best].ck;
+    c->vUsed = cands[best].vt;
+    return E3D_OK;
   }
   setLastError("wavefield checkpoints do not fit in device memory", __FILE__, __LINE__);
   return E3D_ERR_OOM;
@@ -1294,42 +1336,62 @@ static int resizeVStorage(Context* c, int nF32, int nF16) {
   return E3D_OK;
 }
 
+// Grid of the slice kernels for nf consecutive fields: each block covers
+// kSliceThreads * kSliceVecPerThread * 4 values of one y slice.
+static dim3 sliceGrid(const Context* c, int nf) {
+  const long long per = (long long)kSliceThreads * kSliceVecPerThread * 4;
+  return dim3((unsigned)((c->g.yStride + per - 1) / per), (unsigned)c->d.ny, (unsigned)nf);
+}
+
+// Four-wide slice access: slices and fields start on 4-value boundaries and
+// the FP32 and 16-bit arrays are 16- and 8-byte aligned.
+static bool sliceVec(const Context* c, const void* f32, const void* h16) {
+  return c->g.yStride % 4 == 0 && c->g.n % 4 == 0 && (uintptr_t)f32 % 16 == 0 && (uintptr_t)h16 % 8 == 0;
+}
+
+// Scaled 16-bit copy of nf consecutive fields of n values: slice maxima into
+// the scratch, then the packed values and one unscaling factor per (field, y).
+template <typename H>
+static int packSlices(Context* c, const float* a, int nf, int topExp, H* out, float* scales) {
+  const long long n = c->g.n, ys = c->g.yStride;
+  float* smax = (float*)c->scratch;
+  const dim3 grid = sliceGrid(c, nf);
+  const bool vec = sliceVec(c, a, out);
+  E3D_CUDA_TRY(cudaMemsetAsync(smax, 0, (size_t)nf * c->d.ny * sizeof(float), c->st));
+  c->launches += 2;
+  if (vec) kSliceMaxAbs<true><<<grid, kSliceThreads, 0, c->st>>>(a, n, ys, smax);
+  else kSliceMaxAbs<false><<<grid, kSliceThreads, 0, c->st>>>(a, n, ys, smax);
+  E3D_LAUNCH_CHECK();
+  if (vec) kPackSlices<H, true><<<grid, kSliceThreads, 0, c->st>>>(a, n, ys, smax, topExp, out, scales);
+  else kPackSlices<H, false><<<grid, kSliceThreads, 0, c->st>>>(a, n, ys, smax, topExp, out, scales);
+  E3D_LAUNCH_CHECK();
+  return E3D_OK;
+}
+
+template <typename H>
+static int unpackSlices(Context* c, const H* in, int nf, const float* scales, float* a) {
+  const long long n = c->g.n, ys = c->g.yStride;
+  const dim3 grid = sliceGrid(c, nf);
+  c->launches++;
+  if (sliceVec(c, a, in)) kUnpackSlices<H, true><<<grid, kSliceThreads, 0, c->st>>>(in, n, ys, scales, a);
+  else kUnpackSlices<H, false><<<grid, kSliceThreads, 0, c->st>>>(in, n, ys, scales, a);
+  E3D_LAUNCH_CHECK();
+  return E3D_OK;
+}
+
 // Per-(field, y-slice) scaled FP16 copy of the three velocity fields of slot v.
 static int packVelocity(Context* c, const float* v, void* store) {
-  const long long n = c->g.n, ys = c->g.yStride;
-  const int ny = c->d.ny;
-  __half* h = (__half*)store;
   float* scales = (float*)((char*)store + vHalfBytes(c));
-  float* smax = (float*)c->scratch;
-  const unsigned blocks = (unsigned)((n + 255) / 256);
-  for (int k = 0; k < 3; k++) {
-    c->launches += 2;
-    kSliceMaxAbs<<<ny, 256, 0, c->st>>>(v + (size_t)k * n, ys, smax);
-    E3D_LAUNCH_CHECK();
-    kPackSlices<__half><<<blocks, 256, 0, c->st>>>(v + (size_t)k * n, ys, n, smax, 14, h + (size_t)k * n,
-                                                   scales + (size_t)k * ny);
-    E3D_LAUNCH_CHECK();
-  }
-  return E3D_OK;
+  return packSlices(c, v, 3, 14, (__half*)store, scales);
 }
 
 static int unpackVelocity(Context* c, const void* store, float* v) {
-  const long long n = c->g.n, ys = c->g.yStride;
-  const int ny = c->d.ny;
-  const __half* h = (const __half*)store;
   const float* scales = (const float*)((const char*)store + vHalfBytes(c));
-  const unsigned blocks = (unsigned)((n + 255) / 256);
-  for (int k = 0; k < 3; k++) {
-    c->launches++;
-    kUnpackSlices<__half><<<blocks, 256, 0, c->st>>>(h + (size_t)k * n, ys, n, scales + (size_t)k * ny,
-                                                     v + (size_t)k * n);
-    E3D_LAUNCH_CHECK();
-  }
-  return E3D_OK;
+  return unpackSlices(c, (const __half*)store, 3, scales, v);
 }
 
 static int packState(Context* c, int seg) {
-  const long long n = c->g.n, ys = c->g.yStride;
+  const long long n = c->g.n;
   const int ny = c->d.ny;
   Fields9* parts[2] = {&c->s0, &c->s1};
   if (c->ckptUsed == CKPT_F32) {
@@ -1341,48 +1403,34 @@ static int packState(Context* c, int seg) {
     return E3D_OK;
   }
   float* scales = c->ckptScale[seg];
-  float* smax = (float*)c->scratch;
   for (int h = 0; h < 2; h++)
     for (int k = 0; k < NCOMP; k++) {
       const int f = h * NCOMP + k;
-      c->launches += 2;
-      kSliceMaxAbs<<<ny, 256, 0, c->st>>>(parts[h]->p[k], ys, smax);
-      E3D_LAUNCH_CHECK();
-      const unsigned blocks = (unsigned)((n + 255) / 256);
       if (c->ckptUsed == CKPT_F16)
-        kPackSlices<__half><<<blocks, 256, 0, c->st>>>(parts[h]->p[k], ys, n, smax, 14,
-                                                       (__half*)c->ckpt[seg] + (size_t)f * n, scales + (size_t)f * ny);
+        E3D_RET(packSlices(c, parts[h]->p[k], 1, 14, (__half*)c->ckpt[seg] + (size_t)f * n, scales + (size_t)f * ny));
       else
-        kPackSlices<__nv_bfloat16><<<blocks, 256, 0, c->st>>>(parts[h]->p[k], ys, n, smax, 0,
-                                                              (__nv_bfloat16*)c->ckpt[seg] + (size_t)f * n,
-                                                              scales + (size_t)f * ny);
-      E3D_LAUNCH_CHECK();
+        E3D_RET(packSlices(c, parts[h]->p[k], 1, 0, (__nv_bfloat16*)c->ckpt[seg] + (size_t)f * n,
+                           scales + (size_t)f * ny));
     }
   return E3D_OK;
 }
 
 static int unpackState(Context* c, int seg) {
-  const long long n = c->g.n, ys = c->g.yStride;
+  const long long n = c->g.n;
   const int ny = c->d.ny;
   Fields9* parts[2] = {&c->s0, &c->s1};
   for (int h = 0; h < 2; h++)
     for (int k = 0; k < NCOMP; k++) {
       const int f = h * NCOMP + k;
-      if (c->ckptUsed == CKPT_F32) {
+      if (c->ckptUsed == CKPT_F32)
         E3D_CUDA_TRY(cudaMemcpyAsync(parts[h]->p[k], (float*)c->ckpt[seg] + (size_t)f * n, n * sizeof(float),
                                      cudaMemcpyDeviceToDevice, c->st));
-      } else {
-        const unsigned blocks = (unsigned)((n + 255) / 256);
-        c->launches++;
-        if (c->ckptUsed == CKPT_F16)
-          kUnpackSlices<__half><<<blocks, 256, 0, c->st>>>((const __half*)c->ckpt[seg] + (size_t)f * n, ys, n,
-                                                           c->ckptScale[seg] + (size_t)f * ny, parts[h]->p[k]);
-        else
-          kUnpackSlices<__nv_bfloat16><<<blocks, 256, 0, c->st>>>(
-              (const __nv_bfloat16*)c->ckpt[seg] + (size_t)f * n, ys, n, c->ckptScale[seg] + (size_t)f * ny,
-              parts[h]->p[k]);
-        E3D_LAUNCH_CHECK();
-      }
+      else if (c->ckptUsed == CKPT_F16)
+        E3D_RET(unpackSlices(c, (const __half*)c->ckpt[seg] + (size_t)f * n, 1, c->ckptScale[seg] + (size_t)f * ny,
+                             parts[h]->p[k]));
+      else
+        E3D_RET(unpackSlices(c, (const __nv_bfloat16*)c->ckpt[seg] + (size_t)f * n, 1,
+                             c->ckptScale[seg] + (size_t)f * ny, parts[h]->p[k]));
     }
   return E3D_OK;
 }
@@ -1408,7 +1456,7 @@ static int prepareCheckpoints(Context* c, int& L, int& nseg) {
     }
     c->ckptSegLen = L;
   }
-  E3D_RET(scratchAtLeast(c, (size_t)c->d.ny * sizeof(float)));
+  E3D_RET(scratchAtLeast(c, (size_t)3 * c->d.ny * sizeof(float)));  // slice maxima of three fields
   return E3D_OK;
 }
 
@@ -1441,17 +1489,22 @@ static int traceSpread(Context* c, const TraceMap& m, int nReg, const float* irr
 }
 
 // Source-side forward pass over all coarse blocks, saving the state at the
-// start of block s*L-1 for every segment s >= 1.  When recSig is non-null the
+// start of block segStart(s)-1 for every segment s >= 1 and decimating the
+// velocity of the last segment into the velocity slots (the adjoint pass
+// then starts without recomputing it).  When recSig is non-null the
 // receivers are recorded too (this is the nonlinear forward of FWI): into a
 // time-major regular-grid array, or, with a trace map, through a two-slice
 // ring converted to irregular traces as each coarse slice completes.
 static int sourcePassWithCheckpoints(Context* c, const DevSignals& srcSet, const DevSignals* recSet,
                                      const float* srcSig, float* recSig, const TraceMap* map) {
   int L = 0, nseg = 0;
+  c->ckptValid = false;
+  c->tailValid = false;
   E3D_RET(prepareCheckpoints(c, L, nseg));
   E3D_RET(allocFields(c, c->s0, true));
   E3D_RET(allocFields(c, c->s1, true));
-  const int nts = c->d.nts, sub = c->d.sub;
+  const int nts = c->d.nts, sub = c->d.sub, blocks = nts - 1;
+  const long long n = c->g.n;
   const size_t nr = recSet ? (size_t)recSet->off[NCOMP] : 0;
   const size_t rows = map ? (size_t)NCOMP * map->nIrreg : 0;
   float* ring = nullptr;
@@ -1462,15 +1515,35 @@ static int sourcePassWithCheckpoints(Context* c, const DevSignals& srcSet, const
   } else if (recSig) {
     E3D_CUDA_TRY(cudaMemsetAsync(recSig, 0, std::max<size_t>(nr, 1) * nts * sizeof(float), c->st));
   }
-  for (int b = 0; b < nts - 1; b++) {
-    if ((b + 1) % L == 0 && (b + 1) / L < nseg) E3D_RET(packState(c, (b + 1) / L));
+  // the last segment's velocity V[tailBeg .. nts-1], laid out as the adjoint
+  // pass's recomputation lays it out (FP32: one slot per time; FP16: a
+  // two-slot FP32 ring packed into the FP16 slots as each time completes)
+  const bool vc = c->vUsed == V_F16;
+  const int tailBeg = segStart(blocks, L, nseg, nseg - 1);
+  auto A = [&](int t) -> float* {
+    if (t < tailBeg || t >= nts) return nullptr;
+    return vc ? c->vSlots[(t - tailBeg) % 2] : c->vSlots[t - tailBeg];
+  };
+  const int nClear = vc ? 2 : nts - tailBeg;
+  for (int i = 0; i < nClear; i++)
+    E3D_CUDA_TRY(cudaMemsetAsync(c->vSlots[i], 0, (size_t)3 * n * sizeof(float), c->st));
+  int nextCk = 1;
+  for (int b = 0; b < blocks; b++) {
+    if (nextCk < nseg && b == segStart(blocks, L, nseg, nextCk) - 1) E3D_RET(packState(c, nextCk++));
+    const bool decimate = b >= tailBeg - 1;  // block tailBeg-1 feeds V[tailBeg] through its right weights
     for (int it2 = 1; it2 <= sub; it2++) {
       StepPtrs p = makeStep(c, c->s0, c->s1);
+      if (decimate) setSourceAcc(c, p, it2, A(b), A(b + 1));
       E3D_RET(launchStep(c, STEP_FWD, p));
       E3D_RET(launchInject(c, p, srcSet, srcSig, b, it2 - 1));
       if (ring) E3D_RET(launchRecordSlices(c, p, *recSet, ring + (b % 2) * nr, ring + ((b + 1) % 2) * nr, it2));
       else if (recSig) E3D_RET(launchRecord(c, p, *recSet, recSig, b, it2));
       swapF(c->s0, c->s1);
+    }
+    if (vc && b >= tailBeg) {
+      // V[b] is complete: store it and reuse its slot for V[b+2]
+      E3D_RET(packVelocity(c, A(b), c->vStore[b - tailBeg]));
+      E3D_CUDA_TRY(cudaMemsetAsync(A(b), 0, (size_t)3 * n * sizeof(float), c->st));
     }
     if (ring) {
       // slice b is complete; its ring slot is reused for slice b+2
@@ -1478,14 +1551,18 @@ static int sourcePassWithCheckpoints(Context* c, const DevSignals& srcSet, const
       if (nr) E3D_CUDA_TRY(cudaMemsetAsync(ring + (b % 2) * nr, 0, nr * sizeof(float), c->st));
     }
   }
+  // V[nts-1] has no block of its own: complete after block nts-2
+  if (vc) E3D_RET(packVelocity(c, A(nts - 1), c->vStore[nts - 1 - tailBeg]));
   if (ring) E3D_RET(traceGather(c, *map, (int)nr, ring + ((nts - 1) % 2) * nr, recSig + (size_t)(nts - 1) * rows));
   c->ckptValid = true;
+  c->tailValid = true;
   return E3D_OK;
 }
 
 // Adjoint pass (BornElasticAdjGpu_3D phase B) consuming the checkpoints:
 // segments are processed last to first; each recomputes its velocity slots
-// from its checkpoint, then runs its adjoint blocks and imaging.  With a
+// from its checkpoint (the last one only when the forward pass's copy has been
+// overwritten since), then runs its adjoint blocks and imaging.  With a
 // trace map the residual is irregular and time-major; each coarse slice is
 // spread to the regular acquisition points just before the block that
 // injects it.
@@ -1537,36 +1614,42 @@ static int adjointPassFromCheckpoints(Context* c, const DevSignals& srcSet, cons
     if (t < 0 || t >= nts) return nullptr;
     return vc ? c->vSlots[(t - winStart) % 2] : c->vSlots[t - winStart];
   };
+  // the forward pass left the last segment's velocity in the slots; processing
+  // any earlier segment overwrites them
+  const bool tailKept = c->tailValid;
+  if (nseg > 1) c->tailValid = false;
   for (int s = nseg - 1; s >= 0; s--) {
-    const int bBeg = s * L;
-    const int bEnd = std::min(bBeg + L, blocks);  // adjoint blocks [bBeg, bEnd)
+    const int bBeg = segStart(blocks, L, nseg, s);
+    const int bEnd = segStart(blocks, L, nseg, s + 1);  // adjoint blocks [bBeg, bEnd)
     const int lastBlock = std::min(bEnd + 1, blocks - 1);
     winStart = bBeg;
-    // recompute V[bBeg .. min(bEnd+1, nts-1)] from the checkpoint
-    const int nClear = vc ? 2 : std::min(bEnd + 2, nts - 1) - bBeg + 1;
-    for (int i = 0; i < nClear; i++)
-      E3D_CUDA_TRY(cudaMemsetAsync(c->vSlots[i], 0, (size_t)3 * n * sizeof(float), c->st));
-    int firstBlock = 0;
-    if (s == 0) {
-      E3D_RET(zeroFields(c, c->s0));
-      E3D_RET(zeroFields(c, c->s1));
-    } else {
-      E3D_RET(unpackState(c, s));
-      // block bBeg-1 only feeds V[bBeg] through its right weights
-      E3D_RET(sourceBlock(c, bBeg - 1, srcSet, srcSig, nullptr, A(bBeg)));
-      firstBlock = bBeg;
-    }
-    for (int b = firstBlock; b <= lastBlock; b++) {
-      E3D_RET(sourceBlock(c, b, srcSet, srcSig, A(b), A(b + 1)));
-      if (vc) {
-        // V[b] is complete: store it and reuse its slot for V[b+2]
-        E3D_RET(packVelocity(c, A(b), c->vStore[b - bBeg]));
-        E3D_CUDA_TRY(cudaMemsetAsync(A(b), 0, (size_t)3 * n * sizeof(float), c->st));
+    if (!(tailKept && s == nseg - 1)) {
+      // recompute V[bBeg .. min(bEnd+1, nts-1)] from the checkpoint
+      const int nClear = vc ? 2 : std::min(bEnd + 2, nts - 1) - bBeg + 1;
+      for (int i = 0; i < nClear; i++)
+        E3D_CUDA_TRY(cudaMemsetAsync(c->vSlots[i], 0, (size_t)3 * n * sizeof(float), c->st));
+      int firstBlock = 0;
+      if (s == 0) {
+        E3D_RET(zeroFields(c, c->s0));
+        E3D_RET(zeroFields(c, c->s1));
+      } else {
+        E3D_RET(unpackState(c, s));
+        // block bBeg-1 only feeds V[bBeg] through its right weights
+        E3D_RET(sourceBlock(c, bBeg - 1, srcSet, srcSig, nullptr, A(bBeg)));
+        firstBlock = bBeg;
       }
+      for (int b = firstBlock; b <= lastBlock; b++) {
+        E3D_RET(sourceBlock(c, b, srcSet, srcSig, A(b), A(b + 1)));
+        if (vc) {
+          // V[b] is complete: store it and reuse its slot for V[b+2]
+          E3D_RET(packVelocity(c, A(b), c->vStore[b - bBeg]));
+          E3D_CUDA_TRY(cudaMemsetAsync(A(b), 0, (size_t)3 * n * sizeof(float), c->st));
+        }
+      }
+      // V[nts-1] has no block of its own: complete after block nts-2
+      if (vc && lastBlock + 1 == nts - 1 && nts - 1 <= bEnd + 1)
+        E3D_RET(packVelocity(c, A(nts - 1), c->vStore[nts - 1 - bBeg]));
     }
-    // V[nts-1] has no block of its own: complete after block nts-2
-    if (vc && lastBlock + 1 == nts - 1 && nts - 1 <= bEnd + 1)
-      E3D_RET(packVelocity(c, A(nts - 1), c->vStore[nts - 1 - bBeg]));
     if (vc)
       for (int t = bEnd; t <= std::min(bEnd + 1, nts - 1); t++)
         E3D_RET(unpackVelocity(c, c->vStore[t - bBeg], V(t)));
@@ -1711,10 +1794,13 @@ int setVelocityStorage(Context* c, int type) {
   E3D_ARG(c && type >= -1 && type <= 1, "bad velocity slot storage type");
   c->vType = type;
   c->ckptValid = false;
+  c->tailValid = false;
   return E3D_OK;
 }
 
 int velocityStorage(const Context* c) { return c->vUsed; }
+
+int checkpointType(const Context* c) { return c->ckptUsed; }
 
 // ---------------------------------------------------------------------------
 // Allocation-free nonlinear propagation.  Some callers cannot allocate device

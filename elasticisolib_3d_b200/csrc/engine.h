@@ -100,6 +100,7 @@ int fwiGradientDevice(Context* c, const DevSignals& srcSet, const DevSignals& re
 // Source velocity slot storage of the checkpoint plan: -1 auto, 0 FP32, 1 FP16 per-slice scaled.
 int setVelocityStorage(Context* c, int type);
 int velocityStorage(const Context* c);
+int checkpointType(const Context* c);
 
 // Allocation-free nonlinear propagation on the current device: the wavefield
 // levels and the taper live in a fixed 64 MiB device array (staticWorkBytes());

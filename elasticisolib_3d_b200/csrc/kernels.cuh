@@ -1139,18 +1139,56 @@ __global__ void kImaging(ImagingPtrs q, GridConst g) {
 // bf16 with one fp32 scale per (field, y) slice (max-abs / 2^14 for fp16,
 // max-abs for bf16), or copied raw in fp32.
 // ---------------------------------------------------------------------------
-__global__ void kSliceMaxAbs(const float* a, long long ys, float* out) {
-  const long long base = (long long)blockIdx.x * ys;
+// Slice maxima, packing and unpacking run on a (chunk, y slice, field) grid:
+// nf fields of n values each, slice y of field f at f*n + y*ys.  With VEC the
+// slices are read and written four values at a time (ys and n multiples of 4,
+// 16-byte aligned fields).
+constexpr int kSliceThreads = 256;
+constexpr int kSliceVecPerThread = 4;
+
+__device__ __forceinline__ unsigned sliceChunkBegin() { return blockIdx.x * kSliceThreads + threadIdx.x; }
+
+// 16-bit storage types as raw bits, so that four values move as one 8-byte word
+__device__ __forceinline__ unsigned halfBits(__half h) { return __half_as_ushort(h); }
+__device__ __forceinline__ unsigned halfBits(__nv_bfloat16 h) { return __bfloat16_as_ushort(h); }
+template <typename H>
+__device__ __forceinline__ float halfValue(unsigned bits);
+template <>
+__device__ __forceinline__ float halfValue<__half>(unsigned bits) {
+  return __half2float(__ushort_as_half((unsigned short)bits));
+}
+template <>
+__device__ __forceinline__ float halfValue<__nv_bfloat16>(unsigned bits) {
+  return __bfloat162float(__ushort_as_bfloat16((unsigned short)bits));
+}
+
+// out[f*ny + y] = max |a| over slice y of field f; out must be zeroed first.
+// NaN values are ignored, as by fmaxf; the block maxima combine through an
+// unsigned atomicMax, which orders non-negative floats by their bit patterns.
+template <bool VEC>
+__global__ void __launch_bounds__(kSliceThreads) kSliceMaxAbs(const float* a, long long n, long long ys, float* out) {
+  const long long base = (long long)blockIdx.z * n + (long long)blockIdx.y * ys;
+  const unsigned stride = gridDim.x * kSliceThreads;
   float m = 0.0f;
-  for (long long i = threadIdx.x; i < ys; i += blockDim.x) m = fmaxf(m, fabsf(a[base + i]));
+  if (VEC) {
+    const float4* v = reinterpret_cast<const float4*>(a + base);
+    const unsigned nv = (unsigned)(ys / 4);
+    for (unsigned j = sliceChunkBegin(); j < nv; j += stride) {
+      const float4 q = __ldg(v + j);
+      m = fmaxf(fmaxf(m, fabsf(q.x)), fmaxf(fabsf(q.y), fmaxf(fabsf(q.z), fabsf(q.w))));
+    }
+  } else {
+    for (long long j = sliceChunkBegin(); j < ys; j += stride) m = fmaxf(m, fabsf(__ldg(a + base + j)));
+  }
   for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
-  __shared__ float red[32];
+  __shared__ float red[kSliceThreads / 32];
   if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
   __syncthreads();
   if (threadIdx.x < 32) {
-    m = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0f;
+    m = threadIdx.x < kSliceThreads / 32 ? red[threadIdx.x] : 0.0f;
     for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
-    if (threadIdx.x == 0) out[blockIdx.x] = m;
+    if (threadIdx.x == 0 && m > 0.0f)
+      atomicMax(reinterpret_cast<unsigned*>(out) + (size_t)blockIdx.z * gridDim.y + blockIdx.y, __float_as_uint(m));
   }
 }
 
@@ -1158,13 +1196,13 @@ __global__ void kSliceMaxAbs(const float* a, long long ys, float* out) {
 // lands in [2^(topExp-1), 2^topExp): scaling and unscaling are exact, and sh is
 // clamped to +-126 so that slices whose maximum is tiny or subnormal (far from
 // the wavefront) keep finite scales.  A zero or non-finite maximum stores zeros.
-template <typename H>
-__global__ void kPackSlices(const float* a, long long ys, long long n, const float* smax, int topExp, H* out,
-                            float* scales) {
-  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const long long y = i / ys;
-  const float m = smax[y];
+// scales[f*ny + y] receives the unscaling factor.
+template <typename H, bool VEC>
+__global__ void __launch_bounds__(kSliceThreads) kPackSlices(const float* a, long long n, long long ys,
+                                                             const float* smax, int topExp, H* out, float* scales) {
+  const size_t slice = (size_t)blockIdx.z * gridDim.y + blockIdx.y;
+  const long long base = (long long)blockIdx.z * n + (long long)blockIdx.y * ys;
+  const float m = smax[slice];
   float s = 0.0f, inv = 0.0f;
   if (m > 0.0f && isfinite(m)) {
     int e;
@@ -1173,15 +1211,40 @@ __global__ void kPackSlices(const float* a, long long ys, long long n, const flo
     s = ldexpf(1.0f, sh);
     inv = ldexpf(1.0f, -sh);
   }
-  if (i % ys == 0) scales[y] = inv;
-  out[i] = H(a[i] * s);
+  if (blockIdx.x == 0 && threadIdx.x == 0) scales[slice] = inv;
+  const unsigned stride = gridDim.x * kSliceThreads;
+  if (VEC) {
+    const float4* v = reinterpret_cast<const float4*>(a + base);
+    const unsigned nv = (unsigned)(ys / 4);
+    for (unsigned j = sliceChunkBegin(); j < nv; j += stride) {
+      const float4 q = __ldg(v + j);
+      const uint2 w = make_uint2(halfBits(H(q.x * s)) | halfBits(H(q.y * s)) << 16,
+                                 halfBits(H(q.z * s)) | halfBits(H(q.w * s)) << 16);
+      *reinterpret_cast<uint2*>(out + base + 4 * (long long)j) = w;
+    }
+  } else {
+    for (long long j = sliceChunkBegin(); j < ys; j += stride) out[base + j] = H(__ldg(a + base + j) * s);
+  }
 }
 
-template <typename H>
-__global__ void kUnpackSlices(const H* in, long long ys, long long n, const float* scales, float* a) {
-  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  a[i] = float(in[i]) * scales[i / ys];
+template <typename H, bool VEC>
+__global__ void __launch_bounds__(kSliceThreads) kUnpackSlices(const H* in, long long n, long long ys,
+                                                               const float* scales, float* a) {
+  const size_t slice = (size_t)blockIdx.z * gridDim.y + blockIdx.y;
+  const long long base = (long long)blockIdx.z * n + (long long)blockIdx.y * ys;
+  const float sc = scales[slice];
+  const unsigned stride = gridDim.x * kSliceThreads;
+  if (VEC) {
+    float4* v = reinterpret_cast<float4*>(a + base);
+    const unsigned nv = (unsigned)(ys / 4);
+    for (unsigned j = sliceChunkBegin(); j < nv; j += stride) {
+      const uint2 w = __ldg(reinterpret_cast<const uint2*>(in + base + 4 * (long long)j));
+      v[j] = make_float4(halfValue<H>(w.x & 0xffffu) * sc, halfValue<H>(w.x >> 16) * sc,
+                         halfValue<H>(w.y & 0xffffu) * sc, halfValue<H>(w.y >> 16) * sc);
+    }
+  } else {
+    for (long long j = sliceChunkBegin(); j < ys; j += stride) a[base + j] = float(in[base + j]) * sc;
+  }
 }
 
 }  // namespace e3d

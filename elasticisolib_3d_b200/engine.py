@@ -92,6 +92,11 @@ class Propagator:
         N.call("e3d_synchronize", self._h)
 
     @property
+    def checkpoint_type(self):
+        """State storage of the current checkpoints: "fp32", "fp16" or "bf16"."""
+        return ("fp32", "fp16", "bf16")[int(N.lib().e3d_checkpoint_type(self._h))]
+
+    @property
     def checkpoint_segment(self):
         return int(N.lib().e3d_checkpoint_segment(self._h))
 

@@ -6,8 +6,9 @@ Per shot the device runs, through the engine's C ABI:
   2. the L2 residual at the irregular receivers (spaceInterpGpu_3D forward);
   3. the Born adjoint of the residual (BornElasticAdjGpu_3D semantics: exact
      transpose stepper, decimated adjoint field, imaging condition), with the
-     source-side velocity recomputed per segment from the checkpoints instead
-     of the reference's pinned-host snapshot storage;
+     source-side velocity of the last checkpoint segment kept from the
+     forward pass and that of the earlier segments recomputed from the
+     checkpoints, instead of the reference's pinned-host snapshot storage;
   4. the post-processing of BornElasticShotsGpu_3D::adjoint
      (BornElasticShotsGpu_3D.cpp:528-605): scaling by the density planes and
      2*dtw, unstaggering, giving (d rho, d lambda, d mu).

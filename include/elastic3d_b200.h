@@ -233,11 +233,15 @@ int e3d_set_graph_loop(e3d_context* ctx, int on);
 /* Autotuner hook: the number of y chunks each (z, x) tile column of the
  * stepper grid is split into (CTAs = z tiles * x tiles * chunks); 0 = automatic. */
 int e3d_set_stepper_chunks(e3d_context* ctx, int chunks);
-/* Checkpoint storage: type -1 = the first plan that fits among fp32 states with
- * fp32 velocity slots, fp16 states with fp32 slots, fp16 states with fp16 slots
- * (default); 0 = fp32, 1 = fp16, 2 = bf16 (16-bit types carry one scale per
- * y-slice and field);
- * segment = coarse blocks per segment (0 = largest that fits);
+/* Checkpoint storage: type -1 = chosen among fp32 states with fp32 velocity
+ * slots, fp16 states with fp32 slots, fp16 states with fp16 slots (default);
+ * 0 = fp32, 1 = fp16, 2 = bf16 (16-bit types carry one scale per y-slice and
+ * field).  Each candidate takes the longest segment that fits; the one that
+ * recomputes the fewest source blocks wins, a 16-bit plan only where it saves
+ * more than 5% (states) / 15% (velocity slots) of the blocks.  The forward pass
+ * keeps the last segment's velocity, so only the earlier segments are recomputed;
+ * segment = coarse blocks per segment (0 = automatic), segments aligned to the
+ * end of the record;
  * budget_bytes > 0: device bytes for checkpoints and velocity slots; 0: 85% of the
  * free memory; < 0: 85% of the free memory minus |budget_bytes| kept for the caller. */
 int e3d_set_checkpoint_policy(e3d_context* ctx, int type, int segment, double budget_bytes);
@@ -255,11 +259,13 @@ long long e3d_cells_per_step(const e3d_context* ctx);
 /* Coarse blocks per checkpoint segment chosen by the last checkpointed forward (0 before). */
 int e3d_checkpoint_segment(const e3d_context* ctx);
 /* Storage of the decimated source velocity kept per segment for the imaging
- * condition: -1 = fp32 when the plan fits else fp16 (default), 0 = fp32,
+ * condition: -1 = as the checkpoint plan chooses (default), 0 = fp32,
  * 1 = fp16 with one scale per y-slice and field. */
 int e3d_set_velocity_storage(e3d_context* ctx, int type);
 /* Velocity slot storage of the current plan (0 fp32, 1 fp16). */
 int e3d_velocity_storage(const e3d_context* ctx);
+/* State storage of the current checkpoints (0 fp32, 1 fp16, 2 bf16). */
+int e3d_checkpoint_type(const e3d_context* ctx);
 
 /* Host-buffer propagations.  src_pos/rec_pos: 7 tables; n_src/n_rec: 7 counts. */
 int e3d_nl_forward(e3d_context* ctx, const float* const* model9, float* const* data9,

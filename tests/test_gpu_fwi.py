@@ -7,6 +7,7 @@ import torch
 from fwi_case import OracleFwi, explosive, survey
 from elasticisolib_3d_b200 import fwi as F
 from elasticisolib_3d_b200 import hostprep as H
+from elasticisolib_3d_b200.engine import COMP_GRID
 
 pytestmark = pytest.mark.gpu
 
@@ -222,3 +223,44 @@ def test_source_term_gradient_against_finite_differences():
           f"relative L2 {rel:.3f}", flush=True)
     assert corr > 0.98
     assert rel < 0.2
+
+
+# The forward pass leaves the last checkpoint segment's source velocity in the slots and the
+# gradient starts from it.  A second gradient after the same forward finds those slots reused
+# (more than one segment) and recomputes the last segment from its checkpoint: bit-identical
+# from FP32 states, within the 16-bit plans' own error otherwise.  A Born forward in between
+# overwrites the slots as well.
+@pytest.mark.parametrize("ckpt,segment,velocity,tol", [
+    ("fp32", 0, "fp32", 0.0),
+    ("fp32", 5, "fp32", 0.0),
+    ("fp32", 4, "fp16", 0.0),
+    ("fp16", 5, "fp16", 1e-3),
+])
+def test_gradient_repeats_after_one_forward(ckpt, segment, velocity, tol):
+    sv, true = survey()
+    nts = sv.par.getInt("nts")
+    prob, src, rec = _problem(sv, ckpt, segment, (8, 2, "tma"), velocity)
+    d_obs = OracleFwi(sv).data(true)[0].astype(np.float32)
+    shot = F.make_shot(src, rec, explosive(nts, sv.wavelet), d_obs, "cuda")
+    m = [torch.tensor(sv.elastic[k], device="cuda") for k in range(3)]
+    planes = prob.set_model(*m)
+    loss0, g0 = prob.shot_misfit_and_gradient(shot, planes)
+    res, sig = prob.forward_data(shot, planes)
+    res.sub_(shot.d_obs)
+    grads = []
+    for born_between in (False, True, False):
+        if born_between:
+            spos, rpos = [d.unique for d in src], [d.unique for d in rec]
+            sig9 = [np.zeros((len(spos[COMP_GRID[k]]), nts), np.float32) for k in range(9)]
+            prob.prop.born_forward(sig9, [np.zeros(prob.prop.shape, np.float32)] * 8, spos, rpos)
+        g = torch.zeros_like(planes)
+        prob.prop.fwi_gradient_device(shot.src.pos, shot.src.off, shot.rec.pos, shot.rec.off, sig, res, g,
+                                      shot.tables)
+        grads.append(g)
+    torch.cuda.synchronize()
+    assert torch.equal(grads[0], g0), "gradient from the kept segment differs from a fresh forward+gradient"
+    for g in grads[1:]:
+        err = float((g - g0).norm() / g0.norm())
+        print(f"plan ckpt={ckpt} segment={segment} velocity={velocity} segment length "
+              f"{prob.prop.checkpoint_segment}: repeated gradient rel diff {err:.2e}", flush=True)
+        assert err <= tol
