@@ -76,6 +76,8 @@ def parse():
                          "all-FP32 plan)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--breakdown", action="store_true",
+                    help="after the measurement, print the device time per kernel of one more gradient")
     return ap.parse_args()
 
 
@@ -376,9 +378,32 @@ def run_ours(args):
         if world == 1 and not args.no_cpu:
             out["cpu_baseline"] = cpu_baseline(fd)
         print(json.dumps(out), flush=True)
+    if args.breakdown and world == 1:
+        kernel_breakdown(step)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def kernel_breakdown(step, top=16):
+    """Device time per kernel of one more gradient after the measurement, from the CUDA activity
+    trace (torch.profiler), printed to stderr; the JSON line is not affected."""
+    import collections
+    import torch
+    from torch.profiler import ProfilerActivity, profile
+    with profile(activities=[ProfilerActivity.CUDA]) as prof:
+        step()
+        torch.cuda.synchronize()
+    agg = collections.defaultdict(lambda: [0, 0.0])
+    for ev in prof.events():
+        if ev.device_type == torch.autograd.DeviceType.CUDA:
+            a = agg[ev.name.split("(")[0][:80]]
+            a[0] += 1
+            a[1] += ev.device_time_total
+    tot = sum(v[1] for v in agg.values())
+    print(f"kernel breakdown of one gradient: {tot / 1e3:.1f} ms device time", file=sys.stderr)
+    for name, (cnt, us) in sorted(agg.items(), key=lambda kv: -kv[1][1])[:top]:
+        print(f"  {us / 1e3:9.1f} ms {100 * us / tot:6.2f} % {cnt:7d}  {name}", file=sys.stderr)
 
 
 def main():
