@@ -21,8 +21,9 @@ def _problem(sv, ckpt="fp32", segment=0, variant=(8, 2, "tma"), velocity="auto")
     return prob, src, rec
 
 
-# BF16 states (8-bit mantissa) measured 1.26e-3 on this case, above the 1e-3 bound that the
-# FP32 and FP16 plans meet; they are checked against 3e-3.
+# BF16 states (8-bit mantissa) measured 1.2e-3 - 1.8e-3 on this case, depending on where the
+# segments fall, above the 1e-3 bound that the FP32 and FP16 plans meet; they are checked
+# against 3e-3.
 @pytest.mark.parametrize("ckpt,segment,variant,velocity,tol", [
     ("fp32", 0, (8, 2, "tma"), "auto", 1e-3),
     ("fp32", 3, (8, 2, "plain"), "fp32", 1e-3),
