@@ -50,15 +50,6 @@ PROFILE = {5: "profiles/kStepTma_adjoint_decimated_392x392x104.txt",
            0: "profiles/kStepTma_forward_392x392x104.txt"}
 
 
-def recomputed_blocks(blocks, seg):
-    """Source blocks the gradient's adjoint pass recomputes: every checkpoint segment but the last
-    (segments of `seg` blocks aligned to the end of the record), each from the block before it
-    (none before the first) to two blocks past its end."""
-    nseg = -(-blocks // seg)
-    start = [max(0, blocks - (nseg - s) * seg) for s in range(nseg + 1)]
-    return sum(min(start[s + 1] + 1, blocks - 1) - (start[s] - 1 if s else 0) + 1 for s in range(nseg - 1))
-
-
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -229,6 +220,7 @@ def run_ours(args):
     import torch
     import torch.distributed as dist
     from elasticisolib_3d_b200 import fwi as F
+    from elasticisolib_3d_b200.engine import checkpoint_schedule
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -335,7 +327,7 @@ def run_ours(args):
         steps_per_pass = (fd.nts - 1) * fd.sub
         blocks = fd.nts - 1
         seg = prob.prop.checkpoint_segment or blocks
-        recompute_blocks = recomputed_blocks(blocks, seg)
+        _, recompute_blocks = checkpoint_schedule(blocks, seg)
         # the forward pass decimates from the block before the last segment on
         plain_fwd = max(blocks - seg - 1, 0) if seg < blocks else 0
         cell_updates = cells * (steps_per_pass + recompute_blocks * fd.sub + steps_per_pass)

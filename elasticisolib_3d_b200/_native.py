@@ -67,6 +67,7 @@ SIGNATURES = {
     "e3d_noalloc_work_bytes": ([], ctypes.c_size_t),
     "e3d_velocity_storage": ([P], I),
     "e3d_checkpoint_type": ([P], I),
+    "e3d_checkpoint_schedule": ([I, I, P, I, P], I),
     "e3d_step_only": ([P, I, I], I),
     "e3d_kernel_timing": ([P, I], I),
     "e3d_kernel_timing_read": ([P, I, P, P], I),

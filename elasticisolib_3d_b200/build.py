@@ -15,7 +15,7 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libelastic3d_b200.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 SOURCES = ["engine.cu", "c_abi.cpp", "host_prep.cpp"]
-HEADERS = ["common.cuh", "kernels.cuh", "engine.h", "shot_operators.cpp"]
+HEADERS = ["common.cuh", "kernels.cuh", "engine.h", "schedule.h", "shot_operators.cpp"]
 
 
 def _host_compiler():

@@ -2,10 +2,12 @@
 // reference's process-global state) and the explicit-context API.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <mutex>
 
 #include "../../include/elastic3d_b200.h"
 #include "engine.h"
+#include "schedule.h"
 
 using namespace e3d;
 
@@ -319,6 +321,18 @@ int e3d_set_stream(e3d_context* ctx, void* s, int use_own) {
 long long e3d_cells_per_step(const e3d_context* ctx) { return (ctx && ctx->c) ? cellsPerStep(ctx->c) : 0; }
 
 int e3d_checkpoint_segment(const e3d_context* ctx) { return (ctx && ctx->c) ? checkpointSegment(ctx->c) : 0; }
+
+int e3d_checkpoint_schedule(int blocks, int segment_len, int* seg_start, int max_segments, int* recomputed) {
+  if (blocks < 1 || segment_len < 1) return -E3D_ERR_ARG;
+  const int L = std::min(segment_len, blocks);
+  const int nseg = e3d::schedule::segments(blocks, L);
+  if (seg_start) {
+    if (max_segments < nseg) return -E3D_ERR_ARG;
+    for (int s = 0; s <= nseg; s++) seg_start[s] = e3d::schedule::segStart(blocks, L, nseg, s);
+  }
+  if (recomputed) *recomputed = e3d::schedule::recomputedBlocks(blocks, L);
+  return nseg;
+}
 
 int e3d_nl_forward(e3d_context* ctx, const float* const* model9, float* const* data9, const long long* const* src_pos,
                    const long long* n_src, const long long* const* rec_pos, const long long* n_rec) {

@@ -23,6 +23,7 @@
 
 #include "engine.h"
 #include "kernels.cuh"
+#include "schedule.h"
 
 namespace e3d {
 
@@ -1198,19 +1199,8 @@ static int bornForwardDevice(Context* c, const DevSignals& srcSet, const DevSign
 // ---------------------------------------------------------------------------
 enum { V_F32 = 0, V_F16 = 1 };
 
-static int segStart(int blocks, int L, int nseg, int s) { return std::max(0, blocks - (nseg - s) * L); }
-
-// Source blocks the adjoint pass recomputes: every segment but the last, each
-// from the block before it (none before the first) to two blocks past its end.
-static int recomputedBlocks(int blocks, int L) {
-  const int nseg = (blocks + L - 1) / L;
-  int r = 0;
-  for (int s = 0; s + 1 < nseg; s++) {
-    const int b0 = s == 0 ? 0 : segStart(blocks, L, nseg, s) - 1;
-    r += std::min(segStart(blocks, L, nseg, s + 1) + 1, blocks - 1) - b0 + 1;
-  }
-  return r;
-}
+using schedule::recomputedBlocks;
+using schedule::segStart;
 
 static size_t ckptBytesPerState(const Context* c, int type) {
   const size_t eb = type == CKPT_F32 ? 4 : 2;
@@ -1227,7 +1217,8 @@ static double vSlotBytes(const Context* c, int vt) {
 }
 
 // Checkpoints plus velocity slots of a plan with segment length L.  FP32 slots
-// hold V[s*L .. s*L+L+2]; FP16 slots hold V[s*L .. s*L+L+1] plus three FP32
+// hold V[b .. b+L+2] of a segment starting at block b (the last one partial,
+// from the recompute's final block); FP16 slots hold V[b .. b+L+1] plus three FP32
 // working slots (two accumulators while recomputing, a three-deep ring for
 // the imaging condition).
 static double planBytes(const Context* c, int ck, int vt, int L) {

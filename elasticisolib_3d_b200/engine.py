@@ -26,6 +26,19 @@ def _geom(pos7):
     return P, C, pos
 
 
+def checkpoint_schedule(blocks, segment_len):
+    """Checkpoint schedule of a record of `blocks` coarse blocks (nts - 1) with segments of
+    `segment_len` blocks, as the engine runs it: (first block of each segment followed by
+    `blocks`, source blocks the adjoint pass recomputes).  Host arithmetic only."""
+    nmax = -(-int(blocks) // max(1, min(int(segment_len), int(blocks))))
+    starts = (ctypes.c_int * (nmax + 1))()
+    rec = ctypes.c_int(0)
+    n = int(N.lib().e3d_checkpoint_schedule(int(blocks), int(segment_len), starts, nmax, ctypes.byref(rec)))
+    if n < 0:
+        raise ValueError(f"bad checkpoint schedule arguments: blocks={blocks}, segment_len={segment_len}")
+    return list(starts[:n + 1]), rec.value
+
+
 class Propagator:
     def __init__(self, nz, nx, ny, nts, sub, minPad, dz, dx, dy, dts, alphaCos=0.99, device=0, fix_q1=0,
                  q2compat=1, q3compat=1, free_surface=0):

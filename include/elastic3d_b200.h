@@ -266,6 +266,17 @@ int e3d_set_velocity_storage(e3d_context* ctx, int type);
 int e3d_velocity_storage(const e3d_context* ctx);
 /* State storage of the current checkpoints (0 fp32, 1 fp16, 2 bf16). */
 int e3d_checkpoint_type(const e3d_context* ctx);
+/* The checkpoint schedule of a record of `blocks` coarse blocks (nts - 1) cut
+ * into segments of `segment_len` blocks, as the checkpointed passes run it:
+ * returns the segment count nseg, or -E3D_ERR_ARG.  seg_start (room for
+ * max_segments + 1 values, may be NULL) receives the first block of each
+ * segment and then `blocks`: segments are aligned to the end of the record
+ * and the first holds the remainder.  *recomputed (may be NULL) receives the
+ * source blocks the adjoint pass recomputes (every segment but the last, whose
+ * velocity the forward pass keeps).  No device work; no counterpart in the
+ * reference, whose Born adjoint stores the whole source wavefield on the host
+ * (BornElasticGpuFunctions_3D.cu:1268-1316). */
+int e3d_checkpoint_schedule(int blocks, int segment_len, int* seg_start, int max_segments, int* recomputed);
 
 /* Host-buffer propagations.  src_pos/rec_pos: 7 tables; n_src/n_rec: 7 counts. */
 int e3d_nl_forward(e3d_context* ctx, const float* const* model9, float* const* data9,
