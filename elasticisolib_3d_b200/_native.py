@@ -75,6 +75,7 @@ SIGNATURES = {
     "e3d_medium_planes": ([I, I, I, F, P, P], I),
     "e3d_stagger": ([I, I, I, I, I, I, P, P], I),
     "e3d_space_interp_linear": ([P, P, P, LL, I, I, I, F, F, F, F, F, F, P, F, I, F, F, F, P, P, P, P, P], I),
+    "e3d_space_interp": ([I, I, P, P, P, LL, I, I, I, F, F, F, F, F, F, P, F, I, F, F, F, I, P, P, P, P, P], I),
 }
 
 _lib = None

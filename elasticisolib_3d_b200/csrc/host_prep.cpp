@@ -50,6 +50,140 @@ void stagger(int nz, int nx, int ny, int axis, bool adjoint, bool add, const flo
   }
 }
 
+struct Pads {
+  int fat, zPadMinus, zPadPlus, xPadMinus, xPadPlus, yPad;
+};
+struct Grid {
+  int nz, nx, ny;
+  float oz, ox, oy, dz, dx, dy;
+};
+
+// spaceInterpGpu_3D::checkOutOfBounds (spaceInterpGpu_3D.cpp:178-213): every
+// device inside the model interior (float arithmetic, with a tolerance)
+bool devicesInside(const Grid& g, const Pads& p, const float* z, const float* x, const float* y, long long nDev,
+                   float tol) {
+  const int nzS = g.nz - 2 * p.fat - p.zPadMinus - p.zPadPlus;
+  const int nxS = g.nx - 2 * p.fat - p.xPadMinus - p.xPadPlus;
+  const int nyS = g.ny - 2 * p.fat - 2 * p.yPad;
+  const float zMin = g.oz + (p.fat + p.zPadMinus) * g.dz;
+  const float xMin = g.ox + (p.fat + p.xPadMinus) * g.dx;
+  const float yMin = g.oy + (p.fat + p.yPad) * g.dy;
+  const float zMax = zMin + (nzS - 1) * g.dz;
+  const float xMax = xMin + (nxS - 1) * g.dx;
+  const float yMax = yMin + (nyS - 1) * g.dy;
+  for (long long i = 0; i < nDev; i++)
+    if (z[i] - zMax > tol || z[i] - zMin < -tol || x[i] - xMax > tol || x[i] - xMin < -tol || y[i] - yMax > tol ||
+        y[i] - yMin < -tol)
+      return false;
+  return true;
+}
+
+// Trilinear pole (spaceInterpGpu_3D.cpp:216-270): the 8 corners of the cell
+// holding the point, z fastest, with the reference's float/double mix
+// (w = 1 - frac rounded to float; each weight is the reference's own product
+// expression, some evaluated in float and some in double, and the second pole
+// of a dipole carries a (-1.0) factor in front).  dyPole is the y sampling the
+// offset is divided by.  False when a corner leaves the model interior.
+bool linearPole(const Grid& g, const Pads& p, float zd, float xd, float yd, float dyPole, bool second,
+                long long* index, float* weight) {
+  float wz = (zd - g.oz) / g.dz;
+  float wx = (xd - g.ox) / g.dx;
+  float wy = (yd - g.oy) / dyPole;
+  const long long zr = (long long)wz, xr = (long long)wx, yr = (long long)wy;
+  wz = wz - zr; wz = 1.0 - wz;
+  wx = wx - xr; wx = 1.0 - wx;
+  wy = wy - yr; wy = 1.0 - wy;
+  if (yr < p.fat + p.yPad || yr + 1 >= g.ny - p.fat - p.yPad || xr < p.fat + p.xPadMinus ||
+      xr + 1 >= g.nx - p.fat - p.xPadPlus || zr < p.fat + p.zPadMinus || zr + 1 >= g.nz - p.fat - p.zPadPlus)
+    return false;
+  const long long nz = g.nz, nzx = (long long)g.nz * g.nx;
+  const long long b = yr * nzx + xr * nz + zr;
+  const long long off[8] = {0, 1, nz, nz + 1, nzx, nzx + 1, nzx + nz, nzx + nz + 1};
+  for (int k = 0; k < 8; k++) index[k] = b + off[k];
+  if (!second) {
+    weight[0] = wz * wx * wy;
+    weight[1] = (1.0 - wz) * wx * wy;
+    weight[2] = wz * (1.0 - wx) * wy;
+    weight[3] = (1.0 - wz) * (1.0 - wx) * wy;
+    weight[4] = wz * wx * (1.0 - wy);
+    weight[5] = (1.0 - wz) * wx * (1.0 - wy);
+    weight[6] = wz * (1.0 - wx) * (1.0 - wy);
+    weight[7] = (1.0 - wz) * (1.0 - wx) * (1.0 - wy);
+  } else {
+    weight[0] = (-1.0) * wz * wx * wy;
+    weight[1] = (-1.0) * (1.0 - wz) * wx * wy;
+    weight[2] = (-1.0) * wz * (1.0 - wx) * wy;
+    weight[3] = (-1.0) * (1.0 - wz) * (1.0 - wx) * wy;
+    weight[4] = (-1.0) * wz * wx * (1.0 - wy);
+    weight[5] = (-1.0) * (1.0 - wz) * wx * (1.0 - wy);
+    weight[6] = (-1.0) * wz * (1.0 - wx) * (1.0 - wy);
+    weight[7] = (-1.0) * (1.0 - wz) * (1.0 - wx) * (1.0 - wy);
+  }
+  return true;
+}
+
+// sin(a)/a in double with its limit 1 at a = 0: below |a| = 1.2e-4 the Taylor
+// series 1 - a^2/6 + a^4/120 (its next term is below 1e-20 there).
+double sincOfArg(double a) {
+  if (std::fabs(a) < 1.2e-4) {
+    const double a2 = a * a;
+    return 1.0 - a2 / 6.0 + a2 * a2 / 120.0;
+  }
+  return std::sin(a) / a;
+}
+
+// Windowless sinc pole (spaceInterpGpu_3D.cpp:351-413): the 2h points per
+// axis r-h+1 .. r+h around the cell corner r below the point, y then x then z
+// (z fastest); weight sinc(pi wz) sinc(pi wx) sinc(pi wy) in double, stored
+// as float, with w = (device - point) / d in float.  The reference's bounds
+// test is inverted and rejects every in-bounds stencil; here the stencil must
+// lie inside the array (false otherwise).
+bool sincPole(const Grid& g, int h, float zd, float xd, float yd, long long* index, float* weight) {
+  const float zReg = (zd - g.oz) / g.dz;
+  const float xReg = (xd - g.ox) / g.dx;
+  const float yReg = (yd - g.oy) / g.dy;
+  const long long zr = (long long)zReg, xr = (long long)xReg, yr = (long long)yReg;
+  if (yr - h + 1 < 0 || yr + h >= g.ny || xr - h + 1 < 0 || xr + h >= g.nx || zr - h + 1 < 0 || zr + h >= g.nz)
+    return false;
+  const int nf1 = 2 * h;
+  for (int iy = 0; iy < nf1; iy++)
+    for (int ix = 0; ix < nf1; ix++)
+      for (int iz = 0; iz < nf1; iz++) {
+        const long long py = yr + iy - h + 1, px = xr + ix - h + 1, pz = zr + iz - h + 1;
+        const float yCur = py * g.dy + g.oy;
+        const float xCur = px * g.dx + g.ox;
+        const float zCur = pz * g.dz + g.oz;
+        const float wy = (yd - yCur) / g.dy;
+        const float wx = (xd - xCur) / g.dx;
+        const float wz = (zd - zCur) / g.dz;
+        const long long k = ((long long)iy * nf1 + ix) * nf1 + iz;
+        index[k] = (long long)g.nz * g.nx * py + (long long)g.nz * px + pz;
+        weight[k] = (float)(sincOfArg(M_PI * wz) * sincOfArg(M_PI * wx) * sincOfArg(M_PI * wy));
+      }
+  return true;
+}
+
+// spaceInterpGpu_3D::convertIrregToReg (spaceInterpGpu_3D.cpp:113-138): unique
+// grid points in first-seen order, keyed, as the reference's std::map<int,int>
+// is, by the index converted to int; slot[i] = position of index[i] among them.
+void uniquePoints(const long long* index, long long n, long long* unique, long long* slot, long long* nUnique) {
+  std::unordered_map<long long, long long> seen;
+  seen.reserve((size_t)(n * 2 + 16));
+  long long nu = 0;
+  for (long long i = 0; i < n; i++) {
+    const long long key = (long long)(int)index[i];
+    auto it = seen.find(key);
+    if (it == seen.end()) {
+      seen.emplace(key, nu);
+      unique[nu] = index[i];
+      slot[i] = nu++;
+    } else {
+      slot[i] = it->second;
+    }
+  }
+  *nUnique = nu;
+}
+
 }  // namespace
 
 extern "C" {
@@ -102,103 +236,72 @@ int e3d_medium_planes(int nz, int nx, int ny, float dtw, const float* elastic, f
   return E3D_OK;
 }
 
-// spaceInterpGpu_3D::checkOutOfBounds + calcLinearWeights + convertIrregToReg
-// (spaceInterpGpu_3D.cpp:113-138, 178-348)
-int e3d_space_interp_linear(const float* z, const float* x, const float* y, long long nDev, int nz, int nx, int ny,
-                            float oz, float ox, float oy, float dz, float dx, float dy, const int* pads,
-                            float tol, int dipole, float zshift, float xshift, float yshift, long long* index,
-                            float* weight, long long* unique, long long* slot, long long* nUnique) {
+// spaceInterpGpu_3D: checkOutOfBounds + calcLinearWeights / calcSincWeights +
+// convertIrregToReg (spaceInterpGpu_3D.cpp:113-138, 178-480).
+int e3d_space_interp(int method, int hFilter, const float* z, const float* x, const float* y, long long nDev, int nz,
+                     int nx, int ny, float oz, float ox, float oy, float dz, float dx, float dy, const int* pads,
+                     float tol, int dipole, float zshift, float xshift, float yshift, int compat, long long* index,
+                     float* weight, long long* unique, long long* slot, long long* nUnique) {
   if (nDev < 0 || !pads || !index || !weight || !unique || !slot || !nUnique || (nDev > 0 && (!z || !x || !y))) {
     setLastError("bad spaceInterp arguments", __FILE__, __LINE__);
     return E3D_ERR_ARG;
   }
-  const int fat = pads[0], zPadMinus = pads[1], zPadPlus = pads[2], xPadMinus = pads[3], xPadPlus = pads[4],
-            yPad = pads[5];
-  // bounds of the model interior (float arithmetic)
-  const int nzS = nz - 2 * fat - zPadMinus - zPadPlus;
-  const int nxS = nx - 2 * fat - xPadMinus - xPadPlus;
-  const int nyS = ny - 2 * fat - 2 * yPad;
-  const float zMin = oz + (fat + zPadMinus) * dz;
-  const float xMin = ox + (fat + xPadMinus) * dx;
-  const float yMin = oy + (fat + yPad) * dy;
-  const float zMax = zMin + (nzS - 1) * dz;
-  const float xMax = xMin + (nxS - 1) * dx;
-  const float yMax = yMin + (nyS - 1) * dy;
-  for (long long i = 0; i < nDev; i++) {
-    if (z[i] - zMax > tol || z[i] - zMin < -tol || x[i] - xMax > tol || x[i] - xMin < -tol || y[i] - yMax > tol ||
-        y[i] - yMin < -tol) {
-      setLastError("acquisition device outside the model interior", __FILE__, __LINE__);
-      return E3D_ERR_BOUNDS;
-    }
+  if (method == E3D_INTERP_LINEAR && hFilter != 1) {
+    setLastError("linear interpolation requires a half filter length of 1", __FILE__, __LINE__);
+    return E3D_ERR_ARG;
   }
-  const int nf = dipole ? 16 : 8;
-  // the reference stores the dipole shifts in int members (spaceInterpGpu_3D.h:25)
-  const int zs = (int)zshift, xs = (int)xshift, ys = (int)yshift;
+  if ((method != E3D_INTERP_LINEAR && method != E3D_INTERP_SINC) || hFilter < 1 || hFilter > 16) {
+    setLastError("unsupported interpolation method or half filter length", __FILE__, __LINE__);
+    return E3D_ERR_ARG;
+  }
+  const Pads pd{pads[0], pads[1], pads[2], pads[3], pads[4], pads[5]};
+  const Grid g{nz, nx, ny, oz, ox, oy, dz, dx, dy};
+  if (!devicesInside(g, pd, z, x, y, nDev, tol)) {
+    setLastError("acquisition device outside the model interior", __FILE__, __LINE__);
+    return E3D_ERR_BOUNDS;
+  }
+  const int nf1 = 2 * hFilter;
+  const long long nPole = (long long)nf1 * nf1 * nf1;
+  const long long nf = dipole ? 2 * nPole : nPole;
+  // the reference keeps the dipole shifts in int members (spaceInterpGpu_3D.h:25)
+  const float zs = compat ? (float)(int)zshift : zshift;
+  const float xs = compat ? (float)(int)xshift : xshift;
+  const float ys = compat ? (float)(int)yshift : yshift;
   for (long long d = 0; d < nDev; d++) {
     for (int part = 0; part < (dipole ? 2 : 1); part++) {
-      float wz, wx, wy;
-      if (part == 0) {
-        wz = (z[d] - oz) / dz;
-        wx = (x[d] - ox) / dx;
-        wy = (y[d] - oy) / dy;
-      } else {  // dipole point; the reference divides the y offset by dz
-        wz = (z[d] + zs - oz) / dz;
-        wx = (x[d] + xs - ox) / dx;
-        wy = (y[d] + ys - oy) / dz;
+      long long* ix = index + d * nf + part * nPole;
+      float* w = weight + d * nf + part * nPole;
+      const float zd = part ? z[d] + zs : z[d];
+      const float xd = part ? x[d] + xs : x[d];
+      const float yd = part ? y[d] + ys : y[d];
+      bool ok;
+      if (method == E3D_INTERP_LINEAR) {
+        // the reference divides the second pole's y offset by dz; the second
+        // pole enters with negative weights
+        ok = linearPole(g, pd, zd, xd, yd, part && compat ? dz : dy, part == 1, ix, w);
+      } else {
+        ok = sincPole(g, hFilter, zd, xd, yd, ix, w);
+        // the reference's sinc dipole keeps positive weights; the corrected form
+        // subtracts the second pole as the linear dipole does
+        if (part && !compat)
+          for (long long k = 0; k < nPole; k++) w[k] = -w[k];
       }
-      const long long zr = (long long)wz, xr = (long long)wx, yr = (long long)wy;
-      wz = wz - zr; wz = 1.0 - wz;
-      wx = wx - xr; wx = 1.0 - wx;
-      wy = wy - yr; wy = 1.0 - wy;
-      if (yr < fat + yPad || yr + 1 >= ny - fat - yPad || xr < fat + xPadMinus || xr + 1 >= nx - fat - xPadPlus ||
-          zr < fat + zPadMinus || zr + 1 >= nz - fat - zPadPlus) {
-        setLastError("interpolation stencil outside the model interior", __FILE__, __LINE__);
+      if (!ok) {
+        setLastError("interpolation stencil outside the grid", __FILE__, __LINE__);
         return E3D_ERR_BOUNDS;
       }
-      const long long i1 = d * nf + part * 8;
-      const long long b = yr * nz * nx + xr * nz + zr;
-      const long long off[8] = {0, 1, nz, nz + 1, (long long)nz * nx, (long long)nz * nx + 1,
-                                (long long)nz * nx + nz, (long long)nz * nx + nz + 1};
-      for (int k = 0; k < 8; k++) index[i1 + k] = b + off[k];
-      if (part == 0) {
-        weight[i1 + 0] = wz * wx * wy;
-        weight[i1 + 1] = (1.0 - wz) * wx * wy;
-        weight[i1 + 2] = wz * (1.0 - wx) * wy;
-        weight[i1 + 3] = (1.0 - wz) * (1.0 - wx) * wy;
-        weight[i1 + 4] = wz * wx * (1.0 - wy);
-        weight[i1 + 5] = (1.0 - wz) * wx * (1.0 - wy);
-        weight[i1 + 6] = wz * (1.0 - wx) * (1.0 - wy);
-        weight[i1 + 7] = (1.0 - wz) * (1.0 - wx) * (1.0 - wy);
-      } else {
-        weight[i1 + 0] = (-1.0) * wz * wx * wy;
-        weight[i1 + 1] = (-1.0) * (1.0 - wz) * wx * wy;
-        weight[i1 + 2] = (-1.0) * wz * (1.0 - wx) * wy;
-        weight[i1 + 3] = (-1.0) * (1.0 - wz) * (1.0 - wx) * wy;
-        weight[i1 + 4] = (-1.0) * wz * wx * (1.0 - wy);
-        weight[i1 + 5] = (-1.0) * (1.0 - wz) * wx * (1.0 - wy);
-        weight[i1 + 6] = (-1.0) * wz * (1.0 - wx) * (1.0 - wy);
-        weight[i1 + 7] = (-1.0) * (1.0 - wz) * (1.0 - wx) * (1.0 - wy);
-      }
     }
   }
-  // unique grid points in first-seen order; the reference keys an
-  // std::map<int,int> by the index converted to int
-  std::unordered_map<long long, long long> seen;
-  seen.reserve((size_t)(nDev * nf * 2 + 16));
-  long long nu = 0;
-  for (long long i = 0; i < nDev * nf; i++) {
-    const long long key = (long long)(int)index[i];
-    auto it = seen.find(key);
-    if (it == seen.end()) {
-      seen.emplace(key, nu);
-      unique[nu] = index[i];
-      slot[i] = nu++;
-    } else {
-      slot[i] = it->second;
-    }
-  }
-  *nUnique = nu;
+  uniquePoints(index, nDev * nf, unique, slot, nUnique);
   return E3D_OK;
+}
+
+int e3d_space_interp_linear(const float* z, const float* x, const float* y, long long nDev, int nz, int nx, int ny,
+                            float oz, float ox, float oy, float dz, float dx, float dy, const int* pads,
+                            float tol, int dipole, float zshift, float xshift, float yshift, long long* index,
+                            float* weight, long long* unique, long long* slot, long long* nUnique) {
+  return e3d_space_interp(E3D_INTERP_LINEAR, 1, z, x, y, nDev, nz, nx, ny, oz, ox, oy, dz, dx, dy, pads, tol, dipole,
+                          zshift, xshift, yshift, 1, index, weight, unique, slot, nUnique);
 }
 
 }  // extern "C"

@@ -103,14 +103,15 @@ class spaceInterpGpu_3D {
                     py::array_t<float, py::array::c_style | py::array::forcecast> x,
                     py::array_t<float, py::array::c_style | py::array::forcecast> y, std::shared_ptr<hypercube> grid,
                     int nt, std::shared_ptr<paramObj> par, int dipole = 0, float zShift = 0.f, float xShift = 0.f,
-                    float yShift = 0.f, std::string method = "linear", int hFilter1d = 1)
+                    float yShift = 0.f, std::string method = "linear", int hFilter1d = 1, int compat = 1)
       : nt_(nt) {
-    if (method != "linear") throw std::runtime_error("only linear spatial interpolation is supported");
-    if (hFilter1d != 1) throw std::runtime_error("linear interpolation requires hFilter1d = 1");
+    if (method != "linear" && method != "sinc") throw std::runtime_error("unsupported spatial interpolation method");
+    if (method == "linear" && hFilter1d != 1) throw std::runtime_error("linear interpolation requires hFilter1d = 1");
+    if (hFilter1d < 1 || hFilter1d > 16) throw std::runtime_error("hFilter1d must be 1 .. 16");
     const long long n = (long long)z.size();
     if ((long long)x.size() != n || (long long)y.size() != n) throw std::runtime_error("coordinate sizes differ");
     const axis az = grid->getAxis(1), ax = grid->getAxis(2), ay = grid->getAxis(3);
-    nf_ = dipole ? 16 : 8;
+    nf_ = 8 * hFilter1d * hFilter1d * hFilter1d * (dipole ? 2 : 1);
     nIrreg_ = n;
     index_.resize((size_t)n * nf_);
     weight_.resize((size_t)n * nf_);
@@ -119,9 +120,10 @@ class spaceInterpGpu_3D {
     const int pads[6] = {par->getInt("fat", py::int_(4)), par->getInt("zPadMinus"), par->getInt("zPadPlus"),
                          par->getInt("xPadMinus"), par->getInt("xPadPlus"), par->getInt("yPad")};
     long long nu = 0;
-    check(e3d_space_interp_linear(z.data(), x.data(), y.data(), n, az.n, ax.n, ay.n, az.o, ax.o, ay.o, az.d, ax.d,
-                                  ay.d, pads, par->getFloat("errorTolerance", py::float_(1e-6)), dipole, zShift,
-                                  xShift, yShift, index_.data(), weight_.data(), uniq.data(), slot_.data(), &nu));
+    check(e3d_space_interp(method == "sinc" ? E3D_INTERP_SINC : E3D_INTERP_LINEAR, hFilter1d, z.data(), x.data(),
+                           y.data(), n, az.n, ax.n, ay.n, az.o, ax.o, ay.o, az.d, ax.d, ay.d, pads,
+                           par->getFloat("errorTolerance", py::float_(1e-6)), dipole, zShift, xShift, yShift, compat,
+                           index_.data(), weight_.data(), uniq.data(), slot_.data(), &nu));
     unique_.assign(uniq.begin(), uniq.begin() + nu);
   }
   const std::vector<long long>& getRegPosUnique() const { return unique_; }
@@ -641,10 +643,10 @@ PYBIND11_MODULE(pyElastic_iso_float_3D, m) {
       .def(py::init<py::array_t<float, py::array::c_style | py::array::forcecast>,
                     py::array_t<float, py::array::c_style | py::array::forcecast>,
                     py::array_t<float, py::array::c_style | py::array::forcecast>, std::shared_ptr<hypercube>, int,
-                    std::shared_ptr<paramObj>, int, float, float, float, std::string, int>(),
+                    std::shared_ptr<paramObj>, int, float, float, float, std::string, int, int>(),
            py::arg("zCoord"), py::arg("xCoord"), py::arg("yCoord"), py::arg("grid"), py::arg("nt"), py::arg("par"),
            py::arg("dipole") = 0, py::arg("zShift") = 0.f, py::arg("xShift") = 0.f, py::arg("yShift") = 0.f,
-           py::arg("method") = "linear", py::arg("hFilter1d") = 1)
+           py::arg("method") = "linear", py::arg("hFilter1d") = 1, py::arg("compat") = 1)
       .def("getRegPosUnique", &spaceInterpGpu_3D::getRegPosUnique)
       .def("getNDeviceReg", &spaceInterpGpu_3D::getNDeviceReg)
       .def("getNDeviceIrreg", &spaceInterpGpu_3D::getNDeviceIrreg);

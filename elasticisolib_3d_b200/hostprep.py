@@ -169,39 +169,44 @@ class spaceInterpGpu_3D:
     """Acquisition devices mapped onto one (possibly staggered) grid.
 
     Same constructor meaning as the reference (spaceInterpGpu_3D.cpp:13-79):
-    coordinates, grid axes, nt, parameters, dipole flag and shifts, method and
-    half filter length.  Only the linear method is usable in the reference
-    (its sinc bounds checks always throw, quirk Q4), so only linear is built.
+    coordinates, grid axes, nt, parameters, dipole flag and shifts, method
+    ("linear" or "sinc") and half filter length (1 for linear).  The reference's
+    sinc path rejects every in-bounds stencil (its bounds test is inverted); here
+    that test is written the right way round.  `compat` (not a reference
+    argument): True keeps the reference's dipole arithmetic (shifts truncated to
+    int, the linear second pole's y offset divided by dz, the sinc second pole
+    with positive weights); False corrects it.
     """
 
     def __init__(self, zCoord, xCoord, yCoord, axes, nt, par: ParamObj, dipole=0, zDipoleShift=0.0,
-                 xDipoleShift=0.0, yDipoleShift=0.0, interpMethod="linear", hFilter1d=1):
-        if interpMethod != "linear":
-            raise NotImplementedError("only linear spatial interpolation is supported (the reference sinc path "
-                                      "always rejects its input)")
-        if hFilter1d != 1:
+                 xDipoleShift=0.0, yDipoleShift=0.0, interpMethod="linear", hFilter1d=1, compat=True):
+        methods = {"linear": 0, "sinc": 1}
+        if interpMethod not in methods:
+            raise NotImplementedError(f"spatial interpolation method {interpMethod!r} is not supported")
+        if interpMethod == "linear" and hFilter1d != 1:
             raise RuntimeError("linear interpolation requires hFilter1d = 1")
         z = N.as_f32(zCoord).reshape(-1)
         x = N.as_f32(xCoord).reshape(-1)
         y = N.as_f32(yCoord).reshape(-1)
         self.nt = int(nt)
+        self.method = interpMethod
         za, xa, ya = axes
         self.shape = (ya.n, xa.n, za.n)
         pads6 = (N.ctypes.c_int * 6)(par.getInt("fat"), par.getInt("zPadMinus"), par.getInt("zPadPlus"),
                                      par.getInt("xPadMinus"), par.getInt("xPadPlus"), par.getInt("yPad"))
-        nf = 16 if dipole else 8
+        nf = (2 * int(hFilter1d)) ** 3 * (2 if dipole else 1)
         n = z.shape[0]
         self.index = np.empty((n, nf), dtype=np.int64)
         self.weight = np.empty((n, nf), dtype=np.float32)
         uniq = np.empty(max(n * nf, 1), dtype=np.int64)
         self.slot = np.empty((n, nf), dtype=np.int64)
         nu = N.ctypes.c_longlong(0)
-        N.call("e3d_space_interp_linear", z.ctypes.data, x.ctypes.data, y.ctypes.data, n, za.n, xa.n, ya.n,
-               float(np.float32(za.o)), float(np.float32(xa.o)), float(np.float32(ya.o)), float(np.float32(za.d)),
-               float(np.float32(xa.d)), float(np.float32(ya.d)), pads6,
-               float(np.float32(par.getFloat("errorTolerance", 1e-6))), int(dipole), float(zDipoleShift),
-               float(xDipoleShift), float(yDipoleShift), self.index.ctypes.data, self.weight.ctypes.data,
-               uniq.ctypes.data, self.slot.ctypes.data, N.ctypes.byref(nu))
+        N.call("e3d_space_interp", methods[interpMethod], int(hFilter1d), z.ctypes.data, x.ctypes.data,
+               y.ctypes.data, n, za.n, xa.n, ya.n, float(np.float32(za.o)), float(np.float32(xa.o)),
+               float(np.float32(ya.o)), float(np.float32(za.d)), float(np.float32(xa.d)), float(np.float32(ya.d)),
+               pads6, float(np.float32(par.getFloat("errorTolerance", 1e-6))), int(dipole), float(zDipoleShift),
+               float(xDipoleShift), float(yDipoleShift), int(bool(compat)), self.index.ctypes.data,
+               self.weight.ctypes.data, uniq.ctypes.data, self.slot.ctypes.data, N.ctypes.byref(nu))
         self.unique = uniq[:nu.value].copy()
 
     # accessors named after the reference's (spaceInterpGpu_3D.h:54-66)
@@ -253,6 +258,20 @@ def grid_axes(nz, nx, ny, oz, ox, oy, dz, dx, dy):
     return [(Z, X, Y), (Z, Xs, Y), (Z, X, Ys), (Zs, X, Y), (Zs, Xs, Y), (Z, Xs, Ys), (Zs, X, Ys)]
 
 
-def build_devices(z, x, y, axes7, nt, par, dipole=0, shifts=(0.0, 0.0, 0.0)):
-    """The seven spaceInterpGpu_3D objects of one device set (buildSourceGeometry_3D)."""
-    return [spaceInterpGpu_3D(z, x, y, ax, nt, par, dipole, *shifts) for ax in axes7]
+def build_devices(z, x, y, axes7, nt, par, dipole=None, shifts=None, method=None, hFilter1d=None, compat=True):
+    """The seven spaceInterpGpu_3D objects of one device set (buildSourceGeometry_3D /
+    buildReceiversGeometry_3D, Elastic_iso_float_3D.py:21-195).  Unless given, the dipole flag,
+    its shifts, the method and the sinc half length come from the parameters as the reference
+    reads them: dipole, zDipoleShift, xDipoleShift, yDipoleShift, spaceInterpMethod ("linear"
+    by default) and hFilter1d (1 for linear)."""
+    if dipole is None:
+        dipole = par.getInt("dipole", 0)
+    if shifts is None:
+        shifts = (par.getFloat("zDipoleShift", 0.0), par.getFloat("xDipoleShift", 0.0),
+                  par.getFloat("yDipoleShift", 0.0))
+    if method is None:
+        method = par.getString("spaceInterpMethod", "linear")
+    if hFilter1d is None:
+        hFilter1d = 1 if method == "linear" else par.getInt("hFilter1d", 1)
+    return [spaceInterpGpu_3D(z, x, y, ax, nt, par, dipole, *shifts, interpMethod=method, hFilter1d=hFilter1d,
+                              compat=compat) for ax in axes7]

@@ -408,6 +408,27 @@ int e3d_space_interp_linear(const float* z, const float* x, const float* y, long
                             long long* index, float* weight, long long* unique, long long* slot,
                             long long* n_unique);
 
+/* spaceInterpGpu_3D with a choice of method (spaceInterpGpu_3D.cpp:13-79,
+ * 178-480): E3D_INTERP_LINEAR (h_filter must be 1) or E3D_INTERP_SINC with
+ * h_filter points on each side per axis.  nFilter = (2*h_filter)^3 points per
+ * pole, z fastest then x then y, doubled with dipole.  Sinc weights are
+ * sinc(wz) sinc(wx) sinc(wy), sinc(w) = sin(pi w)/(pi w), in double stored as
+ * float; the stencil must lie inside the array.  The reference's sinc path
+ * rejects every in-bounds stencil (its bounds test is inverted), so no output
+ * of it exists to match: this is that path with the test written the right
+ * way round.  compat = 1 keeps the reference's dipole arithmetic (shifts
+ * truncated to int; the linear second pole's y offset divided by dz; the sinc
+ * second pole with positive weights); compat = 0 corrects it (float shifts,
+ * dy, negative second-pole weights for both methods).  With compat = 1 and
+ * the linear method this is e3d_space_interp_linear. */
+#define E3D_INTERP_LINEAR 0
+#define E3D_INTERP_SINC 1
+int e3d_space_interp(int method, int h_filter, const float* z, const float* x, const float* y, long long n_dev,
+                     int nz, int nx, int ny, float oz, float ox, float oy, float dz, float dx, float dy,
+                     const int* pads6, float error_tolerance, int dipole, float zshift, float xshift, float yshift,
+                     int compat, long long* index, float* weight, long long* unique, long long* slot,
+                     long long* n_unique);
+
 #ifdef __cplusplus
 }
 #endif

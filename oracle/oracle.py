@@ -185,21 +185,14 @@ class GridAxis:
     d: float
 
 
-def space_interp_linear(z, x, y, axes, pads, nt, dipole=0, shifts=(0.0, 0.0, 0.0)):
-    """calcLinearWeights + convertIrregToReg with the reference's float arithmetic.
-
-    axes: (zAxis, xAxis, yAxis) GridAxis of the (possibly shifted) grid.
-    pads: dict with fat, zPadMinus, zPadPlus, xPadMinus, xPadPlus, yPad.
-    The dipole shifts are stored as int by the reference class (truncated), and
-    the dipole y weight divides by dz (spaceInterpGpu_3D.h:25, .cpp:287).
-    """
-    f32, f64 = np.float32, np.float64
+def _check_inside(z, x, y, axes, pads):
+    """checkOutOfBounds (spaceInterpGpu_3D.cpp:178-212): devices inside the model interior,
+    float arithmetic with the error tolerance."""
+    f32 = np.float32
     za, xa, ya = axes
     oz, dz, ox, dx, oy, dy = (f32(za.o), f32(za.d), f32(xa.o), f32(xa.d), f32(ya.o), f32(ya.d))
     nz, nx, ny = za.n, xa.n, ya.n
-    z = np.asarray(z, dtype=f32); x = np.asarray(x, dtype=f32); y = np.asarray(y, dtype=f32)
     fat = pads["fat"]
-    # checkOutOfBounds (spaceInterpGpu_3D.cpp:178-212)
     tol = f32(pads.get("errorTolerance", 1e-6))
     nzS = nz - 2 * fat - pads["zPadMinus"] - pads["zPadPlus"]
     nxS = nx - 2 * fat - pads["xPadMinus"] - pads["xPadPlus"]
@@ -215,10 +208,45 @@ def space_interp_linear(z, x, y, axes, pads, nt, dipole=0, shifts=(0.0, 0.0, 0.0
     if np.any(bad):
         raise RuntimeError("spaceInterpGpu_3D: device out of bounds")
 
+
+def _unique_slots(idx):
+    """convertIrregToReg (spaceInterpGpu_3D.cpp:113-138): unique indices in first-seen order,
+    keyed as the reference's std::map<int,int> is, by the index converted to int."""
+    flat = idx.reshape(-1).astype(np.int32).astype(np.int64)
+    seen = {}
+    uniq = []
+    slots = np.empty(flat.shape, dtype=np.int64)
+    for i, v in enumerate(flat.tolist()):
+        s = seen.get(v)
+        if s is None:
+            s = len(uniq)
+            seen[v] = s
+            uniq.append(v)
+        slots[i] = s
+    return np.asarray(uniq, dtype=np.int64), slots.reshape(idx.shape)
+
+
+def space_interp_linear(z, x, y, axes, pads, nt, dipole=0, shifts=(0.0, 0.0, 0.0), compat=True):
+    """calcLinearWeights + convertIrregToReg with the reference's float arithmetic.
+
+    axes: (zAxis, xAxis, yAxis) GridAxis of the (possibly shifted) grid.
+    pads: dict with fat, zPadMinus, zPadPlus, xPadMinus, xPadPlus, yPad.
+    With compat the dipole shifts are truncated to int, as the reference class stores
+    them, and the dipole y weight divides by dz (spaceInterpGpu_3D.h:25, .cpp:287);
+    without, the shifts stay float and y divides by dy.
+    """
+    f32, f64 = np.float32, np.float64
+    za, xa, ya = axes
+    oz, dz, ox, dx, oy, dy = (f32(za.o), f32(za.d), f32(xa.o), f32(xa.d), f32(ya.o), f32(ya.d))
+    nz, nx, ny = za.n, xa.n, ya.n
+    z = np.asarray(z, dtype=f32); x = np.asarray(x, dtype=f32); y = np.asarray(y, dtype=f32)
+    fat = pads["fat"]
+    _check_inside(z, x, y, axes, pads)
+
     def corners(zc, xc, yc, sign):
         wz = (zc - oz) / dz
         wx = (xc - ox) / dx
-        wy = (yc - oy) / (dz if sign < 0 else dy)
+        wy = (yc - oy) / (dz if sign < 0 and compat else dy)
         zr = wz.astype(np.int64); xr = wx.astype(np.int64); yr = wy.astype(np.int64)
         wz = f32(1.0) - (wz - zr.astype(f32))
         wx = f32(1.0) - (wx - xr.astype(f32))
@@ -250,24 +278,74 @@ def space_interp_linear(z, x, y, axes, pads, nt, dipole=0, shifts=(0.0, 0.0, 0.0
 
     idx, w = corners(z, x, y, +1)
     if dipole:
-        sz, sx, sy = (int(s) for s in shifts)
-        idx2, w2 = corners(z + f32(sz), x + f32(sx), y + f32(sy), -1)
+        sz, sx, sy = (f32(int(s)) if compat else f32(s) for s in shifts)
+        idx2, w2 = corners(z + sz, x + sx, y + sy, -1)
         idx = np.concatenate([idx, idx2], axis=1)
         w = np.concatenate([w, w2], axis=1)
-    # convertIrregToReg: unique indices in first-seen order (std::map<int,int> keys)
-    flat = idx.reshape(-1).astype(np.int32).astype(np.int64)
-    seen = {}
-    uniq = []
-    slots = np.empty(flat.shape, dtype=np.int64)
-    for i, v in enumerate(flat.tolist()):
-        s = seen.get(v)
-        if s is None:
-            s = len(uniq)
-            seen[v] = s
-            uniq.append(v)
-        slots[i] = s
-    return SpaceInterp(index=idx, weight=w, unique=np.asarray(uniq, dtype=np.int64),
-                       slot=slots.reshape(idx.shape), nt=nt)
+    uniq, slots = _unique_slots(idx)
+    return SpaceInterp(index=idx, weight=w, unique=uniq, slot=slots, nt=nt)
+
+
+def _sinc_of_arg(a):
+    """sin(a)/a in float64 with its limit 1 at 0: the Taylor series 1 - a^2/6 + a^4/120 below
+    |a| = 1.2e-4 (the published small-argument form of boost::math::sinc_pi, the function the
+    reference calls, spaceInterpGpu_3D.cpp:409)."""
+    a = np.asarray(a, dtype=np.float64)
+    small = np.abs(a) < 1.2e-4
+    a2 = a * a
+    safe = np.where(small, 1.0, a)
+    return np.where(small, 1.0 - a2 / 6.0 + a2 * a2 / 120.0, np.sin(safe) / safe)
+
+
+def space_interp_sinc(z, x, y, axes, pads, nt, h, dipole=0, shifts=(0.0, 0.0, 0.0), compat=True):
+    """calcSincWeights + convertIrregToReg (spaceInterpGpu_3D.cpp:351-480).
+
+    Per device, the 2h points r-h+1 .. r+h on each axis around the cell corner r below it,
+    y then x then z (z fastest), with weight sinc(pi wz) sinc(pi wx) sinc(pi wy) in float64
+    stored as float32, w = (device - point) / d in float32.  The reference's bounds test is
+    inverted (it rejects every in-bounds stencil, so its sinc path never returns and no output
+    of it exists: parity unpinned); here the stencil must lie inside the array.  Dipole: the
+    second pole at the shifted position, shifts truncated to int with compat (as the reference
+    class stores them) and with positive weights, as the reference's code has it; without
+    compat, float shifts and negative weights, as the linear dipole.
+    """
+    f32, f64 = np.float32, np.float64
+    za, xa, ya = axes
+    oz, dz, ox, dx, oy, dy = (f32(za.o), f32(za.d), f32(xa.o), f32(xa.d), f32(ya.o), f32(ya.d))
+    nz, nx, ny = za.n, xa.n, ya.n
+    z = np.asarray(z, dtype=f32); x = np.asarray(x, dtype=f32); y = np.asarray(y, dtype=f32)
+    _check_inside(z, x, y, axes, pads)
+    offs = np.arange(2 * h, dtype=np.int64) - h + 1
+
+    def pole(zc, xc, yc):
+        rz = ((zc - oz) / dz).astype(np.int64)
+        rx = ((xc - ox) / dx).astype(np.int64)
+        ry = ((yc - oy) / dy).astype(np.int64)
+        for r, n in ((ry, ny), (rx, nx), (rz, nz)):
+            if np.any(r - h + 1 < 0) or np.any(r + h >= n):
+                raise RuntimeError("spaceInterpGpu_3D: sinc stencil outside the grid")
+        pz, px, py = rz[:, None] + offs, rx[:, None] + offs, ry[:, None] + offs   # (n, 2h)
+        wz = (zc[:, None] - (pz.astype(f32) * dz + oz)) / dz
+        wx = (xc[:, None] - (px.astype(f32) * dx + ox)) / dx
+        wy = (yc[:, None] - (py.astype(f32) * dy + oy)) / dy
+        sz = _sinc_of_arg(np.pi * wz.astype(f64))
+        sx = _sinc_of_arg(np.pi * wx.astype(f64))
+        sy = _sinc_of_arg(np.pi * wy.astype(f64))
+        w = (sz[:, None, None, :] * sx[:, None, :, None]) * sy[:, :, None, None]
+        idx = (nz * nx * py[:, :, None, None] + nz * px[:, None, :, None] + pz[:, None, None, :])
+        n = zc.shape[0]
+        return idx.reshape(n, -1), w.astype(f32).reshape(n, -1)
+
+    idx, w = pole(z, x, y)
+    if dipole:
+        sz, sx, sy = (f32(int(s)) if compat else f32(s) for s in shifts)
+        idx2, w2 = pole(z + sz, x + sx, y + sy)
+        if not compat:
+            w2 = -w2
+        idx = np.concatenate([idx, idx2], axis=1)
+        w = np.concatenate([w, w2], axis=1)
+    uniq, slots = _unique_slots(idx)
+    return SpaceInterp(index=idx, weight=w, unique=uniq, slot=slots, nt=nt)
 
 
 def staggered_axes(nz, nx, ny, oz, ox, oy, dz, dx, dy):
