@@ -1,6 +1,7 @@
 """CPU: the C++ operator module loads, and its host parts (parameters, acquisition mapping)
 agree with the Python host preparation bit for bit."""
 import numpy as np
+import pytest
 
 from operator_case import OperatorCase
 from elasticisolib_3d_b200 import hostprep as H
@@ -22,6 +23,26 @@ def test_space_interp_matches_python_host_preparation():
         cpp = P.spaceInterpGpu_3D(z, x, y, grids[g], c.nts, par)
         np.testing.assert_array_equal(np.asarray(cpp.getRegPosUnique()), c.rec_dev[g].getRegPosUnique())
         assert cpp.getNDeviceIrreg() == c.rec_dev[g].getNDeviceIrreg()
+
+
+@pytest.mark.parametrize("method,h,dipole,compat", [("linear", 1, 1, 1), ("linear", 1, 1, 0), ("sinc", 2, 0, 1),
+                                                     ("sinc", 2, 1, 0)])
+def test_space_interp_methods_match_python_host_preparation(method, h, dipole, compat):
+    c = OperatorCase()
+    par = P.paramObj(dict(c.par))
+    grids = _cpp_grids(c)
+    za, xa, ya = c.axes
+    ax7 = H.grid_axes(za.n, xa.n, ya.n, za.o, xa.o, ya.o, za.d, xa.d, ya.d)
+    # the receivers line the interior's edges, where a shifted linear pole would leave it: use
+    # the sources of every shot
+    z, x, y = (np.concatenate([np.atleast_1d(s[k]) for s in c.sv.src_xyz]) for k in range(3))
+    shifts = (float(za.d), 0.5 * float(xa.d), float(ya.d))
+    for g in (0, 3, 6):
+        cpp = P.spaceInterpGpu_3D(z, x, y, grids[g], c.nts, par, dipole, *shifts, method, h, compat)
+        py = H.spaceInterpGpu_3D(z, x, y, ax7[g], c.nts, c.par, dipole, *shifts, interpMethod=method,
+                                 hFilter1d=h, compat=bool(compat))
+        np.testing.assert_array_equal(np.asarray(cpp.getRegPosUnique()), py.getRegPosUnique())
+        assert cpp.getNDeviceIrreg() == py.getNDeviceIrreg()
 
 
 def test_param_object_defaults():
