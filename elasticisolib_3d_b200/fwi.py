@@ -97,8 +97,8 @@ class DeviceSet:
     """Nine-component concatenated regular-grid points of one device set."""
     pos: torch.Tensor        # (ntot,) int64
     off: list                # 10 offsets
-    slot: list               # per grid: (nIrreg, 8) int64 into that grid's unique list
-    weight: list             # per grid: (nIrreg, 8) float32
+    slot: list               # per grid: (nIrreg, nTaps) int64 into that grid's unique list
+    weight: list             # per grid: (nIrreg, nTaps) float32 (8 trilinear, (2h)^3 sinc, doubled by a dipole)
     n_irreg: int
 
     @staticmethod
