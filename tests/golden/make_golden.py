@@ -11,7 +11,9 @@ Inputs are not stored: they are regenerated from the seeds below by the same
 code (synthetic.small_survey + the oracle's host preparation), and a digest
 of them is stored so a drift in input generation is detected.
 
-Usage (GPU box):  python tests/golden/make_golden.py
+Usage (on a machine with a GPU):  python tests/golden/make_golden.py [COPY_DIR]
+COPY_DIR, when given and present, receives a second copy of the .npz (for
+runs whose working tree does not persist).
 """
 from __future__ import annotations
 
@@ -93,10 +95,8 @@ def main():
     path = os.path.join(ROOT, "tests", "golden", "ref_small.npz")
     os.makedirs(os.path.dirname(path), exist_ok=True)
     np.savez_compressed(path, **out)
-    # a copy in the folder that returns from the GPU box
-    gdir = os.path.join(ROOT, "gpurun_out")
-    if os.path.isdir(gdir):
-        np.savez_compressed(os.path.join(gdir, "ref_small.npz"), **out)
+    if len(sys.argv) > 1 and os.path.isdir(sys.argv[1]):
+        np.savez_compressed(os.path.join(sys.argv[1], "ref_small.npz"), **out)
     print("wrote", path, os.path.getsize(path), "bytes")
 
 
