@@ -1,5 +1,5 @@
-"""GPU: the autograd FWI misfit/gradient against the FP64 oracle (
-gradient relative error <= 1e-3 against FP64)."""
+"""GPU: the autograd FWI misfit/gradient against the FP64 oracle (accuracy bound of the
+compressed-checkpoint path: gradient relative error <= 1e-3 against FP64)."""
 import numpy as np
 import pytest
 import torch

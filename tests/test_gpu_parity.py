@@ -2,7 +2,7 @@
 
 Tolerances: relative L2 over all traces.  FP32 CUDA vs FP32 oracle differ
 only by summation order/FMA contraction (1e-5); FP32 vs the FP64 oracle is
-the north-star accuracy bound (1e-5 for forward traces, 1e-4 for the Born
+the accuracy bound of the FP32 path (1e-5 for forward traces, 1e-4 for the Born
 image, whose imaging condition multiplies two propagated fields).
 """
 import numpy as np

@@ -81,7 +81,7 @@ def test_born_adjoint_pinned(golden, suf):
     assert _rel(got.astype(np.float64).ravel(), fx[f"born_adj_{suf}"].astype(np.float64).ravel()) < TOL[suf]
 
 
-def test_fp32_reference_within_north_star_of_fp64(golden):
+def test_fp32_reference_within_1e5_of_fp64(golden):
     """The reference's own FP32 traces against its FP64 traces (relative L2 <= 1e-5)."""
     fx, _ = golden
     for k in ("nl_fwd", "born_fwd"):
