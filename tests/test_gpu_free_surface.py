@@ -17,47 +17,15 @@ from elasticisolib_3d_b200 import hostprep as H
 from elasticisolib_3d_b200 import synthetic as S
 from elasticisolib_3d_b200._native import E3DError
 from elasticisolib_3d_b200.engine import COMP_GRID, Propagator
+from free_surface_case import half_space, moveout_velocity, oracle_params, prep
 from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu
-FAT = 4
-
-
-def _half_space(nzi, nxi, nyi, pad, d=10.0, nts=40, vp=2500.0, vs=2500.0 / np.sqrt(3.0), rho=2000.0,
-                smooth=0.0, seed=0):
-    """Grid whose first updated row is the free surface (no top pad), sponge elsewhere."""
-    # nz-2*FAT and nx-2*FAT multiples of 16 (the reference's block rule, fdParamElastic_3D QC)
-    zpp = pad + (-(nzi + pad)) % 16
-    xpp = pad + (-(nxi + 2 * pad)) % 16
-    nz = FAT + nzi + zpp + FAT
-    nx = FAT + pad + nxi + xpp + FAT
-    ny = FAT + pad + nyi + pad + FAT
-    axes = (H.Axis(nz, -FAT * d, d), H.Axis(nx, -(FAT + pad) * d, d), H.Axis(ny, -(FAT + pad) * d, d))
-    pads = dict(zPadMinus=0, zPadPlus=zpp, xPadMinus=pad, xPadPlus=xpp, yPad=pad)
-    par = S.base_params(axes, pads, nts, 0.002, 2, 30.0, free_surface=True)
-    shape = (ny, nx, nz)
-    if smooth:
-        vpf, vsf, rhof = S.gaussian_perturbed_model(shape, vp, vs, rho, smooth, 2.0, seed)
-    else:
-        vpf, vsf, rhof = (np.full(shape, v) for v in (vp, vs, rho))
-    return S.elastic_from_velocity(vpf, vsf, rhof), axes, par
-
-
-def _prep(el, axes, par):
-    fd = H.FdParam(el, axes, par)
-    za, xa, ya = axes
-    ax7 = H.grid_axes(za.n, xa.n, ya.n, za.o, xa.o, ya.o, za.d, xa.d, ya.d)
-    return fd, ax7
 
 
 def _prop(fd, free_surface, q2compat=1):
     return Propagator(fd.nz, fd.nx, fd.ny, fd.nts, fd.sub, fd.minPad, float(fd.dz), float(fd.dx), float(fd.dy),
                       float(fd.dts), float(fd.alphaCos), q2compat=q2compat, free_surface=free_surface)
-
-
-def _oracle_params(fd, free_surface):
-    return O.PropParams(fd.nz, fd.nx, fd.ny, fd.nts, fd.sub, fd.minPad, float(fd.dz), float(fd.dx), float(fd.dy),
-                        float(fd.dts), alphaCos=float(fd.alphaCos), free_surface=free_surface)
 
 
 def _rel(a, b):
@@ -68,8 +36,8 @@ def _rel(a, b):
 
 @pytest.mark.parametrize("loader", ["plain", "tma"])
 def test_free_surface_matches_oracle(loader):
-    el, axes, par = _half_space(24, 24, 16, 6, nts=40, smooth=0.08, seed=2)
-    fd, ax7 = _prep(el, axes, par)
+    el, axes, par = half_space(24, 24, 16, 6, nts=40, smooth=0.08, seed=2)
+    fd, ax7 = prep(el, axes, par)
     rng = np.random.default_rng(3)
     src = H.build_devices(np.array([20.0]), np.array([110.0]), np.array([70.0]), ax7, fd.nts, par)
     rz, rx, ry = rng.uniform(0.0, 150.0, 12), rng.uniform(10.0, 220.0, 12), rng.uniform(10.0, 140.0, 12)
@@ -82,12 +50,12 @@ def test_free_surface_matches_oracle(loader):
     pr.set_stepper_variant(8, 2, loader)
     pr.set_medium(fd.planes)
     got = pr.nl_forward(sig, spos, rpos)
-    p = _oracle_params(fd, 1)
+    p = oracle_params(fd, 1)
     ref64 = O.nl_forward_reg(p, fd.planes.astype(np.float64), [s.astype(np.float64) for s in sig], spos, rpos,
                              np.float64)
     assert _rel(got, ref64) < 1e-5
     # without the free surface the traces differ clearly (the check above is not vacuous)
-    ref_nofs = O.nl_forward_reg(_oracle_params(fd, 0), fd.planes, sig, spos, rpos, np.float32)
+    ref_nofs = O.nl_forward_reg(oracle_params(fd, 0), fd.planes, sig, spos, rpos, np.float32)
     assert _rel(got, ref_nofs) > 1e-2
     dat = [rng.standard_normal((len(rpos[COMP_GRID[k]]), fd.nts)).astype(np.float32) for k in range(9)]
     got_a = pr.nl_adjoint(dat, spos, rpos)
@@ -97,8 +65,8 @@ def test_free_surface_matches_oracle(loader):
 
 
 def test_zero_traction_on_the_surface():
-    el, axes, par = _half_space(24, 32, 24, 6, nts=60)
-    fd, ax7 = _prep(el, axes, par)
+    el, axes, par = half_space(24, 32, 24, 6, nts=60)
+    fd, ax7 = prep(el, axes, par)
     src = H.build_devices(np.array([30.0]), np.array([150.0]), np.array([110.0]), ax7, fd.nts, par)
     xs = np.linspace(60.0, 250.0, 8)
     rec = H.build_devices(np.zeros(8), xs, np.full(8, 115.0), ax7, fd.nts, par)
@@ -121,8 +89,8 @@ def test_zero_traction_on_the_surface():
 
 def _surface_vz(free_surface):
     d = 10.0
-    el, axes, par = _half_space(40, 140, 40, 20, d=d, nts=520)
-    fd, ax7 = _prep(el, axes, par)
+    el, axes, par = half_space(40, 140, 40, 20, d=d, nts=520)
+    fd, ax7 = prep(el, axes, par)
     src = H.build_devices(np.array([0.0]), np.array([100.0]), np.array([200.0]), ax7, fd.nts, par)
     xr = np.array([500.0, 1100.0])
     rec = H.build_devices(np.full(2, 10.0), xr, np.full(2, 200.0), ax7, fd.nts, par)
@@ -136,31 +104,18 @@ def _surface_vz(free_surface):
     return vz.astype(np.float64), xr[1] - xr[0]
 
 
-def _moveout_velocity(vz, dx):
-    a, b = vz[0] - vz[0].mean(), vz[1] - vz[1].mean()
-    cc = np.correlate(b, a, mode="full")
-    lag = int(np.argmax(cc)) - (len(a) - 1)
-    # parabolic refinement of the peak
-    i = int(np.argmax(cc))
-    if 0 < i < len(cc) - 1:
-        den = cc[i - 1] - 2 * cc[i] + cc[i + 1]
-        if den != 0:
-            lag += 0.5 * (cc[i - 1] - cc[i + 1]) / den
-    return dx / (lag * 0.002)
-
-
 def test_rayleigh_wave_moveout():
     vs = 2500.0 / np.sqrt(3.0)
     c_r = 0.9194 * vs
     vz, dx = _surface_vz(1)
-    c = _moveout_velocity(vz, dx)
+    c = moveout_velocity(vz, dx)
     assert abs(c - c_r) / c_r < 0.03, (c, c_r)
     assert c < 0.97 * vs
 
 
 def test_born_and_fwi_refuse_the_free_surface():
-    el, axes, par = _half_space(24, 24, 16, 6, nts=20)
-    fd, ax7 = _prep(el, axes, par)
+    el, axes, par = half_space(24, 24, 16, 6, nts=20)
+    fd, ax7 = prep(el, axes, par)
     src = H.build_devices(np.array([20.0]), np.array([110.0]), np.array([70.0]), ax7, fd.nts, par)
     rec = H.build_devices(np.array([0.0]), np.array([50.0]), np.array([50.0]), ax7, fd.nts, par)
     spos = [d.getRegPosUnique() for d in src]
