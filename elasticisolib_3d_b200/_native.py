@@ -15,6 +15,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libelastic3d_b200.so")
 
 E3D_OK = 0
+E3D_ERR_OOM = 4
 STATUS = {0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "call out of order", 4: "out of device memory",
           5: "acquisition device out of bounds"}
 
@@ -68,6 +69,7 @@ SIGNATURES = {
     "e3d_velocity_storage": ([P], I),
     "e3d_checkpoint_type": ([P], I),
     "e3d_checkpoint_schedule": ([I, I, P, I, P], I),
+    "e3d_checkpoint_plan": ([LL, I, I, D, I, I, I, P, P, P, P], I),
     "e3d_step_only": ([P, I, I], I),
     "e3d_kernel_timing": ([P, I], I),
     "e3d_kernel_timing_read": ([P, I, P, P], I),

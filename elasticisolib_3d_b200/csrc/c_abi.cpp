@@ -334,6 +334,21 @@ int e3d_checkpoint_schedule(int blocks, int segment_len, int* seg_start, int max
   return nseg;
 }
 
+int e3d_checkpoint_plan(long long n_cells, int ny, int nts, double budget_bytes, int ckpt_type, int velocity_type,
+                        int segment, int* ckpt_used, int* velocity_used, int* segment_len, double* plan_bytes) {
+  if (n_cells < 1 || ny < 1 || nts < 2 || ckpt_type < -1 || ckpt_type > 2 || velocity_type < -1 ||
+      velocity_type > 1 || segment < 0)
+    return E3D_ERR_ARG;
+  e3d::schedule::Plan p{};
+  if (!e3d::schedule::choosePlan(n_cells, ny, nts, budget_bytes, ckpt_type, velocity_type, segment, p))
+    return E3D_ERR_OOM;
+  if (ckpt_used) *ckpt_used = p.ck;
+  if (velocity_used) *velocity_used = p.vt;
+  if (segment_len) *segment_len = p.L;
+  if (plan_bytes) *plan_bytes = e3d::schedule::planBytes(n_cells, ny, nts, p.ck, p.vt, p.L);
+  return E3D_OK;
+}
+
 int e3d_nl_forward(e3d_context* ctx, const float* const* model9, float* const* data9, const long long* const* src_pos,
                    const long long* n_src, const long long* const* rec_pos, const long long* n_rec) {
   CTX_OR_FAIL(ctx);

@@ -1188,47 +1188,18 @@ static int bornForwardDevice(Context* c, const DevSignals& srcSet, const DevSign
 // goes, so the adjoint pass recomputes every segment but the last (which is
 // the longest, hence the end alignment).
 // The plan (segment length, checkpoint storage, velocity-slot storage) is
-// chosen among
-//   FP32 states + FP32 velocity slots, FP16 states + FP32 slots,
-//   FP16 states + FP16 slots (auto); for an explicit state type T:
-//   T + FP32 slots, T + FP16 slots;
-// each at the longest segment that fits the memory budget, taking the plan
-// that recomputes the fewest blocks once a lower-precision plan is charged a
-// margin (5% of the blocks for 16-bit states, 15% for 16-bit slots): a
-// 16-bit plan is taken only where it removes that much recomputation.
+// schedule::choosePlan's for the memory budget autoBudget gives.
 // ---------------------------------------------------------------------------
 enum { V_F32 = 0, V_F16 = 1 };
 
-using schedule::recomputedBlocks;
 using schedule::segStart;
 
 static size_t ckptBytesPerState(const Context* c, int type) {
-  const size_t eb = type == CKPT_F32 ? 4 : 2;
-  size_t b = (size_t)18 * c->g.n * eb;
-  if (type != CKPT_F32) b += (size_t)18 * c->d.ny * sizeof(float) + 256;
-  return b;
+  return (size_t)schedule::stateBytes(c->g.n, c->d.ny, type);
 }
-
-// FP16 velocity slot: three fields of n halves, padded to 256 B, then 3*ny scales.
-static size_t vHalfBytes(const Context* c) { return ((size_t)3 * c->g.n * 2 + 255) / 256 * 256; }
-static size_t vStoreBytes(const Context* c) { return vHalfBytes(c) + (size_t)3 * c->d.ny * sizeof(float); }
-static double vSlotBytes(const Context* c, int vt) {
-  return vt == V_F32 ? 3.0 * (double)c->g.n * sizeof(float) : (double)vStoreBytes(c);
-}
-
-// Checkpoints plus velocity slots of a plan with segment length L.  FP32 slots
-// hold V[b .. b+L+2] of a segment starting at block b (the last one partial,
-// from the recompute's final block); FP16 slots hold V[b .. b+L+1] plus three FP32
-// working slots (two accumulators while recomputing, a three-deep ring for
-// the imaging condition).
-static double planBytes(const Context* c, int ck, int vt, int L) {
-  const int blocks = c->d.nts - 1;
-  const int nseg = (blocks + L - 1) / L;
-  double b = (double)(nseg - 1) * ckptBytesPerState(c, ck);
-  if (vt == V_F32) b += (L + 3) * vSlotBytes(c, V_F32);
-  else b += (L + 2) * vSlotBytes(c, V_F16) + 3 * vSlotBytes(c, V_F32);
-  return b;
-}
+static size_t vHalfBytes(const Context* c) { return schedule::halfSlotValuesBytes(c->g.n); }
+static size_t vStoreBytes(const Context* c) { return schedule::halfSlotBytes(c->g.n, c->d.ny); }
+static double vSlotBytes(const Context* c, int vt) { return schedule::slotBytes(c->g.n, c->d.ny, vt); }
 
 static double heldBytes(const Context* c) {
   double b = 0;
@@ -1259,54 +1230,19 @@ static double autoBudget(const Context* c, size_t free) {
 }
 
 static int choosePlan(Context* c, int& L) {
-  const int blocks = c->d.nts - 1;
-  struct Cand {
-    int ck, vt;
-  };
-  const Cand autoList[3] = {{CKPT_F32, V_F32}, {CKPT_F16, V_F32}, {CKPT_F16, V_F16}};
-  const Cand typedList[2] = {{c->ckptType, V_F32}, {c->ckptType, V_F16}};
-  const Cand* all = c->ckptType == CKPT_AUTO ? autoList : typedList;
-  const int nAll = c->ckptType == CKPT_AUTO ? 3 : 2;
-  std::vector<Cand> cands;
-  for (int i = 0; i < nAll; i++)
-    if (c->vType < 0 || all[i].vt == c->vType) cands.push_back(all[i]);
   size_t free = 0, total = 0;
   E3D_CUDA_TRY(cudaMemGetInfo(&free, &total));
   // memory this context already holds for checkpoints and velocity slots counts as available
   const double budget = autoBudget(c, free) + heldBytes(c);
-  if (c->segment > 0) {
-    // explicit segment length: the first candidate that fits it, else the last
-    const int l = std::min(c->segment, blocks);
-    for (size_t i = 0; i < cands.size(); i++)
-      if (planBytes(c, cands[i].ck, cands[i].vt, l) <= budget || i + 1 == cands.size()) {
-        c->ckptUsed = cands[i].ck;
-        c->vUsed = cands[i].vt;
-        L = l;
-        return E3D_OK;
-      }
+  schedule::Plan plan{};
+  if (!schedule::choosePlan(c->g.n, c->d.ny, c->d.nts, budget, c->ckptType, c->vType, c->segment, plan)) {
+    setLastError("wavefield checkpoints do not fit in device memory", __FILE__, __LINE__);
+    return E3D_ERR_OOM;
   }
-  int best = -1;
-  double bestCost = 0;
-  for (size_t i = 0; i < cands.size(); i++) {
-    const Cand& k = cands[i];
-    int l = blocks;
-    while (l >= 1 && planBytes(c, k.ck, k.vt, l) > budget) l--;
-    if (l < 1) continue;
-    const double cost = recomputedBlocks(blocks, l) + blocks * ((k.ck != CKPT_F32 ? 0.05 : 0.0) +
-                                                                (k.vt == V_F16 ? 0.15 : 0.0));
-    if (best < 0 || cost < bestCost) {
-      best = (int)i;
-      bestCost = cost;
-      L = l;
-    }
-  }
-  if (best >= 0) {
-    c->ckptUsed = cands[best].ck;
-    c->vUsed = cands[best].vt;
-    return E3D_OK;
-  }
-  setLastError("wavefield checkpoints do not fit in device memory", __FILE__, __LINE__);
-  return E3D_ERR_OOM;
+  c->ckptUsed = plan.ck;
+  c->vUsed = plan.vt;
+  L = plan.L;
+  return E3D_OK;
 }
 
 static int resizeVStorage(Context* c, int nF32, int nF16) {

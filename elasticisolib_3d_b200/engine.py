@@ -39,6 +39,22 @@ def checkpoint_schedule(blocks, segment_len):
     return list(starts[:n + 1]), rec.value
 
 
+def checkpoint_plan(n_cells, ny, nts, budget_bytes, ckpt="auto", velocity="auto", segment=0):
+    """The checkpoint plan the engine chooses for a padded grid of n_cells cells in ny y slices,
+    nts coarse samples and budget_bytes for checkpoints and velocity slots: (state storage,
+    velocity-slot storage, segment length, plan bytes), or None when nothing fits.  Host
+    arithmetic only."""
+    ck, vt, L, b = ctypes.c_int(0), ctypes.c_int(0), ctypes.c_int(0), ctypes.c_double(0)
+    st = int(N.lib().e3d_checkpoint_plan(int(n_cells), int(ny), int(nts), float(budget_bytes), CKPT_TYPES[ckpt],
+                                         {"auto": -1, "fp32": 0, "fp16": 1}[velocity], int(segment),
+                                         ctypes.byref(ck), ctypes.byref(vt), ctypes.byref(L), ctypes.byref(b)))
+    if st == N.E3D_ERR_OOM:
+        return None
+    if st != N.E3D_OK:
+        raise ValueError(f"bad checkpoint plan arguments (status {st})")
+    return ("fp32", "fp16", "bf16")[ck.value], ("fp32", "fp16")[vt.value], L.value, b.value
+
+
 class Propagator:
     def __init__(self, nz, nx, ny, nts, sub, minPad, dz, dx, dy, dts, alphaCos=0.99, device=0, fix_q1=0,
                  q2compat=1, q3compat=1, free_surface=0):

@@ -277,6 +277,16 @@ int e3d_checkpoint_type(const e3d_context* ctx);
  * reference, whose Born adjoint stores the whole source wavefield on the host
  * (BornElasticGpuFunctions_3D.cu:1268-1316). */
 int e3d_checkpoint_schedule(int blocks, int segment_len, int* seg_start, int max_segments, int* recomputed);
+/* The checkpoint plan the checkpointed passes choose for a padded grid of
+ * n_cells cells in ny y slices, nts coarse samples and budget_bytes of device
+ * memory for checkpoints and velocity slots (the passes use 85% of the free
+ * memory, less the caller's reserve and the adjoint pass's working fields):
+ * ckpt_type / velocity_type / segment as in e3d_set_checkpoint_policy and
+ * e3d_set_velocity_storage.  Outputs (each may be NULL): the state and slot
+ * storage types, the segment length and the plan's bytes.  E3D_ERR_OOM when
+ * nothing fits.  No device work. */
+int e3d_checkpoint_plan(long long n_cells, int ny, int nts, double budget_bytes, int ckpt_type, int velocity_type,
+                        int segment, int* ckpt_used, int* velocity_used, int* segment_len, double* plan_bytes);
 
 /* Host-buffer propagations.  src_pos/rec_pos: 7 tables; n_src/n_rec: 7 counts. */
 int e3d_nl_forward(e3d_context* ctx, const float* const* model9, float* const* data9,

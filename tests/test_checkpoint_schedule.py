@@ -64,3 +64,54 @@ def test_recompute_shrinks_with_the_segment():
     """Longer segments recompute fewer blocks; one segment recomputes none."""
     counts = [checkpoint_schedule(999, L)[1] for L in (50, 100, 200, 500, 998, 999)]
     assert counts == sorted(counts, reverse=True) and counts[-1] == 0
+
+
+# ---- memory plan (e3d_checkpoint_plan: the choice the checkpointed passes make) -------------
+from elasticisolib_3d_b200.engine import checkpoint_plan  # noqa: E402
+
+N288, NY288 = 288 ** 3, 288
+
+
+def test_plan_fits_its_budget_and_prefers_full_precision_when_all_fits():
+    plan = checkpoint_plan(N288, NY288, 1000, 1e13)
+    assert plan[:3] == ("fp32", "fp32", 999)
+    for budget in (3e10, 6e10, 1.0e11, 1.4e11):
+        ck, vt, L, b = checkpoint_plan(N288, NY288, 1000, budget)
+        assert b <= budget
+
+
+def test_plan_takes_16_bit_slots_only_for_a_large_cut_in_recomputation():
+    # 288^3 cells, 1000 samples, 143.6 GB: FP32 slots hold about half the record, FP16 slots
+    # nearly all of it -- the FP16 plan removes ~490 recomputed blocks and wins
+    ck, vt, L, _ = checkpoint_plan(N288, NY288, 1000, 143.6e9)
+    assert (ck, vt) == ("fp16", "fp16") and L > 900
+    assert checkpoint_schedule(999, L)[1] < 50
+    # the all-FP32 plan for the same budget recomputes ~half the record
+    ck, vt, L32, _ = checkpoint_plan(N288, NY288, 1000, 143.6e9, "fp32", "fp32")
+    assert (ck, vt) == ("fp32", "fp32") and checkpoint_schedule(999, L32)[1] > 400
+    # 392^3, 2500 samples: 16-bit slots would cut recomputation by less than their margin
+    ck, vt, L, _ = checkpoint_plan(392 * 392 * 388, 388, 2500, 150e9)
+    assert (ck, vt) == ("fp16", "fp32") and 100 < L < 250
+
+
+def test_plan_respects_explicit_types_and_segment():
+    for ckpt in ("fp32", "fp16", "bf16"):
+        assert checkpoint_plan(N288, NY288, 1000, 1e11, ckpt)[0] == ckpt
+    for vel in ("fp32", "fp16"):
+        assert checkpoint_plan(N288, NY288, 1000, 1e11, velocity=vel)[1] == vel
+    assert checkpoint_plan(N288, NY288, 1000, 1e11, "fp32", "fp32", segment=7)[2] == 7
+    assert checkpoint_plan(N288, NY288, 1000, 1e9) is None
+
+
+def test_plan_cost_falls_with_more_memory():
+    """The chosen plan's cost -- recomputed blocks plus the precision margins (5 % of the blocks
+    for 16-bit states, 15 % for 16-bit slots) -- never rises with the budget.  Recomputation
+    alone may: with 250 GB the all-FP32 plan recomputing 138 blocks beats FP16 slots for the
+    whole record, whose margin is 200 blocks."""
+    prev = None
+    for budget in (3e10, 5e10, 8e10, 1.2e11, 1.6e11, 2.5e11, 3.5e11):
+        ck, vt, L, _ = checkpoint_plan(N288, NY288, 1000, budget)
+        cost = checkpoint_schedule(999, L)[1] + 999 * (0.05 * (ck != "fp32") + 0.15 * (vt == "fp16"))
+        assert prev is None or cost <= prev + 1e-9
+        prev = cost
+    assert prev == 0
