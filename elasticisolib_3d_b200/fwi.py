@@ -290,10 +290,21 @@ class FwiProblem:
         self.data_mask = None
         self.grad_mask = None
 
-    def distribute(self, group=None):
-        """Shard the shots over the ranks of `group` (torch.distributed, one rank per GPU)."""
+    def distribute(self, group=None, dealing="static", store=None, tag="fwi"):
+        """Share the shots among the ranks of `group` (torch.distributed, one rank per GPU).
+        dealing "static": rank r takes shots r, r+world, ...; "dynamic": every rank takes the next
+        undealt shot from a counter in `store` (a torch.distributed Store; by default a client of
+        the rendezvous store at MASTER_ADDR:MASTER_PORT), so that ranks with cheaper shots take
+        more of them.  `tag` names the counters; problems evaluated in the same job need distinct
+        tags."""
+        if dealing not in ("static", "dynamic"):
+            raise ValueError(f"unknown shot dealing {dealing!r}")
         self.distributed = True
         self.group = group
+        self.dealing = dealing
+        self.store = store
+        self.tag = tag
+        self.evaluations = 0
         return self
 
     def _bind_stream(self):
@@ -356,6 +367,34 @@ def shard_shots(n_shots, rank, world):
     return list(range(rank, n_shots, world))
 
 
+def rendezvous_store(timeout_s=300.0):
+    """A client of the store torch.distributed's env:// initialisation (and torchrun) serve at
+    MASTER_ADDR:MASTER_PORT."""
+    import datetime
+    import os
+    return torch.distributed.TCPStore(os.environ["MASTER_ADDR"], int(os.environ["MASTER_PORT"]), is_master=False,
+                                      timeout=datetime.timedelta(seconds=timeout_s))
+
+
+class ShotQueue:
+    """Dynamic dealing of n_shots shots over the ranks that iterate queues with the same key:
+    each step takes the next undealt shot from an atomic counter in a torch.distributed Store,
+    as the reference deals shots to GPUs from an OpenMP loop with a dynamic schedule
+    (nonlinearPropElasticShotsGpu_3D.cpp:178-204).  Every shot is dealt exactly once."""
+
+    def __init__(self, n_shots, key, store):
+        self.n_shots = int(n_shots)
+        self.key = key
+        self.store = store
+
+    def __iter__(self):
+        while True:
+            i = int(self.store.add(self.key, 1)) - 1
+            if i >= self.n_shots:
+                return
+            yield i
+
+
 def reduce_misfit(total, grads, group=None):
     """Sum the misfit and the (rho, lambda, mu) gradient over the ranks of `group`: one
     all-reduce of a flat buffer (NCCL over NVLink between GPUs; the reference sums shot
@@ -398,6 +437,11 @@ class ElasticFwiMisfit(torch.autograd.Function):
         planes = problem.set_model(rho.float().contiguous(), lam.float().contiguous(), mu.float().contiguous())
         if shot_ids is not None:
             ids = shot_ids
+        elif problem.distributed and getattr(problem, "dealing", "static") == "dynamic":
+            if problem.store is None:
+                problem.store = rendezvous_store()
+            ids = ShotQueue(len(problem.shots), f"e3d/shots/{problem.tag}/{problem.evaluations}", problem.store)
+            problem.evaluations += 1
         elif problem.distributed:
             ids = shard_shots(len(problem.shots), torch.distributed.get_rank(problem.group),
                               torch.distributed.get_world_size(problem.group))

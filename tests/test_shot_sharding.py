@@ -68,3 +68,46 @@ def test_two_rank_reduction_matches_serial_sum():
         assert abs(loss - serial_loss) < 1e-9
         for a, b in zip(grads, serial):
             assert torch.allclose(a, b, atol=1e-5)
+
+
+def _dynamic_worker(rank, world, port, n_shots, shape, out):
+    import time
+    from elasticisolib_3d_b200.fwi import ShotQueue, rendezvous_store
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        store = rendezvous_store(timeout_s=60.0)
+        results = []
+        for evaluation in range(2):  # two evaluations: distinct counters, every shot dealt in each
+            total = torch.zeros((), dtype=torch.float64)
+            grads = [torch.zeros(shape) for _ in range(3)]
+            mine = []
+            for i in ShotQueue(n_shots, f"e3d/shots/test/{evaluation}", store):
+                time.sleep(0.02 if rank == 0 else 0.12)  # rank 1's shots are six times as costly
+                l, g = _fake_shot(i, shape)
+                total += l
+                for a, b in zip(grads, g):
+                    a += b
+                mine.append(i)
+            total, grads = reduce_misfit(total, grads)
+            results.append((mine, float(total), [g.clone() for g in grads]))
+        out[rank] = results
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.timeout(120)
+def test_dynamic_dealing_covers_every_shot_once_and_balances():
+    n_shots, shape = 12, (3, 4, 5)
+    mgr = mp.Manager()
+    out = mgr.dict()
+    mp.start_processes(_dynamic_worker, args=(2, _free_port(), n_shots, shape, out), nprocs=2, join=True,
+                       start_method="spawn")
+    serial_loss = sum(float(_fake_shot(i, shape)[0]) for i in range(n_shots))
+    for evaluation in range(2):
+        m0, m1 = out[0][evaluation][0], out[1][evaluation][0]
+        assert sorted(m0 + m1) == list(range(n_shots))
+        assert len(m0) > len(m1)  # the faster rank took more shots
+        for r in range(2):
+            assert abs(out[r][evaluation][1] - serial_loss) < 1e-9
