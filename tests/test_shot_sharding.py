@@ -52,7 +52,7 @@ def test_shards_cover_every_shot_once():
 @pytest.mark.timeout(120)
 def test_two_rank_reduction_matches_serial_sum():
     n_shots, shape = 5, (3, 4, 6)
-    mgr = mp.Manager()
+    mgr = mp.get_context("spawn").Manager()
     out = mgr.dict()
     mp.start_processes(_worker, args=(2, _free_port(), n_shots, shape, out), nprocs=2, join=True,
                        start_method="spawn")
@@ -100,7 +100,7 @@ def _dynamic_worker(rank, world, port, n_shots, shape, out):
 @pytest.mark.timeout(120)
 def test_dynamic_dealing_covers_every_shot_once_and_balances():
     n_shots, shape = 12, (3, 4, 5)
-    mgr = mp.Manager()
+    mgr = mp.get_context("spawn").Manager()
     out = mgr.dict()
     mp.start_processes(_dynamic_worker, args=(2, _free_port(), n_shots, shape, out), nprocs=2, join=True,
                        start_method="spawn")
