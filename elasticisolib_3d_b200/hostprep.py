@@ -20,6 +20,16 @@ FAT = 4
 SUB_MAX = 100
 
 
+def _as_int(v):
+    """int of a parameter value; a decimal string such as "7.5" truncates, as a float does."""
+    if isinstance(v, str):
+        try:
+            return int(v)
+        except ValueError:
+            return int(float(v))
+    return int(v)
+
+
 class ParamObj(dict):
     """Minimal stand-in for SEP's paramObj: getInt/getFloat/getString with defaults.
 
@@ -38,7 +48,7 @@ class ParamObj(dict):
         return default
 
     def getInt(self, key, default=_missing):
-        return self._get(key, default, int)
+        return self._get(key, default, _as_int)
 
     def getFloat(self, key, default=_missing):
         return self._get(key, default, float)

@@ -10,6 +10,8 @@ and the C++ shot operators they wrap:
   BornElasticShotsGpu_3D            (BornElasticShotsGpu_3D.cpp:143-605, BornElasticGpu_3D.cpp:70-330,
                                      seismicElasticOperator3D.cpp:74-228)
   ElasticDatComp_3D                 (seis_utils/python/dataCompModule_3D.py)
+  buildSourceGeometry_3D, buildReceiversGeometry_3D (Elastic_iso_float_3D.py:21-385), with the
+                                     geometry passed as an array instead of a SEP file
 
 Vectors are numpy arrays (or objects with getNdArray(), such as SEP vectors)
 in the numpy view of the reference's hypercubes, slowest axis first:
@@ -55,6 +57,79 @@ def _axes_of(elastic, par):
     return (H.Axis(par.getInt("nz"), par.getFloat("oz", 0.0), par.getFloat("dz")),
             H.Axis(par.getInt("nx"), par.getFloat("ox", 0.0), par.getFloat("dx")),
             H.Axis(par.getInt("ny"), par.getFloat("oy", 0.0), par.getFloat("dy")))
+
+
+def _interp_params(par, receivers):
+    """Dipole, shifts, method and sinc half length as the reference's geometry builders read them
+    (Elastic_iso_float_3D.py:21-60, 194-240): the receiver builder reads the dipole shifts with
+    getInt (truncating them), the source builder with getFloat; sinc sources default hFilter1d
+    to 1, sinc receivers require it."""
+    get = par.getInt if receivers else par.getFloat
+    dipole = par.getInt("dipole", 0)
+    shifts = tuple(float(get(k, 0)) for k in ("zDipoleShift", "xDipoleShift", "yDipoleShift"))
+    method = par.getString("spaceInterpMethod", "linear")
+    if method == "linear":
+        h = 1
+    elif method == "sinc":
+        h = par.getInt("hFilter1d") if receivers else par.getInt("hFilter1d", 1)
+    else:
+        raise ValueError(f"spatial interpolation method {method!r} is not implemented")
+    return dipole, shifts, method, h
+
+
+def _geometry(par, elastic, geom, receivers):
+    za, xa, ya = _axes_of(elastic, par)
+    axes7 = H.grid_axes(za.n, xa.n, ya.n, za.o, xa.o, ya.o, za.d, xa.d, ya.d)
+    g = np.asarray(_nd(geom), dtype=np.float32)
+    if g.ndim != 3 or g.shape[0] != 3:
+        raise ValueError("geometry must be (3, nPoints, nExp) in the numpy view: x, y, z rows")
+    dipole, shifts, method, h = _interp_params(par, receivers)
+    nts = par.getInt("nts")
+    vecs = [[] for _ in range(7)]
+    for e in builtins.range(g.shape[2]):
+        devs = H.build_devices(g[2, :, e], g[0, :, e], g[1, :, e], axes7, nts, par, dipole=dipole, shifts=shifts,
+                               method=method, hFilter1d=h)
+        for k in builtins.range(7):
+            vecs[k].append(devs[k])
+    return vecs
+
+
+def buildSourceGeometry_3D(parObject, elasticParam, sourceGeom):
+    """The reference's source-geometry builder (Elastic_iso_float_3D.py:21-191) with the geometry
+    passed as an array instead of read from the SEP file `sourceGeomFile` (SEP IO is not part of
+    this library): sourceGeom (3, nSimSou, nExp) in the numpy view, rows x, y, z.  Returns the
+    seven per-grid lists of spaceInterpGpu_3D objects (center, x, y, z, xz, xy, yz; one per shot)
+    and the shot axis."""
+    n_exp = parObject.getInt("nExp", -1)
+    if n_exp == -1:
+        raise ValueError("buildSourceGeometry_3D: the total number of shots (nExp) is required")
+    g = np.asarray(_nd(sourceGeom))
+    if g.ndim != 3 or g.shape[2] != n_exp:
+        raise ValueError(f"nExp ({n_exp}) not consistent with the number of shots in the geometry "
+                         f"({g.shape[2] if g.ndim == 3 else 'bad shape'})")
+    return (*_geometry(parObject, elasticParam, g, receivers=False), H.Axis(n_exp, 0.0, 1.0))
+
+
+def buildReceiversGeometry_3D(parObject, elasticParam, receiverGeom):
+    """The reference's receiver-geometry builder (Elastic_iso_float_3D.py:194-385) with the geometry
+    passed as an array instead of read from `receiverGeomFile`: receiverGeom (3, nReceiverPerShot,
+    nExp or 1) in the numpy view, rows x, y, z; one shot-independent set when its last axis is 1.
+    Returns the seven per-grid lists and the receiver axis."""
+    n_exp = parObject.getInt("nExp", -1)
+    if n_exp == -1:
+        raise ValueError("buildReceiversGeometry_3D: the total number of shots (nExp) is required")
+    n_rec = parObject.getInt("nReceiverPerShot", -1)
+    if n_rec == -1:
+        raise ValueError("buildReceiversGeometry_3D: the number of receivers per shot (nReceiverPerShot) is "
+                         "required")
+    g = np.asarray(_nd(receiverGeom))
+    if g.ndim != 3:
+        raise ValueError("geometry must be (3, nReceiverPerShot, nExp or 1)")
+    if g.shape[2] != 1 and g.shape[2] != n_exp:
+        raise ValueError(f"number of shots ({n_exp}) not consistent with the receivers' geometry ({g.shape[2]})")
+    if g.shape[1] != n_rec:
+        raise ValueError(f"nReceiverPerShot ({n_rec}) not consistent with the receivers' geometry ({g.shape[1]})")
+    return (*_geometry(parObject, elasticParam, g, receivers=True), H.Axis(n_rec, 0.0, 1.0))
 
 
 def scale_signals(reg9, devices7, planes, dx, dy, dz):
