@@ -639,6 +639,27 @@ PYBIND11_MODULE(pyElastic_iso_float_3D, m) {
       .def(py::init<std::shared_ptr<hypercube>, py::array_t<float, py::array::c_style>>())
       .def("getHyper", &float4DReg::getHyper)
       .def("getNdArray", &float4DReg::getNdArray);
+  py::class_<fdParamElastic_3D, std::shared_ptr<fdParamElastic_3D>>(m, "fdParamElastic_3D")
+      .def(py::init<const float4DReg&, std::shared_ptr<paramObj>>(), py::arg("elasticParam"), py::arg("par"))
+      .def_readonly("nz", &fdParamElastic_3D::nz)
+      .def_readonly("nx", &fdParamElastic_3D::nx)
+      .def_readonly("ny", &fdParamElastic_3D::ny)
+      .def_readonly("nts", &fdParamElastic_3D::nts)
+      .def_readonly("sub", &fdParamElastic_3D::sub)
+      .def_readonly("minPad", &fdParamElastic_3D::minPad)
+      .def_readonly("freeSurface", &fdParamElastic_3D::freeSurface)
+      .def_readonly("dz", &fdParamElastic_3D::dz)
+      .def_readonly("dx", &fdParamElastic_3D::dx)
+      .def_readonly("dy", &fdParamElastic_3D::dy)
+      .def_readonly("dts", &fdParamElastic_3D::dts)
+      .def_readonly("dtw", &fdParamElastic_3D::dtw)
+      .def_readonly("alphaCos", &fdParamElastic_3D::alphaCos)
+      // the eight 2dtw-scaled medium planes, (8, ny, nx, nz), copied out
+      .def("getPlanes", [](const fdParamElastic_3D& f) {
+        py::array_t<float> out({(ssize_t)8, (ssize_t)f.ny, (ssize_t)f.nx, (ssize_t)f.nz});
+        std::copy(f.planes.begin(), f.planes.end(), out.mutable_data());
+        return out;
+      });
   py::class_<spaceInterpGpu_3D, std::shared_ptr<spaceInterpGpu_3D>>(m, "spaceInterpGpu_3D")
       .def(py::init<py::array_t<float, py::array::c_style | py::array::forcecast>,
                     py::array_t<float, py::array::c_style | py::array::forcecast>,

@@ -51,3 +51,21 @@ def test_param_object_defaults():
     assert abs(par.getFloat("dts") - 0.002) < 1e-9
     assert par.getInt("nGpu", 1) == 1
     assert par.getString("iGpu", "-1") == "-1"
+
+
+def test_cpp_fd_param_matches_python():
+    """The C++ operators' fdParamElastic_3D: time axes, minPad and the eight medium planes equal
+    the Python host preparation's, bit for bit; the same QC rejects a Courant violation."""
+    c = OperatorCase()
+    za, xa, ya = c.axes
+    h = P.hypercube([P.axis(za.n, za.o, za.d), P.axis(xa.n, xa.o, xa.d), P.axis(ya.n, ya.o, ya.d), P.axis(3)])
+    el = np.ascontiguousarray(c.sv.elastic, dtype=np.float32)
+    cpp = P.fdParamElastic_3D(P.float4DReg(h, el.copy()), P.paramObj(dict(c.par)))
+    py = H.FdParam(el, c.axes, c.par)
+    assert (cpp.nz, cpp.nx, cpp.ny, cpp.nts, cpp.sub, cpp.minPad) == (py.nz, py.nx, py.ny, py.nts, py.sub, py.minPad)
+    assert np.float32(cpp.dtw) == py.dtw
+    np.testing.assert_array_equal(cpp.getPlanes().view(np.int32), py.planes.view(np.int32))
+    bad = dict(c.par)
+    bad["dts"] = 0.05
+    with pytest.raises(RuntimeError, match="Courant"):
+        P.fdParamElastic_3D(P.float4DReg(h, el.copy()), P.paramObj(bad))
