@@ -57,3 +57,16 @@ def test_rejections():
     el, axes, par, _ = _case(sub=60)               # internal 120 > SUB_MAX
     with pytest.raises(RuntimeError, match="SUB_MAX"):
         H.FdParam(el, axes, par)
+
+
+def test_parfile_parsing():
+    """SEP parfile / command-line style 'key=value' tokens, with the getters' conversions."""
+    par = H.ParamObj.from_parfile("nts=1000 dts=0.002 sub=2\n# a comment line\nspaceInterpMethod=sinc "
+                                  "zDipoleShift=7.5 fMax=40")
+    assert par.getInt("nts") == 1000 and abs(par.getFloat("dts") - 0.002) < 1e-12
+    assert par.getString("spaceInterpMethod") == "sinc"
+    assert par.getInt("zDipoleShift") == 7 and par.getFloat("zDipoleShift") == 7.5
+    assert par.getInt("fMax") == 40 and par.getFloat("fMax") == 40.0
+    assert par.getInt("nExp", -1) == -1
+    with pytest.raises(KeyError):
+        par.getInt("nExp")
