@@ -33,3 +33,37 @@ def test_library_exports_every_declared_symbol():
 def test_bindings_cover_every_declared_symbol():
     missing = [n for n in _declared() if n not in N.SIGNATURES]
     assert not missing, missing
+
+
+# ---- the seam's host-side argument and state checks (no device work reached) ----------------
+E3D_ERR_ARG, E3D_ERR_STATE = 1, 3
+SPARE_SLOT = 15   # the last slot: no other test uses it
+
+
+def _init(lib, **kw):
+    a = dict(dz=10.0, dx=10.0, dy=10.0, nz=40, nx=40, ny=32, nts=20, dts=0.002, sub=4, minPad=6, blockSize=16,
+             alphaCos=0.99, nGpu=1, iGpuId=0, iGpuAlloc=0)
+    a.update(kw)
+    return lib.initNonlinearElasticGpu_3D(*a.values())
+
+
+def test_seam_rejects_bad_arguments_without_a_gpu():
+    lib = N.lib()
+    assert _init(lib, nGpu=0) == E3D_ERR_ARG
+    assert _init(lib, nGpu=17) == E3D_ERR_ARG
+    assert _init(lib, sub=100) == E3D_ERR_ARG           # SUB_MAX
+    assert b"SUB_MAX" in lib.e3d_last_error()
+    assert lib.deallocateNonlinearElasticGpu_3D(16, 0) == E3D_ERR_ARG                  # slots 0..15
+    assert lib.allocatePinBornElasticGpu_3D(40, 32, 40, 2, 1, 0, 0, 0) == E3D_ERR_ARG   # nts < 3
+    assert lib.allocatePinBornElasticGpu_3D(40, 32, 40, 20, 1, 0, 0, 0) == 0
+
+
+def test_seam_refuses_propagation_on_an_unallocated_slot():
+    lib = N.lib()
+    nulls = [None] * 18
+    geom = []
+    for _ in range(14):
+        geom += [None, 0]
+    st = lib.propElasticFwdGpu_3D(*nulls, *geom, 40, 32, 40, SPARE_SLOT, 0)
+    assert st == E3D_ERR_STATE
+    assert b"not allocated" in lib.e3d_last_error()
