@@ -43,3 +43,19 @@ def test_trace_map_matches_space_interp(method, h, dipole):
         np.testing.assert_allclose(irr[k * n:(k + 1) * n], fwd, rtol=1e-5, atol=1e-5)
         adj = dev.adjoint(False, None, irr[k * n:(k + 1) * n].astype(np.float32))
         np.testing.assert_allclose(back[rec.comp(k)], adj, rtol=1e-4, atol=1e-4)
+
+
+def test_empty_device_sets():
+    """No receivers: empty tables, empty traces, and a trace map with no rows (the engine's
+    gather and spread launch nothing for it)."""
+    sv = S.small_survey(seed=5, nzi=16, nxi=16, nyi=16, pad=4, nts=7, nrec=5)
+    za, xa, ya = sv.axes
+    ax7 = H.grid_axes(za.n, xa.n, ya.n, za.o, xa.o, ya.o, za.d, xa.d, ya.d)
+    e = np.zeros(0, np.float32)
+    d7 = H.build_devices(e, e, e, ax7, 7, sv.par)
+    assert all(d.getNDeviceReg() == 0 and d.getNDeviceIrreg() == 0 for d in d7)
+    assert d7[0].forward(False, np.zeros((0, 7), np.float32)).shape == (0, 7)
+    assert d7[0].adjoint(False, None, np.zeros((0, 7), np.float32)).shape == (0, 7)
+    rec = F.DeviceSet.from_devices(d7, "cpu")
+    tt = F.TraceTables.from_set(rec, "cpu")
+    assert tt.n_irreg == 0 and tt.slot.numel() == 0 and tt.row_ptr.tolist() == [0]
