@@ -229,7 +229,9 @@ def run_ours(args):
     device = torch.device("cuda", local)
     if world > 1:
         import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=1800), device_id=device)
+        # bounded so that ranks left waiting on a failed peer end with an error: the longest gap
+        # between collectives is one gradient (about 90 s at the default size) plus set-up skew
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=device)
 
     sv, fd, prob = build_problem(args, device)
     # every rank holds its own shot; under torchrun the misfit and gradient of the step are
