@@ -290,13 +290,14 @@ class FwiProblem:
         self.data_mask = None
         self.grad_mask = None
 
-    def distribute(self, group=None, dealing="static", store=None, tag="fwi"):
+    def distribute(self, group=None, dealing="static", store=None, tag="fwi", broadcast=True):
         """Share the shots among the ranks of `group` (torch.distributed, one rank per GPU).
         dealing "static": rank r takes shots r, r+world, ...; "dynamic": every rank takes the next
         undealt shot from a counter in `store` (a torch.distributed Store; by default a client of
         the rendezvous store at MASTER_ADDR:MASTER_PORT), so that ranks with cheaper shots take
         more of them.  `tag` names the counters; problems evaluated in the same job need distinct
-        tags."""
+        tags.  broadcast: every evaluation first broadcasts (rho, lambda, mu) from the group's
+        first rank, so that all ranks propagate in the same medium even if their copies drifted."""
         if dealing not in ("static", "dynamic"):
             raise ValueError(f"unknown shot dealing {dealing!r}")
         self.distributed = True
@@ -305,6 +306,7 @@ class FwiProblem:
         self.store = store
         self.tag = tag
         self.evaluations = 0
+        self.broadcast = broadcast
         return self
 
     def _bind_stream(self):
@@ -395,6 +397,21 @@ class ShotQueue:
             yield i
 
 
+def broadcast_model(tensors, group=None):
+    """Overwrite (rho, lambda, mu) on every rank of `group` with the first rank's copy (one
+    broadcast of a flat buffer); a no-op without an initialised process group."""
+    if not (torch.distributed.is_available() and torch.distributed.is_initialized()):
+        return tensors
+    flat = torch.cat([t.detach().reshape(-1).float() for t in tensors])
+    src = torch.distributed.get_global_rank(group, 0) if group is not None else 0
+    torch.distributed.broadcast(flat, src=src, group=group)
+    out, off = [], 0
+    for t in tensors:
+        out.append(flat[off:off + t.numel()].view_as(t).to(t.dtype))
+        off += t.numel()
+    return out
+
+
 def reduce_misfit(total, grads, group=None):
     """Sum the misfit and the (rho, lambda, mu) gradient over the ranks of `group`: one
     all-reduce of a flat buffer (NCCL over NVLink between GPUs; the reference sums shot
@@ -434,7 +451,10 @@ class ElasticFwiMisfit(torch.autograd.Function):
 
     @staticmethod
     def forward(ctx, rho, lam, mu, problem: FwiProblem, shot_ids=None):
-        planes = problem.set_model(rho.float().contiguous(), lam.float().contiguous(), mu.float().contiguous())
+        model = [rho.float().contiguous(), lam.float().contiguous(), mu.float().contiguous()]
+        if problem.distributed and getattr(problem, "broadcast", False):
+            model = [m.contiguous() for m in broadcast_model(model, problem.group)]
+        planes = problem.set_model(*model)
         if shot_ids is not None:
             ids = shot_ids
         elif problem.distributed and getattr(problem, "dealing", "static") == "dynamic":
@@ -462,7 +482,7 @@ class ElasticFwiMisfit(torch.autograd.Function):
                 src_terms.append((shot, src_adj))
         g = planes_to_model(g8, planes, problem.fd.dtw)
         if src_terms:
-            g = tuple(a + b for a, b in zip(g, _source_scaling_gradient(rho, lam, mu, problem, src_terms)))
+            g = tuple(a + b for a, b in zip(g, _source_scaling_gradient(*model, problem, src_terms)))
         if problem.grad_mask is not None:
             g = tuple(gk * problem.grad_mask[k] for k, gk in enumerate(g))
         if problem.distributed:

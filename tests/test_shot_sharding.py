@@ -111,3 +111,28 @@ def test_dynamic_dealing_covers_every_shot_once_and_balances():
         assert len(m0) > len(m1)  # the faster rank took more shots
         for r in range(2):
             assert abs(out[r][evaluation][1] - serial_loss) < 1e-9
+
+
+def _broadcast_worker(rank, world, port, out):
+    from elasticisolib_3d_b200.fwi import broadcast_model
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        g = torch.Generator().manual_seed(7 + rank)   # every rank starts from a different medium
+        model = [torch.rand((3, 4, 5), generator=g) + 1.0 for _ in range(3)]
+        out[rank] = [t.clone() for t in broadcast_model(model)]
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.timeout(120)
+def test_model_broadcast_makes_every_rank_use_the_first_ranks_medium():
+    mgr = mp.get_context("spawn").Manager()
+    out = mgr.dict()
+    mp.start_processes(_broadcast_worker, args=(2, _free_port(), out), nprocs=2, join=True, start_method="spawn")
+    g = torch.Generator().manual_seed(7)
+    ref = [torch.rand((3, 4, 5), generator=g) + 1.0 for _ in range(3)]
+    for r in range(2):
+        for a, b in zip(out[r], ref):
+            assert torch.equal(a, b)
