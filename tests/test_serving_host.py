@@ -1,0 +1,60 @@
+"""CPU: the gradient server's host logic -- requests dealt to devices by grid (a device keeps the
+grids it was given), submission order kept per device and in the results, errors reported after
+the other devices finish.  The per-request GPU work is replaced by a recorder."""
+import threading
+from types import SimpleNamespace
+
+import pytest
+
+from elasticisolib_3d_b200.serving import GradientRequest, GradientServer
+
+
+def _fd(n, nts):
+    return SimpleNamespace(nz=n, nx=n, ny=n, nts=nts, sub=4, minPad=40, dz=10.0, dx=10.0, dy=10.0, dts=0.002)
+
+
+def _requests():
+    grids = [_fd(200, 1000), _fd(300, 2000), _fd(200, 1000), _fd(330, 3000), _fd(300, 2000), _fd(200, 1500)]
+    return [GradientRequest(fd, None, None, None, None, None) for fd in grids]
+
+
+def test_requests_are_dealt_by_grid_in_submission_order(monkeypatch):
+    server = GradientServer(devices=(0, 1), autotune=False)
+    seen, lock = [], threading.Lock()
+
+    def fake(dev, req):
+        with lock:
+            seen.append((dev, id(req)))
+        req.result = (float(dev), id(req))
+        return req.result
+
+    monkeypatch.setattr(server, "_serve_one", fake)
+    reqs = _requests()
+    out = server.serve(reqs)
+    assert [o[1] for o in out] == [id(r) for r in reqs]          # results in submission order
+    dev_of = dict((i, d) for d, i in seen)
+    # same grid (shape and record) -> same device; four distinct grids over two devices
+    assert dev_of[id(reqs[0])] == dev_of[id(reqs[2])]
+    assert dev_of[id(reqs[1])] == dev_of[id(reqs[4])]
+    assert {dev_of[id(r)] for r in reqs} == {0, 1}
+    for d in (0, 1):                                              # per-device order kept
+        ids = [i for dd, i in seen if dd == d]
+        assert ids == [id(r) for r in reqs if dev_of[id(r)] == d]
+
+
+def test_a_failing_device_is_reported_after_the_others(monkeypatch):
+    server = GradientServer(devices=(0, 1), autotune=False)
+    done = []
+
+    def fake(dev, req):
+        if dev == 1:
+            raise RuntimeError("device 1 failed")
+        done.append(id(req))
+        req.result = (0.0, None)
+        return req.result
+
+    monkeypatch.setattr(server, "_serve_one", fake)
+    reqs = _requests()
+    with pytest.raises(RuntimeError, match="device 1 failed"):
+        server.serve(reqs)
+    assert done  # device 0 finished its requests
