@@ -58,3 +58,34 @@ def test_a_failing_device_is_reported_after_the_others(monkeypatch):
     with pytest.raises(RuntimeError, match="device 1 failed"):
         server.serve(reqs)
     assert done  # device 0 finished its requests
+
+
+def test_least_recently_used_problems_close_to_admit_a_new_grid(monkeypatch):
+    import torch
+    from elasticisolib_3d_b200 import serving as SV
+
+    opened, closed = [], []
+
+    class FakeProblem:
+        def __init__(self, fd, device=None, ckpt=None, variant=None):
+            self.fd = fd
+            self.prop = SimpleNamespace(close=lambda: closed.append(fd.nz))
+            opened.append(fd.nz)
+
+    total = 3 * SV._estimate_bytes(_fd(200, 1000)) + 3 * (2 << 30)   # room for about three 200^3 grids
+    open_problems = lambda: sum(len(p) for p in server.open.values())   # noqa: E731
+    monkeypatch.setattr(SV.F, "FwiProblem", FakeProblem)
+    monkeypatch.setattr(torch.cuda, "synchronize", lambda dev=None: None)
+    monkeypatch.setattr(torch.cuda, "empty_cache", lambda: None)
+    monkeypatch.setattr(torch.cuda, "mem_get_info",
+                        lambda dev=None: (total - open_problems() * (SV._estimate_bytes(_fd(200, 1000)) + (2 << 30)),
+                                          total))
+    server = SV.GradientServer(devices=(0,), autotune=False)
+    a, b, c, d = _fd(200, 1000), _fd(201, 1000), _fd(202, 1000), _fd(203, 1000)
+    server._problem(0, a)
+    server._problem(0, b)
+    server._problem(0, a)          # a is now the most recently used
+    server._problem(0, c)          # fits: three open
+    server._problem(0, d)          # does not fit: b (least recently used) closes first
+    assert closed and closed[0] == 201
+    assert opened == [200, 201, 202, 203]
