@@ -192,3 +192,25 @@ def test_stagger_operators_match_oracle_bitwise(axis):
     name = "zxy"[axis]
     np.testing.assert_array_equal(H.stagger(f, name), O.stagger_forward(f, axis))
     np.testing.assert_array_equal(H.stagger(f, name, adjoint=True), O.stagger_adjoint(f, axis))
+
+
+def test_coinciding_devices_share_grid_points():
+    """Two devices at one position (and a third sharing a cell corner): unique points appear once,
+    in first-seen order, both devices' taps point at the same slots, and the adjoint accumulates
+    both signals there -- as the reference's std::map-keyed convertIrregToReg does."""
+    axes_h, axes_o = _grid()
+    za, xa, ya = axes_o
+    z0 = za.o + 20.5 * za.d
+    x0 = xa.o + 17.25 * xa.d
+    y0 = ya.o + 15.75 * ya.d
+    z = np.array([z0, z0, z0 + za.d], np.float32)
+    x = np.array([x0, x0, x0], np.float32)
+    y = np.array([y0, y0, y0], np.float32)
+    nat = H.spaceInterpGpu_3D(z, x, y, axes_h, 4, _par())
+    ref = O.space_interp_linear(z, x, y, axes_o, PADS, 4)
+    _same(nat, ref)
+    assert len(set(nat.unique.tolist())) == len(nat.unique) == 12     # 8 + 4 new corners
+    np.testing.assert_array_equal(nat.slot[0], nat.slot[1])
+    sig = np.ones((3, 4), np.float32)
+    reg = nat.adjoint(False, None, sig)
+    np.testing.assert_allclose(reg.sum(axis=0), np.full(4, 3.0), rtol=1e-6)   # weights sum to 1 per device
