@@ -214,3 +214,27 @@ def test_coinciding_devices_share_grid_points():
     sig = np.ones((3, 4), np.float32)
     reg = nat.adjoint(False, None, sig)
     np.testing.assert_allclose(reg.sum(axis=0), np.full(4, 3.0), rtol=1e-6)   # weights sum to 1 per device
+
+
+def test_torch_medium_planes_and_gradient_post_processing_on_the_cpu():
+    """The FWI path's torch restatements (fwi.medium_planes, fwi.planes_to_model), run on CPU
+    tensors, equal the native medium planes and the oracle's Born gradient post-processing bit
+    for bit (on the GPU they are compared through the gradient's FP64 parity)."""
+    import torch
+    from elasticisolib_3d_b200 import fwi as F
+    rng = np.random.default_rng(3)
+    ny, nx, nz = 10, 12, 14
+    vp = rng.uniform(2000, 4000, (ny, nx, nz))
+    vs = vp / 1.8
+    rho = rng.uniform(1800, 2600, (ny, nx, nz))
+    el = np.stack([rho, rho * (vp ** 2 - 2 * vs ** 2), rho * vs ** 2]).astype(np.float32)
+    dtw = np.float32(0.25e-3)
+    tp = F.medium_planes(*[torch.from_numpy(el[k]) for k in range(3)], dtw)
+    hp = H.medium_planes(el, dtw)
+    for k in range(8):
+        np.testing.assert_array_equal(tp[k].numpy().view(np.int32), hp[k].view(np.int32))
+    g8 = rng.standard_normal((8, ny, nx, nz)).astype(np.float32)
+    tm = F.planes_to_model(torch.from_numpy(g8), torch.from_numpy(hp), dtw)
+    om = O.born_planes_to_model(g8, hp[0:3], dtw)
+    for k in range(3):
+        np.testing.assert_array_equal(tm[k].numpy().view(np.int32), np.asarray(om[k]).view(np.int32))
