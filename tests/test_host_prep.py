@@ -238,3 +238,23 @@ def test_torch_medium_planes_and_gradient_post_processing_on_the_cpu():
     om = O.born_planes_to_model(g8, hp[0:3], dtw)
     for k in range(3):
         np.testing.assert_array_equal(tm[k].numpy().view(np.int32), np.asarray(om[k]).view(np.int32))
+
+
+def test_torch_source_scaling_on_the_cpu():
+    """fwi.scale_sources (the FWI path's device-side medium scaling of the regular-grid source
+    signals, nonlinearPropElasticGpu_3D.cpp:200-277) on CPU tensors equals the oracle's bit for bit."""
+    import torch
+    from operator_case import OperatorCase
+    from elasticisolib_3d_b200 import fwi as F
+    from elasticisolib_3d_b200.engine import COMP_GRID
+    c = OperatorCase()
+    src7 = c.src_dev[0]
+    rng = np.random.default_rng(2)
+    reg = [rng.standard_normal((len(src7[COMP_GRID[k]].unique), c.nts)).astype(np.float32) for k in range(9)]
+    planes = H.medium_planes(c.sv.elastic, np.float32(c.dtw))
+    dz, dx, dy = c.d
+    got = F.scale_sources(torch.from_numpy(np.concatenate(reg, axis=0).T.copy()), F.DeviceSet.from_devices(src7, "cpu"),
+                          torch.from_numpy(planes), np.float32(dx), np.float32(dy), np.float32(dz))
+    ref = [r.copy() for r in reg]
+    O.scale_signals(ref, c.o_src[0], planes, dx, dy, dz)
+    np.testing.assert_array_equal(got.numpy().view(np.int32), np.concatenate(ref, axis=0).T.view(np.int32))
