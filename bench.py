@@ -8,17 +8,22 @@ Workload (the FWI-gradient configuration): 300^3 interior + 40-cell sponge
 Gaussian anomalies; the gradient is taken at the background model.  Inputs are
 seeded synthetic data (no dataset is involved).
 
-One step = one shot's FWI gradient per GPU: nonlinear forward with on-device
-checkpoints, residual at the receivers, Born adjoint of the residual with the
-source wavefield recomputed from the checkpoints, and the Born model
-post-processing, through ``ElasticFwiMisfit`` (autograd forward+backward);
-with several GPUs the misfit and gradient are then summed over ranks (one
-NCCL all-reduce of the flat gradient).
+One step = one shot's FWI gradient per GPU through ``ElasticFwiMisfit``
+(autograd forward + backward): the model and the observed traces are copied in
+from pinned host memory, the nonlinear forward runs with on-device
+checkpoints, the residual is formed at the receivers, the Born adjoint of the
+residual runs with the source wavefield recomputed from the checkpoints, and
+the gradient (and the misfit) are copied back to pinned host memory.  One
+timed loop gives both figures: ``value`` from the device time between the
+input copies and the gradient copy of each step (inputs resident in HBM),
+``e2e`` from the whole loop including the copies.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
 Multi-GPU (torchrun): every rank takes its own shot each step (weak scaling) and
-the gradients are summed with one all-reduce; the time is the max over ranks.
+the misfit and gradient are summed with one all-reduce; the time is the max over
+ranks.  --impl reference times the oracle port of the path on the host cores
+(rank 0 only), without loading this package's native library.
 """
 from __future__ import annotations
 
@@ -38,16 +43,28 @@ sys.path.insert(0, ROOT)
 
 METRIC = "FWI gradient shots/s (Born-adjoint gradient, 300^3+40 sponge, 2500 samples)"
 UNIT = "shots/s"
-# Algorithmic bytes per updated cell of the three stepper launches of a gradient (fp32 fields):
-#   0 forward (checkpointed forward pass): read old 9 + current 9 + medium 8, write new 9 = 140 B
-#   3 forward with the 3 velocity fields decimated into two accumulators (source recompute): +48 B
-#   5 dual-state exact adjoint (raw + premultiplied levels: +36 B) with all 9 fields decimated
-#     into two accumulators (+144 B) = 320 B
-STEPPER_BYTES = {0: 140.0, 3: 188.0, 5: 320.0}
-STEPPER_NAMES = {0: "forward stepper (kStepTma<0>)", 3: "forward stepper + 3-field decimation (kStepTma<0>)",
-                 5: "exact-adjoint stepper, dual state + 9-field decimation (kStepTma<2>)"}
-PROFILE = {5: "profiles/kStepTma_adjoint_decimated_392x392x104.txt",
-           0: "profiles/kStepTma_forward_392x392x104.txt"}
+# Timed kernel kinds of the gradient (e3d_kernel_timing_read) and their algorithmic bytes per
+# updated cell (fp32 fields):
+#   0 forward stepper: read old 9 + current 9 + medium 8, write new 9 = 140 B (the forward pass
+#     and the source recompute, whose fine levels go to a ring of sub+1 levels)
+#   2 dual-state exact-adjoint stepper: read old raw 9, current premultiplied 9, medium 8, write
+#     new raw 9 and new premultiplied 9 = 176 B
+#   6 block imaging, once per coarse block: read the sub adjoint levels (sub*36 B), V(t-1..t+2)
+#     (48 B), the eight image planes (32 B) and write them (32 B) = 256 B at sub = 4
+#   7 source-velocity decimation, once per recomputed block: read sub levels x 3 fields (48 B),
+#     V[b] (12 B), write V[b] and V[b+1] (24 B) = 84 B at sub = 4
+#   with --decimation acc: 3 = forward + 3-field accumulators (188 B), 5 = dual adjoint + 9-field
+#     accumulators (320 B)
+KIND_NAMES = {0: "forward stepper (kStepSplit<0,3,3>: velocity and stress CTA roles)",
+              2: "dual-state exact-adjoint stepper (kStepTma<2,8,2>)",
+              6: "block imaging from the adjoint ring (kImagingTma)", 7: "source-velocity decimation (kDecimateVelocity)",
+              3: "forward stepper + 3-field decimation accumulators", 5: "dual adjoint stepper + 9-field accumulators"}
+PROFILE = {0: "profiles/kStepSplit_forward_392x392x104.txt", 2: "profiles/kStepTma_adjoint_dual_392x392x104.txt",
+           6: "profiles/kImagingTma_392x392x104.txt"}
+
+
+def kind_bytes(kind, sub):
+    return {0: 140.0, 2: 176.0, 6: sub * 36.0 + 48.0 + 64.0, 7: sub * 12.0 + 36.0, 3: 188.0, 5: 320.0}[kind]
 
 
 def parse():
@@ -58,14 +75,18 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--nts", type=int, default=2500)
     ap.add_argument("--interior", type=int, default=300)
-    ap.add_argument("--variant", default="tma", choices=["tma", "plain", "auto"],
-                    help="stepper: tma (8-wide, 2 stages, TMA; default), plain (plain loads, no dual-state "
+    ap.add_argument("--variant", default="split", choices=["split", "tma", "plain", "auto"],
+                    help="stepper: split (default: velocity and stress updates as two CTA roles with 3-stage TMA "
+                         "pipelines for the forward-type steps, the 2-stage TMA stepper for the dual-state "
+                         "adjoint), tma (2-stage TMA stepper for every step), plain (plain loads, no dual-state "
                          "adjoint), auto (autotuned)")
     ap.add_argument("--ckpt", default="auto", choices=["auto", "fp32", "fp16", "bf16"])
     ap.add_argument("--velocity", default="auto", choices=["auto", "fp32", "fp16"],
                     help="storage of the decimated source velocity slots (fp32 with --ckpt fp32: the "
                          "all-FP32 plan)")
-    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--decimation", default="ring", choices=["ring", "acc"],
+                    help="gradient passes: decimate from a ring of fine levels once per coarse block (ring) "
+                         "or through accumulators fused into every fine step (acc)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--breakdown", action="store_true",
                     help="after the measurement, print the device time per kernel of one more gradient")
@@ -124,18 +145,23 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+
+
 def build_problem(args, device):
+    """Background survey, the FWI problem on it and one shot whose observed traces are the
+    nonlinear forward of the true model (computed on the device)."""
     import torch
     from elasticisolib_3d_b200 import fwi as F
     from elasticisolib_3d_b200 import hostprep as H
     from elasticisolib_3d_b200 import synthetic as S
     n = args.interior
-    sv = S.fwi_gradient_survey(nzi=n, nxi=n, nyi=n, nts=args.nts, true_model=False)
-    svt = S.fwi_gradient_survey(nzi=n, nxi=n, nyi=n, nts=args.nts, true_model=True)
+    sv, true_el = S.fwi_gradient_survey(nzi=n, nxi=n, nyi=n, nts=args.nts, with_true=True)
     fd = H.FdParam(sv.elastic, sv.axes, sv.par)
     ax7 = H.grid_axes(*(a.n for a in sv.axes), *(a.o for a in sv.axes), *(a.d for a in sv.axes))
-    variant = {"tma": (8, 2, "tma"), "plain": (8, 2, "plain"), "auto": "auto"}[args.variant]
-    prob = F.FwiProblem(fd, device=device, ckpt=args.ckpt, variant=variant, velocity=args.velocity)
+    variant = {"split": (8, 3, "split-fwd"), "tma": (8, 2, "tma"), "plain": (8, 2, "plain"),
+               "auto": "auto"}[args.variant]
+    prob = F.FwiProblem(fd, device=device, ckpt=args.ckpt, variant=variant, velocity=args.velocity,
+                        decimation_ring=args.decimation == "ring")
     rank = int(os.environ.get("RANK", "0"))
     shot_id = rank % len(sv.src_xyz)
     src = H.build_devices(*sv.src_xyz[shot_id], ax7, fd.nts, sv.par)
@@ -144,8 +170,7 @@ def build_problem(args, device):
     for k in (3, 4, 5):
         irr[k][0] = sv.wavelet
     shot = F.make_shot(src, rec, irr, None, device)
-    # observed data: nonlinear forward on the true model
-    mt = [torch.tensor(svt.elastic[k], device=device) for k in range(3)]
+    mt = [torch.tensor(true_el[k], device=device) for k in range(3)]
     planes = prob.set_model(*mt)
     shot.d_obs, _ = prob.forward_data(shot, planes)
     del planes, mt
@@ -154,63 +179,97 @@ def build_problem(args, device):
     return sv, fd, prob
 
 
-def cpu_baseline(fd, n_sample_fwd=2, n_sample_adj=1):
-    """Oracle (C++/OpenMP restatement) stepper timed on the host cores over a bounded sample of the
-    same grid, extrapolated to one gradient (2 forward-type passes + 1 adjoint pass)."""
-    import ctypes
+def oracle_grid(args):
+    """Grid, medium planes and propagation constants of the workload for the host-core runs,
+    from the oracle's own host preparation (this package's native library is not loaded)."""
+    from elasticisolib_3d_b200 import synthetic as S
     from oracle import oracle as O
-    L = O.lib()
-    threads = L.oracle_num_threads(os.cpu_count() or 1)
-    p = O.PropParams(fd.nz, fd.nx, fd.ny, fd.nts, fd.sub, fd.minPad, float(fd.dz), float(fd.dx), float(fd.dy),
-                     float(fd.dts))
-    shape = (fd.ny, fd.nx, fd.nz)
-    rng = np.random.default_rng(0)
-    med = [np.asarray(fd.planes[k]) for k in range(8)]
-    p0 = [np.zeros(shape, np.float32) for _ in range(9)]
-    p1 = [rng.standard_normal(shape, dtype=np.float32) * 1e-3 for _ in range(9)]
-    a, k1 = O._ptrs(p0)
-    b, k2 = O._ptrs(p1)
-    m, k3 = O._ptrs(med)
-    prm = p.c()
-    t0 = time.perf_counter()
-    for _ in range(n_sample_fwd):
-        L.oracle_step_f32(ctypes.byref(prm), a, b, m, 0, 1)
-    t_fwd = (time.perf_counter() - t0) / n_sample_fwd
-    t0 = time.perf_counter()
-    for _ in range(n_sample_adj):
-        L.oracle_step_f32(ctypes.byref(prm), a, b, m, 2, 1)
-    t_adj = (time.perf_counter() - t0) / n_sample_adj
-    steps = (fd.nts - 1) * fd.sub
-    t_shot = 2 * steps * t_fwd + steps * t_adj
-    return {"value": 1.0 / t_shot, "unit": UNIT, "cores": int(threads), "kind": "port",
-            "sample": f"{n_sample_fwd} forward + {n_sample_adj} exact-adjoint fine steps of the oracle stepper "
-                      f"(FP32, fused sponge) on the full {fd.nz}x{fd.nx}x{fd.ny} grid, extrapolated to "
-                      f"2x{steps} forward + {steps} adjoint steps per gradient"}
+    n = args.interior
+    sv = S.fwi_gradient_survey(nzi=n, nxi=n, nyi=n, nts=args.nts)
+    par = sv.par
+    nts, dts = par.getInt("nts"), par.getFloat("dts")
+    sub, _, dtw = O.time_axes(nts, dts, par.getInt("sub"))
+    za, xa, ya = sv.axes
+    # one sponge width for all faces: the smaller z and x pads (fdParamElastic_3D.cpp minPad rule)
+    min_pad = min(par.getInt("zPadMinus"), par.getInt("zPadPlus"), par.getInt("xPadMinus"), par.getInt("xPadPlus"))
+    p = O.PropParams(za.n, xa.n, ya.n, nts, sub, min_pad, float(za.d), float(xa.d), float(ya.d), float(dts))
+    med = O.medium_planes(sv.elastic, dtw)
+    return p, med
+
+
+class OracleSteps:
+    """The oracle's FP32 stepper (C++/OpenMP restatement of the reference's kernels, sponge fused)
+    on the full grid, on all host cores; one sample = 2 forward + 1 exact-adjoint fine steps, the
+    mix of a gradient (forward pass, source wavefield, adjoint pass)."""
+
+    def __init__(self, p, med):
+        import ctypes
+        from oracle import oracle as O
+        self.ctypes = ctypes
+        self.L = O.lib()
+        self.threads = int(self.L.oracle_num_threads(os.cpu_count() or 1))
+        shape = (p.ny, p.nx, p.nz)
+        rng = np.random.default_rng(0)
+        self.keep = [np.ascontiguousarray(m, dtype=np.float32) for m in med]
+        self.p0 = [np.zeros(shape, np.float32) for _ in range(9)]
+        self.p1 = [rng.standard_normal(shape, dtype=np.float32) * 1e-3 for _ in range(9)]
+        self.a, _ = O._ptrs(self.p0)
+        self.b, _ = O._ptrs(self.p1)
+        self.m, _ = O._ptrs(self.keep)
+        self.prm = p.c()
+        self.steps_per_gradient = (p.nts - 1) * p.sub  # fine steps of each of the three passes
+
+    def sample(self):
+        """Seconds of one 2-forward + 1-adjoint sample."""
+        L, by = self.L, self.ctypes.byref
+        t0 = time.perf_counter()
+        L.oracle_step_f32(by(self.prm), self.a, self.b, self.m, 0, 1)
+        L.oracle_step_f32(by(self.prm), self.a, self.b, self.m, 0, 1)
+        L.oracle_step_f32(by(self.prm), self.a, self.b, self.m, 2, 1)
+        return time.perf_counter() - t0
+
+
+def cpu_baseline(args, n_samples=4):
+    """The oracle port timed on the host cores over a bounded sample of the same workload
+    (n_samples samples of 2 forward + 1 adjoint fine steps on the full grid after one warm-up
+    sample), extrapolated to one gradient."""
+    p, med = oracle_grid(args)
+    o = OracleSteps(p, med)
+    o.sample()
+    t = statistics.mean(o.sample() for _ in range(n_samples))
+    return {"value": 1.0 / (t * o.steps_per_gradient), "unit": UNIT, "cores": o.threads, "kind": "port",
+            "sample": f"{n_samples} samples of 2 forward + 1 exact-adjoint fine steps of the oracle's FP32 stepper "
+                      f"on the full {p.nz}x{p.nx}x{p.ny} grid ({3 * n_samples} fine steps after 3 warm-up steps), "
+                      f"extrapolated to the gradient's 3 x {o.steps_per_gradient} fine steps"}
 
 
 def run_reference(args):
-    """Reference arm: the reference's path has no CPU implementation, so the oracle port runs on the
-    host cores (rank 0 only)."""
+    """Reference arm: the reference's path has no CPU implementation, so the oracle port (its
+    kernels restated in C++/OpenMP) runs on the host cores, rank 0 only.  One step = one bounded
+    sample of the workload: 2 forward + 1 exact-adjoint fine steps on the full grid (1/9996 of a
+    gradient); shots/s is extrapolated from the timed window of K samples."""
     if int(os.environ.get("RANK", "0")) != 0:
         return
-    from elasticisolib_3d_b200 import hostprep as H
-    from elasticisolib_3d_b200 import synthetic as S
-    n = args.interior
-    sv = S.fwi_gradient_survey(nzi=n, nxi=n, nyi=n, nts=args.nts)
-    fd = H.FdParam(sv.elastic, sv.axes, sv.par)
-    vals = []
-    for i in range(args.warmup + args.steps):
-        cb = cpu_baseline(fd, 1, 1)
-        if i >= args.warmup:
-            vals.append(cb["value"])
-    v = float(np.mean(vals))
-    cb["value"] = v
+    p, med = oracle_grid(args)
+    o = OracleSteps(p, med)
+    for _ in range(args.warmup):
+        o.sample()
+    times = [o.sample() for _ in range(args.steps)]
+    t = statistics.mean(times)
+    v = 1.0 / (t * o.steps_per_gradient)
+    cb = {"value": v, "unit": UNIT, "cores": o.threads, "kind": "port",
+          "sample": f"{args.steps} timed samples (after {args.warmup} warm-up samples) of 2 forward + 1 exact-adjoint "
+                    f"fine steps of the oracle's FP32 stepper on the full {p.nz}x{p.nx}x{p.ny} grid, i.e. a window of "
+                    f"{3 * args.steps} fine steps after {3 * args.warmup}; shots/s extrapolated to the gradient's "
+                    f"3 x {o.steps_per_gradient} fine steps"}
     out = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
-           "warmup": args.warmup, "ms_per_step": 1e3 / v, "higher_is_better": True, "scaling": "weak",
+           "warmup": args.warmup, "ms_per_step": 1e3 * t, "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)", "impl": "reference",
-           "config": {"workload": f"fwi-gradient {args.interior}^3+40 sponge ({fd.nz}x{fd.nx}x{fd.ny}), "
-                                  f"{fd.nts} samples ({(fd.nts - 1) * fd.sub} fine steps), 150x150 receivers x 9 "
-                                  f"components, Ricker 10 Hz, one shot per step",
+           "config": {"workload": f"fwi-gradient {args.interior}^3+40 sponge ({p.nz}x{p.nx}x{p.ny}), {p.nts} samples "
+                                  f"({(p.nts - 1) * p.sub} fine steps), 150x150 receivers x 9 components, Ricker 10 Hz, "
+                                  f"one shot per gradient",
+                      "step": "one bounded sample: 2 forward + 1 exact-adjoint fine steps on the full grid; "
+                              "ms_per_step is the sample's time, value the extrapolated gradient throughput",
                       "l2_flush": "inputs larger than L2"},
            "cpu_baseline": cb, "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out), flush=True)
@@ -230,92 +289,73 @@ def run_ours(args):
     if world > 1:
         import datetime
         # bounded so that ranks left waiting on a failed peer end with an error: the longest gap
-        # between collectives is one gradient (about 90 s at the default size) plus set-up skew
+        # between collectives is one gradient plus set-up skew
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=device)
 
     sv, fd, prob = build_problem(args, device)
     # every rank holds its own shot; under torchrun the misfit and gradient of the step are
     # summed over ranks with one all-reduce, as an FWI iteration needs
     prob.distributed = world > 1
-    m = [torch.tensor(sv.elastic[k], device=device, requires_grad=True) for k in range(3)]
+    cb = cpu_baseline(args) if (world == 1 and rank == 0 and not args.no_cpu) else None
 
-    def step():
-        loss = F.ElasticFwiMisfit.apply(m[0], m[1], m[2], prob, [0])
+    # inputs and output in pinned host memory: the model, the shot's observed traces, the gradient
+    shot = prob.shots[0]
+    host_model = [torch.from_numpy(np.ascontiguousarray(sv.elastic[k])).pin_memory() for k in range(3)]
+    host_obs = shot.d_obs.cpu().pin_memory()
+    host_grad = [torch.empty_like(h).pin_memory() for h in host_model]
+    h2d = sum(h.numel() * 4 for h in host_model) + host_obs.numel() * 4
+    d2h = sum(h.numel() * 4 for h in host_grad) + 8
+    stream = torch.cuda.current_stream(device)
+
+    def step(ev=None):
+        if ev:
+            ev[0].record(stream)
+        md = [h.to(device, non_blocking=True).requires_grad_(True) for h in host_model]
+        shot.d_obs.copy_(host_obs, non_blocking=True)
+        if ev:
+            ev[1].record(stream)
+        loss = F.ElasticFwiMisfit.apply(md[0], md[1], md[2], prob, [0])
         loss.backward()
-        for x in m:
-            x.grad = None
-        return loss
+        if ev:
+            ev[2].record(stream)
+        for hg, x in zip(host_grad, md):
+            hg.copy_(x.grad, non_blocking=True)
+        lv = loss.item()
+        if ev:
+            ev[3].record(stream)
+        return lv
 
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
 
-    stream = torch.cuda.current_stream(device)
     prob.prop.kernel_timing(16)
-    for mode in STEPPER_BYTES:
-        prob.prop.kernel_timing_read(mode)
+    for kind in KIND_NAMES:
+        prob.prop.kernel_timing_read(kind)
     launches0 = prob.prop.launch_count
+    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(args.steps)]
     clocks = ClockSampler(local)
     clocks.start()
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(args.steps):
-        step()
-    e1.record(stream)
+    loss_value = None
+    for i in range(args.steps):
+        loss_value = step(evs[i])
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
     clk = clocks.stop()
     launches = prob.prop.launch_count - launches0
-    ms = e0.elapsed_time(e1)
-    sampled = {mode: prob.prop.kernel_timing_read(mode) for mode in STEPPER_BYTES}
+    device_ms = sum(e[1].elapsed_time(e[2]) for e in evs)   # inputs resident, gradient on the device
+    e2e_ms = evs[0][0].elapsed_time(evs[-1][3])              # the whole loop, copies included
+    sampled = {kind: prob.prop.kernel_timing_read(kind) for kind in KIND_NAMES}
     prob.prop.kernel_timing(0)
-    stepper_bytes, stepper_names = dict(STEPPER_BYTES), dict(STEPPER_NAMES)
-    if args.variant == "plain":
-        # plain loads: the adjoint runs on the raw state only (medium applied at the halo), no dual level
-        stepper_bytes[5] = 284.0
-        stepper_names = {0: "forward stepper (kStep<0>, plain loads)",
-                         3: "forward stepper + 3-field decimation (kStep<0>, plain loads)",
-                         5: "exact-adjoint stepper + 9-field decimation (kStep<2>, plain loads)"}
-    t = torch.tensor([ms], device=device, dtype=torch.float64)
+    t = torch.tensor([device_ms, e2e_ms], device=device, dtype=torch.float64)
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
-    value = world * args.steps / (ms_max / 1e3)
-
-    # end to end through the public API: model and observed data from pinned host memory,
-    # gradient back to pinned host memory, every step
-    e2e = None
-    if not args.no_e2e:
-        host_model = [torch.from_numpy(np.ascontiguousarray(sv.elastic[k])).pin_memory() for k in range(3)]
-        shot = prob.shots[0]
-        host_obs = shot.d_obs.cpu().pin_memory()
-        host_grad = [torch.empty_like(h).pin_memory() for h in host_model]
-        torch.cuda.synchronize()
-        if world > 1:
-            dist.barrier()
-        a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a0.record(stream)
-        for _ in range(args.steps):
-            md = [h.to(device, non_blocking=True).requires_grad_(True) for h in host_model]
-            shot.d_obs = host_obs.to(device, non_blocking=True)
-            loss = F.ElasticFwiMisfit.apply(md[0], md[1], md[2], prob, [0])
-            loss.backward()
-            for hg, x in zip(host_grad, md):
-                hg.copy_(x.grad, non_blocking=True)
-            lv = loss.item()
-        a1.record(stream)
-        torch.cuda.synchronize()
-        t2 = torch.tensor([a0.elapsed_time(a1)], device=device, dtype=torch.float64)
-        if world > 1:
-            dist.all_reduce(t2, op=dist.ReduceOp.MAX)
-        h2d = sum(h.numel() * 4 for h in host_model) + host_obs.numel() * 4
-        d2h = sum(h.numel() * 4 for h in host_grad) + 8
-        e2e = {"value": world * args.steps / (float(t2.item()) / 1e3), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
-               "d2h_bytes_per_step": int(d2h), "loss": lv}
+    device_ms, e2e_ms = float(t[0].item()), float(t[1].item())
+    value = world * args.steps / (device_ms / 1e3)
 
     if rank == 0:
         cells = prob.prop.cells_per_step
@@ -323,54 +363,59 @@ def run_ours(args):
         if os.path.exists(peaks_path):
             with open(peaks_path) as f:
                 peak = float(json.load(f)["hbm_gbs"])
-            peak_src = "measured"
+            peak_src = "measured (MEASURED_PEAKS.json hbm_gbs)"
         else:
             peak, peak_src = 6650.0, "fallback"
         steps_per_pass = (fd.nts - 1) * fd.sub
         blocks = fd.nts - 1
         seg = prob.prop.checkpoint_segment or blocks
         _, recompute_blocks = checkpoint_schedule(blocks, seg)
-        # the forward pass decimates from the block before the last segment on
-        plain_fwd = max(blocks - seg - 1, 0) if seg < blocks else 0
         cell_updates = cells * (steps_per_pass + recompute_blocks * fd.sub + steps_per_pass)
-        launches_per_step = {0: plain_fwd * fd.sub, 3: (blocks - plain_fwd + recompute_blocks) * fd.sub,
-                             5: steps_per_pass}
+        ring = args.decimation == "ring"
+        # launches of each kind in one gradient
+        per_step = ({0: steps_per_pass + recompute_blocks * fd.sub, 2: steps_per_pass, 6: blocks,
+                     7: recompute_blocks + seg + 1} if ring else
+                    {0: max(blocks - seg - 1, 0) * fd.sub, 3: (min(seg + 1, blocks) + recompute_blocks) * fd.sub,
+                     5: steps_per_pass})
         kernels = {}
-        for mode, (avg, cnt) in sampled.items():
-            if cnt == 0:
-                continue  # e.g. the plain forward stepper when the whole record is decimated in the forward pass
+        for kind, (avg, cnt) in sampled.items():
+            if cnt == 0 or kind not in per_step:
+                continue
             traffic_per_cell = None
-            prof = os.path.join(ROOT, PROFILE[mode]) if mode in PROFILE and args.variant != "plain" else None
+            prof = os.path.join(ROOT, PROFILE[kind]) if kind in PROFILE and args.variant == "split" else None
             if prof and os.path.exists(prof):
                 for line in open(prof):
                     if line.startswith("dram_bytes_per_cell:"):
                         traffic_per_cell = float(line.split(":")[1])
-            ach = stepper_bytes[mode] * cells / (avg / 1e3) / 1e9 if avg > 0 else None
-            kernels[mode] = {"kernel": stepper_names[mode], "bound": "hbm", "achieved": ach, "peak": peak,
+            nbytes = kind_bytes(kind, fd.sub)
+            ach = nbytes * cells / (avg / 1e3) / 1e9 if avg > 0 else None
+            kernels[kind] = {"kernel": KIND_NAMES[kind], "bound": "hbm", "achieved": ach, "peak": peak,
                              "peak_source": peak_src, "unit": "GB/s", "frac": (ach / peak) if ach else None,
                              "traffic": traffic_per_cell * cells if traffic_per_cell else None,
-                             "algorithmic_bytes_per_cell": stepper_bytes[mode], "avg_launch_ms": avg,
-                             "sampled_launches": cnt,
-                             "share_of_step_est": avg * launches_per_step[mode] / (ms_max / args.steps)}
-        # the dominant kernel: largest estimated share of the step
-        dom = max(kernels, key=lambda m: kernels[m]["share_of_step_est"] or 0.0)
+                             "algorithmic_bytes_per_cell": nbytes, "cells_per_launch": cells,
+                             "avg_launch_ms": avg, "sampled_launches": cnt, "launches_per_step": per_step[kind],
+                             "share_of_step_est": avg * per_step[kind] / (device_ms / args.steps)}
+        dom = max(kernels, key=lambda k: kernels[k]["share_of_step_est"] or 0.0)
         roofline = dict(kernels[dom])
-        roofline["other_kernels"] = [kernels[m] for m in kernels if m != dom]
+        roofline["other_kernels"] = [kernels[k] for k in kernels if k != dom]
         out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-               "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+               "warmup": args.warmup, "ms_per_step": device_ms / args.steps, "higher_is_better": True,
                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
                "config": {"workload": f"fwi-gradient {args.interior}^3+40 sponge ({fd.nz}x{fd.nx}x{fd.ny}), "
                                       f"{fd.nts} samples ({steps_per_pass} fine steps), 150x150 receivers x 9 "
                                       f"components, Ricker 10 Hz, one shot per step per GPU",
                           "parallelism": f"shots sharded over {world} GPU(s)",
                           "l2_flush": "inputs larger than L2 (each field 238 MB, working set > 14 GB)",
-                          "checkpoint_segment_blocks": seg, "stepper": args.variant, "checkpoints": prob.prop.checkpoint_type,
-                          "velocity_slots": prob.prop.velocity_storage},
-               "gcell_updates_per_s": world * args.steps * cell_updates / (ms_max / 1e3) / 1e9,
+                          "checkpoint_segment_blocks": seg, "recomputed_blocks": recompute_blocks,
+                          "stepper": args.variant, "decimation": args.decimation,
+                          "checkpoints": prob.prop.checkpoint_type, "velocity_slots": prob.prop.velocity_storage},
+               "gcell_updates_per_s": world * args.steps * cell_updates / (device_ms / 1e3) / 1e9,
                "roofline": roofline,
-               "gpu_launches": int(launches), "clocks": clk, "e2e": e2e}
-        if world == 1 and not args.no_cpu:
-            out["cpu_baseline"] = cpu_baseline(fd)
+               "gpu_launches": int(launches), "clocks": clk,
+               "e2e": {"value": world * args.steps / (e2e_ms / 1e3), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+                       "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_ms / args.steps, "loss": loss_value}}
+        if cb is not None:
+            out["cpu_baseline"] = cb
         print(json.dumps(out), flush=True)
     if args.breakdown and world == 1:
         kernel_breakdown(step)

@@ -67,6 +67,8 @@ SIGNATURES = {
     "e3d_nl_propagate_device_noalloc": ([P, P, I, P, P, P, P, P, P, P], I),
     "e3d_noalloc_work_bytes": ([], ctypes.c_size_t),
     "e3d_velocity_storage": ([P], I),
+    "e3d_set_decimation_ring": ([P, I], I),
+    "e3d_set_imaging_chunks": ([P, I], I),
     "e3d_checkpoint_type": ([P], I),
     "e3d_checkpoint_schedule": ([I, I, P, I, P], I),
     "e3d_checkpoint_plan": ([LL, I, I, D, I, I, I, P, P, P, P], I),

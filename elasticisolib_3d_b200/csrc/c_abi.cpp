@@ -460,6 +460,16 @@ int e3d_velocity_storage(const e3d_context* ctx) { return (ctx && ctx->c) ? velo
 
 int e3d_checkpoint_type(const e3d_context* ctx) { return (ctx && ctx->c) ? checkpointType(ctx->c) : -1; }
 
+int e3d_set_imaging_chunks(e3d_context* ctx, int chunks) {
+  CTX_OR_FAIL(ctx);
+  return setImagingChunks(ctx->c, chunks);
+}
+
+int e3d_set_decimation_ring(e3d_context* ctx, int on) {
+  CTX_OR_FAIL(ctx);
+  return setDecimationRing(ctx->c, on);
+}
+
 int e3d_nl_propagate_device_noalloc(const e3d_desc* desc, const float* const* planes8_dev, int adjoint,
                                     const long long* src_pos_dev, const int* src_off10,
                                     const long long* rec_pos_dev, const int* rec_off10, float* src_sig_dev,

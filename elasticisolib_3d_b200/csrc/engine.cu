@@ -68,8 +68,11 @@ struct Context {
   float* med[NMED] = {};
   bool haveMedium = false;
   int tx = 8;
-  int stages = 2;            // shared-memory pipeline depth of the stepper
-  int loader = 2;            // 0: plain loads, 1: cp.async, 2: TMA bulk tensor copies
+  int stages = 3;            // shared-memory pipeline depth of the stepper
+  // 0: plain loads, 1: cp.async, 2: TMA bulk tensor copies, 3-5: TMA forms with a rotating
+  // y-window, 6: split velocity/stress roles for every mode, 7 (default): split roles for the
+  // forward and time-reversed steps, loader 2's two-stage stepper for the exact adjoint
+  int loader = 7;
   int yChunks = 0;           // y chunks per (z, x) tile column of the stepper grid (0: automatic)
   int numSMs = 148;          // multiprocessors of the device
   int graphLoop = 1;         // 1: replay coarse blocks of the nonlinear loop as a CUDA graph
@@ -89,6 +92,13 @@ struct Context {
   size_t traceRingFloats = 0;
   Fields9 ss[2];             // secondary sources (forward) / decimated adjoint field (adjoint)
   Fields9 q0, q1;            // premultiplied adjoint levels (dual-state exact adjoint)
+  // Rings of fine time levels for the gradient's passes (empty: decimation
+  // accumulators fused into the stepper instead).  Level m lives in
+  // lev[m mod size]; the first two entries are the s0/s1 (source) and w0/w1
+  // (adjoint) buffers, so those always point into the ring.
+  std::vector<Fields9> srcRing, adjRing;
+  int ringMode = 1;          // 1: decimate from rings when sub allows it
+  int imgChunks = 0;         // y chunks of the y-marching imaging launch (0: automatic)
   float* pertDev[NMED] = {};
   // checkpoints
   int ckptType = CKPT_AUTO;
@@ -108,7 +118,7 @@ struct Context {
   // launch accounting and sampled stepper timing
   long long launches = 0;
   int timingEvery = 0;       // 0: off; n: time every n-th stepper launch
-  long long stepCounter = 0;
+  long long kindCounter[8] = {};
   std::vector<cudaEvent_t> evPool;
   struct Timed { int mode; cudaEvent_t a, b; };
   std::vector<Timed> timed;
@@ -281,12 +291,20 @@ int setMedium(Context* c, const float* const* planes, bool onDevice) {
 
 int setStepperVariant(Context* c, int tx, int stages, int loader) {
   E3D_ARG(c && (tx == 8 || tx == 16), "tile width must be 8 or 16");
-  E3D_ARG(stages == 2 || stages == 3, "pipeline depth must be 2 or 3");
-  E3D_ARG(loader >= 0 && loader <= 5, "loader must be 0 (plain), 1 (cp.async), 2-5 (TMA forms)");
+  E3D_ARG(loader >= 0 && loader <= 7, "loader must be 0 (plain), 1 (cp.async), 2-5 (TMA forms), 6-7 (split TMA)");
+  E3D_ARG(stages == 2 || stages == 3 || (loader >= 6 && stages == 4),
+          "pipeline depth must be 2 or 3 (4 with the split stepper)");
   E3D_ARG(!(tx == 16 && stages == 3), "16-wide tiles fit two stages at most");
+  E3D_ARG(loader < 6 || tx == 8, "the split stepper uses 8-wide tiles");
   c->tx = tx;
   c->stages = stages;
   c->loader = loader;
+  return E3D_OK;
+}
+
+int setImagingChunks(Context* c, int chunks) {
+  E3D_ARG(c && chunks >= 0, "bad chunk count");
+  c->imgChunks = chunks;
   return E3D_OK;
 }
 
@@ -332,6 +350,25 @@ static StepPtrs makeStep(Context* c, Fields9& o, const Fields9& cur) {
   }
   for (int k = 0; k < NMED; k++) p.m[k] = c->med[k];
   return p;
+}
+
+// A step that writes its new level into `nw` (a ring slot) instead of over the old level.
+static StepPtrs makeRingStep(Context* c, Fields9& o, const Fields9& cur, Fields9& nw) {
+  StepPtrs p = makeStep(c, o, cur);
+  for (int k = 0; k < NCOMP; k++) p.nw[k] = nw.p[k];
+  return p;
+}
+
+// The pointers the post-step kernels (injection, recording, refresh, source
+// extraction) act on: the new level as their "o".
+static StepPtrs afterStep(const StepPtrs& p) {
+  StepPtrs q = p;
+  if (p.nw[0])
+    for (int k = 0; k < NCOMP; k++) {
+      q.o[k] = p.nw[k];
+      q.nw[k] = nullptr;
+    }
+  return q;
 }
 
 // Opt a kernel into its dynamic shared memory once per device (function
@@ -431,6 +468,53 @@ static int launchTma(Context* c, const StepPtrs& p, dim3 grid, int yChunk) {
   return E3D_OK;
 }
 
+static int chooseChunks(const Context* c, long long tiles, int nyi, int perSM = 2);
+
+// Split stepper: role V maps (stress halos and leads, old velocities, rho planes) and role S maps
+// (velocity halos and leads, old stresses, lambda/mu planes).
+static int buildSplitMaps(Context* c, const StepPtrs& p, SplitMaps& mp) {
+  const CUtensorMap* m = nullptr;
+  const int vHalo[5] = {SXX, SXY, SXZ, SYZ, SZZ}, vLead[3] = {SXY, SYY, SYZ};
+  int i = 0;
+  for (int f : vHalo) { E3D_RET(tensorMap(c, p.c[f], SZ, 8 + 2 * HALO, &m)); mp.v[i++] = *m; }
+  for (int f : vLead) { E3D_RET(tensorMap(c, p.c[f], TZ, 8, &m)); mp.v[i++] = *m; }
+  for (int k = VX; k <= VZ; k++) { E3D_RET(tensorMap(c, p.o[k], TZ, 8, &m)); mp.v[i++] = *m; }
+  for (int k = RHOX; k <= RHOZ; k++) { E3D_RET(tensorMap(c, p.m[k], TZ, 8, &m)); mp.v[i++] = *m; }
+  i = 0;
+  for (int f = VX; f <= VZ; f++) { E3D_RET(tensorMap(c, p.c[f], SZ, 8 + 2 * HALO, &m)); mp.s[i++] = *m; }
+  for (int f = VX; f <= VZ; f++) { E3D_RET(tensorMap(c, p.c[f], TZ, 8, &m)); mp.s[i++] = *m; }
+  for (int k = SXX; k <= SYZ; k++) { E3D_RET(tensorMap(c, p.o[k], TZ, 8, &m)); mp.s[i++] = *m; }
+  for (int k = L2M; k <= MUYZ; k++) { E3D_RET(tensorMap(c, p.m[k], TZ, 8, &m)); mp.s[i++] = *m; }
+  return E3D_OK;
+}
+
+template <int MODE, int STAGES, int MINB>
+static int launchSplit(Context* c, const StepPtrs& p, int tiz, int tix, int nyi) {
+  constexpr size_t smem = (size_t)STAGES * SPL_STAGE_F * sizeof(float);
+  static std::atomic<unsigned long long> configured{0};
+  E3D_RET(ensureSmemAttr((const void*)kStepSplit<MODE, STAGES, MINB>, smem, configured));
+  SplitMaps mp;
+  E3D_RET(buildSplitMaps(c, p, mp));
+  // y runs measured best on B200 (392^3 and 288^3 grids, 3 stages): about 32 planes for the
+  // forward and time-reversed steps (0.84-0.85 of the copy bandwidth), about 10 for the
+  // dual-state exact adjoint (0.78-0.79; 0.59-0.64 with one long run)
+  int chunks = c->yChunks > 0 ? std::min(c->yChunks, nyi) : (nyi + (MODE == STEP_ADJ_EXACT ? 9 : 31)) /
+                                                                (MODE == STEP_ADJ_EXACT ? 10 : 32);
+  chunks = std::max(chunks, 1);
+  const int yChunk = (nyi + chunks - 1) / chunks;
+  chunks = (nyi + yChunk - 1) / yChunk;
+  kStepSplit<MODE, STAGES, MINB><<<dim3(tiz, tix, 2 * chunks), dim3(TZ, 8), smem, c->st>>>(mp, p, c->g, yChunk,
+                                                                                              chunks);
+  return E3D_OK;
+}
+
+template <int MODE>
+static int launchSplitVariant(Context* c, const StepPtrs& p, int tiz, int tix, int nyi) {
+  if (c->stages == 4) return launchSplit<MODE, 4, 2>(c, p, tiz, tix, nyi);
+  if (c->stages == 2) return launchSplit<MODE, 2, 3>(c, p, tiz, tix, nyi);
+  return launchSplit<MODE, 3, 3>(c, p, tiz, tix, nyi);
+}
+
 template <int MODE, int TX, int STAGES, bool OM_SMEM, int MINB>
 static int launchTma2(Context* c, const StepPtrs& p, dim3 grid, int yChunk) {
   constexpr size_t smem = (size_t)STAGES * Tma2Layout<TX, OM_SMEM>::STAGE_F * sizeof(float);
@@ -465,6 +549,7 @@ static int launchVariant(Context* c, const StepPtrs& p, dim3 grid, int yChunk) {
       default: return launchTma2<MODE, 8, 3, false, 2>(c, p, grid, yChunk);
     }
   }
+  if (c->loader >= 6) return launchTma<MODE, 8, 2>(c, p, grid, yChunk);  // split loaders: fused steps
   if (c->loader == 2) {
     switch (key) {
       case 82: return launchTma<MODE, 8, 2>(c, p, grid, yChunk);
@@ -492,36 +577,51 @@ static cudaEvent_t takeEvent(Context* c) {
   return e;
 }
 
-// Every stepper launch goes through here: counts it and, when sampling is
-// on, brackets every n-th one with CUDA events on the launching stream.
-static int launchStep(Context* c, int mode, const StepPtrs& p) {
-  c->launches++;
-  const bool sample = !c->inCapture && c->timingEvery > 0 && (c->stepCounter++ % c->timingEvery) == 0;
+// Sampled launch timing: with sampling on, every n-th launch of each timed
+// kind is bracketed with CUDA events on the launching stream.  Kinds: stepper
+// modes 0..2, the same with a fused decimation or secondary source 3..5, the
+// block imaging of the decimation ring 6, its velocity decimation 7.
+struct TimedLaunch {
+  Context* c;
+  int kind;
   cudaEvent_t a = nullptr, b = nullptr;
-  if (sample) {
+  TimedLaunch(Context* cc, int k) : c(cc), kind(k) {
+    if (c->inCapture || c->timingEvery <= 0) return;
+    if ((c->kindCounter[kind]++ % c->timingEvery) != 0) return;
     a = takeEvent(c);
     b = takeEvent(c);
     if (a && b) cudaEventRecord(a, c->st);
   }
-  const int st = launchStepRaw(c, mode, p);
-  if (sample && a && b) {
+  ~TimedLaunch() {
+    if (!(a && b)) {
+      if (a) c->evPool.push_back(a);
+      if (b) c->evPool.push_back(b);
+      return;
+    }
     cudaEventRecord(b, c->st);
-    // launches that also fuse a decimation or a secondary source are kept apart (mode + 3)
-    const bool fused = p.accL[0] != nullptr || p.ssL[0] != nullptr;
-    c->timed.push_back({mode + (fused ? 3 : 0), a, b});
+    c->timed.push_back({kind, a, b});
   }
-  return st;
+};
+
+// Every stepper launch goes through here: counts it and samples its time.
+static int launchStep(Context* c, int mode, const StepPtrs& p) {
+  c->launches++;
+  // launches that also fuse a decimation or a secondary source are kept apart (mode + 3)
+  const bool fused = p.accL[0] != nullptr || p.ssL[0] != nullptr;
+  TimedLaunch t(c, mode + (fused ? 3 : 0));
+  return launchStepRaw(c, mode, p);
 }
 
 int setKernelTiming(Context* c, int every) {
   E3D_ARG(c && every >= 0, "bad timing interval");
   c->timingEvery = every;
-  c->stepCounter = 0;
+  for (auto& k : c->kindCounter) k = 0;
   return E3D_OK;
 }
 
 int readKernelTiming(Context* c, int mode, double* avgMs, long long* count) {
   E3D_ARG(c && avgMs && count, "null argument");
+  E3D_ARG(mode >= 0 && mode < 8, "bad timed kind");
   double sum = 0;
   long long n = 0;
   std::vector<Context::Timed> keep;
@@ -546,6 +646,25 @@ int readKernelTiming(Context* c, int mode, double* avgMs, long long* count) {
 
 long long launchCount(const Context* c) { return c->launches; }
 
+// y chunks of a y-marching launch over `tiles` (z, x) tile columns: the CTAs
+// run in waves of perSM per SM, and each CTA pays about two planes of pipeline
+// start-up, so pick the chunk count (y runs of at least 24 planes) that
+// minimises waves * (planes per CTA + 2).
+static int chooseChunks(const Context* c, long long tiles, int nyi, int perSM) {
+  int chunks = 1;
+  const long long slots = (long long)perSM * c->numSMs;
+  long long bestCost = -1;
+  for (int ch = 1; ch <= std::max(1, nyi / 24); ch++) {
+    const long long waves = (tiles * ch + slots - 1) / slots;
+    const long long cost = waves * ((nyi + ch - 1) / ch + 2);
+    if (bestCost < 0 || cost < bestCost) {
+      bestCost = cost;
+      chunks = ch;
+    }
+  }
+  return chunks;
+}
+
 static int launchStepRaw(Context* c, int mode, const StepPtrs& p) {
   const GridConst& g = c->g;
   const int tiz = (g.nz - 2 * FAT + TZ - 1) / TZ;
@@ -553,25 +672,22 @@ static int launchStepRaw(Context* c, int mode, const StepPtrs& p) {
   const int nyi = g.ny - 2 * FAT;
   // enough CTAs for several waves over 148 SMs, chunks of at least 32 planes
   const long long tiles = (long long)tiz * tix;
-  // y chunks: the CTAs of a launch run in waves of two per SM, and each CTA
-  // pays about two planes of pipeline start-up, so pick the chunk count (y runs
-  // of at least 24 planes) that minimises waves * (planes per CTA + 2).
-  // Measured on B200: at 288^3 this takes the forward from 0.54 to 0.67 of the
-  // copy bandwidth (10 chunks instead of 2); at 392^3 it keeps the long runs.
-  int chunks = 1;
-  {
-    const long long slots = 2LL * c->numSMs;
-    long long bestCost = -1;
-    for (int ch = 1; ch <= std::max(1, nyi / 24); ch++) {
-      const long long waves = (tiles * ch + slots - 1) / slots;
-      const long long cost = waves * ((nyi + ch - 1) / ch + 2);
-      if (bestCost < 0 || cost < bestCost) {
-        bestCost = cost;
-        chunks = ch;
-      }
-    }
-  }
+  // y chunks (chooseChunks).  Measured on B200: at 288^3 this takes the forward
+  // from 0.54 to 0.67 of the copy bandwidth (10 chunks instead of 2); at 392^3
+  // it keeps the long runs.
+  int chunks = chooseChunks(c, tiles, nyi);
   const bool dual = mode == STEP_ADJ_EXACT && p.oP[0] != nullptr;
+  // the split stepper (loader 6; loader 7: all but the exact adjoint, which keeps kStepTma) takes
+  // every step without a fused decimation or secondary source
+  if ((c->loader == 6 || (c->loader == 7 && mode != STEP_ADJ_EXACT)) && g.nz % 4 == 0 && p.accL[0] == nullptr &&
+      p.ssL[0] == nullptr) {
+    const int tixS = (g.nx - 2 * FAT + 7) / 8;
+    if (mode == STEP_FWD) E3D_RET(launchSplitVariant<STEP_FWD>(c, p, tiz, tixS, nyi));
+    else if (mode == STEP_ADJ_REVERSED) E3D_RET(launchSplitVariant<STEP_ADJ_REVERSED>(c, p, tiz, tixS, nyi));
+    else E3D_RET(launchSplitVariant<STEP_ADJ_EXACT>(c, p, tiz, tixS, nyi));
+    E3D_LAUNCH_CHECK();
+    return E3D_OK;
+  }
   // The dual-state adjoint runs faster on short y runs: measured on B200 at
   // 392x392x388, about 16 planes per CTA with the 9-field decimation fused
   // (0.64 -> 0.75 of the copy bandwidth) and about 32 without it; the other
@@ -586,7 +702,7 @@ static int launchStepRaw(Context* c, int mode, const StepPtrs& p) {
   if (dual) {
     E3D_ARG(g.nz % 4 == 0, "dual-state adjoint needs nz % 4 == 0");
     if (c->tx == 16) E3D_RET((launchTma<STEP_ADJ_EXACT, 16, 2>(c, p, grid, yChunk)));
-    else if (c->stages == 3) E3D_RET((launchTma<STEP_ADJ_EXACT, 8, 3>(c, p, grid, yChunk)));
+    else if (c->stages == 3 && c->loader < 6) E3D_RET((launchTma<STEP_ADJ_EXACT, 8, 3>(c, p, grid, yChunk)));
     else E3D_RET((launchTma<STEP_ADJ_EXACT, 8, 2>(c, p, grid, yChunk)));
   } else if (pipe) {
     if (mode == STEP_FWD) E3D_RET(launchVariant<STEP_FWD>(c, p, grid, yChunk));
@@ -654,6 +770,29 @@ static int launchExtractSource(Context* c, const StepPtrs& p, const DevSignals& 
   kExtractSource<<<(n + 127) / 128, 128, 0, c->st>>>(p, c->g, ss, out + (size_t)its * ntot,
                                                      out + (size_t)(its + 1) * ntot, c->filt[k],
                                                      c->filt[c->hfilt + k]);
+  E3D_LAUNCH_CHECK();
+  return E3D_OK;
+}
+
+static int launchRefresh(Context* c, const StepPtrs& p, const DevSignals& s);
+
+// Receiver injection (slices its, its+1, filter weights k) and premultiplied refresh of the dual
+// adjoint in one launch when the three normal-stress tables have equal counts (they share the
+// center grid); otherwise the two launches.
+static int launchInjectRefresh(Context* c, const StepPtrs& p, const DevSignals& s, const float* sigL,
+                               const float* sigR, int k) {
+  const int nc = s.off[SXX + 1] - s.off[SXX];
+  if (p.accL[0] != nullptr || s.off[SYY + 1] - s.off[SYY] != nc || s.off[SZZ + 1] - s.off[SZZ] != nc) {
+    E3D_RET(launchInjectSlices(c, p, s, sigL, sigR, k));
+    return launchRefresh(c, p, s);
+  }
+  SparseSet ss;
+  ss.pos = s.pos;
+  for (int i = 0; i <= NCOMP; i++) ss.off[i] = s.off[i];
+  const int n = s.off[NCOMP];
+  if (n == 0) return E3D_OK;
+  c->launches++;
+  kInjectRefresh<<<(n + 127) / 128, 128, 0, c->st>>>(p, c->g, ss, sigL, sigR, c->filt[k], c->filt[c->hfilt + k]);
   E3D_LAUNCH_CHECK();
   return E3D_OK;
 }
@@ -1115,6 +1254,130 @@ static int launchImaging(Context* c, bool adjoint, int t, float* vPrev, float* v
   return E3D_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Rings of fine time levels (the gradient's passes).  With a ring the stepper
+// writes level m+1 into its own slot, so the sub levels of a coarse block are
+// all still there when the block ends, and one launch per block decimates them
+// (source velocity) or decimates and images them (adjoint) instead of the
+// stepper reading and writing two accumulators at every fine step.
+// ---------------------------------------------------------------------------
+static int ringLevels(const Context* c) {
+  return (c->ringMode && c->d.sub <= RING_SUB_MAX) ? std::max(c->d.sub + 1, 3) : 0;
+}
+
+static Fields9& ringAt(std::vector<Fields9>& r, long long m) {
+  const long long R = (long long)r.size();
+  return r[(size_t)(((m % R) + R) % R)];
+}
+
+// Allocate a ring of `levels` levels whose first two are a and b; every level zeroed.
+static int ensureRing(Context* c, std::vector<Fields9>& ring, Fields9& a, Fields9& b, int levels) {
+  if (ring.empty()) {
+    E3D_RET(allocFields(c, a, false));
+    E3D_RET(allocFields(c, b, false));
+    ring.push_back(a);
+    ring.push_back(b);
+    while ((int)ring.size() < levels) {
+      Fields9 f;
+      E3D_RET(allocFields(c, f, false));
+      ring.push_back(f);
+    }
+  }
+  E3D_ARG((int)ring.size() == levels, "ring size changed");
+  for (auto& f : ring) E3D_RET(zeroFields(c, f));
+  return E3D_OK;
+}
+
+// Source velocity of the block whose last fine level is mEnd (fine steps 1..sub
+// are levels mEnd-sub+1..mEnd): the left part into vLeft (leftMode 1 added to
+// the right part of the previous block already there, 2 written, 0 skipped)
+// and the right part written into vRight (may be null).
+static int launchDecimate(Context* c, long long mEnd, float* vLeft, int leftMode, float* vRight) {
+  DecimatePtrs d{};
+  const int sub = c->d.sub;
+  d.nlev = sub;
+  for (int t = 0; t < sub; t++) {
+    Fields9& L = ringAt(c->srcRing, mEnd - sub + 1 + t);
+    for (int k = 0; k < 3; k++) d.lev[t][k] = L.p[k];
+    d.wl[t] = c->filt[t + 1];
+    d.wr[t] = c->filt[c->hfilt + t + 1];
+  }
+  d.vl = leftMode ? vLeft : nullptr;
+  d.vlMode = leftMode;
+  d.vr = vRight;
+  d.n = c->g.n;
+  if (!d.vl && !d.vr) return E3D_OK;
+  bool vec = c->g.n % 4 == 0;
+  for (int t = 0; t < sub; t++)
+    for (int k = 0; k < 3; k++) vec = vec && ((uintptr_t)d.lev[t][k] % 16 == 0);
+  vec = vec && (!d.vl || (uintptr_t)d.vl % 16 == 0) && (!d.vr || (uintptr_t)d.vr % 16 == 0);
+  const long long items = vec ? c->g.n / 4 : c->g.n;
+  const unsigned gx = (unsigned)std::min<long long>((items + 255) / 256, (long long)c->numSMs * 8);
+  c->launches++;
+  TimedLaunch tl(c, 7);
+  if (vec) kDecimateVelocity<true><<<dim3(gx, 3), 256, 0, c->st>>>(d);
+  else kDecimateVelocity<false><<<dim3(gx, 3), 256, 0, c->st>>>(d);
+  E3D_LAUNCH_CHECK();
+  return E3D_OK;
+}
+
+// Adjoint imaging of block its from the adjoint ring; the block's last fine
+// level (it2 = 0) is mEnd, so level it2 is mEnd - it2.  v[0..3] = V(its-1..its+2).
+static int launchImagingBlock(Context* c, long long mEnd, float* const v[4], bool carryIn, bool leftImage,
+                              Fields9& carry) {
+  ImagingBlockPtrs q{};
+  const int sub = c->d.sub;
+  q.nlev = sub;
+  // in the order the fine steps ran (it2 = sub-1 first), as the fused decimation summed them
+  for (int j = 0; j < sub; j++) {
+    const int it2 = sub - 1 - j;
+    Fields9& L = ringAt(c->adjRing, mEnd - it2);
+    for (int k = 0; k < NCOMP; k++) q.lev[j][k] = L.p[k];
+    q.wl[j] = c->filt[it2];
+    q.wr[j] = c->filt[c->hfilt + it2];
+  }
+  const long long n = c->g.n;
+  for (int t = 0; t < 4; t++)
+    for (int k = 0; k < 3; k++) q.v[t][k] = vComp(v[t], k, n);
+  for (int k = 0; k < NCOMP; k++) q.carry[k] = carry.p[k];
+  q.carryIn = carryIn ? 1 : 0;
+  q.leftImage = leftImage ? 1 : 0;
+  for (int k = 0; k < NMED; k++) q.pert[k] = c->pertDev[k];
+  q.dtsInv = c->dtsInv;
+  q.q3compat = c->d.q3compat;
+  c->launches++;
+  TimedLaunch tl(c, 6);
+  if (c->d.nz % 4 == 0 && c->loader >= 2) {
+    // y-marching TMA form: tensor maps of the velocity fields (cached per pointer)
+    ImagingMaps mp;
+    const CUtensorMap* m = nullptr;
+    for (int t = 0; t < 2; t++)
+      for (int k = 0; k < 3; k++) {
+        const float* src = q.v[t + 1][k] ? q.v[t + 1][k] : q.v[2][k];  // time 0 absent: any valid field
+        E3D_RET(tensorMap(c, src, SZ, IMG_TX + 2 * HALO, &m));
+        mp.halo[t][k] = *m;
+        E3D_RET(tensorMap(c, src, TZ, IMG_TX, &m));
+        mp.lead[t][k] = *m;
+      }
+    constexpr size_t smem = (size_t)2 * IMG_STAGE_F * sizeof(float);
+    static std::atomic<unsigned long long> configured{0};
+    E3D_RET(ensureSmemAttr((const void*)kImagingTma, smem, configured));
+    const int tiz = (c->g.nz - 2 * FAT + TZ - 1) / TZ;
+    const int tix = (c->g.nx - 2 * FAT + IMG_TX - 1) / IMG_TX;
+    const int nyi = c->g.ny - 2 * FAT;
+    const int chunks0 = c->imgChunks > 0 ? std::min(c->imgChunks, nyi) : chooseChunks(c, (long long)tiz * tix, nyi);
+    const int yChunk = (nyi + chunks0 - 1) / chunks0;
+    const int chunks = (nyi + yChunk - 1) / yChunk;
+    kImagingTma<<<dim3(tiz, tix, chunks), dim3(TZ, IMG_TX), smem, c->st>>>(mp, q, c->g, yChunk);
+  } else {
+    dim3 block(32, 8);
+    dim3 grid((c->d.nz - 2 * FAT + 31) / 32, (c->d.nx - 2 * FAT + 7) / 8, c->d.ny - 2 * FAT);
+    kImagingBlock<<<grid, block, 0, c->st>>>(q, c->g);
+  }
+  E3D_LAUNCH_CHECK();
+  return E3D_OK;
+}
+
 static int ensurePert(Context* c) {
   for (int k = 0; k < NMED; k++)
     if (!c->pertDev[k]) E3D_RET(devAlloc(c, (void**)&c->pertDev[k], (size_t)c->g.n * sizeof(float)));
@@ -1214,8 +1477,15 @@ static double heldBytes(const Context* c) {
 static double pendingAdjointBytes(const Context* c) {
   const double f = (double)c->g.n * sizeof(float);
   double b = 0;
-  if (!c->w0.p[0]) b += 18 * f;
-  if (!c->ss[0].p[0]) b += 18 * f;
+  const int R = ringLevels(c);
+  if (R) {
+    // the adjoint ring (w0, w1 and R-2 more levels) and the carried decimation
+    if (c->adjRing.empty()) b += (double)(R - 2) * NCOMP * f + (c->w0.p[0] ? 0 : 18 * f);
+    if (!c->ss[0].p[0]) b += NCOMP * f;
+  } else {
+    if (!c->w0.p[0]) b += 18 * f;
+    if (!c->ss[0].p[0]) b += 18 * f;
+  }
   if (!c->q0.p[0] && c->loader >= 2) b += 18 * f;
   return b;
 }
@@ -1373,7 +1643,7 @@ static int prepareCheckpoints(Context* c, int& L, int& nseg) {
     c->ckpt.assign(nseg, nullptr);
     c->ckptScale.assign(nseg, nullptr);
     c->ckptAllocType = c->ckptUsed;
-    E3D_RET(resizeVStorage(c, c->vUsed == V_F32 ? L + 3 : 3, c->vUsed == V_F32 ? 0 : L + 2));
+    E3D_RET(resizeVStorage(c, c->vUsed == V_F32 ? L + 3 : 4, c->vUsed == V_F32 ? 0 : L + 2));
     c->vAllocType = c->vUsed;
     for (int s = 1; s < nseg; s++) {
       const size_t eb = c->ckptUsed == CKPT_F32 ? 4 : 2;
@@ -1422,8 +1692,12 @@ static int traceSpread(Context* c, const TraceMap& m, int nReg, const float* irr
 // receivers are recorded too (this is the nonlinear forward of FWI): into a
 // time-major regular-grid array, or, with a trace map, through a two-slice
 // ring converted to irregular traces as each coarse slice completes.
+static int sourcePassRing(Context* c, const DevSignals& srcSet, const DevSignals* recSet, const float* srcSig,
+                          float* recSig, const TraceMap* map);
+
 static int sourcePassWithCheckpoints(Context* c, const DevSignals& srcSet, const DevSignals* recSet,
                                      const float* srcSig, float* recSig, const TraceMap* map) {
+  if (ringLevels(c)) return sourcePassRing(c, srcSet, recSet, srcSig, recSig, map);
   int L = 0, nseg = 0;
   c->ckptValid = false;
   c->tailValid = false;
@@ -1493,16 +1767,20 @@ static int sourcePassWithCheckpoints(Context* c, const DevSignals& srcSet, const
 // trace map the residual is irregular and time-major; each coarse slice is
 // spread to the regular acquisition points just before the block that
 // injects it.
+static int adjointPassRing(Context* c, const DevSignals& srcSet, const DevSignals& recSet, const float* srcSig,
+                           const float* resid, const TraceMap* map, float* srcAdj);
+
 static int adjointPassFromCheckpoints(Context* c, const DevSignals& srcSet, const DevSignals& recSet,
                                       const float* srcSig, const float* resid, const TraceMap* map,
                                       float* srcAdj = nullptr) {
   E3D_ARG(c->ckptValid, "no checkpoints for this shot");
+  if (ringLevels(c)) return adjointPassRing(c, srcSet, recSet, srcSig, resid, map, srcAdj);
   const int nts = c->d.nts, sub = c->d.sub, L = c->ckptSegLen;
   const int blocks = nts - 1;
   const int nseg = (blocks + L - 1) / L;
   const long long n = c->g.n;
   const bool vc = c->vUsed == V_F16;
-  E3D_RET(resizeVStorage(c, std::max<int>(vc ? 3 : L + 3, (int)c->vSlots.size()),
+  E3D_RET(resizeVStorage(c, std::max<int>(vc ? 4 : L + 3, (int)c->vSlots.size()),
                          std::max<int>(vc ? L + 2 : 0, (int)c->vStore.size())));
   E3D_RET(allocFields(c, c->w0, true));
   E3D_RET(allocFields(c, c->w1, true));
@@ -1624,6 +1902,220 @@ static int adjointPassFromCheckpoints(Context* c, const DevSignals& srcSet, cons
   return E3D_OK;
 }
 
+// ---------------------------------------------------------------------------
+// The checkpointed passes with rings of fine levels (the same schedule, loop
+// order and checkpoints as the two functions above; only the decimation
+// moves out of the stepper into one launch per coarse block).
+// ---------------------------------------------------------------------------
+
+// One coarse block (its) of the source-side forward propagation on the source
+// ring from level m, injecting srcSig; then the block's velocity decimated
+// into vLeft (leftMode as launchDecimate) and vRight.  m advances by sub.
+static int sourceBlockRing(Context* c, long long& m, int its, const DevSignals& srcSet, const float* srcSig,
+                           float* vLeft, int leftMode, float* vRight) {
+  auto S = [&](long long k) -> Fields9& { return ringAt(c->srcRing, k); };
+  for (int it2 = 1; it2 <= c->d.sub; it2++) {
+    StepPtrs p = makeRingStep(c, S(m - 1), S(m), S(m + 1));
+    E3D_RET(launchStep(c, STEP_FWD, p));
+    E3D_RET(launchInject(c, afterStep(p), srcSet, srcSig, its, it2 - 1));
+    m++;
+  }
+  if ((vLeft && leftMode) || vRight) E3D_RET(launchDecimate(c, m, vLeft, leftMode, vRight));
+  c->s0 = S(m - 1);
+  c->s1 = S(m);
+  return E3D_OK;
+}
+
+static int sourcePassRing(Context* c, const DevSignals& srcSet, const DevSignals* recSet, const float* srcSig,
+                          float* recSig, const TraceMap* map) {
+  int L = 0, nseg = 0;
+  c->ckptValid = false;
+  c->tailValid = false;
+  // the ring is allocated before the plan, so that the free memory the plan sees excludes it
+  E3D_RET(ensureRing(c, c->srcRing, c->s0, c->s1, ringLevels(c)));
+  E3D_RET(prepareCheckpoints(c, L, nseg));
+  const int nts = c->d.nts, sub = c->d.sub, blocks = nts - 1;
+  const size_t nr = recSet ? (size_t)recSet->off[NCOMP] : 0;
+  const size_t rows = map ? (size_t)NCOMP * map->nIrreg : 0;
+  float* ring = nullptr;
+  if (recSig && map) {
+    E3D_RET(traceRingAtLeast(c, 2 * nr));
+    ring = c->traceRing;
+    E3D_CUDA_TRY(cudaMemsetAsync(ring, 0, std::max<size_t>(2 * nr, 1) * sizeof(float), c->st));
+  } else if (recSig) {
+    E3D_CUDA_TRY(cudaMemsetAsync(recSig, 0, std::max<size_t>(nr, 1) * nts * sizeof(float), c->st));
+  }
+  // the last segment's velocity V[tailBeg .. nts-1] (FP32: one slot per time;
+  // FP16: a two-slot FP32 ring packed into the FP16 slots as each time completes)
+  const bool vc = c->vUsed == V_F16;
+  const int tailBeg = segStart(blocks, L, nseg, nseg - 1);
+  auto A = [&](int t) -> float* {
+    if (t < tailBeg || t >= nts) return nullptr;
+    return vc ? c->vSlots[(t - tailBeg) % 2] : c->vSlots[t - tailBeg];
+  };
+  auto S = [&](long long k) -> Fields9& { return ringAt(c->srcRing, k); };
+  long long m = 0;  // levels -1 and 0 are the zero initial state
+  int nextCk = 1;
+  for (int b = 0; b < blocks; b++) {
+    if (nextCk < nseg && b == segStart(blocks, L, nseg, nextCk) - 1) {
+      c->s0 = S(m - 1);
+      c->s1 = S(m);
+      E3D_RET(packState(c, nextCk++));
+    }
+    for (int it2 = 1; it2 <= sub; it2++) {
+      StepPtrs p = makeRingStep(c, S(m - 1), S(m), S(m + 1));
+      E3D_RET(launchStep(c, STEP_FWD, p));
+      const StepPtrs q = afterStep(p);
+      E3D_RET(launchInject(c, q, srcSet, srcSig, b, it2 - 1));
+      if (ring) E3D_RET(launchRecordSlices(c, q, *recSet, ring + (b % 2) * nr, ring + ((b + 1) % 2) * nr, it2));
+      else if (recSig) E3D_RET(launchRecord(c, q, *recSet, recSig, b, it2));
+      m++;
+    }
+    // block tailBeg-1 feeds V[tailBeg] through its right weights only; V[0] has no earlier block
+    if (b >= tailBeg - 1) E3D_RET(launchDecimate(c, m, A(b), b < tailBeg ? 0 : (b == 0 ? 2 : 1), A(b + 1)));
+    if (vc && b >= tailBeg) {
+      // V[b] is complete: store it; its slot next receives V[b+2], written by block b+1
+      E3D_RET(packVelocity(c, A(b), c->vStore[b - tailBeg]));
+    }
+    if (ring) {
+      // slice b is complete; its ring slot is reused for slice b+2
+      E3D_RET(traceGather(c, *map, (int)nr, ring + (b % 2) * nr, recSig + (size_t)b * rows));
+      if (nr) E3D_CUDA_TRY(cudaMemsetAsync(ring + (b % 2) * nr, 0, nr * sizeof(float), c->st));
+    }
+  }
+  // V[nts-1] has no block of its own: complete after block nts-2
+  if (vc) E3D_RET(packVelocity(c, A(nts - 1), c->vStore[nts - 1 - tailBeg]));
+  if (ring) E3D_RET(traceGather(c, *map, (int)nr, ring + ((nts - 1) % 2) * nr, recSig + (size_t)(nts - 1) * rows));
+  c->s0 = S(m - 1);
+  c->s1 = S(m);
+  c->ckptValid = true;
+  c->tailValid = true;
+  return E3D_OK;
+}
+
+// Adjoint pass with the adjoint levels in a ring: after the last fine step of
+// block its, one launch decimates its levels into the right part R (coarse
+// sample its+1) and the left part L (its) and images both.  V(its-1) belongs
+// to the segment's window except at its first block, whose L is carried to the
+// next block processed (the last block of the previous segment), as the fused
+// decimation carried its accumulator.
+static int adjointPassRing(Context* c, const DevSignals& srcSet, const DevSignals& recSet, const float* srcSig,
+                           const float* resid, const TraceMap* map, float* srcAdj) {
+  const int nts = c->d.nts, sub = c->d.sub, L = c->ckptSegLen;
+  const int blocks = nts - 1;
+  const int nseg = (blocks + L - 1) / L;
+  const bool vc = c->vUsed == V_F16;
+  E3D_RET(resizeVStorage(c, std::max<int>(vc ? 4 : L + 3, (int)c->vSlots.size()),
+                         std::max<int>(vc ? L + 2 : 0, (int)c->vStore.size())));
+  E3D_RET(ensureRing(c, c->adjRing, c->w0, c->w1, ringLevels(c)));
+  Fields9& carry = c->ss[0];
+  E3D_RET(allocFields(c, carry, true));  // L of the block after the last one: zero
+  const bool dual = c->loader >= 2 && c->d.nz % 4 == 0;
+  if (dual) {
+    E3D_RET(allocFields(c, c->q0, true));
+    E3D_RET(allocFields(c, c->q1, true));
+  }
+  const size_t nr = (size_t)recSet.off[NCOMP];
+  const size_t rows = map ? (size_t)NCOMP * map->nIrreg : 0;
+  if (srcAdj)
+    E3D_CUDA_TRY(cudaMemsetAsync(srcAdj, 0, (size_t)std::max(srcSet.off[NCOMP], 1) * nts * sizeof(float), c->st));
+  if (map) {
+    E3D_RET(traceRingAtLeast(c, 2 * nr));
+    E3D_RET(traceSpread(c, *map, (int)nr, resid + (size_t)(nts - 1) * rows, c->traceRing + ((nts - 1) % 2) * nr));
+  }
+  auto dataSlice = [&](int t) -> const float* {
+    return map ? c->traceRing + (t % 2) * nr : resid + (size_t)t * nr;
+  };
+  int winStart = 0, winEnd = -1;  // velocity window [winStart, winEnd] of the current segment
+  int held[4] = {-1, -1, -1, -1};  // FP16 slots: the time unpacked in FP32 slot t % 4
+  // FP32 velocity of coarse time t for the imaging condition
+  auto V = [&](int t) -> float* {
+    if (t < 0 || t >= nts) return nullptr;
+    if (vc) return held[t % 4] == t ? c->vSlots[t % 4] : nullptr;
+    const int i = t - winStart;
+    return (i >= 0 && i < (int)c->vSlots.size()) ? c->vSlots[i] : nullptr;
+  };
+  auto unpackV = [&](int t) -> int {
+    if (!vc || t < winStart || t > winEnd || held[t % 4] == t) return E3D_OK;
+    E3D_RET(unpackVelocity(c, c->vStore[t - winStart], c->vSlots[t % 4]));
+    held[t % 4] = t;
+    return E3D_OK;
+  };
+  // accumulation slot of V[t] while the segment is recomputed
+  auto Acc = [&](int t) -> float* {
+    if (t < 0 || t >= nts) return nullptr;
+    return vc ? c->vSlots[(t - winStart) % 2] : c->vSlots[t - winStart];
+  };
+  auto W = [&](long long k) -> Fields9& { return ringAt(c->adjRing, k); };
+  long long ma = 0;  // adjoint levels -1 and 0: the zero final state
+  const bool tailKept = c->tailValid;
+  if (nseg > 1) c->tailValid = false;
+  for (int s = nseg - 1; s >= 0; s--) {
+    const int bBeg = segStart(blocks, L, nseg, s);
+    const int bEnd = segStart(blocks, L, nseg, s + 1);  // adjoint blocks [bBeg, bEnd)
+    const int lastBlock = std::min(bEnd + 1, blocks - 1);
+    winStart = bBeg;
+    winEnd = std::min(bEnd + 1, nts - 1);
+    if (!(tailKept && s == nseg - 1)) {
+      // recompute V[bBeg .. min(bEnd+1, nts-1)] from the checkpoint
+      long long m = 0;
+      int firstBlock = 0;
+      auto S = [&](long long k) -> Fields9& { return ringAt(c->srcRing, k); };
+      if (s == 0) {
+        E3D_RET(zeroFields(c, S(-1)));
+        E3D_RET(zeroFields(c, S(0)));
+      } else {
+        c->s0 = S(-1);
+        c->s1 = S(0);
+        E3D_RET(unpackState(c, s));
+        // block bBeg-1 only feeds V[bBeg] through its right weights
+        E3D_RET(sourceBlockRing(c, m, bBeg - 1, srcSet, srcSig, nullptr, 0, Acc(bBeg)));
+        firstBlock = bBeg;
+      }
+      for (int b = firstBlock; b <= lastBlock; b++) {
+        E3D_RET(sourceBlockRing(c, m, b, srcSet, srcSig, Acc(b), b == 0 ? 2 : 1, Acc(b + 1)));
+        // V[b] is complete: store it; its slot next receives V[b+2], written by block b+1
+        if (vc) E3D_RET(packVelocity(c, Acc(b), c->vStore[b - bBeg]));
+      }
+      // V[nts-1] has no block of its own: complete after block nts-2
+      if (vc && lastBlock + 1 == nts - 1 && nts - 1 <= bEnd + 1)
+        E3D_RET(packVelocity(c, Acc(nts - 1), c->vStore[nts - 1 - bBeg]));
+    }
+    for (int i = 0; i < 4; i++) held[i] = -1;  // the recompute used the FP32 slots
+    // adjoint blocks, last to first
+    for (int its = bEnd - 1; its >= bBeg; its--) {
+      const bool leftImage = its > bBeg;
+      for (int t = its + 2; t >= (leftImage ? its - 1 : its); t--) E3D_RET(unpackV(t));
+      if (map) E3D_RET(traceSpread(c, *map, (int)nr, resid + (size_t)its * rows, c->traceRing + (its % 2) * nr));
+      for (int it2 = sub - 1; it2 >= 0; it2--) {
+        StepPtrs p = makeRingStep(c, W(ma - 1), W(ma), W(ma + 1));
+        if (dual) {
+          for (int k = 0; k < NCOMP; k++) {
+            p.c[k] = c->q1.p[k];
+            p.oP[k] = c->q0.p[k];
+          }
+        }
+        E3D_RET(launchStep(c, STEP_ADJ_EXACT, p));
+        const StepPtrs q = afterStep(p);
+        if (dual) E3D_RET(launchInjectRefresh(c, q, recSet, dataSlice(its), dataSlice(its + 1), it2 + 1));
+        else E3D_RET(launchInjectSlices(c, q, recSet, dataSlice(its), dataSlice(its + 1), it2 + 1));
+        // transpose of the source injection of forward step (its, it2+1): the exact
+        // adjoint of the nonlinear propagation with respect to the scaled source signals
+        if (srcAdj) E3D_RET(launchExtractSource(c, q, srcSet, srcAdj, its, it2));
+        ma++;
+        if (dual) swapF(c->q0, c->q1);
+      }
+      float* const v[4] = {leftImage ? V(its - 1) : nullptr, V(its), V(its + 1), V(its + 2)};
+      E3D_RET(launchImagingBlock(c, ma, v, its == bEnd - 1, leftImage, carry));
+    }
+  }
+  // final imaging at t = 0: the carried left part of block 0
+  E3D_RET(launchImaging(c, true, 0, nullptr, V(0), V(1), carry));
+  c->w0 = W(ma - 1);
+  c->w1 = W(ma);
+  return E3D_OK;
+}
+
 static int bornAdjointDevice(Context* c, const DevSignals& srcSet, const DevSignals& recSet, const float* srcSig,
                              const float* resid) {
   E3D_RET(sourcePassWithCheckpoints(c, srcSet, nullptr, srcSig, nullptr, nullptr));
@@ -1726,6 +2218,14 @@ int setVelocityStorage(Context* c, int type) {
 }
 
 int velocityStorage(const Context* c) { return c->vUsed; }
+
+int setDecimationRing(Context* c, int on) {
+  E3D_ARG(c && (on == 0 || on == 1), "bad decimation mode");
+  c->ringMode = on;
+  c->ckptValid = false;
+  c->tailValid = false;
+  return E3D_OK;
+}
 
 int checkpointType(const Context* c) { return c->ckptUsed; }
 

@@ -101,6 +101,11 @@ int fwiGradientDevice(Context* c, const DevSignals& srcSet, const DevSignals& re
 int setVelocityStorage(Context* c, int type);
 int velocityStorage(const Context* c);
 int checkpointType(const Context* c);
+// Decimation of the gradient's passes: 1 (default) from rings of fine levels, one
+// launch per coarse block; 0 through accumulators fused into every fine step.
+int setDecimationRing(Context* c, int on);
+// y chunks of the y-marching block imaging launch (0: automatic).
+int setImagingChunks(Context* c, int chunks);
 
 // Allocation-free nonlinear propagation on the current device: the wavefield
 // levels and the taper live in a fixed 64 MiB device array (staticWorkBytes());

@@ -21,7 +21,8 @@ constexpr int HALO = 4;
 constexpr int SZ = TZ + 2 * HALO;  // shared tile row length (z)
 
 struct StepPtrs {
-  float* o[NCOMP];        // old level in, new level out (in place)
+  float* o[NCOMP];        // old level in; new level out when nw is null (in place)
+  float* nw[NCOMP];       // new level out (null: written over the old level)
   const float* c[NCOMP];  // current level
   const float* m[NMED];   // medium planes
   // optional Born secondary source injected inside the step (may be null)
@@ -220,7 +221,7 @@ __global__ void __launch_bounds__(TZ * TX) kStep(StepPtrs p, GridConst g, int yC
         float v = G * ov[k] + up[k];
         if (hasSS) v += __ldg(p.ssL[k] + ic) * p.ssWl + __ldg(p.ssR[k] + ic) * p.ssWr;
         v *= G;
-        p.o[k][ic] = v;
+        (p.nw[0] ? p.nw[k] : p.o[k])[ic] = v;
         if (hasAcc && k < p.nAcc) {
           p.accL[k][ic] += v * p.accWl;
           if (p.accR[0] != nullptr) p.accR[k][ic] += v * p.accWr;
@@ -399,7 +400,7 @@ __global__ void __launch_bounds__(TZ * TX) kStepPipe(StepPtrs p, GridConst g, in
         float v = G * ov[k * L::INT_F] + up[k];
         if (hasSS) v += __ldg(p.ssL[k] + ic) * p.ssWl + __ldg(p.ssR[k] + ic) * p.ssWr;
         v *= G;
-        p.o[k][ic] = v;
+        (p.nw[0] ? p.nw[k] : p.o[k])[ic] = v;
         if (hasAcc && k < p.nAcc) {
           p.accL[k][ic] += v * p.accWl;
           if (p.accR[0] != nullptr) p.accR[k][ic] += v * p.accWr;
@@ -624,7 +625,7 @@ __global__ void __launch_bounds__(TZ * TX) kStepTma(const __grid_constant__ TmaM
       }
 #pragma unroll
       for (int k = 0; k < NCOMP; k++) {
-        p.o[k][ic] = nv[k];
+        (p.nw[0] ? p.nw[k] : p.o[k])[ic] = nv[k];
         if (hasAcc && k < p.nAcc) {
           p.accL[k][ic] = preL[k] + nv[k] * p.accWl;
           if (hasR) p.accR[k][ic] = preR[k] + nv[k] * p.accWr;
@@ -644,6 +645,213 @@ __global__ void __launch_bounds__(TZ * TX) kStepTma(const __grid_constant__ TmaM
     }
     slot = (slot + 1 == STAGES) ? 0 : slot + 1;
   }
+}
+
+// ---------------------------------------------------------------------------
+// Split stepper.  Within one step the velocity update reads only the current
+// stresses and the stress update only the current velocities, so a launch can
+// run them as two independent CTA roles: role V (blockIdx.z < yChunksV)
+// advances vx, vy, vz; role S the six stresses.  Each role stages half the
+// fields (five or three halo boxes, three y-window leads, its old level and
+// medium: 5504 floats either way) and keeps three y-windows instead of six,
+// so a CTA holds fewer registers and STAGES-deep TMA pipelines fit at higher
+// occupancy.  The bytes moved and the arithmetic of every component are those
+// of kStepTma (modes 0..2, the dual state of mode 2 included); the fused
+// decimation and secondary sources stay with kStepTma.
+// ---------------------------------------------------------------------------
+struct SplitMaps {
+  CUtensorMap v[14];  // halo SXX, SXY, SXZ, SYZ, SZZ; lead SXY, SYY, SYZ; old VX, VY, VZ; med RHOX, RHOY, RHOZ
+  CUtensorMap s[17];  // halo VX, VY, VZ; lead VX, VY, VZ; old SXX..SYZ; med L2M, LAM, MUXZ, MUXY, MUYZ
+};
+constexpr int SPL_HALO_F = SZ * (8 + 2 * HALO);
+constexpr int SPL_INT_F = TZ * 8;
+constexpr int SPL_STAGE_F = 5 * SPL_HALO_F + 9 * SPL_INT_F;  // = 3 * SPL_HALO_F + 14 * SPL_INT_F
+static_assert(5 * SPL_HALO_F + 9 * SPL_INT_F == 3 * SPL_HALO_F + 14 * SPL_INT_F, "role stages differ");
+
+template <bool ROLE_S>
+struct SplitRole {
+  static constexpr int NH = ROLE_S ? 3 : 5;      // halo boxes
+  static constexpr int NO = ROLE_S ? 6 : 3;      // old-level (and new-level) components
+  static constexpr int NM = ROLE_S ? 5 : 3;      // medium planes
+  static constexpr int C0 = ROLE_S ? SXX : VX;   // first component of the role
+  static constexpr int M0 = ROLE_S ? L2M : RHOX; // first medium plane of the role
+  static constexpr int LEAD_OFF = NH * SPL_HALO_F;
+  static constexpr int OLD_OFF = LEAD_OFF + 3 * SPL_INT_F;
+  static constexpr int MED_OFF = OLD_OFF + NO * SPL_INT_F;
+  __device__ static constexpr int lead(int q) {  // y-window fields (component, base)
+    return ROLE_S ? (q == 0 ? VX : q == 1 ? VY : VZ) : (q == 0 ? SXY : q == 1 ? SYY : SYZ);
+  }
+  __device__ static constexpr int base(int q) {
+    return ROLE_S ? (q == 1 ? -3 : -4) : (q == 1 ? -4 : -3);
+  }
+};
+
+template <bool ROLE_S>
+__device__ __forceinline__ void splitIssuePlane(const CUtensorMap* mp, float* st, unsigned long long* bar, int y,
+                                                int z0, int x0) {
+  using R = SplitRole<ROLE_S>;
+  mbarExpectTx(bar, (unsigned)SPL_STAGE_F * 4u);
+#pragma unroll
+  for (int t = 0; t < R::NH; t++) tmaLoad3d(st + t * SPL_HALO_F, &mp[t], z0 - HALO, x0 - HALO, y, bar);
+#pragma unroll
+  for (int q = 0; q < 3; q++)
+    tmaLoad3d(st + R::LEAD_OFF + q * SPL_INT_F, &mp[R::NH + q], z0, x0, y + R::base(q) + 7, bar);
+#pragma unroll
+  for (int k = 0; k < R::NO; k++) tmaLoad3d(st + R::OLD_OFF + k * SPL_INT_F, &mp[R::NH + 3 + k], z0, x0, y, bar);
+#pragma unroll
+  for (int k = 0; k < R::NM; k++)
+    tmaLoad3d(st + R::MED_OFF + k * SPL_INT_F, &mp[R::NH + 3 + R::NO + k], z0, x0, y, bar);
+}
+
+template <int MODE, bool ROLE_S, int STAGES>
+__device__ __forceinline__ void splitRole(const CUtensorMap* mp, const StepPtrs& p, const GridConst& g, int yChunk,
+                                          int chunk, float* smem, unsigned long long* bars) {
+  using R = SplitRole<ROLE_S>;
+  constexpr int TXS = 8;
+  const int tz = threadIdx.x, tx = threadIdx.y;
+  const int tid = tx * TZ + tz;
+  const int z0 = FAT + blockIdx.x * TZ, x0 = FAT + blockIdx.y * TXS;
+  const int iz = z0 + tz, ix = x0 + tx;
+  const bool active = (iz < g.nz - FAT) && (ix < g.nx - FAT);
+  const int yBeg = FAT + chunk * yChunk;
+  const int yEnd = min(yBeg + yChunk, g.ny - FAT);
+  const long long ys = g.yStride;
+  const long long col = (long long)ix * g.nz + iz;
+  if (tid == 0) {
+    for (int s = 0; s < STAGES; s++) mbarInit(&bars[s], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  __syncthreads();
+  if (tid == 0) {
+    for (int s = 0; s < STAGES - 1; s++)
+      if (yBeg + s < yEnd) splitIssuePlane<ROLE_S>(mp, smem + s * SPL_STAGE_F, &bars[s], yBeg + s, z0, x0);
+  }
+  float w[3][8];
+  if (active) {
+#pragma unroll
+    for (int q = 0; q < 3; q++)
+#pragma unroll
+      for (int k = 0; k < 7; k++) w[q][k] = __ldg(p.c[R::lead(q)] + (long long)(yBeg + R::base(q) + k) * ys + col);
+  }
+  const int dzx = min(min(topDistance(g, iz), ix - FAT), min(g.nz - iz - 1 - FAT, g.nx - ix - 1 - FAT));
+  const float Gzx = (active && dzx < g.minPad) ? __ldg(g.taper + dzx) : 1.0f;
+  const int lc = (tx + HALO) * SZ + (tz + HALO);
+  const int li = tx * TZ + tz;
+  float* const* dst = p.nw[0] ? p.nw : p.o;
+  int slot = 0;
+  unsigned parity = 0;
+  for (int y = yBeg; y < yEnd; y++) {
+    const int dyy = min(y - FAT, g.ny - y - 1 - FAT);
+    const float Gy = dyy < g.minPad ? __ldg(g.taper + dyy) : 1.0f;
+    const bool ok = mbarWaitBounded(&bars[slot], (parity >> slot) & 1u);
+    if (__syncthreads_or(!ok)) {
+      if (tid == 0) {
+        atomicExch(&g_e3dPipeError, 1u);
+        for (int s = 0; s < STAGES; s++) mbarWaitBounded(&bars[s], (parity >> s) & 1u);
+      }
+      __syncthreads();
+      return;
+    }
+    parity ^= 1u << slot;
+    if (tid == 0) {
+      const int yn = y + STAGES - 1;
+      int ns = slot + STAGES - 1;
+      if (ns >= STAGES) ns -= STAGES;
+      if (yn < yEnd) splitIssuePlane<ROLE_S>(mp, smem + ns * SPL_STAGE_F, &bars[ns], yn, z0, x0);
+    }
+    const float* st = smem + slot * SPL_STAGE_F;
+    if (active) {
+      const long long ic = (long long)y * ys + col;
+#pragma unroll
+      for (int q = 0; q < 3; q++) w[q][7] = st[R::LEAD_OFF + q * SPL_INT_F + li];
+      const float* cz = g.cz;
+      const float* cx = g.cx;
+      const float* cy = g.cy;
+      const float* mv = st + R::MED_OFF + li;
+      const float* ov = st + R::OLD_OFF + li;
+      const float G = dyy < dzx ? Gy : Gzx;
+      float up[6], nv[6];
+      if (!ROLE_S) {
+        const float* tSXX = st;
+        const float* tSXY = st + SPL_HALO_F;
+        const float* tSXZ = st + 2 * SPL_HALO_F;
+        const float* tSYZ = st + 3 * SPL_HALO_F;
+        const float* tSZZ = st + 4 * SPL_HALO_F;
+        const float fvx = dMinus(tSXX, lc, SZ, cx) + dWin(w[0], cy) + dPlus(tSXZ, lc, 1, cz);
+        const float fvy = dPlus(tSXY, lc, SZ, cx) + dWin(w[1], cy) + dPlus(tSYZ, lc, 1, cz);
+        const float fvz = dPlus(tSXZ, lc, SZ, cx) + dWin(w[2], cy) + dMinus(tSZZ, lc, 1, cz);
+        const float rhox = mv[0], rhoy = mv[SPL_INT_F], rhoz = mv[2 * SPL_INT_F];
+        if (MODE == STEP_ADJ_EXACT) {
+          up[0] = -fvx; up[1] = -fvy; up[2] = -fvz;
+        } else {
+          const float sgn = (MODE == STEP_FWD) ? 1.0f : -1.0f;
+          up[0] = sgn * (rhox * fvx);
+          up[1] = sgn * (rhoy * fvy);
+          up[2] = sgn * (rhoz * fvz);
+        }
+#pragma unroll
+        for (int k = 0; k < 3; k++) nv[k] = G * (G * ov[k * SPL_INT_F] + up[k]);
+#pragma unroll
+        for (int k = 0; k < 3; k++) dst[VX + k][ic] = nv[k];
+        if (MODE == STEP_ADJ_EXACT && p.oP[0]) {
+          p.oP[VX][ic] = nv[0] * rhox;
+          p.oP[VY][ic] = nv[1] * rhoy;
+          p.oP[VZ][ic] = nv[2] * rhoz;
+        }
+      } else {
+        const float* tVX = st;
+        const float* tVY = st + SPL_HALO_F;
+        const float* tVZ = st + 2 * SPL_HALO_F;
+        const float dvx_dx = dPlus(tVX, lc, SZ, cx);
+        const float dvy_dy = dWin(w[1], cy);
+        const float dvz_dz = dPlus(tVZ, lc, 1, cz);
+        const float fxy = dWin(w[0], cy) + dMinus(tVY, lc, SZ, cx);
+        const float fxz = dMinus(tVX, lc, 1, cz) + dMinus(tVZ, lc, SZ, cx);
+        const float fyz = dWin(w[2], cy) + dMinus(tVY, lc, 1, cz);
+        const float l2m = mv[0], lam = mv[SPL_INT_F];
+        const float muxz = mv[2 * SPL_INT_F], muxy = mv[3 * SPL_INT_F], muyz = mv[4 * SPL_INT_F];
+        // local order SXX, SYY, SZZ, SXZ, SXY, SYZ (the component order from SXX on)
+        if (MODE == STEP_ADJ_EXACT) {
+          up[0] = -dvx_dx; up[1] = -dvy_dy; up[2] = -dvz_dz;
+          up[3] = -fxz; up[4] = -fxy; up[5] = -fyz;
+        } else {
+          const float sgn = (MODE == STEP_FWD) ? 1.0f : -1.0f;
+          up[0] = sgn * (l2m * dvx_dx + lam * (dvy_dy + dvz_dz));
+          up[1] = sgn * (l2m * dvy_dy + lam * (dvx_dx + dvz_dz));
+          up[2] = sgn * (l2m * dvz_dz + lam * (dvx_dx + dvy_dy));
+          up[3] = sgn * (muxz * fxz);
+          up[4] = sgn * (muxy * fxy);
+          up[5] = sgn * (muyz * fyz);
+        }
+#pragma unroll
+        for (int k = 0; k < 6; k++) nv[k] = G * (G * ov[k * SPL_INT_F] + up[k]);
+#pragma unroll
+        for (int k = 0; k < 6; k++) dst[SXX + k][ic] = nv[k];
+        if (MODE == STEP_ADJ_EXACT && p.oP[0]) {
+          p.oP[SXX][ic] = nv[0] * l2m + (nv[1] + nv[2]) * lam;
+          p.oP[SYY][ic] = nv[1] * l2m + (nv[0] + nv[2]) * lam;
+          p.oP[SZZ][ic] = nv[2] * l2m + (nv[0] + nv[1]) * lam;
+          p.oP[SXZ][ic] = nv[3] * muxz;
+          p.oP[SXY][ic] = nv[4] * muxy;
+          p.oP[SYZ][ic] = nv[5] * muyz;
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < 3; q++)
+#pragma unroll
+        for (int k = 0; k < 7; k++) w[q][k] = w[q][k + 1];
+    }
+    slot = (slot + 1 == STAGES) ? 0 : slot + 1;
+  }
+}
+
+template <int MODE, int STAGES, int MINB>
+__global__ void __launch_bounds__(TZ * 8, MINB) kStepSplit(const __grid_constant__ SplitMaps mp, StepPtrs p,
+                                                            GridConst g, int yChunk, int chunksV) {
+  extern __shared__ __align__(1024) float smem[];
+  __shared__ __align__(8) unsigned long long bars[STAGES];
+  if ((int)blockIdx.z < chunksV) splitRole<MODE, false, STAGES>(mp.v, p, g, yChunk, blockIdx.z, smem, bars);
+  else splitRole<MODE, true, STAGES>(mp.s, p, g, yChunk, blockIdx.z - chunksV, smem, bars);
 }
 
 // Recompute the premultiplied level at injected points (dual-state mode 2):
@@ -673,6 +881,49 @@ __global__ void kRefreshPremultiplied(StepPtrs p, SparseSet s) {
       p.oP[SZZ][i] = szz * l2m + (sxx + syy) * lam;
     }
   }
+}
+
+// Injection into the raw new level and the refresh of its premultiplied copy
+// at the injected points in one launch (dual-state mode 2): kInject followed by
+// kRefreshPremultiplied, without decimation accumulators.  The normal stresses
+// share the center-grid points (equal counts, the same order), so the thread of
+// the r-th sxx entry injects sxx, syy and szz at that point before
+// premultiplying the three.
+__global__ void kInjectRefresh(StepPtrs p, GridConst g, SparseSet s, const float* sigL, const float* sigR, float wl,
+                               float wr) {
+  const int ntot = s.off[NCOMP];
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= ntot) return;
+  int k = 0;
+#pragma unroll
+  for (int c = 1; c < NCOMP; c++) k += (j >= s.off[c]);
+  if (k == SYY || k == SZZ) return;
+  const long long i = s.pos[j];
+  const int iz = (int)(i % g.nz);
+  const int ix = (int)((i / g.nz) % g.nx);
+  const int iy = (int)(i / g.yStride);
+  const float G = taperAt(g, iz, ix, iy);
+  if (k == SXX) {
+    const int r = j - s.off[SXX];
+    float v[3];
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      const int jj = s.off[SXX + c] + r;
+      const float add = G * (sigL[jj] * wl + sigR[jj] * wr);
+      v[c] = p.o[SXX + c][i] + add;
+      p.o[SXX + c][i] = v[c];
+    }
+    const float l2m = __ldg(p.m[L2M] + i), lam = __ldg(p.m[LAM] + i);
+    p.oP[SXX][i] = v[0] * l2m + (v[1] + v[2]) * lam;
+    p.oP[SYY][i] = v[1] * l2m + (v[0] + v[2]) * lam;
+    p.oP[SZZ][i] = v[2] * l2m + (v[0] + v[1]) * lam;
+    return;
+  }
+  const float add = G * (sigL[j] * wl + sigR[j] * wr);
+  const float v = p.o[k][i] + add;
+  p.o[k][i] = v;
+  const int med = k == VX ? RHOX : k == VY ? RHOY : k == VZ ? RHOZ : k == SXZ ? MUXZ : k == SXY ? MUXY : MUYZ;
+  p.oP[k][i] = v * __ldg(p.m[med] + i);
 }
 
 // ---------------------------------------------------------------------------
@@ -809,7 +1060,7 @@ __device__ __forceinline__ bool tma2Plane(Tma2State<MODE, TX, STAGES, OM_SMEM>& 
       float v = G * ovr[k] + up[k];
       if (hasSS) v += __ldg(p.ssL[k] + ic) * p.ssWl + __ldg(p.ssR[k] + ic) * p.ssWr;
       v *= G;
-      p.o[k][ic] = v;
+      (p.nw[0] ? p.nw[k] : p.o[k])[ic] = v;
       if (hasAcc && k < p.nAcc) {
         p.accL[k][ic] += v * p.accWl;
         if (p.accR[0] != nullptr) p.accR[k][ic] += v * p.accWr;
@@ -1131,6 +1382,343 @@ __global__ void kImaging(ImagingPtrs q, GridConst g) {
     q.pert[5][i] += q.ss[SXZ][i] * exz;
     q.pert[6][i] += q.ss[SXY][i] * exy;
     q.pert[7][i] += q.ss[SYZ][i] * eyz;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Decimation from a ring of fine levels.  The gradient's passes keep the
+// fine time levels of one coarse block in a ring of buffers (the stepper
+// writes each new level beside the old one instead of over it) and decimate
+// once per block, so that the steppers carry no accumulators: the reference's
+// interpWavefieldVxVyVz_3D / extractInterpAdjointWavefield_3D
+// (kernelsElaGpu_3D.cu:1646-1672, 1694-1714) weight every fine level of block
+// b by the time-interpolation filter into the coarse samples b (left weight)
+// and b+1 (right weight).
+// ---------------------------------------------------------------------------
+constexpr int RING_SUB_MAX = 8;  // longest block (internal sub) decimated from a ring
+
+// Source velocity (3 fields): V[b] (left) and V[b+1] (right) from the levels of block b.
+//   vl: 3 fields at vl + k*n; vlMode 0 skip, 1 accumulate onto V[b] (which holds
+//   the right part of block b-1), 2 write; vr: written (the first part of V[b+1]).
+struct DecimatePtrs {
+  const float* lev[RING_SUB_MAX][3];
+  float wl[RING_SUB_MAX], wr[RING_SUB_MAX];
+  int nlev;
+  float* vl;
+  float* vr;
+  int vlMode;
+  long long n;
+};
+
+template <bool VEC>
+__global__ void __launch_bounds__(256) kDecimateVelocity(DecimatePtrs d) {
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  const long long start = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int k = blockIdx.y;  // velocity component
+  if (VEC) {
+    const long long nv = d.n / 4;
+    for (long long j = start; j < nv; j += stride) {
+      float4 l = make_float4(0.f, 0.f, 0.f, 0.f), r = l;
+      if (d.vl && d.vlMode == 1) l = reinterpret_cast<const float4*>(d.vl + k * d.n)[j];
+      for (int t = 0; t < d.nlev; t++) {
+        const float4 v = __ldg(reinterpret_cast<const float4*>(d.lev[t][k]) + j);
+        l.x = fmaf(v.x, d.wl[t], l.x); l.y = fmaf(v.y, d.wl[t], l.y);
+        l.z = fmaf(v.z, d.wl[t], l.z); l.w = fmaf(v.w, d.wl[t], l.w);
+        r.x = fmaf(v.x, d.wr[t], r.x); r.y = fmaf(v.y, d.wr[t], r.y);
+        r.z = fmaf(v.z, d.wr[t], r.z); r.w = fmaf(v.w, d.wr[t], r.w);
+      }
+      if (d.vl && d.vlMode) reinterpret_cast<float4*>(d.vl + k * d.n)[j] = l;
+      if (d.vr) reinterpret_cast<float4*>(d.vr + k * d.n)[j] = r;
+    }
+  } else {
+    for (long long j = start; j < d.n; j += stride) {
+      float l = (d.vl && d.vlMode == 1) ? d.vl[k * d.n + j] : 0.f, r = 0.f;
+      for (int t = 0; t < d.nlev; t++) {
+        const float v = __ldg(d.lev[t][k] + j);
+        l = fmaf(v, d.wl[t], l);
+        r = fmaf(v, d.wr[t], r);
+      }
+      if (d.vl && d.vlMode) d.vl[k * d.n + j] = l;
+      if (d.vr) d.vr[k * d.n + j] = r;
+    }
+  }
+}
+
+// Velocity terms of the Born imaging condition at one coarse time (the
+// derivatives of imagingElaAdjGpu_3D, kernelsElaGpu_3D.cu:1440-1641, as kImaging).
+struct VelTerms {
+  float dvx_dx, dvy_dy, dvz_dz, exz, exy, eyz, tder[3];
+};
+__device__ __forceinline__ VelTerms velTerms(const float* const* vPrev, const float* const* vCur,
+                                             const float* const* vNext, long long i, const GridConst& g,
+                                             float dtsInv, int q3compat) {
+  const long long xs = g.nz, ys = g.yStride;
+  const float* vx = vCur[0];
+  const float* vy = vCur[1];
+  const float* vz = vCur[2];
+  VelTerms t;
+  t.dvx_dx = gPlus(vx, i, xs, g.cx);
+  t.dvy_dy = gPlus(vy, i, ys, g.cy);
+  t.dvz_dz = gPlus(vz, i, 1, g.cz);
+  t.exz = gMinus(vx, i, 1, g.cz) + gMinus(vz, i, xs, g.cx);
+  t.exy = gMinus(vx, i, ys, g.cy) + gMinus(vy, i, xs, g.cx);
+  t.eyz = q3compat ? t.exz : (gMinus(vz, i, ys, g.cy) + gMinus(vy, i, 1, g.cz));
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    const float a = vPrev[k] ? __ldg(vPrev[k] + i) : 0.0f;
+    const float b = vNext[k] ? __ldg(vNext[k] + i) : 0.0f;
+    t.tder[k] = (a - b) * dtsInv;
+  }
+  return t;
+}
+
+// Imaging contributions of the decimated adjoint field a (9 components) at one coarse time.
+__device__ __forceinline__ void imagingTerms(const VelTerms& t, const float* a, float* out) {
+  const float div = t.dvx_dx + t.dvy_dy + t.dvz_dz;
+  out[0] = a[VX] * t.tder[0];
+  out[1] = a[VY] * t.tder[1];
+  out[2] = a[VZ] * t.tder[2];
+  out[3] = (a[SXX] + a[SYY] + a[SZZ]) * div;
+  out[4] = 2.0f * (t.dvx_dx * a[SXX] + t.dvy_dy * a[SYY] + t.dvz_dz * a[SZZ]);
+  out[5] = a[SXZ] * t.exz;
+  out[6] = a[SXY] * t.exy;
+  out[7] = a[SYZ] * t.eyz;
+}
+
+// Adjoint imaging of one coarse block `its` from the ring of its fine adjoint
+// levels (9 fields each, after injection): R = sum_t wr[t] lev[t] belongs to
+// the coarse sample its+1, L = sum_t wl[t] lev[t] to its.
+//   pert += I(V at its+1, R [+ carry when carryIn])      v[1..3] = V(its..its+2)
+//   leftImage: pert += I(V at its, L)                     v[0..2] = V(its-1..its+1)
+//   else:      carry = L (imaged with the block before, whose right part completes it)
+struct ImagingBlockPtrs {
+  const float* lev[RING_SUB_MAX][NCOMP];
+  float wl[RING_SUB_MAX], wr[RING_SUB_MAX];
+  int nlev;
+  const float* v[4][3];  // V(its-1), V(its), V(its+1), V(its+2); null outside the record
+  float* carry[NCOMP];
+  int carryIn, leftImage;
+  float* pert[NMED];
+  float dtsInv;
+  int q3compat;
+};
+
+__global__ void __launch_bounds__(256) kImagingBlock(ImagingBlockPtrs q, GridConst g) {
+  const int iz = FAT + blockIdx.x * blockDim.x + threadIdx.x;
+  const int ix = FAT + blockIdx.y * blockDim.y + threadIdx.y;
+  const int iy = FAT + blockIdx.z;
+  if (iz >= g.nz - FAT || ix >= g.nx - FAT) return;
+  const long long i = (long long)iy * g.yStride + (long long)ix * g.nz + iz;
+  float L[NCOMP], R[NCOMP];
+#pragma unroll
+  for (int k = 0; k < NCOMP; k++) {
+    L[k] = 0.f;
+    R[k] = q.carryIn ? q.carry[k][i] : 0.f;
+  }
+  for (int t = 0; t < q.nlev; t++) {
+    const float wl = q.wl[t], wr = q.wr[t];
+#pragma unroll
+    for (int k = 0; k < NCOMP; k++) {
+      const float a = __ldg(q.lev[t][k] + i);
+      L[k] = fmaf(a, wl, L[k]);
+      R[k] = fmaf(a, wr, R[k]);
+    }
+  }
+  float acc[NMED];
+  {
+    const VelTerms t1 = velTerms(q.v[1], q.v[2], q.v[3], i, g, q.dtsInv, q.q3compat);
+    imagingTerms(t1, R, acc);
+  }
+  if (q.leftImage) {
+    const VelTerms t0 = velTerms(q.v[0], q.v[1], q.v[2], i, g, q.dtsInv, q.q3compat);
+    float accL[NMED];
+    imagingTerms(t0, L, accL);
+#pragma unroll
+    for (int k = 0; k < NMED; k++) acc[k] += accL[k];
+  } else {
+#pragma unroll
+    for (int k = 0; k < NCOMP; k++) q.carry[k][i] = L[k];
+  }
+#pragma unroll
+  for (int k = 0; k < NMED; k++) q.pert[k][i] += acc[k];
+}
+
+// ---------------------------------------------------------------------------
+// kImagingBlock as a 2.5D y-march: a CTA owns a 32(z) x 8(x) tile column and
+// walks a chunk of y planes.  Per plane one elected thread issues TMA box
+// copies of the three source velocities of the two coarse times the block
+// images (halo boxes for the z/x derivatives, lead boxes for 8-deep register
+// y-windows) into a 2-stage mbarrier pipeline; the adjoint levels, the time-
+// derivative neighbours and the image planes are read with coalesced loads
+// issued before the wait.  Same arithmetic, term by term, as kImagingBlock.
+// Time index 1 = V(its+1) (right part), 0 = V(its) (left part, leftImage).
+// Every wait is bounded as in kStepTma.
+// ---------------------------------------------------------------------------
+struct ImagingMaps {
+  CUtensorMap halo[2][3];  // [time][vx, vy, vz], halo box
+  CUtensorMap lead[2][3];  // [time][vx, vy, vz], interior box
+};
+constexpr int IMG_TX = 8;
+constexpr int IMG_HALO_F = SZ * (IMG_TX + 2 * HALO);  // floats per halo box
+constexpr int IMG_INT_F = TZ * IMG_TX;                // floats per interior box
+constexpr int IMG_STAGE_F = 6 * IMG_HALO_F + 6 * IMG_INT_F;
+// y-window bases: vy enters a forward y derivative (dvy/dy), vx and vz backward ones (exy, eyz)
+__device__ constexpr int imgBase(int f) { return f == 1 ? -3 : -4; }
+
+__device__ __forceinline__ void imgIssuePlane(const ImagingMaps& mp, float* st, unsigned long long* bar, int y,
+                                              int z0, int x0, int ntimes) {
+  const unsigned bytes = (unsigned)(ntimes * 3 * (IMG_HALO_F + IMG_INT_F)) * 4u;
+  mbarExpectTx(bar, bytes);
+  for (int t = 2 - ntimes; t < 2; t++)
+#pragma unroll
+    for (int f = 0; f < 3; f++) {
+      tmaLoad3d(st + (t * 3 + f) * IMG_HALO_F, &mp.halo[t][f], z0 - HALO, x0 - HALO, y, bar);
+      tmaLoad3d(st + 6 * IMG_HALO_F + (t * 3 + f) * IMG_INT_F, &mp.lead[t][f], z0, x0, y + imgBase(f) + 7, bar);
+    }
+}
+
+// Velocity terms at one cell from the shared tiles (halo boxes of vx, vy, vz) and the y-windows
+__device__ __forceinline__ VelTerms tileVelTerms(const float* tx_, const float* ty_, const float* tz_,
+                                                 const float* wx, const float* wy, const float* wz, int lc,
+                                                 const GridConst& g, float prev[3], float next[3], float dtsInv,
+                                                 int q3compat) {
+  VelTerms t;
+  t.dvx_dx = dPlus(tx_, lc, SZ, g.cx);
+  t.dvy_dy = dWin(wy, g.cy);
+  t.dvz_dz = dPlus(tz_, lc, 1, g.cz);
+  t.exz = dMinus(tx_, lc, 1, g.cz) + dMinus(tz_, lc, SZ, g.cx);
+  t.exy = dWin(wx, g.cy) + dMinus(ty_, lc, SZ, g.cx);
+  t.eyz = q3compat ? t.exz : (dWin(wz, g.cy) + dMinus(ty_, lc, 1, g.cz));
+#pragma unroll
+  for (int k = 0; k < 3; k++) t.tder[k] = (prev[k] - next[k]) * dtsInv;
+  return t;
+}
+
+__global__ void __launch_bounds__(TZ * IMG_TX) kImagingTma(const __grid_constant__ ImagingMaps mp,
+                                                           ImagingBlockPtrs q, GridConst g, int yChunk) {
+  extern __shared__ __align__(1024) float smem[];
+  __shared__ __align__(8) unsigned long long bars[2];
+  const int tz = threadIdx.x, tx = threadIdx.y;
+  const int tid = tx * TZ + tz;
+  const int z0 = FAT + blockIdx.x * TZ, x0 = FAT + blockIdx.y * IMG_TX;
+  const int iz = z0 + tz, ix = x0 + tx;
+  const bool active = (iz < g.nz - FAT) && (ix < g.nx - FAT);
+  const int yBeg = FAT + blockIdx.z * yChunk;
+  const int yEnd = min(yBeg + yChunk, g.ny - FAT);
+  const long long ys = g.yStride;
+  const long long col = (long long)ix * g.nz + iz;
+  const int ntimes = q.leftImage ? 2 : 1;
+  const int t0 = 2 - ntimes;  // first time index present
+
+  if (tid == 0) {
+    for (int s = 0; s < 2; s++) mbarInit(&bars[s], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  __syncthreads();
+  if (tid == 0 && yBeg < yEnd) imgIssuePlane(mp, smem, &bars[0], yBeg, z0, x0, ntimes);
+  // y-windows: w[t][f][k] holds plane y + imgBase(f) + k of field f at time t
+  float w[2][3][8];
+  if (active) {
+#pragma unroll
+    for (int t = 0; t < 2; t++)
+#pragma unroll
+      for (int f = 0; f < 3; f++)
+#pragma unroll
+        for (int k = 0; k < 7; k++)
+          w[t][f][k] = (t >= t0) ? __ldg(q.v[t + 1][f] + (long long)(yBeg + imgBase(f) + k) * ys + col) : 0.f;
+  }
+  const int lc = (tx + HALO) * SZ + (tz + HALO);
+  const int li = tx * TZ + tz;
+  int slot = 0;
+  unsigned parity = 0;
+  for (int y = yBeg; y < yEnd; y++) {
+    const long long ic = (long long)y * ys + col;
+    // coalesced per-cell loads, issued ahead of the wait
+    float L[NCOMP], R[NCOMP], pv[NMED], nxt[3], prv[3], cur0[3];
+    if (active) {
+#pragma unroll
+      for (int k = 0; k < NCOMP; k++) {
+        L[k] = 0.f;
+        R[k] = q.carryIn ? q.carry[k][ic] : 0.f;
+      }
+      for (int j = 0; j < q.nlev; j++) {
+        const float wl = q.wl[j], wr = q.wr[j];
+#pragma unroll
+        for (int k = 0; k < NCOMP; k++) {
+          const float a = __ldg(q.lev[j][k] + ic);
+          L[k] = fmaf(a, wl, L[k]);
+          R[k] = fmaf(a, wr, R[k]);
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < 3; k++) {
+        nxt[k] = q.v[3][k] ? __ldg(q.v[3][k] + ic) : 0.f;                        // V(its+2)
+        prv[k] = (q.leftImage && q.v[0][k]) ? __ldg(q.v[0][k] + ic) : 0.f;       // V(its-1)
+        cur0[k] = q.leftImage ? 0.f : __ldg(q.v[1][k] + ic);                     // V(its) without its tile
+      }
+#pragma unroll
+      for (int k = 0; k < NMED; k++) pv[k] = q.pert[k][ic];
+    }
+    const bool ok = mbarWaitBounded(&bars[slot], (parity >> slot) & 1u);
+    if (__syncthreads_or(!ok)) {
+      if (tid == 0) {
+        atomicExch(&g_e3dPipeError, 1u);
+        for (int s = 0; s < 2; s++) mbarWaitBounded(&bars[s], (parity >> s) & 1u);
+      }
+      __syncthreads();
+      return;
+    }
+    parity ^= 1u << slot;
+    if (tid == 0 && y + 1 < yEnd) imgIssuePlane(mp, smem + (slot ^ 1) * IMG_STAGE_F, &bars[slot ^ 1], y + 1, z0, x0, ntimes);
+    const float* st = smem + slot * IMG_STAGE_F;
+    if (active) {
+#pragma unroll
+      for (int t = 0; t < 2; t++)
+#pragma unroll
+        for (int f = 0; f < 3; f++)
+          if (t >= t0) w[t][f][7] = st[6 * IMG_HALO_F + (t * 3 + f) * IMG_INT_F + li];
+      const float* h1x = st + 3 * IMG_HALO_F;
+      const float* h1y = st + 4 * IMG_HALO_F;
+      const float* h1z = st + 5 * IMG_HALO_F;
+      // right part: V(its+1); prev = V(its) (its tile when present), next = V(its+2)
+      float prevR[3];
+      if (q.leftImage) {
+        prevR[0] = st[0 * IMG_HALO_F + lc];
+        prevR[1] = st[1 * IMG_HALO_F + lc];
+        prevR[2] = st[2 * IMG_HALO_F + lc];
+      } else {
+        prevR[0] = cur0[0];
+        prevR[1] = cur0[1];
+        prevR[2] = cur0[2];
+      }
+      float acc[NMED];
+      {
+        const VelTerms t1 = tileVelTerms(h1x, h1y, h1z, w[1][0], w[1][1], w[1][2], lc, g, prevR, nxt, q.dtsInv,
+                                         q.q3compat);
+        imagingTerms(t1, R, acc);
+      }
+      if (q.leftImage) {
+        float nextL[3] = {h1x[lc], h1y[lc], h1z[lc]};  // V(its+1)
+        const VelTerms tl = tileVelTerms(st, st + IMG_HALO_F, st + 2 * IMG_HALO_F, w[0][0], w[0][1], w[0][2], lc,
+                                         g, prv, nextL, q.dtsInv, q.q3compat);
+        float accL[NMED];
+        imagingTerms(tl, L, accL);
+#pragma unroll
+        for (int k = 0; k < NMED; k++) acc[k] += accL[k];
+      } else {
+#pragma unroll
+        for (int k = 0; k < NCOMP; k++) q.carry[k][ic] = L[k];
+      }
+#pragma unroll
+      for (int k = 0; k < NMED; k++) q.pert[k][ic] = pv[k] + acc[k];
+#pragma unroll
+      for (int t = 0; t < 2; t++)
+#pragma unroll
+        for (int f = 0; f < 3; f++)
+#pragma unroll
+          for (int k = 0; k < 7; k++) w[t][f][k] = w[t][f][k + 1];
+    }
+    slot ^= 1;
   }
 }
 

@@ -56,14 +56,14 @@ inline double slotBytes(long long n, int ny, int vt) {
 
 // Checkpoints plus velocity slots of a plan with segment length L.  FP32 slots
 // hold V[b .. b+L+2] of a segment starting at block b (the last one partial,
-// from the recompute's final block); FP16 slots hold V[b .. b+L+1] plus three
-// FP32 working slots (two accumulators while recomputing, a three-deep ring
-// for the imaging condition).
+// from the recompute's final block); FP16 slots hold V[b .. b+L+1] plus four
+// FP32 working slots (two accumulators while recomputing, a four-deep window
+// V(t-1..t+2) for the imaging condition of a block).
 inline double planBytes(long long n, int ny, int nts, int ck, int vt, int L) {
   const int nseg = segments(nts - 1, L);
   double b = (double)(nseg - 1) * stateBytes(n, ny, ck);
   if (vt == kSlotF32) b += (L + 3) * slotBytes(n, ny, kSlotF32);
-  else b += (L + 2) * slotBytes(n, ny, kSlotF16) + 3 * slotBytes(n, ny, kSlotF32);
+  else b += (L + 2) * slotBytes(n, ny, kSlotF16) + 4 * slotBytes(n, ny, kSlotF32);
   return b;
 }
 

@@ -92,9 +92,10 @@ class Propagator:
             planes = [N.as_f32(planes8[k]) for k in range(8)]
             N.call("e3d_set_medium", self._h, N.ptr_array(planes), 0)
 
-    LOADERS = {"plain": 0, "cpasync": 1, "tma": 2, "tma-ring": 3, "tma-ring-ldg": 4, "tma-ring-ldg2": 5}
+    LOADERS = {"plain": 0, "cpasync": 1, "tma": 2, "tma-ring": 3, "tma-ring-ldg": 4, "tma-ring-ldg2": 5, "split": 6,
+               "split-fwd": 7}
 
-    def set_stepper_variant(self, tx=8, stages=2, loader="tma"):
+    def set_stepper_variant(self, tx=8, stages=3, loader="split-fwd"):
         """Stepper variant: x tile width (8/16), shared-memory stages (2/3) and plane loader."""
         N.call("e3d_set_stepper_variant", self._h, int(tx), int(stages), self.LOADERS[loader])
 
@@ -173,11 +174,12 @@ class Propagator:
         return pert
 
     def kernel_timing(self, every):
-        """Sample every n-th stepper launch with CUDA events (0 = off)."""
+        """Sample every n-th launch of each timed kind with CUDA events (0 = off)."""
         N.call("e3d_kernel_timing", self._h, int(every))
 
     def kernel_timing_read(self, mode):
-        """(mean ms, count) of the sampled stepper launches of one mode since the last read."""
+        """(mean ms, count) of the sampled launches of one kind since the last read: stepper modes 0..2,
+        the same with a fused decimation or secondary source 3..5, block imaging 6, velocity decimation 7."""
         avg = ctypes.c_double(0)
         cnt = ctypes.c_longlong(0)
         N.call("e3d_kernel_timing_read", self._h, int(mode), ctypes.byref(avg), ctypes.byref(cnt))
@@ -233,3 +235,12 @@ class Propagator:
     @property
     def velocity_storage(self):
         return ("fp32", "fp16")[int(N.lib().e3d_velocity_storage(self._h))]
+
+    def set_decimation_ring(self, on=True):
+        """Gradient passes: decimate fine levels from a ring once per coarse block (True, default) or
+        through accumulators at every fine step (False)."""
+        N.call("e3d_set_decimation_ring", self._h, 1 if on else 0)
+
+    def set_imaging_chunks(self, chunks=0):
+        """y chunks of the block imaging launch (0 = automatic)."""
+        N.call("e3d_set_imaging_chunks", self._h, int(chunks))

@@ -157,24 +157,31 @@ def batched_forward_survey(nts=2000, seed=1, nshots=16, coarse=8):
     return Survey(el, axes, par, src, rec, ricker(nts, dts, 15.0, 1.0 / 15.0), "batched-forward-400x400x300+40")
 
 
+def _with_anomalies(shape, vp, vs, rho):
+    """The true model of the FWI survey: two Gaussian anomalies (+-8% vp/vs, +-3% rho) on the background."""
+    iy, ix, iz = [np.arange(n, dtype=np.float64) for n in shape]
+    for sgn, cz in ((1.0, 0.35), (-1.0, 0.65)):
+        cy, cx, czz = shape[0] / 2, shape[1] / 2, shape[2] * cz
+        r2 = (((iy - cy) ** 2)[:, None, None] + ((ix - cx) ** 2)[None, :, None] + ((iz - czz) ** 2)[None, None, :]) \
+            / (0.08 * min(shape)) ** 2
+        g = np.exp(-r2)
+        vp = vp * (1 + sgn * 0.08 * g)
+        vs = vs * (1 + sgn * 0.08 * g)
+        rho = rho * (1 + sgn * 0.03 * g)
+    return vp, vs, rho
+
+
 def fwi_gradient_survey(nzi=300, nxi=300, nyi=300, pad=40, nts=2500, nshots=32, nrec=150, fdom=10.0, seed=3,
-               true_model=False):
+               true_model=False, with_true=False):
     """FWI gradient survey (300^3 interior + 40 sponge by default): smooth background (vp 2500, vs vp/1.732, rho 2000 with
-    +-10% smooth perturbations) plus, for the true model, two Gaussian anomalies (+-8% vp/vs, +-3% rho)."""
+    +-10% smooth perturbations) plus, for the true model, two Gaussian anomalies (+-8% vp/vs, +-3% rho).
+    with_true=True returns (survey on the background, true (rho, lambda, mu)) from one random field."""
     d = 10.0
     axes, pads = make_grid(nzi, nxi, nyi, pad, d)
     shape = (axes[2].n, axes[1].n, axes[0].n)
     vp, vs, rho = gaussian_perturbed_model(shape, 2500.0, 2500.0 / 1.732, 2000.0, 0.10, 5.0, seed)
-    if true_model:
-        iy, ix, iz = np.meshgrid(*[np.arange(n) for n in shape], indexing="ij")
-        for sgn, cz in ((1.0, 0.35), (-1.0, 0.65)):
-            cy, cx, czz = shape[0] / 2, shape[1] / 2, shape[2] * cz
-            r2 = ((iy - cy) ** 2 + (ix - cx) ** 2 + (iz - czz) ** 2) / (0.08 * min(shape)) ** 2
-            g = np.exp(-r2)
-            vp = vp * (1 + sgn * 0.08 * g)
-            vs = vs * (1 + sgn * 0.08 * g)
-            rho = rho * (1 + sgn * 0.03 * g)
-    el = elastic_from_velocity(vp, vs, rho)
+    true_el = elastic_from_velocity(*_with_anomalies(shape, vp, vs, rho)) if (true_model or with_true) else None
+    el = true_el if true_model else elastic_from_velocity(vp, vs, rho)
     dts = 0.002
     par = base_params(axes, pads, nts, dts, 2, 25.0)
     z0 = (axes[0].n - 2 * FAT - pads["zPadMinus"] - pads["zPadPlus"])
@@ -190,7 +197,8 @@ def fwi_gradient_survey(nzi=300, nxi=300, nyi=300, pad=40, nts=2500, nshots=32, 
     X, Y = np.meshgrid(gx, gy, indexing="ij")
     rec = (np.full(X.size, 10.0), X.reshape(-1), Y.reshape(-1))
     del z0
-    return Survey(el, axes, par, src, rec, ricker(nts, dts, fdom, 1.0 / fdom), f"fwi-{nzi}x{nxi}x{nyi}")
+    sv = Survey(el, axes, par, src, rec, ricker(nts, dts, fdom, 1.0 / fdom), f"fwi-{nzi}x{nxi}x{nyi}")
+    return (sv, true_el) if with_true else sv
 
 
 def small_survey(seed=0, nzi=32, nxi=32, nyi=24, pad=4, nts=20, sub_par=2, d=10.0, nrec=6, nshots=1):

@@ -221,8 +221,11 @@ int e3d_context_destroy(e3d_context* ctx);
 /* Eight medium planes (see allocateNonlinearElasticGpu_3D); on_device != 0 for device pointers. */
 int e3d_set_medium(e3d_context* ctx, const float* const* planes8, int on_device);
 /* Stepper variant (autotuner hook): tile width along x (8 or 16), shared-memory
- * pipeline depth (2 or 3 stages) and plane loader (0 plain loads, 1 cp.async,
- * 2 TMA bulk tensor copies; 1 and 2 need nz % 4 == 0). */
+ * pipeline depth (2 or 3 stages; 2 to 4 with loader 6) and plane loader (0 plain
+ * loads, 1 cp.async, 2 TMA bulk tensor copies, 3-5 TMA with a rotating y-window,
+ * 6 TMA with the velocity and stress updates of a step as two CTA roles of one
+ * launch, 8-wide tiles, 7 the same for the forward and time-reversed steps with
+ * the exact adjoint on loader 2's stepper; 1 to 7 need nz % 4 == 0). */
 int e3d_set_stepper_variant(e3d_context* ctx, int tx, int stages, int loader);
 /* Nonlinear propagation (e3d_nl_* and the seam's propElastic*Gpu_3D): on = 1
  * (default) captures one coarse block as a CUDA graph after running the first
@@ -266,6 +269,18 @@ int e3d_set_velocity_storage(e3d_context* ctx, int type);
 int e3d_velocity_storage(const e3d_context* ctx);
 /* State storage of the current checkpoints (0 fp32, 1 fp16, 2 bf16). */
 int e3d_checkpoint_type(const e3d_context* ctx);
+/* How the checkpointed passes decimate fine levels into coarse samples (the
+ * reference's interpWavefieldVxVyVz_3D and extractInterpAdjointWavefield_3D,
+ * kernelsElaGpu_3D.cu:1646-1672, 1694-1714, which run at every fine step):
+ * on = 1 (default): the fine levels of a coarse block stay in a ring of
+ * sub+1 levels and one launch per block decimates them (the adjoint's launch
+ * also applies the imaging condition); on = 0: two coarse accumulators are
+ * read and written by the stepper at every fine step.  Blocks longer than 8
+ * fine steps always use the accumulators.  Invalidates the checkpoints. */
+int e3d_set_decimation_ring(e3d_context* ctx, int on);
+/* y chunks of the block imaging launch of the decimation ring (0 = automatic:
+ * the rule of the stepper grids).  A tuning knob; no counterpart in the reference. */
+int e3d_set_imaging_chunks(e3d_context* ctx, int chunks);
 /* The checkpoint schedule of a record of `blocks` coarse blocks (nts - 1) cut
  * into segments of `segment_len` blocks, as the checkpointed passes run it:
  * returns the segment count nseg, or -E3D_ERR_ARG.  seg_start (room for
@@ -377,13 +392,15 @@ int e3d_nl_propagate_device_noalloc(const e3d_desc* desc, const float* const* pl
 /* Size in bytes of the fixed device array used by e3d_nl_propagate_device_noalloc. */
 size_t e3d_noalloc_work_bytes(void);
 
-/* Sampled stepper timing for roofline reporting: every n-th stepper launch is
- * bracketed by CUDA events on the launching stream (n = 0 switches it off). */
+/* Sampled kernel timing for roofline reporting: every n-th launch of each
+ * timed kind is bracketed by CUDA events on the launching stream (n = 0
+ * switches it off). */
 int e3d_kernel_timing(e3d_context* ctx, int every);
-/* Mean duration in ms and number of the sampled launches of one stepper mode
- * since the previous read (waits for them to finish).  mode 0..2: bare steps
- * of that mode; 3..5: the same modes with a fused decimation into coarse
- * accumulators or a fused Born secondary source. */
+/* Mean duration in ms and number of the sampled launches of one kind since
+ * the previous read (waits for them to finish).  mode 0..2: bare steps of that
+ * stepper mode; 3..5: the same modes with a fused decimation into coarse
+ * accumulators or a fused Born secondary source; 6: the block imaging of the
+ * decimation ring; 7: its source-velocity decimation. */
 int e3d_kernel_timing_read(e3d_context* ctx, int mode, double* avg_ms, long long* count);
 /* Number of kernel launches this context has issued. */
 long long e3d_launch_count(const e3d_context* ctx);

@@ -28,7 +28,7 @@ def test_autotuner_picks_a_variant_that_keeps_parity():
     got = pr.nl_forward(sig, spos, rpos)
     assert rel_l2(got, O.nl_forward_reg(p, med, sig, spos, rpos, np.float32)) < 1e-5
     best_g, per = AT.autotune_gradient(pr, steps=2, warmup=1)
-    assert best_g[2] == "tma" and len(per[best_g]) == 3
+    assert best_g[2] in AT.TMA_LOADERS and len(per[best_g]) == 2
 
 
 def test_born_dot_test_on_the_born_configuration_grid():

@@ -12,9 +12,9 @@ from elasticisolib_3d_b200.engine import COMP_GRID
 pytestmark = pytest.mark.gpu
 
 
-def _problem(sv, ckpt="fp32", segment=0, variant=(8, 2, "tma"), velocity="auto"):
+def _problem(sv, ckpt="fp32", segment=0, variant=(8, 2, "tma"), velocity="auto", ring=True):
     fd = H.FdParam(sv.elastic, sv.axes, sv.par)
-    prob = F.FwiProblem(fd, ckpt=ckpt, segment=segment, variant=variant, velocity=velocity)
+    prob = F.FwiProblem(fd, ckpt=ckpt, segment=segment, variant=variant, velocity=velocity, decimation_ring=ring)
     ax7 = H.grid_axes(*(a.n for a in sv.axes), *(a.o for a in sv.axes), *(a.d for a in sv.axes))
     src = H.build_devices(*sv.src_xyz[0], ax7, fd.nts, sv.par)
     rec = H.build_devices(*sv.rec_xyz, ax7, fd.nts, sv.par)
@@ -24,20 +24,24 @@ def _problem(sv, ckpt="fp32", segment=0, variant=(8, 2, "tma"), velocity="auto")
 # BF16 states (8-bit mantissa) measured 1.2e-3 - 1.8e-3 on this case, depending on where the
 # segments fall, above the 1e-3 bound that the FP32 and FP16 plans meet; they are checked
 # against 3e-3.
-@pytest.mark.parametrize("ckpt,segment,variant,velocity,tol", [
-    ("fp32", 0, (8, 2, "tma"), "auto", 1e-3),
-    ("fp32", 3, (8, 2, "plain"), "fp32", 1e-3),
-    ("fp16", 4, (8, 2, "tma"), "auto", 1e-3),
-    ("fp16", 5, (8, 2, "tma"), "fp16", 1e-3),
-    ("fp32", 1, (8, 2, "tma"), "fp16", 1e-3),
-    ("bf16", 4, (8, 2, "tma"), "fp16", 3e-3),
+@pytest.mark.parametrize("ckpt,segment,variant,velocity,tol,ring", [
+    ("fp32", 0, (8, 2, "tma"), "auto", 1e-3, True),
+    ("fp32", 3, (8, 2, "plain"), "fp32", 1e-3, True),
+    ("fp16", 4, (8, 2, "tma"), "auto", 1e-3, True),
+    ("fp16", 5, (8, 2, "tma"), "fp16", 1e-3, True),
+    ("fp32", 1, (8, 2, "tma"), "fp16", 1e-3, True),
+    ("bf16", 4, (8, 2, "tma"), "fp16", 3e-3, True),
+    ("fp32", 3, (8, 2, "tma"), "fp32", 1e-3, False),
+    ("fp16", 4, (8, 2, "tma"), "fp16", 1e-3, False),
+    ("fp32", 0, (8, 3, "split"), "fp32", 1e-3, True),
+    ("fp16", 3, (8, 3, "split"), "fp16", 1e-3, True),
 ])
-def test_fwi_gradient_matches_fp64_oracle(ckpt, segment, variant, velocity, tol):
+def test_fwi_gradient_matches_fp64_oracle(ckpt, segment, variant, velocity, tol, ring):
     sv, true = survey()
     orc = OracleFwi(sv)
     d_obs, _ = orc.data(true)
     loss_ref, g_ref = orc.misfit_and_gradient(sv.elastic, d_obs)
-    prob, src, rec = _problem(sv, ckpt, segment, variant, velocity)
+    prob, src, rec = _problem(sv, ckpt, segment, variant, velocity, ring)
     prob.shots.append(F.make_shot(src, rec, explosive(sv.par.getInt("nts"), sv.wavelet), d_obs.astype(np.float32),
                                   "cuda"))
     m = [torch.tensor(sv.elastic[k], device="cuda", requires_grad=True) for k in range(3)]
@@ -47,12 +51,45 @@ def test_fwi_gradient_matches_fp64_oracle(ckpt, segment, variant, velocity, tol)
         assert prob.prop.velocity_storage == velocity
     g = np.stack([x.grad.double().cpu().numpy() for x in m])
     errs = [float(np.linalg.norm(g[k] - g_ref[k]) / np.linalg.norm(g_ref[k])) for k in range(3)]
-    print(f"plan ckpt={ckpt} segment={segment} velocity={prob.prop.velocity_storage}: misfit rel err "
+    print(f"plan ckpt={ckpt} segment={segment} velocity={prob.prop.velocity_storage} ring={ring}: misfit rel err "
           f"{abs(loss.item() - loss_ref) / loss_ref:.2e}, gradient rel err rho {errs[0]:.2e} lambda {errs[1]:.2e} "
           f"mu {errs[2]:.2e}", flush=True)
     assert abs(loss.item() - loss_ref) / loss_ref < 1e-4
     for k in range(3):
         assert errs[k] < tol, (k, errs[k])
+
+
+@pytest.mark.parametrize("ckpt,segment,variant,velocity", [
+    ("fp32", 0, (8, 2, "tma"), "fp32"),
+    ("fp32", 1, (8, 2, "tma"), "fp32"),
+    ("fp16", 3, (8, 2, "tma"), "fp16"),
+    ("fp32", 2, (8, 2, "plain"), "fp32"),
+    ("fp32", 5, (8, 2, "cpasync"), "fp16"),
+    ("fp32", 3, (8, 3, "split"), "fp32"),
+])
+def test_ring_decimation_matches_fused_accumulators(ckpt, segment, variant, velocity):
+    """The gradient with the fine levels of each block decimated from a ring (one launch per block,
+    imaging fused) equals the one with the decimation accumulators fused into every fine step: the
+    same sums in another order, so FP32 rounding apart (relative 1e-5), for segment lengths that put
+    one-block segments, segment starts at block 0 and the kept last segment on the path."""
+    sv, true = survey()
+    orc = OracleFwi(sv)
+    d_obs, _ = orc.data(true)
+    grads, losses = [], []
+    for ring in (False, True):
+        prob, src, rec = _problem(sv, ckpt, segment, variant, velocity, ring)
+        prob.shots.append(F.make_shot(src, rec, explosive(sv.par.getInt("nts"), sv.wavelet),
+                                      d_obs.astype(np.float32), "cuda"))
+        m = [torch.tensor(sv.elastic[k], device="cuda", requires_grad=True) for k in range(3)]
+        loss = F.ElasticFwiMisfit.apply(m[0], m[1], m[2], prob)
+        loss.backward()
+        losses.append(loss.item())
+        grads.append(np.stack([x.grad.double().cpu().numpy() for x in m]))
+    assert abs(losses[0] - losses[1]) <= 1e-7 * abs(losses[0])
+    for k in range(3):
+        err = float(np.linalg.norm(grads[1][k] - grads[0][k]) / np.linalg.norm(grads[0][k]))
+        print(f"ring vs fused, plan {ckpt}/{velocity} segment {segment} {variant[2]}: component {k} {err:.2e}")
+        assert err < 1e-5, (k, err)
 
 
 def test_predicted_traces_match_fp64_oracle():

@@ -22,7 +22,8 @@ def _prop(p, **kw):
 
 VARIANTS = [(8, 2, "plain"), (16, 2, "plain"), (8, 2, "cpasync"), (8, 3, "cpasync"), (16, 2, "cpasync"),
             (8, 2, "tma"), (8, 3, "tma"), (16, 2, "tma"), (8, 2, "tma-ring"), (16, 2, "tma-ring"),
-            (8, 2, "tma-ring-ldg"), (8, 3, "tma-ring-ldg"), (8, 2, "tma-ring-ldg2")]
+            (8, 2, "tma-ring-ldg"), (8, 3, "tma-ring-ldg"), (8, 2, "tma-ring-ldg2"),
+            (8, 2, "split"), (8, 3, "split"), (8, 4, "split")]
 
 
 @pytest.mark.parametrize("tx,stages,loader", VARIANTS)
@@ -42,7 +43,7 @@ def test_nl_forward_matches_oracle(tx, stages, loader):
     assert rel_l2(got, ref64) < 1e-5
 
 
-@pytest.mark.parametrize("loader", ["plain", "tma"])
+@pytest.mark.parametrize("loader", ["plain", "tma", "split"])
 def test_nl_adjoint_matches_oracle(loader):
     sv, p, med, src, rec, dtw = prepared(seed=2)
     rng = np.random.default_rng(6)
@@ -50,7 +51,7 @@ def test_nl_adjoint_matches_oracle(loader):
     rpos = [d.unique for d in rec]
     dat = random_signals(rpos, p.nts, rng)
     pr = _prop(p)
-    pr.set_stepper_variant(8, 2, loader)
+    pr.set_stepper_variant(8, 3 if loader == "split" else 2, loader)
     pr.set_medium(med)
     got = pr.nl_adjoint(dat, spos, rpos)
     ref = O.nl_adjoint_reg(p, med, dat, spos, rpos, np.float32)
@@ -71,7 +72,8 @@ def test_born_forward_matches_oracle():
     assert rel_l2(got, ref) < 1e-5
 
 
-@pytest.mark.parametrize("segment,loader", [(0, "plain"), (1, "plain"), (3, "plain"), (0, "tma"), (3, "tma")])
+@pytest.mark.parametrize("segment,loader", [(0, "plain"), (1, "plain"), (3, "plain"), (0, "tma"), (3, "tma"),
+                                            (0, "split"), (1, "split"), (3, "split")])
 def test_born_adjoint_matches_oracle(segment, loader):
     sv, p, med, src, rec, dtw = prepared(seed=4)
     rng = np.random.default_rng(8)
@@ -82,7 +84,7 @@ def test_born_adjoint_matches_oracle(segment, loader):
     pr = _prop(p)
     pr.set_medium(med)
     pr.set_checkpoint_policy("fp32", segment)
-    pr.set_stepper_variant(8, 2, loader)
+    pr.set_stepper_variant(8, 3 if loader == "split" else 2, loader)
     got = pr.born_adjoint(sig, dat, spos, rpos)
     ref = O.born_adjoint_reg(p, med, sig, dat, spos, rpos, None, np.float32)
     assert rel_l2(got, ref) < 1e-5
