@@ -78,7 +78,7 @@ struct Plan {
 // fits it, else the last one.  Otherwise each candidate takes the longest
 // segment that fits, and the plan that recomputes the fewest source blocks
 // wins once a lower-precision plan is charged a margin (5% of the blocks for
-// 16-bit states, 15% for 16-bit slots).  False when nothing fits.
+// 16-bit states, 5% for 16-bit slots).  False when nothing fits.
 inline bool choosePlan(long long n, int ny, int nts, double budget, int ckptType, int vType, int segment,
                        Plan& out) {
   const int blocks = nts - 1;
@@ -105,7 +105,7 @@ inline bool choosePlan(long long n, int ny, int nts, double budget, int ckptType
     while (l >= 1 && planBytes(n, ny, nts, cands[i].ck, cands[i].vt, l) > budget) l--;
     if (l < 1) continue;
     const double cost = recomputedBlocks(blocks, l) +
-                        blocks * ((cands[i].ck != kStateF32 ? 0.05 : 0.0) + (cands[i].vt == kSlotF16 ? 0.15 : 0.0));
+                        blocks * ((cands[i].ck != kStateF32 ? 0.05 : 0.0) + (cands[i].vt == kSlotF16 ? 0.05 : 0.0));
     if (best < 0 || cost < bestCost) {
       best = i;
       bestCost = cost;

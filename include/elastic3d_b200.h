@@ -241,7 +241,7 @@ int e3d_set_stepper_chunks(e3d_context* ctx, int chunks);
  * 0 = fp32, 1 = fp16, 2 = bf16 (16-bit types carry one scale per y-slice and
  * field).  Each candidate takes the longest segment that fits; the one that
  * recomputes the fewest source blocks wins, a 16-bit plan only where it saves
- * more than 5% (states) / 15% (velocity slots) of the blocks.  The forward pass
+ * more than 5% (states) / 5% (velocity slots) of the blocks.  The forward pass
  * keeps the last segment's velocity, so only the earlier segments are recomputed;
  * segment = coarse blocks per segment (0 = automatic), segments aligned to the
  * end of the record;

@@ -80,7 +80,7 @@ def test_plan_fits_its_budget_and_prefers_full_precision_when_all_fits():
         assert b <= budget
 
 
-def test_plan_takes_16_bit_slots_only_for_a_large_cut_in_recomputation():
+def test_plan_takes_16_bit_slots_where_they_cut_recomputation():
     # 288^3 cells, 1000 samples, 143.6 GB: FP32 slots hold about half the record, FP16 slots
     # nearly all of it -- the FP16 plan removes ~490 recomputed blocks and wins
     ck, vt, L, _ = checkpoint_plan(N288, NY288, 1000, 143.6e9)
@@ -89,9 +89,13 @@ def test_plan_takes_16_bit_slots_only_for_a_large_cut_in_recomputation():
     # the all-FP32 plan for the same budget recomputes ~half the record
     ck, vt, L32, _ = checkpoint_plan(N288, NY288, 1000, 143.6e9, "fp32", "fp32")
     assert (ck, vt) == ("fp32", "fp32") and checkpoint_schedule(999, L32)[1] > 400
-    # 392^3, 2500 samples: 16-bit slots would cut recomputation by less than their margin
+    # 392^3, 2500 samples: FP16 slots double the segment (about 330 blocks against 160 with FP32
+    # slots), which removes about 190 recomputed blocks, more than their 5 % margin of 125
     ck, vt, L, _ = checkpoint_plan(392 * 392 * 388, 388, 2500, 150e9)
-    assert (ck, vt) == ("fp16", "fp32") and 100 < L < 250
+    assert (ck, vt) == ("fp16", "fp16") and 300 < L < 450
+    ck, vt, L32, _ = checkpoint_plan(392 * 392 * 388, 388, 2500, 150e9, velocity="fp32")
+    assert (ck, vt) == ("fp16", "fp32") and 100 < L32 < 250
+    assert checkpoint_schedule(2499, L32)[1] - checkpoint_schedule(2499, L)[1] > 0.05 * 2499
 
 
 def test_plan_respects_explicit_types_and_segment():
@@ -105,13 +109,12 @@ def test_plan_respects_explicit_types_and_segment():
 
 def test_plan_cost_falls_with_more_memory():
     """The chosen plan's cost -- recomputed blocks plus the precision margins (5 % of the blocks
-    for 16-bit states, 15 % for 16-bit slots) -- never rises with the budget.  Recomputation
-    alone may: with 250 GB the all-FP32 plan recomputing 138 blocks beats FP16 slots for the
-    whole record, whose margin is 200 blocks."""
+    for 16-bit states, 5 % for 16-bit slots) -- never rises with the budget, and with enough
+    memory the all-FP32 plan recomputes nothing."""
     prev = None
     for budget in (3e10, 5e10, 8e10, 1.2e11, 1.6e11, 2.5e11, 3.5e11):
         ck, vt, L, _ = checkpoint_plan(N288, NY288, 1000, budget)
-        cost = checkpoint_schedule(999, L)[1] + 999 * (0.05 * (ck != "fp32") + 0.15 * (vt == "fp16"))
+        cost = checkpoint_schedule(999, L)[1] + 999 * (0.05 * (ck != "fp32") + 0.05 * (vt == "fp16"))
         assert prev is None or cost <= prev + 1e-9
         prev = cost
     assert prev == 0
