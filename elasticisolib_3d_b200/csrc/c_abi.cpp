@@ -400,6 +400,7 @@ int e3d_nl_propagate_device(e3d_context* ctx, int adjoint, const long long* src_
   DevSignals S, R;
   int st = devSet(src_pos_dev, src_off10, S);
   if (st == E3D_OK) st = devSet(rec_pos_dev, rec_off10, R);
+  if (st == E3D_OK) st = validateDeviceSets(ctx->c, S, R);
   if (st != E3D_OK) return st;
   return nlPropagateDevice(ctx->c, adjoint != 0, S, R, src_sig_dev, rec_sig_dev);
 }
@@ -433,6 +434,7 @@ int e3d_fwi_forward_device(e3d_context* ctx, const long long* src_pos_dev, const
   int st = devSet(src_pos_dev, src_off10, S);
   if (st == E3D_OK) st = devSet(rec_pos_dev, rec_off10, R);
   if (st == E3D_OK) st = traceMap(map, T);
+  if (st == E3D_OK) st = validateDeviceSets(ctx->c, S, R);
   if (st != E3D_OK) return st;
   return fwiForwardDevice(ctx->c, S, R, src_sig_dev, rec_sig_dev, map ? &T : nullptr);
 }
@@ -447,6 +449,7 @@ int e3d_fwi_gradient_device(e3d_context* ctx, const long long* src_pos_dev, cons
   int st = devSet(src_pos_dev, src_off10, S);
   if (st == E3D_OK) st = devSet(rec_pos_dev, rec_off10, R);
   if (st == E3D_OK) st = traceMap(map, T);
+  if (st == E3D_OK) st = validateDeviceSets(ctx->c, S, R);
   if (st != E3D_OK) return st;
   return fwiGradientDevice(ctx->c, S, R, src_sig_dev, residual_dev, grad8_dev, map ? &T : nullptr, src_adj_dev);
 }

@@ -78,6 +78,7 @@ struct Context {
   int graphLoop = 1;         // 1: replay coarse blocks of the nonlinear loop as a CUDA graph
   bool inCapture = false;    // a coarse block is being captured (no timing samples)
   int* blockIndex = nullptr; // device coarse-time index of replayed blocks
+  unsigned* posFlag = nullptr;  // device word of the position-table check
   std::unordered_map<unsigned long long, CUtensorMap> tmaps;  // (pointer, box) -> tensor map
   std::vector<void*> owned;  // every device allocation of this context
   // working wavefields (primary propagation)
@@ -1068,6 +1069,41 @@ int setGraphLoop(Context* c, int on) {
 // than the legacy default stream) the remaining blocks replay one captured
 // block (two when sub is odd, for the two pointer parities), the coarse index
 // living on the device.
+// Device position tables checked before any injection or recording (the host
+// path checks host tables the same way): every entry an updated cell.  flagDev
+// is a device word the check may overwrite; the result is read back on `st`.
+static int checkDevicePositions(const DevSignals* const* sets, int nsets, int nz, int nx, int ny, unsigned* flagDev,
+                                cudaStream_t st) {
+  bool any = false;
+  for (int i = 0; i < nsets; i++) any = any || sets[i]->off[NCOMP] > 0;
+  if (!any) return E3D_OK;
+  E3D_CUDA_TRY(cudaMemsetAsync(flagDev, 0, sizeof(unsigned), st));
+  for (int i = 0; i < nsets; i++) {
+    const int n = sets[i]->off[NCOMP];
+    if (n == 0) continue;
+    E3D_ARG(sets[i]->pos != nullptr, "null position table");
+    kCheckPositions<<<(n + 255) / 256, 256, 0, st>>>(sets[i]->pos, n, nz, nx, ny, flagDev);
+    E3D_LAUNCH_CHECK();
+  }
+  unsigned bad = 0;
+  E3D_CUDA_TRY(cudaMemcpyAsync(&bad, flagDev, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+  E3D_CUDA_TRY(cudaStreamSynchronize(st));
+  if (bad) {
+    setLastError("device position table holds a point inside the FAT ring or outside the grid", __FILE__, __LINE__);
+    return E3D_ERR_BOUNDS;
+  }
+  return E3D_OK;
+}
+
+int validateDeviceSets(Context* c, const DevSignals& a, const DevSignals& b) {
+  E3D_ARG(c != nullptr, "null context");
+  E3D_CUDA_TRY(cudaSetDevice(c->d.device));
+  if (!c->posFlag) E3D_RET(devAlloc(c, (void**)&c->posFlag, sizeof(unsigned)));
+  const DevSignals* sets[2] = {&a, &b};
+  c->launches += (a.off[NCOMP] > 0) + (b.off[NCOMP] > 0);
+  return checkDevicePositions(sets, 2, c->d.nz, c->d.nx, c->d.ny, c->posFlag, c->st);
+}
+
 int nlPropagateDevice(Context* c, bool adjoint, const DevSignals& srcSet, const DevSignals& recSet, float* srcSig,
                       float* recSig) {
   E3D_ARG(c && c->haveMedium, "medium not set");
@@ -2245,19 +2281,38 @@ constexpr int kStaticMaxDevices = 64;
 static __device__ __align__(256) unsigned char g_e3dStaticWork[kStaticWorkBytes];
 static std::mutex g_staticWorkMutex;
 static void* g_staticWorkAddr[kStaticMaxDevices] = {};
+static CUcontext g_staticWorkCtx[kStaticMaxDevices] = {};  // context the cached address belongs to
 
 size_t staticWorkBytes() { return kStaticWorkBytes; }
 
+// cuCtxGetCurrent through the runtime's driver entry point (no libcuda link dependency)
+static CUresult (*ctxGetCurrent())(CUcontext*) {
+  static CUresult (*fn)(CUcontext*) = nullptr;
+  if (!fn) {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (CUresult(*)(CUcontext*))f;
+  }
+  return fn;
+}
+
 // Device address of the static work array on the current device.  The name
 // g_e3dStaticWork is a host-side stand-in in host code, so its device address
-// is looked up once per device (with that device current) and cached.
+// is looked up once per device (with that device current) and cached, and
+// looked up again when the device's primary context is no longer the one the
+// address was taken in (after cudaDeviceReset).
 static int staticWorkAddress(int dev, float** out) {
   if (dev < 0 || dev >= kStaticMaxDevices) {
     setLastError("device ordinal beyond the static work table", __FILE__, __LINE__);
     return E3D_ERR_ARG;
   }
+  E3D_CUDA_TRY(cudaSetDevice(dev));  // makes the device's primary context current
+  CUcontext cur = nullptr;
+  if (auto fn = ctxGetCurrent()) fn(&cur);
   std::lock_guard<std::mutex> lock(g_staticWorkMutex);
-  if (!g_staticWorkAddr[dev]) {
+  if (!g_staticWorkAddr[dev] || g_staticWorkCtx[dev] != cur) {
     void* p = nullptr;
     const cudaError_t e = cudaGetSymbolAddress(&p, g_e3dStaticWork);
     if (e != cudaSuccess || !p) {
@@ -2265,6 +2320,7 @@ static int staticWorkAddress(int dev, float** out) {
       return E3D_ERR_CUDA;
     }
     g_staticWorkAddr[dev] = p;
+    g_staticWorkCtx[dev] = cur;
   }
   *out = (float*)g_staticWorkAddr[dev];
   return E3D_OK;
@@ -2283,13 +2339,14 @@ int nlPropagateStatic(const ContextDesc& d, const float* const* planes, bool adj
   E3D_ARG(recSet.off[NCOMP] == 0 || recSig, "null receiver signals");
   const long long n = (long long)d.nz * d.nx * d.ny;
   const size_t fieldsBytes = ((size_t)2 * NCOMP * n * sizeof(float) + 255) / 256 * 256;
-  const size_t need = fieldsBytes + (size_t)PAD_MAX * sizeof(float);
+  // the two levels, the taper and one word for the position-table check
+  const size_t need = fieldsBytes + (size_t)PAD_MAX * sizeof(float) + 256;
   if (n >= (1LL << 34) || need > kStaticWorkBytes) {
     char msg[256];
     snprintf(msg, sizeof(msg),
              "grid of %lld cells needs %zu bytes of static work memory; the allocation-free entry point holds "
              "%zu bytes (18 fields of at most %zu cells)",
-             n, need, kStaticWorkBytes, (kStaticWorkBytes - (size_t)PAD_MAX * sizeof(float)) / (18 * sizeof(float)));
+             n, need, kStaticWorkBytes, (kStaticWorkBytes - (size_t)PAD_MAX * sizeof(float) - 256) / (18 * sizeof(float)));
     setLastError(msg, __FILE__, __LINE__);
     return E3D_ERR_ARG;
   }
@@ -2318,15 +2375,23 @@ int nlPropagateStatic(const ContextDesc& d, const float* const* planes, bool adj
     filt[i] = (float)(left * scale);
     filt[i + hfilt] = (float)(right * scale);
   }
-  float taper[PAD_MAX];
-  for (int i = 0; i < PAD_MAX; i++) taper[i] = 1.f;
+  TaperArg taper;
+  for (int i = 0; i < PAD_MAX; i++) taper.v[i] = 1.f;
   for (int i = 0; i < d.minPad; i++) {
     float arg = (float)(M_PI / (1.0 * d.minPad) * 1.0 * (d.minPad - i));
-    taper[i] = (float)(d.alphaCos + (1.0 - d.alphaCos) * std::cos(arg));
+    taper.v[i] = (float)(d.alphaCos + (1.0 - d.alphaCos) * std::cos(arg));
   }
   float* taperDev = (float*)((char*)work + fieldsBytes);
-  // the array keeps the previous call's contents: both levels start at zero
-  E3D_CUDA_TRY(cudaMemcpyAsync(taperDev, taper, sizeof(taper), cudaMemcpyHostToDevice, st));
+  unsigned* flagDev = (unsigned*)((char*)work + fieldsBytes + (size_t)PAD_MAX * sizeof(float));
+  {
+    // device positions: every entry an updated cell, checked before anything is written
+    const DevSignals* sets[2] = {&srcSet, &recSet};
+    E3D_RET(checkDevicePositions(sets, 2, d.nz, d.nx, d.ny, flagDev, st));
+  }
+  // the taper travels as a kernel argument; the array keeps the previous call's
+  // contents, so both levels start at zero
+  kWriteTaper<<<1, 128, 0, st>>>(taper, taperDev);
+  E3D_LAUNCH_CHECK();
   E3D_CUDA_TRY(cudaMemsetAsync(work, 0, (size_t)2 * NCOMP * n * sizeof(float), st));
   g.taper = taperDev;
   Fields9 a, b;
@@ -2339,7 +2404,9 @@ int nlPropagateStatic(const ContextDesc& d, const float* const* planes, bool adj
   const int tix = (g.nx - 2 * FAT + TXS - 1) / TXS;
   const int nyi = g.ny - 2 * FAT;
   const long long tiles = (long long)tiz * tix;
-  int chunks = (int)std::min<long long>((4LL * 148 + tiles - 1) / tiles, std::max(1, nyi / 32));
+  int sms = 148;
+  E3D_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  int chunks = (int)std::min<long long>((4LL * sms + tiles - 1) / tiles, std::max(1, nyi / 32));
   chunks = std::max(chunks, 1);
   const int yChunk = (nyi + chunks - 1) / chunks;
   chunks = (nyi + yChunk - 1) / yChunk;

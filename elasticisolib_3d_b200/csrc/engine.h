@@ -70,6 +70,9 @@ struct DevSignals {
 };
 int nlPropagateDevice(Context* c, bool adjoint, const DevSignals& srcSet, const DevSignals& recSet,
                       float* srcSig, float* recSig);
+// Device position tables: every entry an updated cell (E3D_ERR_BOUNDS otherwise); waits on the
+// context's stream.  The device-pointer entry points call it before any propagation.
+int validateDeviceSets(Context* c, const DevSignals& a, const DevSignals& b);
 // 1 (default): nonlinear propagation replays captured coarse blocks as CUDA graphs.
 int setGraphLoop(Context* c, int on);
 // Irregular receivers as linear combinations of the regular acquisition

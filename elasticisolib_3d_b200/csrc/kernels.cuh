@@ -1168,6 +1168,31 @@ __device__ __forceinline__ void injectAt(const StepPtrs& p, const GridConst& g, 
   }
 }
 
+// Check of a device position table before any injection or recording: every
+// entry must be an updated cell (not in the FAT ring, not outside the grid), as
+// the host path requires of host tables.  Reads the table only; a bad entry
+// sets *bad, which the host reads back.
+__global__ void kCheckPositions(const long long* pos, int n, int nz, int nx, int ny, unsigned* bad) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  const long long p = pos[j];
+  const long long ys = (long long)nz * nx;
+  bool ok = p >= 0 && p < ys * ny;
+  if (ok) {
+    const long long iz = p % nz, ix = (p / nz) % nx, iy = p / ys;
+    ok = iz >= FAT && iz < nz - FAT && ix >= FAT && ix < nx - FAT && iy >= FAT && iy < ny - FAT;
+  }
+  if (!ok) atomicOr(bad, 1u);
+}
+
+// The sponge taper written from kernel arguments (no host buffer involved).
+struct TaperArg {
+  float v[PAD_MAX];
+};
+__global__ void kWriteTaper(TaperArg t, float* out) {
+  for (int i = threadIdx.x; i < PAD_MAX; i += blockDim.x) out[i] = t.v[i];
+}
+
 __global__ void kInject(StepPtrs p, GridConst g, SparseSet s, const float* sigL, const float* sigR, float wl,
                         float wr) {
   injectAt(p, g, s, sigL, sigR, wl, wr);

@@ -417,17 +417,20 @@ def broadcast_model(tensors, group=None):
 
 def reduce_misfit(total, grads, group=None):
     """Sum the misfit and the (rho, lambda, mu) gradient over the ranks of `group`: one
-    all-reduce of a flat buffer (NCCL over NVLink between GPUs; the reference sums shot
-    gradients on the host, BornElasticShotsGpu_3D.cpp:528-540)."""
+    all-reduce of the flat gradient (NCCL over NVLink between GPUs; the reference sums shot
+    gradients on the host, BornElasticShotsGpu_3D.cpp:528-540) and one of the misfit in its own
+    precision (FP64), so that the distributed misfit keeps the digits the single-rank one has."""
     if not (torch.distributed.is_available() and torch.distributed.is_initialized()):
         return total, grads
-    flat = torch.cat([total.reshape(1).to(grads[0].dtype)] + [g.reshape(-1) for g in grads])
+    flat = torch.cat([g.reshape(-1) for g in grads])
+    tot = total.reshape(1).clone()
     torch.distributed.all_reduce(flat, group=group)
-    out, off = [], 1
+    torch.distributed.all_reduce(tot, group=group)
+    out, off = [], 0
     for g in grads:
         out.append(flat[off:off + g.numel()].view_as(g))
         off += g.numel()
-    return flat[0].to(total.dtype), out
+    return tot[0], out
 
 
 def _source_scaling_gradient(rho, lam, mu, problem, src_terms):

@@ -37,8 +37,11 @@ class GradientRequest:
 
 
 def _key(fd):
+    """Everything of a request's fdParamElastic_3D that its FwiProblem is built from: the grid, the
+    time axes, the sponge (width and taper constant) and the free-surface flag (a free-surface
+    request must reach FwiProblem, which refuses it, rather than reuse a problem without one)."""
     return (fd.nz, fd.nx, fd.ny, fd.nts, fd.sub, fd.minPad, float(fd.dz), float(fd.dx), float(fd.dy),
-            float(fd.dts))
+            float(fd.dts), float(getattr(fd, "alphaCos", 0.99)), int(getattr(fd, "freeSurface", 0)))
 
 
 def _estimate_bytes(fd):

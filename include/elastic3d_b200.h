@@ -320,7 +320,12 @@ int e3d_born_adjoint(e3d_context* ctx, const float* const* src9, const float* co
 /* Device-buffer propagations.  Signals are time-major [nts][ntot] with the
  * nine components concatenated; pos_dev is the matching int64 table and
  * off10[k]..off10[k+1] is component k's range.  Work is queued on the
- * context's stream; call e3d_synchronize before reading outputs. */
+ * context's stream; call e3d_synchronize before reading outputs.
+ * Before anything is written, a read-only kernel checks the position tables
+ * (e3d_nl_propagate_device, e3d_fwi_forward_device, e3d_fwi_gradient_device
+ * and e3d_nl_propagate_device_noalloc): an entry inside the FAT ring or outside
+ * the grid returns E3D_ERR_BOUNDS, as the host-buffer calls do for host
+ * tables.  The check waits for the stream once per call. */
 int e3d_nl_propagate_device(e3d_context* ctx, int adjoint, const long long* src_pos_dev, const int* src_off10,
                             const long long* rec_pos_dev, const int* rec_off10, float* src_sig_dev,
                             float* rec_sig_dev);
@@ -372,8 +377,8 @@ int e3d_fwi_gradient_device(e3d_context* ctx, const long long* src_pos_dev, cons
  * wavefield levels and the sponge taper live in one fixed device array of
  * e3d_noalloc_work_bytes() = 64 MiB, which every GPU that loads this library
  * holds until the process exits.  That limits the grid to nz*nx*ny of about
- * 0.93 M cells (18 float fields); larger grids return E3D_ERR_ARG with the
- * sizes in e3d_last_error().  No context is needed: the propagation runs on
+ * 0.93 M cells (18 float fields, the taper and one status word); larger grids
+ * return E3D_ERR_ARG with the sizes in e3d_last_error().  No context is needed: the propagation runs on
  * the calling thread's current device, on `stream` (NULL = legacy default
  * stream), with the stepper of the "plain" variant; desc->device is ignored
  * and desc->free_surface must be 0.
@@ -381,7 +386,9 @@ int e3d_fwi_gradient_device(e3d_context* ctx, const long long* src_pos_dev, cons
  * time-major signals as for e3d_nl_propagate_device (the output signals are
  * overwritten).  The first call on a device looks up the device address of
  * the array (cudaGetSymbolAddress, with the device current) and caches it;
- * make that first call before any stream capture.  Every call on a device
+ * make that first call before any stream capture.  The cached address
+ * belongs to the device's primary context; a call that finds another primary
+ * context current (after cudaDeviceReset) looks the address up again.  Every call on a device
  * uses the same array and clears it at the start, so calls that overlap on
  * the GPU (on different streams, or from different threads) race and give
  * wrong results; order them on one stream. */

@@ -89,3 +89,39 @@ def test_least_recently_used_problems_close_to_admit_a_new_grid(monkeypatch):
     server._problem(0, d)          # does not fit: b (least recently used) closes first
     assert closed and closed[0] == 201
     assert opened == [200, 201, 202, 203]
+
+
+def test_requests_differing_only_in_the_sponge_or_free_surface_get_their_own_problem(monkeypatch):
+    """The problem cache is keyed by everything FwiProblem takes from the request's parameters: a
+    request whose taper constant (alphaCos) differs gets its own problem, and a free-surface request
+    reaches FwiProblem (which refuses it) instead of reusing a problem built without one."""
+    import torch
+    from elasticisolib_3d_b200 import serving as SV
+
+    built = []
+
+    class FakeProblem:
+        def __init__(self, fd, device=None, ckpt=None, variant=None):
+            if getattr(fd, "freeSurface", 0):
+                raise ValueError("free surface")
+            built.append(fd)
+            self.fd = fd
+            self.prop = SimpleNamespace(close=lambda: None)
+
+    monkeypatch.setattr(SV.F, "FwiProblem", FakeProblem)
+    monkeypatch.setattr(torch.cuda, "synchronize", lambda dev=None: None)
+    monkeypatch.setattr(torch.cuda, "mem_get_info", lambda dev=None: (1 << 50, 1 << 50))
+    server = SV.GradientServer(devices=(0,), autotune=False)
+    a = _fd(200, 1000)
+    a.alphaCos, a.freeSurface = 0.99, 0
+    b = SimpleNamespace(**vars(a))
+    b.alphaCos = 0.95
+    pa = server._problem(0, a)
+    pb = server._problem(0, b)
+    assert pa is not pb and pb.fd.alphaCos == 0.95
+    assert server._problem(0, SimpleNamespace(**vars(a))) is pa      # identical parameters: reused
+    fs = SimpleNamespace(**vars(a))
+    fs.freeSurface = 1
+    with pytest.raises(ValueError, match="free surface"):
+        server._problem(0, fs)
+    assert len(built) == 2

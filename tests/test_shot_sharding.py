@@ -13,7 +13,9 @@ from elasticisolib_3d_b200.fwi import reduce_misfit, shard_shots
 
 def _fake_shot(i, shape):
     g = torch.Generator().manual_seed(100 + i)
-    return torch.tensor(float(i + 1) ** 2, dtype=torch.float64), [torch.randn(shape, generator=g) for _ in range(3)]
+    # misfits with digits below FP32 resolution: the reduced total must keep them
+    return (torch.tensor(1e8 + float(i + 1) ** 2 + 0.125 * (i + 1), dtype=torch.float64),
+            [torch.randn(shape, generator=g) for _ in range(3)])
 
 
 def _worker(rank, world, port, n_shots, shape, out):
@@ -65,7 +67,7 @@ def test_two_rank_reduction_matches_serial_sum():
             a += b
     for r in range(2):
         loss, grads = out[r]
-        assert abs(loss - serial_loss) < 1e-9
+        assert abs(loss - serial_loss) < 1e-3   # an FP32 misfit would be off by ~10 at 5e8
         for a, b in zip(grads, serial):
             assert torch.allclose(a, b, atol=1e-5)
 
@@ -110,7 +112,7 @@ def test_dynamic_dealing_covers_every_shot_once_and_balances():
         assert sorted(m0 + m1) == list(range(n_shots))
         assert len(m0) > len(m1)  # the faster rank took more shots
         for r in range(2):
-            assert abs(out[r][evaluation][1] - serial_loss) < 1e-9
+            assert abs(out[r][evaluation][1] - serial_loss) < 1e-3
 
 
 def _broadcast_worker(rank, world, port, out):

@@ -99,3 +99,41 @@ def test_noalloc_rejects_oversized_grid():
                                                  off, None, None, None)
     assert st == 1  # E3D_ERR_ARG
     assert b"static work memory" in N.lib().e3d_last_error()
+
+
+def test_noalloc_rejects_positions_in_the_fat_ring():
+    """A position table with an entry inside the FAT ring returns E3D_ERR_BOUNDS before anything is
+    written: the output signals keep their contents, and the next correct call still agrees with the
+    context entry point."""
+    sv, p, med, src, rec, dtw = prepared(seed=8)
+    rng = np.random.default_rng(12)
+    spos7 = [d.unique for d in src]
+    rpos7 = [d.unique for d in rec]
+    spos, soff = _device_set(spos7)
+    rpos, roff = _device_set(rpos7)
+    planes = torch.from_numpy(np.ascontiguousarray(med)).cuda()
+    ssig = _time_major(random_signals(spos7, p.nts, rng))
+    bad = rpos.clone()
+    q = int(bad[0])
+    bad[0] = (q // (p.nz * p.nx)) * p.nz * p.nx + ((q // p.nz) % p.nx) * p.nz + 1   # z = 1: the FAT ring
+    out = torch.full((p.nts, roff[9]), 5.0, device="cuda")
+    desc = N.E3DDesc(0, p.nz, p.nx, p.ny, p.nts, p.sub, p.minPad, p.dz, p.dx, p.dy, p.dts, p.alphaCos, 0, 1, 1)
+    so = (ctypes.c_int * 10)(*soff)
+    ro = (ctypes.c_int * 10)(*roff)
+    stream = torch.cuda.current_stream().cuda_stream
+    st = N.lib().e3d_nl_propagate_device_noalloc(ctypes.byref(desc), N.ptr_array([planes[k] for k in range(8)]), 0,
+                                                 spos.data_ptr(), so, bad.data_ptr(), ro, ssig.data_ptr(),
+                                                 out.data_ptr(), stream)
+    torch.cuda.synchronize()
+    assert st == 5  # E3D_ERR_BOUNDS
+    assert bool((out == 5.0).all())
+    pr = Propagator(p.nz, p.nx, p.ny, p.nts, p.sub, p.minPad, p.dz, p.dx, p.dy, p.dts, p.alphaCos)
+    pr.set_stepper_variant(8, 2, "plain")
+    pr.set_medium(planes)
+    pr.set_stream(torch.cuda.current_stream())
+    ref = torch.zeros((p.nts, roff[9]), device="cuda")
+    pr.nl_propagate_device(False, spos, soff, rpos, roff, ssig, ref)
+    torch.cuda.synchronize()
+    _noalloc(p, planes, False, spos, soff, rpos, roff, ssig, out)
+    assert rel_l2([out.double().cpu().numpy()], [ref.double().cpu().numpy()]) < 1e-5
+    pr.close()
