@@ -69,6 +69,7 @@ SIGNATURES = {
     "e3d_velocity_storage": ([P], I),
     "e3d_set_decimation_ring": ([P, I], I),
     "e3d_set_imaging_chunks": ([P, I], I),
+    "e3d_set_premultiplied_adjoint": ([P, I], I),
     "e3d_checkpoint_type": ([P], I),
     "e3d_checkpoint_schedule": ([I, I, P, I, P], I),
     "e3d_checkpoint_plan": ([LL, I, I, D, I, I, I, P, P, P, P], I),

@@ -463,6 +463,11 @@ int e3d_velocity_storage(const e3d_context* ctx) { return (ctx && ctx->c) ? velo
 
 int e3d_checkpoint_type(const e3d_context* ctx) { return (ctx && ctx->c) ? checkpointType(ctx->c) : -1; }
 
+int e3d_set_premultiplied_adjoint(e3d_context* ctx, int on) {
+  CTX_OR_FAIL(ctx);
+  return setPremultipliedAdjoint(ctx->c, on);
+}
+
 int e3d_set_imaging_chunks(e3d_context* ctx, int chunks) {
   CTX_OR_FAIL(ctx);
   return setImagingChunks(ctx->c, chunks);

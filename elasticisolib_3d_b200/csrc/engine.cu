@@ -100,6 +100,10 @@ struct Context {
   std::vector<Fields9> srcRing, adjRing;
   int ringMode = 1;          // 1: decimate from rings when sub allows it
   int imgChunks = 0;         // y chunks of the y-marching imaging launch (0: automatic)
+  // exact adjoint state of the ring passes: 1 premultiplied-only where the medium's premultiplication
+  // is well conditioned (premCond <= kPremCondMax), 0 always the dual raw + premultiplied state
+  int premMode = 1;
+  double premCond = -1.0;    // condition number of the current medium's premultiplication (-1: unknown)
   float* pertDev[NMED] = {};
   // checkpoints
   int ckptType = CKPT_AUTO;
@@ -119,7 +123,7 @@ struct Context {
   // launch accounting and sampled stepper timing
   long long launches = 0;
   int timingEvery = 0;       // 0: off; n: time every n-th stepper launch
-  long long kindCounter[8] = {};
+  long long kindCounter[9] = {};
   std::vector<cudaEvent_t> evPool;
   struct Timed { int mode; cudaEvent_t a, b; };
   std::vector<Timed> timed;
@@ -287,6 +291,7 @@ int setMedium(Context* c, const float* const* planes, bool onDevice) {
   c->haveMedium = true;
   c->ckptValid = false;
   c->tailValid = false;
+  c->premCond = -1.0;
   return E3D_OK;
 }
 
@@ -469,6 +474,17 @@ static int launchTma(Context* c, const StepPtrs& p, dim3 grid, int yChunk) {
   return E3D_OK;
 }
 
+// The exact adjoint on the premultiplied-only state (8-wide tiles, two stages).
+static int launchTmaPrem(Context* c, const StepPtrs& p, dim3 grid, int yChunk) {
+  constexpr size_t smem = (size_t)2 * PipeLayout<8>::STAGE_F * sizeof(float);
+  static std::atomic<unsigned long long> configured{0};
+  E3D_RET(ensureSmemAttr((const void*)kStepTma<STEP_ADJ_EXACT, 8, 2, true>, smem, configured));
+  TmaMaps mp;
+  E3D_RET(buildMaps<8>(c, p, mp));
+  kStepTma<STEP_ADJ_EXACT, 8, 2, true><<<grid, dim3(TZ, 8), smem, c->st>>>(mp, p, c->g, yChunk);
+  return E3D_OK;
+}
+
 static int chooseChunks(const Context* c, long long tiles, int nyi, int perSM = 2);
 
 // Split stepper: role V maps (stress halos and leads, old velocities, rho planes) and role S maps
@@ -581,7 +597,8 @@ static cudaEvent_t takeEvent(Context* c) {
 // Sampled launch timing: with sampling on, every n-th launch of each timed
 // kind is bracketed with CUDA events on the launching stream.  Kinds: stepper
 // modes 0..2, the same with a fused decimation or secondary source 3..5, the
-// block imaging of the decimation ring 6, its velocity decimation 7.
+// block imaging of the decimation ring 6, its velocity decimation 7, the exact
+// adjoint on the premultiplied-only state 8.
 struct TimedLaunch {
   Context* c;
   int kind;
@@ -609,7 +626,7 @@ static int launchStep(Context* c, int mode, const StepPtrs& p) {
   c->launches++;
   // launches that also fuse a decimation or a secondary source are kept apart (mode + 3)
   const bool fused = p.accL[0] != nullptr || p.ssL[0] != nullptr;
-  TimedLaunch t(c, mode + (fused ? 3 : 0));
+  TimedLaunch t(c, p.prem ? 8 : mode + (fused ? 3 : 0));
   return launchStepRaw(c, mode, p);
 }
 
@@ -622,7 +639,7 @@ int setKernelTiming(Context* c, int every) {
 
 int readKernelTiming(Context* c, int mode, double* avgMs, long long* count) {
   E3D_ARG(c && avgMs && count, "null argument");
-  E3D_ARG(mode >= 0 && mode < 8, "bad timed kind");
+  E3D_ARG(mode >= 0 && mode < 9, "bad timed kind");
   double sum = 0;
   long long n = 0;
   std::vector<Context::Timed> keep;
@@ -677,11 +694,11 @@ static int launchStepRaw(Context* c, int mode, const StepPtrs& p) {
   // from 0.54 to 0.67 of the copy bandwidth (10 chunks instead of 2); at 392^3
   // it keeps the long runs.
   int chunks = chooseChunks(c, tiles, nyi);
-  const bool dual = mode == STEP_ADJ_EXACT && p.oP[0] != nullptr;
+  const bool dual = mode == STEP_ADJ_EXACT && (p.oP[0] != nullptr || p.prem);
   // the split stepper (loader 6; loader 7: all but the exact adjoint, which keeps kStepTma) takes
   // every step without a fused decimation or secondary source
   if ((c->loader == 6 || (c->loader == 7 && mode != STEP_ADJ_EXACT)) && g.nz % 4 == 0 && p.accL[0] == nullptr &&
-      p.ssL[0] == nullptr) {
+      p.ssL[0] == nullptr && !p.prem) {
     const int tixS = (g.nx - 2 * FAT + 7) / 8;
     if (mode == STEP_FWD) E3D_RET(launchSplitVariant<STEP_FWD>(c, p, tiz, tixS, nyi));
     else if (mode == STEP_ADJ_REVERSED) E3D_RET(launchSplitVariant<STEP_ADJ_REVERSED>(c, p, tiz, tixS, nyi));
@@ -700,7 +717,11 @@ static int launchStepRaw(Context* c, int mode, const StepPtrs& p) {
   chunks = (nyi + yChunk - 1) / yChunk;
   dim3 grid(tiz, tix, chunks);
   const bool pipe = (g.nz % 4 == 0) && mode != STEP_ADJ_EXACT && c->loader > 0;
-  if (dual) {
+  if (dual && p.prem) {
+    E3D_ARG(g.nz % 4 == 0 && p.accL[0] == nullptr && p.ssL[0] == nullptr,
+            "premultiplied-only adjoint needs nz % 4 == 0 and no fused decimation");
+    E3D_RET(launchTmaPrem(c, p, grid, yChunk));
+  } else if (dual) {
     E3D_ARG(g.nz % 4 == 0, "dual-state adjoint needs nz % 4 == 0");
     if (c->tx == 16) E3D_RET((launchTma<STEP_ADJ_EXACT, 16, 2>(c, p, grid, yChunk)));
     else if (c->stages == 3 && c->loader < 6) E3D_RET((launchTma<STEP_ADJ_EXACT, 8, 3>(c, p, grid, yChunk)));
@@ -776,6 +797,22 @@ static int launchExtractSource(Context* c, const StepPtrs& p, const DevSignals& 
 }
 
 static int launchRefresh(Context* c, const StepPtrs& p, const DevSignals& s);
+
+// Receiver injection into the premultiplied-only state (slices its, its+1, filter weights k);
+// the three normal-stress tables must have equal counts (the caller checks).
+static int launchInjectPremultiplied(Context* c, const StepPtrs& p, const DevSignals& s, const float* sigL,
+                                     const float* sigR, int k) {
+  SparseSet ss;
+  ss.pos = s.pos;
+  for (int i = 0; i <= NCOMP; i++) ss.off[i] = s.off[i];
+  const int n = s.off[NCOMP];
+  if (n == 0) return E3D_OK;
+  c->launches++;
+  kInjectPremultiplied<<<(n + 127) / 128, 128, 0, c->st>>>(p, c->g, ss, sigL, sigR, c->filt[k],
+                                                          c->filt[c->hfilt + k]);
+  E3D_LAUNCH_CHECK();
+  return E3D_OK;
+}
 
 // Receiver injection (slices its, its+1, filter weights k) and premultiplied refresh of the dual
 // adjoint in one launch when the three normal-stress tables have equal counts (they share the
@@ -1175,12 +1212,15 @@ int nlPropagateHost(Context* c, bool adjoint, float* const* model, float* const*
 
 int stepOnly(Context* c, int mode, int nSteps) {
   E3D_ARG(c && c->haveMedium, "medium not set");
-  E3D_ARG(mode >= 0 && mode <= 5, "bad mode");
+  E3D_ARG(mode >= 0 && mode <= 6, "bad mode");
   // modes 3..5: modes 0..2 with the new level decimated into two coarse
-  // accumulators, as the gradient's passes run them (3 velocity fields for the
-  // source recompute, 9 fields for the adjoint)
-  const bool fused = mode >= 3;
-  const int m = fused ? mode - 3 : mode;
+  // accumulators, as the fused-accumulator passes run them (3 velocity fields for
+  // the source recompute, 9 fields for the adjoint); mode 6: mode 2 on the
+  // premultiplied-only state, as the ring adjoint pass runs it
+  const bool premOnly = mode == 6;
+  E3D_ARG(!premOnly || (c->loader >= 2 && c->d.nz % 4 == 0), "mode 6 needs a TMA loader and nz % 4 == 0");
+  const bool fused = mode >= 3 && !premOnly;
+  const int m = premOnly ? STEP_ADJ_EXACT : fused ? mode - 3 : mode;
   E3D_RET(allocFields(c, c->w0, false));
   E3D_RET(allocFields(c, c->w1, false));
   if (fused) {
@@ -1188,13 +1228,14 @@ int stepOnly(Context* c, int mode, int nSteps) {
     E3D_RET(allocFields(c, c->ss[1], true));
   }
   // the exact adjoint runs on the dual state, as in the adjoint pass, with the TMA loader
-  const bool dual = m == STEP_ADJ_EXACT && c->loader >= 2 && c->d.nz % 4 == 0;
+  const bool dual = m == STEP_ADJ_EXACT && c->loader >= 2 && c->d.nz % 4 == 0 && !premOnly;
   if (dual) {
     E3D_RET(allocFields(c, c->q0, false));
     E3D_RET(allocFields(c, c->q1, false));
   }
   for (int i = 0; i < nSteps; i++) {
     StepPtrs p = makeStep(c, c->w0, c->w1);
+    p.prem = premOnly ? 1 : 0;
     if (dual)
       for (int k = 0; k < NCOMP; k++) {
         p.c[k] = c->q1.p[k];
@@ -1301,6 +1342,41 @@ static int ringLevels(const Context* c) {
   return (c->ringMode && c->d.sub <= RING_SUB_MAX) ? std::max(c->d.sub + 1, 3) : 0;
 }
 
+// The ring passes' exact adjoint runs on the premultiplied-only state where the
+// medium's premultiplication is this well conditioned (the normal-stress block's
+// eigenvalue ratio; every density and shear plane positive): its stepper needs no
+// inverse, but the block imaging recovers the raw decimated fields with one, at
+// a cost of a few float roundings times this ratio.
+constexpr double kPremCondMax = 100.0;
+
+static int premultipliedAdjoint(Context* c, bool& use) {
+  use = false;
+  if (!c->premMode || c->loader < 2 || c->d.nz % 4 != 0 || !c->haveMedium) return E3D_OK;
+  if (c->premCond < 0) {
+    if (!c->posFlag) E3D_RET(devAlloc(c, (void**)&c->posFlag, sizeof(unsigned)));
+    E3D_CUDA_TRY(cudaMemsetAsync(c->posFlag, 0, sizeof(unsigned), c->st));
+    StepPtrs p{};
+    for (int k = 0; k < NMED; k++) p.m[k] = c->med[k];
+    c->launches++;
+    kPremultiplyCondition<<<c->numSMs * 4, 256, 0, c->st>>>(p, c->g, c->posFlag);
+    E3D_LAUNCH_CHECK();
+    unsigned bits = 0;
+    E3D_CUDA_TRY(cudaMemcpyAsync(&bits, c->posFlag, sizeof(unsigned), cudaMemcpyDeviceToHost, c->st));
+    E3D_CUDA_TRY(cudaStreamSynchronize(c->st));
+    float cond;
+    std::memcpy(&cond, &bits, sizeof(float));
+    c->premCond = std::isfinite(cond) ? (double)cond : 1e30;
+  }
+  use = c->premCond <= kPremCondMax;
+  return E3D_OK;
+}
+
+int setPremultipliedAdjoint(Context* c, int on) {
+  E3D_ARG(c && (on == 0 || on == 1), "bad adjoint state mode");
+  c->premMode = on;
+  return E3D_OK;
+}
+
 static Fields9& ringAt(std::vector<Fields9>& r, long long m) {
   const long long R = (long long)r.size();
   return r[(size_t)(((m % R) + R) % R)];
@@ -1360,8 +1436,10 @@ static int launchDecimate(Context* c, long long mEnd, float* vLeft, int leftMode
 // Adjoint imaging of block its from the adjoint ring; the block's last fine
 // level (it2 = 0) is mEnd, so level it2 is mEnd - it2.  v[0..3] = V(its-1..its+2).
 static int launchImagingBlock(Context* c, long long mEnd, float* const v[4], bool carryIn, bool leftImage,
-                              Fields9& carry) {
+                              Fields9& carry, bool prem) {
   ImagingBlockPtrs q{};
+  q.prem = prem ? 1 : 0;
+  for (int k = 0; k < NMED; k++) q.med[k] = c->med[k];
   const int sub = c->d.sub;
   q.nlev = sub;
   // in the order the fine steps ran (it2 = sub-1 first), as the fused decimation summed them
@@ -1522,7 +1600,8 @@ static double pendingAdjointBytes(const Context* c) {
     if (!c->w0.p[0]) b += 18 * f;
     if (!c->ss[0].p[0]) b += 18 * f;
   }
-  if (!c->q0.p[0] && c->loader >= 2) b += 18 * f;
+  const bool prem = R && c->premMode && c->premCond >= 0 && c->premCond <= kPremCondMax;
+  if (!c->q0.p[0] && c->loader >= 2 && !prem) b += 18 * f;
   return b;
 }
 
@@ -1969,6 +2048,10 @@ static int sourcePassRing(Context* c, const DevSignals& srcSet, const DevSignals
   c->tailValid = false;
   // the ring is allocated before the plan, so that the free memory the plan sees excludes it
   E3D_RET(ensureRing(c, c->srcRing, c->s0, c->s1, ringLevels(c)));
+  {
+    bool prem = false;  // known before the plan, which then leaves out the dual state's levels
+    E3D_RET(premultipliedAdjoint(c, prem));
+  }
   E3D_RET(prepareCheckpoints(c, L, nseg));
   const int nts = c->d.nts, sub = c->d.sub, blocks = nts - 1;
   const size_t nr = recSet ? (size_t)recSet->off[NCOMP] : 0;
@@ -2047,7 +2130,12 @@ static int adjointPassRing(Context* c, const DevSignals& srcSet, const DevSignal
   Fields9& carry = c->ss[0];
   E3D_RET(allocFields(c, carry, true));  // L of the block after the last one: zero
   const bool dual = c->loader >= 2 && c->d.nz % 4 == 0;
-  if (dual) {
+  // the premultiplied-only state: the ring holds premultiplied levels and no raw level is kept
+  bool prem = false;
+  const int ncn = recSet.off[SXX + 1] - recSet.off[SXX];
+  if (dual && !srcAdj && recSet.off[SYY + 1] - recSet.off[SYY] == ncn && recSet.off[SZZ + 1] - recSet.off[SZZ] == ncn)
+    E3D_RET(premultipliedAdjoint(c, prem));
+  if (dual && !prem) {
     E3D_RET(allocFields(c, c->q0, true));
     E3D_RET(allocFields(c, c->q1, true));
   }
@@ -2125,7 +2213,9 @@ static int adjointPassRing(Context* c, const DevSignals& srcSet, const DevSignal
       if (map) E3D_RET(traceSpread(c, *map, (int)nr, resid + (size_t)its * rows, c->traceRing + (its % 2) * nr));
       for (int it2 = sub - 1; it2 >= 0; it2--) {
         StepPtrs p = makeRingStep(c, W(ma - 1), W(ma), W(ma + 1));
-        if (dual) {
+        if (prem) {
+          p.prem = 1;
+        } else if (dual) {
           for (int k = 0; k < NCOMP; k++) {
             p.c[k] = c->q1.p[k];
             p.oP[k] = c->q0.p[k];
@@ -2133,16 +2223,17 @@ static int adjointPassRing(Context* c, const DevSignals& srcSet, const DevSignal
         }
         E3D_RET(launchStep(c, STEP_ADJ_EXACT, p));
         const StepPtrs q = afterStep(p);
-        if (dual) E3D_RET(launchInjectRefresh(c, q, recSet, dataSlice(its), dataSlice(its + 1), it2 + 1));
+        if (prem) E3D_RET(launchInjectPremultiplied(c, q, recSet, dataSlice(its), dataSlice(its + 1), it2 + 1));
+        else if (dual) E3D_RET(launchInjectRefresh(c, q, recSet, dataSlice(its), dataSlice(its + 1), it2 + 1));
         else E3D_RET(launchInjectSlices(c, q, recSet, dataSlice(its), dataSlice(its + 1), it2 + 1));
         // transpose of the source injection of forward step (its, it2+1): the exact
         // adjoint of the nonlinear propagation with respect to the scaled source signals
         if (srcAdj) E3D_RET(launchExtractSource(c, q, srcSet, srcAdj, its, it2));
         ma++;
-        if (dual) swapF(c->q0, c->q1);
+        if (dual && !prem) swapF(c->q0, c->q1);
       }
       float* const v[4] = {leftImage ? V(its - 1) : nullptr, V(its), V(its + 1), V(its + 2)};
-      E3D_RET(launchImagingBlock(c, ma, v, its == bEnd - 1, leftImage, carry));
+      E3D_RET(launchImagingBlock(c, ma, v, its == bEnd - 1, leftImage, carry, prem));
     }
   }
   // final imaging at t = 0: the carried left part of block 0

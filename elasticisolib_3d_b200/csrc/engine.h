@@ -109,6 +109,9 @@ int checkpointType(const Context* c);
 int setDecimationRing(Context* c, int on);
 // y chunks of the y-marching block imaging launch (0: automatic).
 int setImagingChunks(Context* c, int chunks);
+// Exact adjoint of the ring passes: 1 (default) the premultiplied-only state where the
+// medium allows it, 0 always the dual raw + premultiplied state.
+int setPremultipliedAdjoint(Context* c, int on);
 
 // Allocation-free nonlinear propagation on the current device: the wavefield
 // levels and the taper live in a fixed 64 MiB device array (staticWorkBytes());

@@ -38,6 +38,8 @@ struct StepPtrs {
   // mode 2 with a dual state: c[] holds the medium-premultiplied current level
   // and the step also writes the premultiplied new level here (may be null)
   float* oP[NCOMP];
+  // mode 2, host side: 1 selects the premultiplied-only state (kStepTma<2,...,PREM>)
+  int prem;
 };
 
 // A "device set" concatenates the regular-grid points of the nine
@@ -487,7 +489,13 @@ __device__ __forceinline__ void tmaIssuePlane(const TmaMaps& mp, float* st, unsi
   for (int k = 0; k < NMED; k++) tmaLoad3d(st + L::MED_OFF + k * L::INT_F, &mp.med[k], z0, x0, y, bar);
 }
 
-template <int MODE, int TX, int STAGES>
+// PREM (mode 2 only): the state is the premultiplied level alone.  With P = M a
+// (M the pointwise, linear premultiplication), the dual update
+// a_new = G (G a_old + up), P_new = M a_new is P_new = G (G P_old + M up): old
+// and current levels are premultiplied, the update's terms are premultiplied
+// like the forward stepper's, and no raw level is read or written (140 B per
+// cell instead of the dual state's 176).
+template <int MODE, int TX, int STAGES, bool PREM = false>
 __global__ void __launch_bounds__(TZ * TX) kStepTma(const __grid_constant__ TmaMaps mp, StepPtrs p, GridConst g,
                                                      int yChunk) {
   using L = PipeLayout<TX>;
@@ -616,6 +624,12 @@ __global__ void __launch_bounds__(TZ * TX) kStepTma(const __grid_constant__ TmaM
       // = taper[min(dzx, dyy)] when that distance is below minPad, else 1
       const float G = dyy < dzx ? Gy : Gzx;
       float nv[NCOMP];
+      if (PREM) {
+        float mup[NCOMP];
+        premultiply(up, rhox, rhoy, rhoz, l2m, lam, muxz, muxy, muyz, mup);
+#pragma unroll
+        for (int k = 0; k < NCOMP; k++) up[k] = mup[k];
+      }
 #pragma unroll
       for (int k = 0; k < NCOMP; k++) {
         float v = G * ov[k * L::INT_F] + up[k];
@@ -631,7 +645,7 @@ __global__ void __launch_bounds__(TZ * TX) kStepTma(const __grid_constant__ TmaM
           if (hasR) p.accR[k][ic] = preR[k] + nv[k] * p.accWr;
         }
       }
-      if (MODE == STEP_ADJ_EXACT) {
+      if (MODE == STEP_ADJ_EXACT && !PREM) {
         float q[NCOMP];
         premultiply(nv, rhox, rhoy, rhoz, l2m, lam, muxz, muxy, muyz, q);
 #pragma unroll
@@ -924,6 +938,67 @@ __global__ void kInjectRefresh(StepPtrs p, GridConst g, SparseSet s, const float
   p.o[k][i] = v;
   const int med = k == VX ? RHOX : k == VY ? RHOY : k == VZ ? RHOZ : k == SXZ ? MUXZ : k == SXY ? MUXY : MUYZ;
   p.oP[k][i] = v * __ldg(p.m[med] + i);
+}
+
+// Injection into a premultiplied-only state (kStepTma<2,...,PREM>): the raw
+// increment G*(sigL*wl + sigR*wr) of each component enters premultiplied,
+// P += M * add, the normal stresses together as in kInjectRefresh.
+__global__ void kInjectPremultiplied(StepPtrs p, GridConst g, SparseSet s, const float* sigL, const float* sigR,
+                                     float wl, float wr) {
+  const int ntot = s.off[NCOMP];
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= ntot) return;
+  int k = 0;
+#pragma unroll
+  for (int c = 1; c < NCOMP; c++) k += (j >= s.off[c]);
+  if (k == SYY || k == SZZ) return;
+  const long long i = s.pos[j];
+  const int iz = (int)(i % g.nz);
+  const int ix = (int)((i / g.nz) % g.nx);
+  const int iy = (int)(i / g.yStride);
+  const float G = taperAt(g, iz, ix, iy);
+  if (k == SXX) {
+    const int r = j - s.off[SXX];
+    float a[3];
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      const int jj = s.off[SXX + c] + r;
+      a[c] = G * (sigL[jj] * wl + sigR[jj] * wr);
+    }
+    const float l2m = __ldg(p.m[L2M] + i), lam = __ldg(p.m[LAM] + i);
+    p.o[SXX][i] += a[0] * l2m + (a[1] + a[2]) * lam;
+    p.o[SYY][i] += a[1] * l2m + (a[0] + a[2]) * lam;
+    p.o[SZZ][i] += a[2] * l2m + (a[0] + a[1]) * lam;
+    return;
+  }
+  const float add = G * (sigL[j] * wl + sigR[j] * wr);
+  const int med = k == VX ? RHOX : k == VY ? RHOY : k == VZ ? RHOZ : k == SXZ ? MUXZ : k == SXY ? MUXY : MUYZ;
+  p.o[k][i] += add * __ldg(p.m[med] + i);
+}
+
+// Largest condition number of the normal-stress block of the premultiplication
+// over the updated cells, as the bits of a non-negative float (for atomicMax);
+// a cell whose block or shear, density planes are not positive counts as +inf.
+__global__ void kPremultiplyCondition(StepPtrs p, GridConst g, unsigned* out) {
+  const float* const* m = p.m;
+  const long long ncell = g.n;
+  float worst = 0.0f;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < ncell;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int iz = (int)(i % g.nz);
+    const int ix = (int)((i / g.nz) % g.nx);
+    const int iy = (int)(i / g.yStride);
+    if (iz < FAT || iz >= g.nz - FAT || ix < FAT || ix >= g.nx - FAT || iy < FAT || iy >= g.ny - FAT) continue;
+    const float a = __ldg(m[L2M] + i), b = __ldg(m[LAM] + i);
+    const float e1 = a - b, e2 = a + 2.0f * b;
+    float c = (e1 > 0.0f && e2 > 0.0f) ? fmaxf(e1, e2) / fminf(e1, e2) : INFINITY;
+    if (!(__ldg(m[RHOX] + i) > 0.0f && __ldg(m[RHOY] + i) > 0.0f && __ldg(m[RHOZ] + i) > 0.0f &&
+          __ldg(m[MUXZ] + i) > 0.0f && __ldg(m[MUXY] + i) > 0.0f && __ldg(m[MUYZ] + i) > 0.0f))
+      c = INFINITY;
+    worst = fmaxf(worst, c);
+  }
+  for (int o = 16; o > 0; o >>= 1) worst = fmaxf(worst, __shfl_xor_sync(0xffffffffu, worst, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(out, __float_as_uint(worst));
 }
 
 // ---------------------------------------------------------------------------
@@ -1526,7 +1601,60 @@ struct ImagingBlockPtrs {
   float* pert[NMED];
   float dtsInv;
   int q3compat;
+  int prem;                // the levels are premultiplied: the sums are converted back to raw values
+  const float* med[NMED];  // medium planes (prem)
 };
+
+// Decimated sums of one block from its levels: L (coarse sample its) and R (its+1), raw values,
+// R including the carried left part of the block after it when carryIn.
+__device__ __forceinline__ void blockSums(const ImagingBlockPtrs& q, long long ic, float* L, float* R) {
+#pragma unroll
+  for (int k = 0; k < NCOMP; k++) {
+    L[k] = 0.f;
+    R[k] = 0.f;
+  }
+  for (int j = 0; j < q.nlev; j++) {
+    const float wl = q.wl[j], wr = q.wr[j];
+#pragma unroll
+    for (int k = 0; k < NCOMP; k++) {
+      const float a = __ldg(q.lev[j][k] + ic);
+      L[k] = fmaf(a, wl, L[k]);
+      R[k] = fmaf(a, wr, R[k]);
+    }
+  }
+  if (q.prem) {
+    // both sums back to raw values: the inverse of premultiply.  The normal stresses invert the
+    // block [[a,b,b],[b,a,b],[b,b,a]] (a = lambda+2mu, b = lambda, scaled), whose inverse is
+    // [[a+b,-b,-b],[-b,a+b,-b],[-b,-b,a+b]] / ((a-b)(a+2b)); the other components divide by their
+    // own plane.  The reciprocals are taken once for both sums.
+    float md[NMED];
+#pragma unroll
+    for (int k = 0; k < NMED; k++) md[k] = __ldg(q.med[k] + ic);
+    const float r[6] = {__frcp_rn(md[RHOX]), __frcp_rn(md[RHOY]), __frcp_rn(md[RHOZ]),
+                        __frcp_rn(md[MUXZ]), __frcp_rn(md[MUXY]), __frcp_rn(md[MUYZ])};
+    const float det = __frcp_rn((md[L2M] - md[LAM]) * (md[L2M] + 2.0f * md[LAM]));
+    const float apb = md[L2M] + md[LAM], lam = md[LAM];
+    float* const sums[2] = {L, R};
+#pragma unroll
+    for (int s = 0; s < 2; s++) {
+      float* v = sums[s];
+      const float xx = v[SXX], yy = v[SYY], zz = v[SZZ];
+      v[VX] *= r[0];
+      v[VY] *= r[1];
+      v[VZ] *= r[2];
+      v[SXX] = (apb * xx - lam * (yy + zz)) * det;
+      v[SYY] = (apb * yy - lam * (xx + zz)) * det;
+      v[SZZ] = (apb * zz - lam * (xx + yy)) * det;
+      v[SXZ] *= r[3];
+      v[SXY] *= r[4];
+      v[SYZ] *= r[5];
+    }
+  }
+  if (q.carryIn) {
+#pragma unroll
+    for (int k = 0; k < NCOMP; k++) R[k] += q.carry[k][ic];
+  }
+}
 
 __global__ void __launch_bounds__(256) kImagingBlock(ImagingBlockPtrs q, GridConst g) {
   const int iz = FAT + blockIdx.x * blockDim.x + threadIdx.x;
@@ -1535,20 +1663,7 @@ __global__ void __launch_bounds__(256) kImagingBlock(ImagingBlockPtrs q, GridCon
   if (iz >= g.nz - FAT || ix >= g.nx - FAT) return;
   const long long i = (long long)iy * g.yStride + (long long)ix * g.nz + iz;
   float L[NCOMP], R[NCOMP];
-#pragma unroll
-  for (int k = 0; k < NCOMP; k++) {
-    L[k] = 0.f;
-    R[k] = q.carryIn ? q.carry[k][i] : 0.f;
-  }
-  for (int t = 0; t < q.nlev; t++) {
-    const float wl = q.wl[t], wr = q.wr[t];
-#pragma unroll
-    for (int k = 0; k < NCOMP; k++) {
-      const float a = __ldg(q.lev[t][k] + i);
-      L[k] = fmaf(a, wl, L[k]);
-      R[k] = fmaf(a, wr, R[k]);
-    }
-  }
+  blockSums(q, i, L, R);
   float acc[NMED];
   {
     const VelTerms t1 = velTerms(q.v[1], q.v[2], q.v[3], i, g, q.dtsInv, q.q3compat);
@@ -1661,20 +1776,7 @@ __global__ void __launch_bounds__(TZ * IMG_TX) kImagingTma(const __grid_constant
     // coalesced per-cell loads, issued ahead of the wait
     float L[NCOMP], R[NCOMP], pv[NMED], nxt[3], prv[3], cur0[3];
     if (active) {
-#pragma unroll
-      for (int k = 0; k < NCOMP; k++) {
-        L[k] = 0.f;
-        R[k] = q.carryIn ? q.carry[k][ic] : 0.f;
-      }
-      for (int j = 0; j < q.nlev; j++) {
-        const float wl = q.wl[j], wr = q.wr[j];
-#pragma unroll
-        for (int k = 0; k < NCOMP; k++) {
-          const float a = __ldg(q.lev[j][k] + ic);
-          L[k] = fmaf(a, wl, L[k]);
-          R[k] = fmaf(a, wr, R[k]);
-        }
-      }
+      blockSums(q, ic, L, R);
 #pragma unroll
       for (int k = 0; k < 3; k++) {
         nxt[k] = q.v[3][k] ? __ldg(q.v[3][k] + ic) : 0.f;                        // V(its+2)

@@ -179,7 +179,8 @@ class Propagator:
 
     def kernel_timing_read(self, mode):
         """(mean ms, count) of the sampled launches of one kind since the last read: stepper modes 0..2,
-        the same with a fused decimation or secondary source 3..5, block imaging 6, velocity decimation 7."""
+        the same with a fused decimation or secondary source 3..5, block imaging 6, velocity decimation 7,
+        the exact adjoint on the premultiplied-only state 8."""
         avg = ctypes.c_double(0)
         cnt = ctypes.c_longlong(0)
         N.call("e3d_kernel_timing_read", self._h, int(mode), ctypes.byref(avg), ctypes.byref(cnt))
@@ -240,6 +241,11 @@ class Propagator:
         """Gradient passes: decimate fine levels from a ring once per coarse block (True, default) or
         through accumulators at every fine step (False)."""
         N.call("e3d_set_decimation_ring", self._h, 1 if on else 0)
+
+    def set_premultiplied_adjoint(self, on=True):
+        """Exact adjoint of the gradient passes on the premultiplied-only state where the medium
+        allows it (True, default), or always on the dual raw + premultiplied state (False)."""
+        N.call("e3d_set_premultiplied_adjoint", self._h, 1 if on else 0)
 
     def set_imaging_chunks(self, chunks=0):
         """y chunks of the block imaging launch (0 = automatic)."""

@@ -258,14 +258,16 @@ class FwiProblem:
     """One propagation grid, its context and shots; shared by forward modelling and gradients."""
 
     def __init__(self, fd: H.FdParam, device="cuda", ckpt="auto", segment=0, variant=(8, 3, "split-fwd"),
-                 velocity="auto", q3compat=1, source_term=False, decimation_ring=True):
+                 velocity="auto", q3compat=1, source_term=False, decimation_ring=True, premultiplied=True):
         """q3compat=1 keeps the reference's Born yz shear term (the xz derivative pair, quirk Q3);
         0 uses the yz pair, the linearisation of the propagator's own yz stress update.
         source_term=True adds the misfit's derivative through the medium scaling of the source
         signals (the exact adjoint sampled at the source points, chained through medium_planes and
         scale_sources by autograd), which the reference's Born-adjoint gradient leaves out.
         decimation_ring=True decimates the fine levels of each coarse block from a ring of levels in
-        one launch per block; False fuses two coarse accumulators into every fine step."""
+        one launch per block; False fuses two coarse accumulators into every fine step.
+        premultiplied=True runs the ring passes' exact adjoint on the premultiplied-only state where
+        the medium allows it; False keeps the dual raw + premultiplied state."""
         if getattr(fd, "freeSurface", 0):
             raise ValueError("FWI gradients with a free surface are not supported (no exact adjoint of it)")
         self.fd = fd
@@ -281,6 +283,7 @@ class FwiProblem:
         self.prop.set_checkpoint_policy(ckpt, segment)
         self.prop.set_velocity_storage(velocity)
         self.prop.set_decimation_ring(decimation_ring)
+        self.prop.set_premultiplied_adjoint(premultiplied)
         self.ckpt, self.segment = ckpt, segment
         self.source_term = source_term
         self.auto_budget = segment == 0

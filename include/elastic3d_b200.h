@@ -281,6 +281,15 @@ int e3d_set_decimation_ring(e3d_context* ctx, int on);
 /* y chunks of the block imaging launch of the decimation ring (0 = automatic:
  * the rule of the stepper grids).  A tuning knob; no counterpart in the reference. */
 int e3d_set_imaging_chunks(e3d_context* ctx, int chunks);
+/* State of the exact adjoint (the transpose of stepFwdGpu_3D's update, as
+ * stepAdjGpuBorn_3D, kernelsElaGpu_3D.cu:825-1177) in the checkpointed passes
+ * with a decimation ring.  on = 1 (default): where the medium allows it -- all
+ * density and shear planes positive and the normal-stress block of the
+ * premultiplication conditioned within 100 -- only the medium-premultiplied
+ * levels are stored (140 B per cell and step), the raw old level being
+ * recovered from them at each step; otherwise, and with on = 0, the raw and
+ * the premultiplied levels both (176 B).  The choice is made per medium. */
+int e3d_set_premultiplied_adjoint(e3d_context* ctx, int on);
 /* The checkpoint schedule of a record of `blocks` coarse blocks (nts - 1) cut
  * into segments of `segment_len` blocks, as the checkpointed passes run it:
  * returns the segment count nseg, or -E3D_ERR_ARG.  seg_start (room for
@@ -407,16 +416,18 @@ int e3d_kernel_timing(e3d_context* ctx, int every);
  * the previous read (waits for them to finish).  mode 0..2: bare steps of that
  * stepper mode; 3..5: the same modes with a fused decimation into coarse
  * accumulators or a fused Born secondary source; 6: the block imaging of the
- * decimation ring; 7: its source-velocity decimation. */
+ * decimation ring; 7: its source-velocity decimation; 8: the exact adjoint on
+ * the premultiplied-only state. */
 int e3d_kernel_timing_read(e3d_context* ctx, int mode, double* avg_ms, long long* count);
 /* Number of kernel launches this context has issued. */
 long long e3d_launch_count(const e3d_context* ctx);
 
-/* Bare stepper (mode 0 forward, 1 time-reversed, 2 exact transpose) applied
- * n_steps times to the context's working wavefields; for benchmarking.
- * Modes 3..5 run modes 0..2 with the new level decimated into two coarse
- * accumulators (3 velocity fields for modes 3 and 4, all 9 fields for 5), as
- * the FWI gradient's source recompute and adjoint passes do. */
+/* Bare stepper (mode 0 forward, 1 time-reversed, 2 exact transpose on the dual
+ * state) applied n_steps times to the context's working wavefields; for
+ * benchmarking.  Modes 3..5 run modes 0..2 with the new level decimated into
+ * two coarse accumulators (3 velocity fields for modes 3 and 4, all 9 fields for
+ * 5), as the fused-accumulator passes do; mode 6 runs mode 2 on the
+ * premultiplied-only state. */
 int e3d_step_only(e3d_context* ctx, int mode, int n_steps);
 
 /* ------------------------------------------------------------------------

@@ -12,9 +12,10 @@ from elasticisolib_3d_b200.engine import COMP_GRID
 pytestmark = pytest.mark.gpu
 
 
-def _problem(sv, ckpt="fp32", segment=0, variant=(8, 2, "tma"), velocity="auto", ring=True):
+def _problem(sv, ckpt="fp32", segment=0, variant=(8, 2, "tma"), velocity="auto", ring=True, prem=True):
     fd = H.FdParam(sv.elastic, sv.axes, sv.par)
-    prob = F.FwiProblem(fd, ckpt=ckpt, segment=segment, variant=variant, velocity=velocity, decimation_ring=ring)
+    prob = F.FwiProblem(fd, ckpt=ckpt, segment=segment, variant=variant, velocity=velocity, decimation_ring=ring,
+                        premultiplied=prem)
     ax7 = H.grid_axes(*(a.n for a in sv.axes), *(a.o for a in sv.axes), *(a.d for a in sv.axes))
     src = H.build_devices(*sv.src_xyz[0], ax7, fd.nts, sv.par)
     rec = H.build_devices(*sv.rec_xyz, ax7, fd.nts, sv.par)
@@ -90,6 +91,51 @@ def test_ring_decimation_matches_fused_accumulators(ckpt, segment, variant, velo
         err = float(np.linalg.norm(grads[1][k] - grads[0][k]) / np.linalg.norm(grads[0][k]))
         print(f"ring vs fused, plan {ckpt}/{velocity} segment {segment} {variant[2]}: component {k} {err:.2e}")
         assert err < 1e-5, (k, err)
+
+
+@pytest.mark.parametrize("ckpt,segment,velocity", [("fp32", 0, "fp32"), ("fp16", 3, "fp16")])
+def test_premultiplied_only_adjoint_matches_dual_state(ckpt, segment, velocity):
+    """The ring adjoint on the premultiplied-only state (raw old level recovered from the
+    premultiplied one at each step) against the dual raw + premultiplied state: the same
+    arithmetic up to the recovery's roundings, relative 1e-5."""
+    sv, true = survey()
+    orc = OracleFwi(sv)
+    d_obs, _ = orc.data(true)
+    grads = []
+    for prem in (False, True):
+        prob, src, rec = _problem(sv, ckpt, segment, (8, 3, "split-fwd"), velocity, True, prem)
+        prob.shots.append(F.make_shot(src, rec, explosive(sv.par.getInt("nts"), sv.wavelet),
+                                      d_obs.astype(np.float32), "cuda"))
+        m = [torch.tensor(sv.elastic[k], device="cuda", requires_grad=True) for k in range(3)]
+        F.ElasticFwiMisfit.apply(m[0], m[1], m[2], prob).backward()
+        grads.append(np.stack([x.grad.double().cpu().numpy() for x in m]))
+    for k in range(3):
+        err = float(np.linalg.norm(grads[1][k] - grads[0][k]) / np.linalg.norm(grads[0][k]))
+        print(f"premultiplied-only vs dual state, {ckpt}/{velocity} segment {segment}: component {k} {err:.2e}")
+        assert err < 1e-5, (k, err)
+
+
+def test_fluid_layer_keeps_the_dual_state_and_matches_fp64_oracle():
+    """A fluid layer (mu = 0) makes the premultiplication singular there, so the adjoint pass keeps
+    the dual raw + premultiplied state; the gradient still matches the FP64 oracle (1e-3)."""
+    sv, true = survey()
+    for el in (sv.elastic, true):
+        el[2, :, :, 10:14] = 0.0          # four fluid rows (shear modulus zero) below the sources
+    orc = OracleFwi(sv)
+    d_obs, _ = orc.data(true)
+    loss_ref, g_ref = orc.misfit_and_gradient(sv.elastic, d_obs)
+    prob, src, rec = _problem(sv, "fp32", 0, (8, 3, "split-fwd"), "fp32")
+    prob.shots.append(F.make_shot(src, rec, explosive(sv.par.getInt("nts"), sv.wavelet), d_obs.astype(np.float32),
+                                  "cuda"))
+    m = [torch.tensor(sv.elastic[k], device="cuda", requires_grad=True) for k in range(3)]
+    loss = F.ElasticFwiMisfit.apply(m[0], m[1], m[2], prob)
+    loss.backward()
+    assert abs(loss.item() - loss_ref) / loss_ref < 1e-4
+    for k in range(3):
+        g = m[k].grad.double().cpu().numpy()
+        err = float(np.linalg.norm(g - g_ref[k]) / np.linalg.norm(g_ref[k]))
+        print(f"fluid layer: gradient component {k} vs FP64 oracle {err:.2e}")
+        assert err < 1e-3, (k, err)
 
 
 def test_predicted_traces_match_fp64_oracle():
