@@ -47,9 +47,9 @@ UNIT = "shots/s"
 # updated cell (fp32 fields):
 #   0 forward stepper: read old 9 + current 9 + medium 8, write new 9 = 140 B (the forward pass
 #     and the source recompute, whose fine levels go to a ring of sub+1 levels)
-#   8 exact-adjoint stepper on the premultiplied-only state: read old 9 + current 9 (both
-#     premultiplied) + medium 8, write new 9 = 140 B (where the medium's premultiplication is
-#     well conditioned)
+#   1 exact-adjoint stepper on the premultiplied-only state (the time-reversed stepper on
+#     premultiplied levels): read old 9 + current 9 (both premultiplied) + medium 8, write new 9
+#     = 140 B (where the medium's premultiplication is well conditioned)
 #   2 the same on the dual state (raw + premultiplied levels): read old raw 9, current
 #     premultiplied 9, medium 8, write new raw 9 and new premultiplied 9 = 176 B
 #   6 block imaging, once per coarse block: read the sub adjoint levels (sub*36 B), V(t-1..t+2)
@@ -60,17 +60,17 @@ UNIT = "shots/s"
 #   with --decimation acc: 3 = forward + 3-field accumulators (188 B), 5 = dual adjoint + 9-field
 #     accumulators (320 B)
 KIND_NAMES = {0: "forward stepper (kStepSplit<0,3,3>: velocity and stress CTA roles)",
-              8: "exact-adjoint stepper, premultiplied-only state (kStepTma<2,8,2,PREM>)",
+              1: "exact-adjoint stepper on premultiplied levels (kStepSplit<1,3,3>, the time-reversed update on P)",
               2: "dual-state exact-adjoint stepper (kStepTma<2,8,2>)",
               6: "block imaging from the adjoint ring (kImagingTma)", 7: "source-velocity decimation (kDecimateVelocity)",
               3: "forward stepper + 3-field decimation accumulators", 5: "dual adjoint stepper + 9-field accumulators"}
 PROFILE = {0: "profiles/kStepSplit_forward_392x392x104.txt", 2: "profiles/kStepTma_adjoint_dual_392x392x104.txt",
-           8: "profiles/kStepTma_adjoint_premultiplied_392x392x104.txt",
+           1: "profiles/kStepSplit_adjoint_premultiplied_392x392x104.txt",
            6: "profiles/kImagingTma_392x392x104.txt"}
 
 
 def kind_bytes(kind, sub, prem=False):
-    return {0: 140.0, 8: 140.0, 2: 176.0, 6: sub * 36.0 + 48.0 + 64.0 + (32.0 if prem else 0.0), 7: sub * 12.0 + 36.0,
+    return {0: 140.0, 1: 140.0, 2: 176.0, 6: sub * 36.0 + 48.0 + 64.0 + (32.0 if prem else 0.0), 7: sub * 12.0 + 36.0,
             3: 188.0, 5: 320.0}[kind]
 
 
@@ -393,8 +393,8 @@ def run_ours(args):
         cell_updates = cells * (steps_per_pass + recompute_blocks * fd.sub + steps_per_pass)
         ring = args.decimation == "ring"
         # launches of each kind in one gradient
-        prem = sampled.get(8, (0, 0))[1] > 0
-        per_step = ({0: steps_per_pass + recompute_blocks * fd.sub, (8 if prem else 2): steps_per_pass, 6: blocks,
+        prem = sampled.get(1, (0, 0))[1] > 0
+        per_step = ({0: steps_per_pass + recompute_blocks * fd.sub, (1 if prem else 2): steps_per_pass, 6: blocks,
                      7: recompute_blocks + seg + 1} if ring else
                     {0: max(blocks - seg - 1, 0) * fd.sub, 3: (min(seg + 1, blocks) + recompute_blocks) * fd.sub,
                      5: steps_per_pass})

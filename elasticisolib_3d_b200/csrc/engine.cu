@@ -123,7 +123,7 @@ struct Context {
   // launch accounting and sampled stepper timing
   long long launches = 0;
   int timingEvery = 0;       // 0: off; n: time every n-th stepper launch
-  long long kindCounter[9] = {};
+  long long kindCounter[8] = {};
   std::vector<cudaEvent_t> evPool;
   struct Timed { int mode; cudaEvent_t a, b; };
   std::vector<Timed> timed;
@@ -474,17 +474,6 @@ static int launchTma(Context* c, const StepPtrs& p, dim3 grid, int yChunk) {
   return E3D_OK;
 }
 
-// The exact adjoint on the premultiplied-only state (8-wide tiles, two stages).
-static int launchTmaPrem(Context* c, const StepPtrs& p, dim3 grid, int yChunk) {
-  constexpr size_t smem = (size_t)2 * PipeLayout<8>::STAGE_F * sizeof(float);
-  static std::atomic<unsigned long long> configured{0};
-  E3D_RET(ensureSmemAttr((const void*)kStepTma<STEP_ADJ_EXACT, 8, 2, true>, smem, configured));
-  TmaMaps mp;
-  E3D_RET(buildMaps<8>(c, p, mp));
-  kStepTma<STEP_ADJ_EXACT, 8, 2, true><<<grid, dim3(TZ, 8), smem, c->st>>>(mp, p, c->g, yChunk);
-  return E3D_OK;
-}
-
 static int chooseChunks(const Context* c, long long tiles, int nyi, int perSM = 2);
 
 // Split stepper: role V maps (stress halos and leads, old velocities, rho planes) and role S maps
@@ -597,8 +586,7 @@ static cudaEvent_t takeEvent(Context* c) {
 // Sampled launch timing: with sampling on, every n-th launch of each timed
 // kind is bracketed with CUDA events on the launching stream.  Kinds: stepper
 // modes 0..2, the same with a fused decimation or secondary source 3..5, the
-// block imaging of the decimation ring 6, its velocity decimation 7, the exact
-// adjoint on the premultiplied-only state 8.
+// block imaging of the decimation ring 6, its velocity decimation 7.
 struct TimedLaunch {
   Context* c;
   int kind;
@@ -626,7 +614,7 @@ static int launchStep(Context* c, int mode, const StepPtrs& p) {
   c->launches++;
   // launches that also fuse a decimation or a secondary source are kept apart (mode + 3)
   const bool fused = p.accL[0] != nullptr || p.ssL[0] != nullptr;
-  TimedLaunch t(c, p.prem ? 8 : mode + (fused ? 3 : 0));
+  TimedLaunch t(c, mode + (fused ? 3 : 0));
   return launchStepRaw(c, mode, p);
 }
 
@@ -639,7 +627,7 @@ int setKernelTiming(Context* c, int every) {
 
 int readKernelTiming(Context* c, int mode, double* avgMs, long long* count) {
   E3D_ARG(c && avgMs && count, "null argument");
-  E3D_ARG(mode >= 0 && mode < 9, "bad timed kind");
+  E3D_ARG(mode >= 0 && mode < 8, "bad timed kind");
   double sum = 0;
   long long n = 0;
   std::vector<Context::Timed> keep;
@@ -694,11 +682,11 @@ static int launchStepRaw(Context* c, int mode, const StepPtrs& p) {
   // from 0.54 to 0.67 of the copy bandwidth (10 chunks instead of 2); at 392^3
   // it keeps the long runs.
   int chunks = chooseChunks(c, tiles, nyi);
-  const bool dual = mode == STEP_ADJ_EXACT && (p.oP[0] != nullptr || p.prem);
+  const bool dual = mode == STEP_ADJ_EXACT && p.oP[0] != nullptr;
   // the split stepper (loader 6; loader 7: all but the exact adjoint, which keeps kStepTma) takes
   // every step without a fused decimation or secondary source
   if ((c->loader == 6 || (c->loader == 7 && mode != STEP_ADJ_EXACT)) && g.nz % 4 == 0 && p.accL[0] == nullptr &&
-      p.ssL[0] == nullptr && !p.prem) {
+      p.ssL[0] == nullptr) {
     const int tixS = (g.nx - 2 * FAT + 7) / 8;
     if (mode == STEP_FWD) E3D_RET(launchSplitVariant<STEP_FWD>(c, p, tiz, tixS, nyi));
     else if (mode == STEP_ADJ_REVERSED) E3D_RET(launchSplitVariant<STEP_ADJ_REVERSED>(c, p, tiz, tixS, nyi));
@@ -717,11 +705,7 @@ static int launchStepRaw(Context* c, int mode, const StepPtrs& p) {
   chunks = (nyi + yChunk - 1) / yChunk;
   dim3 grid(tiz, tix, chunks);
   const bool pipe = (g.nz % 4 == 0) && mode != STEP_ADJ_EXACT && c->loader > 0;
-  if (dual && p.prem) {
-    E3D_ARG(g.nz % 4 == 0 && p.accL[0] == nullptr && p.ssL[0] == nullptr,
-            "premultiplied-only adjoint needs nz % 4 == 0 and no fused decimation");
-    E3D_RET(launchTmaPrem(c, p, grid, yChunk));
-  } else if (dual) {
+  if (dual) {
     E3D_ARG(g.nz % 4 == 0, "dual-state adjoint needs nz % 4 == 0");
     if (c->tx == 16) E3D_RET((launchTma<STEP_ADJ_EXACT, 16, 2>(c, p, grid, yChunk)));
     else if (c->stages == 3 && c->loader < 6) E3D_RET((launchTma<STEP_ADJ_EXACT, 8, 3>(c, p, grid, yChunk)));
@@ -1212,15 +1196,13 @@ int nlPropagateHost(Context* c, bool adjoint, float* const* model, float* const*
 
 int stepOnly(Context* c, int mode, int nSteps) {
   E3D_ARG(c && c->haveMedium, "medium not set");
-  E3D_ARG(mode >= 0 && mode <= 6, "bad mode");
+  E3D_ARG(mode >= 0 && mode <= 5, "bad mode");
   // modes 3..5: modes 0..2 with the new level decimated into two coarse
   // accumulators, as the fused-accumulator passes run them (3 velocity fields for
-  // the source recompute, 9 fields for the adjoint); mode 6: mode 2 on the
-  // premultiplied-only state, as the ring adjoint pass runs it
-  const bool premOnly = mode == 6;
-  E3D_ARG(!premOnly || (c->loader >= 2 && c->d.nz % 4 == 0), "mode 6 needs a TMA loader and nz % 4 == 0");
-  const bool fused = mode >= 3 && !premOnly;
-  const int m = premOnly ? STEP_ADJ_EXACT : fused ? mode - 3 : mode;
+  // the source recompute, 9 fields for the adjoint).  The ring passes' exact
+  // adjoint on the premultiplied-only state is mode 1 on premultiplied levels.
+  const bool fused = mode >= 3;
+  const int m = fused ? mode - 3 : mode;
   E3D_RET(allocFields(c, c->w0, false));
   E3D_RET(allocFields(c, c->w1, false));
   if (fused) {
@@ -1228,14 +1210,13 @@ int stepOnly(Context* c, int mode, int nSteps) {
     E3D_RET(allocFields(c, c->ss[1], true));
   }
   // the exact adjoint runs on the dual state, as in the adjoint pass, with the TMA loader
-  const bool dual = m == STEP_ADJ_EXACT && c->loader >= 2 && c->d.nz % 4 == 0 && !premOnly;
+  const bool dual = m == STEP_ADJ_EXACT && c->loader >= 2 && c->d.nz % 4 == 0;
   if (dual) {
     E3D_RET(allocFields(c, c->q0, false));
     E3D_RET(allocFields(c, c->q1, false));
   }
   for (int i = 0; i < nSteps; i++) {
     StepPtrs p = makeStep(c, c->w0, c->w1);
-    p.prem = premOnly ? 1 : 0;
     if (dual)
       for (int k = 0; k < NCOMP; k++) {
         p.c[k] = c->q1.p[k];
@@ -2213,15 +2194,17 @@ static int adjointPassRing(Context* c, const DevSignals& srcSet, const DevSignal
       if (map) E3D_RET(traceSpread(c, *map, (int)nr, resid + (size_t)its * rows, c->traceRing + (its % 2) * nr));
       for (int it2 = sub - 1; it2 >= 0; it2--) {
         StepPtrs p = makeRingStep(c, W(ma - 1), W(ma), W(ma + 1));
-        if (prem) {
-          p.prem = 1;
-        } else if (dual) {
+        if (dual && !prem) {
           for (int k = 0; k < NCOMP; k++) {
             p.c[k] = c->q1.p[k];
             p.oP[k] = c->q0.p[k];
           }
         }
-        E3D_RET(launchStep(c, STEP_ADJ_EXACT, p));
+        // On premultiplied levels P = M a the exact adjoint's update
+        // a_new = G (G a_old - D(P_cur)), P_new = M a_new reads
+        // P_new = G (G P_old - M D(P_cur)) with M applied term by term: the
+        // time-reversed stepper (stepAdjGpu_3D's update) on P.
+        E3D_RET(launchStep(c, prem ? STEP_ADJ_REVERSED : STEP_ADJ_EXACT, p));
         const StepPtrs q = afterStep(p);
         if (prem) E3D_RET(launchInjectPremultiplied(c, q, recSet, dataSlice(its), dataSlice(its + 1), it2 + 1));
         else if (dual) E3D_RET(launchInjectRefresh(c, q, recSet, dataSlice(its), dataSlice(its + 1), it2 + 1));

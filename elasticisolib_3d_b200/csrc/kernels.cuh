@@ -38,8 +38,6 @@ struct StepPtrs {
   // mode 2 with a dual state: c[] holds the medium-premultiplied current level
   // and the step also writes the premultiplied new level here (may be null)
   float* oP[NCOMP];
-  // mode 2, host side: 1 selects the premultiplied-only state (kStepTma<2,...,PREM>)
-  int prem;
 };
 
 // A "device set" concatenates the regular-grid points of the nine
@@ -489,13 +487,7 @@ __device__ __forceinline__ void tmaIssuePlane(const TmaMaps& mp, float* st, unsi
   for (int k = 0; k < NMED; k++) tmaLoad3d(st + L::MED_OFF + k * L::INT_F, &mp.med[k], z0, x0, y, bar);
 }
 
-// PREM (mode 2 only): the state is the premultiplied level alone.  With P = M a
-// (M the pointwise, linear premultiplication), the dual update
-// a_new = G (G a_old + up), P_new = M a_new is P_new = G (G P_old + M up): old
-// and current levels are premultiplied, the update's terms are premultiplied
-// like the forward stepper's, and no raw level is read or written (140 B per
-// cell instead of the dual state's 176).
-template <int MODE, int TX, int STAGES, bool PREM = false>
+template <int MODE, int TX, int STAGES>
 __global__ void __launch_bounds__(TZ * TX) kStepTma(const __grid_constant__ TmaMaps mp, StepPtrs p, GridConst g,
                                                      int yChunk) {
   using L = PipeLayout<TX>;
@@ -624,12 +616,6 @@ __global__ void __launch_bounds__(TZ * TX) kStepTma(const __grid_constant__ TmaM
       // = taper[min(dzx, dyy)] when that distance is below minPad, else 1
       const float G = dyy < dzx ? Gy : Gzx;
       float nv[NCOMP];
-      if (PREM) {
-        float mup[NCOMP];
-        premultiply(up, rhox, rhoy, rhoz, l2m, lam, muxz, muxy, muyz, mup);
-#pragma unroll
-        for (int k = 0; k < NCOMP; k++) up[k] = mup[k];
-      }
 #pragma unroll
       for (int k = 0; k < NCOMP; k++) {
         float v = G * ov[k * L::INT_F] + up[k];
@@ -645,7 +631,7 @@ __global__ void __launch_bounds__(TZ * TX) kStepTma(const __grid_constant__ TmaM
           if (hasR) p.accR[k][ic] = preR[k] + nv[k] * p.accWr;
         }
       }
-      if (MODE == STEP_ADJ_EXACT && !PREM) {
+      if (MODE == STEP_ADJ_EXACT) {
         float q[NCOMP];
         premultiply(nv, rhox, rhoy, rhoz, l2m, lam, muxz, muxy, muyz, q);
 #pragma unroll
@@ -940,7 +926,7 @@ __global__ void kInjectRefresh(StepPtrs p, GridConst g, SparseSet s, const float
   p.oP[k][i] = v * __ldg(p.m[med] + i);
 }
 
-// Injection into a premultiplied-only state (kStepTma<2,...,PREM>): the raw
+// Injection into a premultiplied-only adjoint state: the raw
 // increment G*(sigL*wl + sigR*wr) of each component enters premultiplied,
 // P += M * add, the normal stresses together as in kInjectRefresh.
 __global__ void kInjectPremultiplied(StepPtrs p, GridConst g, SparseSet s, const float* sigL, const float* sigR,

@@ -179,8 +179,7 @@ class Propagator:
 
     def kernel_timing_read(self, mode):
         """(mean ms, count) of the sampled launches of one kind since the last read: stepper modes 0..2,
-        the same with a fused decimation or secondary source 3..5, block imaging 6, velocity decimation 7,
-        the exact adjoint on the premultiplied-only state 8."""
+        the same with a fused decimation or secondary source 3..5, block imaging 6, velocity decimation 7."""
         avg = ctypes.c_double(0)
         cnt = ctypes.c_longlong(0)
         N.call("e3d_kernel_timing_read", self._h, int(mode), ctypes.byref(avg), ctypes.byref(cnt))

@@ -7,8 +7,8 @@ Modes: 0 forward, 1 time-reversed, 2 exact transpose (run on the dual raw +
 premultiplied state with the TMA loader, as the FWI adjoint pass does);
 3..5 the same with the new level decimated into two coarse accumulators
 (3 velocity fields for 3 and 4; 9 fields for 5), as the fused-accumulator
-passes do; 6 the exact transpose on the premultiplied-only state (140 B per
-cell), as the ring adjoint pass runs it where the medium allows.  The
+passes do.  The ring adjoint pass's exact transpose on the premultiplied-only
+state is mode 1 on premultiplied levels (140 B per cell).  The
 medium is homogeneous (vp 2500 m/s, vs 1443 m/s, rho 2000 kg/m^3, dtw 0.5 ms);
 the wavefields start at zero.  Prints one JSON line with the mean step time
 (CUDA events on the launching stream), the updated cells per step, the
@@ -28,7 +28,7 @@ import torch
 from .engine import Propagator
 from .fwi import medium_planes
 
-BYTES_PER_CELL = {0: 140.0, 1: 140.0, 2: 176.0, 3: 188.0, 4: 188.0, 5: 320.0, 6: 140.0}
+BYTES_PER_CELL = {0: 140.0, 1: 140.0, 2: 176.0, 3: 188.0, 4: 188.0, 5: 320.0}
 
 
 def main(argv=None):
@@ -36,7 +36,7 @@ def main(argv=None):
     ap.add_argument("--nz", type=int, default=392)
     ap.add_argument("--nx", type=int, default=392)
     ap.add_argument("--ny", type=int, default=104)
-    ap.add_argument("--mode", type=int, default=0, choices=[0, 1, 2, 3, 4, 5, 6])
+    ap.add_argument("--mode", type=int, default=0, choices=[0, 1, 2, 3, 4, 5])
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--tx", type=int, default=8)

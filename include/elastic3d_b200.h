@@ -286,9 +286,12 @@ int e3d_set_imaging_chunks(e3d_context* ctx, int chunks);
  * with a decimation ring.  on = 1 (default): where the medium allows it -- all
  * density and shear planes positive and the normal-stress block of the
  * premultiplication conditioned within 100 -- only the medium-premultiplied
- * levels are stored (140 B per cell and step), the raw old level being
- * recovered from them at each step; otherwise, and with on = 0, the raw and
- * the premultiplied levels both (176 B).  The choice is made per medium. */
+ * levels P = M a are stored (140 B per cell and step): the update
+ * a_new = G(G a_old - D(P_cur)) then reads P_new = G(G P_old - M D(P_cur)), the
+ * reference's time-reversed stepper (stepAdjGpu_3D) applied to P, and the
+ * imaging converts its decimated sums back to raw values once per coarse
+ * block; otherwise, and with on = 0, the raw and the premultiplied levels both
+ * (176 B).  The choice is made per medium. */
 int e3d_set_premultiplied_adjoint(e3d_context* ctx, int on);
 /* The checkpoint schedule of a record of `blocks` coarse blocks (nts - 1) cut
  * into segments of `segment_len` blocks, as the checkpointed passes run it:
@@ -416,8 +419,8 @@ int e3d_kernel_timing(e3d_context* ctx, int every);
  * the previous read (waits for them to finish).  mode 0..2: bare steps of that
  * stepper mode; 3..5: the same modes with a fused decimation into coarse
  * accumulators or a fused Born secondary source; 6: the block imaging of the
- * decimation ring; 7: its source-velocity decimation; 8: the exact adjoint on
- * the premultiplied-only state. */
+ * decimation ring; 7: its source-velocity decimation.  The exact adjoint on the
+ * premultiplied-only state runs as mode 1 (see e3d_set_premultiplied_adjoint). */
 int e3d_kernel_timing_read(e3d_context* ctx, int mode, double* avg_ms, long long* count);
 /* Number of kernel launches this context has issued. */
 long long e3d_launch_count(const e3d_context* ctx);
@@ -426,8 +429,7 @@ long long e3d_launch_count(const e3d_context* ctx);
  * state) applied n_steps times to the context's working wavefields; for
  * benchmarking.  Modes 3..5 run modes 0..2 with the new level decimated into
  * two coarse accumulators (3 velocity fields for modes 3 and 4, all 9 fields for
- * 5), as the fused-accumulator passes do; mode 6 runs mode 2 on the
- * premultiplied-only state. */
+ * 5), as the fused-accumulator passes do. */
 int e3d_step_only(e3d_context* ctx, int mode, int n_steps);
 
 /* ------------------------------------------------------------------------
