@@ -94,6 +94,9 @@ def parse():
     ap.add_argument("--decimation", default="ring", choices=["ring", "acc"],
                     help="gradient passes: decimate from a ring of fine levels once per coarse block (ring) "
                          "or through accumulators fused into every fine step (acc)")
+    ap.add_argument("--adjoint-state", default="auto", choices=["auto", "dual"],
+                    help="gradient adjoint pass: premultiplied levels only where the medium allows (auto) or "
+                         "the dual raw + premultiplied state everywhere")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--breakdown", action="store_true",
                     help="after the measurement, print the device time per kernel of one more gradient")
@@ -168,7 +171,7 @@ def build_problem(args, device):
     variant = {"split": (8, 3, "split-fwd"), "tma": (8, 2, "tma"), "plain": (8, 2, "plain"),
                "auto": "auto"}[args.variant]
     prob = F.FwiProblem(fd, device=device, ckpt=args.ckpt, variant=variant, velocity=args.velocity,
-                        decimation_ring=args.decimation == "ring")
+                        decimation_ring=args.decimation == "ring", premultiplied=args.adjoint_state == "auto")
     rank = int(os.environ.get("RANK", "0"))
     shot_id = rank % len(sv.src_xyz)
     src = H.build_devices(*sv.src_xyz[shot_id], ax7, fd.nts, sv.par)

@@ -70,6 +70,7 @@ SIGNATURES = {
     "e3d_set_decimation_ring": ([P, I], I),
     "e3d_set_imaging_chunks": ([P, I], I),
     "e3d_set_premultiplied_adjoint": ([P, I], I),
+    "e3d_nl_forward_batch_device": ([P, I, P, P, P, P, P, P], I),
     "e3d_checkpoint_type": ([P], I),
     "e3d_checkpoint_schedule": ([I, I, P, I, P], I),
     "e3d_checkpoint_plan": ([LL, I, I, D, I, I, I, P, P, P, P], I),

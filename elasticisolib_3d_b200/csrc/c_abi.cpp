@@ -463,6 +463,19 @@ int e3d_velocity_storage(const e3d_context* ctx) { return (ctx && ctx->c) ? velo
 
 int e3d_checkpoint_type(const e3d_context* ctx) { return (ctx && ctx->c) ? checkpointType(ctx->c) : -1; }
 
+int e3d_nl_forward_batch_device(e3d_context* ctx, int shots, const long long* src_pos_dev, const int* src_off10,
+                                const long long* rec_pos_dev, const int* rec_off10, const float* src_sig_dev,
+                                float* rec_sig_dev) {
+  CTX_OR_FAIL(ctx);
+  DevSignals S, R;
+  int st = devSet(src_pos_dev, src_off10, S);
+  if (st == E3D_OK) st = devSet(rec_pos_dev, rec_off10, R);
+  if (st == E3D_OK && shots < 1) st = fail(E3D_ERR_ARG, "shots must be positive");
+  if (st == E3D_OK) st = validateDeviceSets(ctx->c, S, R, shots);
+  if (st != E3D_OK) return st;
+  return nlForwardBatchDevice(ctx->c, shots, S, R, src_sig_dev, rec_sig_dev);
+}
+
 int e3d_set_premultiplied_adjoint(e3d_context* ctx, int on) {
   CTX_OR_FAIL(ctx);
   return setPremultipliedAdjoint(ctx->c, on);

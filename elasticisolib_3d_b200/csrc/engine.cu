@@ -79,6 +79,8 @@ struct Context {
   bool inCapture = false;    // a coarse block is being captured (no timing samples)
   int* blockIndex = nullptr; // device coarse-time index of replayed blocks
   unsigned* posFlag = nullptr;  // device word of the position-table check
+  Fields9 bw0, bw1;          // batched nonlinear forward: the shots' levels, stacked per field
+  int batchShots = 0;
   std::unordered_map<unsigned long long, CUtensorMap> tmaps;  // (pointer, box) -> tensor map
   std::vector<void*> owned;  // every device allocation of this context
   // working wavefields (primary propagation)
@@ -411,9 +413,11 @@ static PFN_cuTensorMapEncodeTiled_v12000 tmaEncoder() {
   return fn;
 }
 
-// 3D map over a (nz, nx, ny) float field with a boxZ x boxX x 1 box, zero fill outside
-static int tensorMap(Context* c, const float* ptr, int boxZ, int boxX, const CUtensorMap** out) {
-  const unsigned long long key = (reinterpret_cast<unsigned long long>(ptr) << 8) ^ (unsigned long long)(boxZ * 64 + boxX);
+// 3D map over a (nz, nx, ny) float field with a boxZ x boxX x 1 box, zero fill outside; with
+// shots > 0 a 4D (nz, nx, ny, shots) map over that many fields stacked at stride n.
+static int tensorMap(Context* c, const float* ptr, int boxZ, int boxX, const CUtensorMap** out, int shots = 0) {
+  const unsigned long long key = (reinterpret_cast<unsigned long long>(ptr) << 8) ^
+                                 (unsigned long long)(boxZ * 64 + boxX) ^ ((unsigned long long)shots << 52);
   auto it = c->tmaps.find(key);
   if (it != c->tmaps.end()) {
     *out = &it->second;
@@ -423,13 +427,13 @@ static int tensorMap(Context* c, const float* ptr, int boxZ, int boxX, const CUt
   E3D_ARG(enc != nullptr, "cuTensorMapEncodeTiled unavailable");
   E3D_ARG((reinterpret_cast<unsigned long long>(ptr) & 15) == 0, "field not 16-byte aligned");
   CUtensorMap m;
-  cuuint64_t dims[3] = {(cuuint64_t)c->d.nz, (cuuint64_t)c->d.nx, (cuuint64_t)c->d.ny};
-  cuuint64_t strides[2] = {(cuuint64_t)c->d.nz * 4, (cuuint64_t)c->g.yStride * 4};
-  cuuint32_t box[3] = {(cuuint32_t)boxZ, (cuuint32_t)boxX, 1};
-  cuuint32_t es[3] = {1, 1, 1};
-  CUresult r = enc(&m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float*>(ptr), dims, strides, box, es,
-                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  cuuint64_t dims[4] = {(cuuint64_t)c->d.nz, (cuuint64_t)c->d.nx, (cuuint64_t)c->d.ny, (cuuint64_t)std::max(shots, 1)};
+  cuuint64_t strides[3] = {(cuuint64_t)c->d.nz * 4, (cuuint64_t)c->g.yStride * 4, (cuuint64_t)c->g.n * 4};
+  cuuint32_t box[4] = {(cuuint32_t)boxZ, (cuuint32_t)boxX, 1, 1};
+  cuuint32_t es[4] = {1, 1, 1, 1};
+  CUresult r = enc(&m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, shots > 0 ? 4 : 3, const_cast<float*>(ptr), dims, strides,
+                   box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                   CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) {
     setLastError("cuTensorMapEncodeTiled failed", __FILE__, __LINE__);
     return E3D_ERR_CUDA;
@@ -477,19 +481,20 @@ static int launchTma(Context* c, const StepPtrs& p, dim3 grid, int yChunk) {
 static int chooseChunks(const Context* c, long long tiles, int nyi, int perSM = 2);
 
 // Split stepper: role V maps (stress halos and leads, old velocities, rho planes) and role S maps
-// (velocity halos and leads, old stresses, lambda/mu planes).
-static int buildSplitMaps(Context* c, const StepPtrs& p, SplitMaps& mp) {
+// (velocity halos and leads, old stresses, lambda/mu planes).  shots > 0: the field maps cover
+// that many shots stacked per field (4D); the medium maps stay 3D.
+static int buildSplitMaps(Context* c, const StepPtrs& p, SplitMaps& mp, int shots = 0) {
   const CUtensorMap* m = nullptr;
   const int vHalo[5] = {SXX, SXY, SXZ, SYZ, SZZ}, vLead[3] = {SXY, SYY, SYZ};
   int i = 0;
-  for (int f : vHalo) { E3D_RET(tensorMap(c, p.c[f], SZ, 8 + 2 * HALO, &m)); mp.v[i++] = *m; }
-  for (int f : vLead) { E3D_RET(tensorMap(c, p.c[f], TZ, 8, &m)); mp.v[i++] = *m; }
-  for (int k = VX; k <= VZ; k++) { E3D_RET(tensorMap(c, p.o[k], TZ, 8, &m)); mp.v[i++] = *m; }
+  for (int f : vHalo) { E3D_RET(tensorMap(c, p.c[f], SZ, 8 + 2 * HALO, &m, shots)); mp.v[i++] = *m; }
+  for (int f : vLead) { E3D_RET(tensorMap(c, p.c[f], TZ, 8, &m, shots)); mp.v[i++] = *m; }
+  for (int k = VX; k <= VZ; k++) { E3D_RET(tensorMap(c, p.o[k], TZ, 8, &m, shots)); mp.v[i++] = *m; }
   for (int k = RHOX; k <= RHOZ; k++) { E3D_RET(tensorMap(c, p.m[k], TZ, 8, &m)); mp.v[i++] = *m; }
   i = 0;
-  for (int f = VX; f <= VZ; f++) { E3D_RET(tensorMap(c, p.c[f], SZ, 8 + 2 * HALO, &m)); mp.s[i++] = *m; }
-  for (int f = VX; f <= VZ; f++) { E3D_RET(tensorMap(c, p.c[f], TZ, 8, &m)); mp.s[i++] = *m; }
-  for (int k = SXX; k <= SYZ; k++) { E3D_RET(tensorMap(c, p.o[k], TZ, 8, &m)); mp.s[i++] = *m; }
+  for (int f = VX; f <= VZ; f++) { E3D_RET(tensorMap(c, p.c[f], SZ, 8 + 2 * HALO, &m, shots)); mp.s[i++] = *m; }
+  for (int f = VX; f <= VZ; f++) { E3D_RET(tensorMap(c, p.c[f], TZ, 8, &m, shots)); mp.s[i++] = *m; }
+  for (int k = SXX; k <= SYZ; k++) { E3D_RET(tensorMap(c, p.o[k], TZ, 8, &m, shots)); mp.s[i++] = *m; }
   for (int k = L2M; k <= MUYZ; k++) { E3D_RET(tensorMap(c, p.m[k], TZ, 8, &m)); mp.s[i++] = *m; }
   return E3D_OK;
 }
@@ -510,7 +515,29 @@ static int launchSplit(Context* c, const StepPtrs& p, int tiz, int tix, int nyi)
   const int yChunk = (nyi + chunks - 1) / chunks;
   chunks = (nyi + yChunk - 1) / yChunk;
   kStepSplit<MODE, STAGES, MINB><<<dim3(tiz, tix, 2 * chunks), dim3(TZ, 8), smem, c->st>>>(mp, p, c->g, yChunk,
-                                                                                              chunks);
+                                                                                              chunks, 1, 0);
+  return E3D_OK;
+}
+
+// One step of `shots` shots stacked per field (fields of n*shots floats), 3-stage split stepper.
+template <int MODE>
+static int launchSplitBatch(Context* c, const StepPtrs& p, int shots) {
+  constexpr size_t smem = (size_t)3 * SPL_STAGE_F * sizeof(float);
+  static std::atomic<unsigned long long> configured{0};
+  E3D_RET(ensureSmemAttr((const void*)kStepSplit<MODE, 3, 3, true>, smem, configured));
+  SplitMaps mp;
+  E3D_RET(buildSplitMaps(c, p, mp, shots));
+  const GridConst& g = c->g;
+  const int tiz = (g.nz - 2 * FAT + TZ - 1) / TZ;
+  const int tix = (g.nx - 2 * FAT + 7) / 8;
+  const int nyi = g.ny - 2 * FAT;
+  int chunks = c->yChunks > 0 ? std::min(c->yChunks, nyi) : (nyi + 31) / 32;
+  chunks = std::max(chunks, 1);
+  const int yChunk = (nyi + chunks - 1) / chunks;
+  chunks = (nyi + yChunk - 1) / yChunk;
+  kStepSplit<MODE, 3, 3, true><<<dim3(tiz * shots, tix, 2 * chunks), dim3(TZ, 8), smem, c->st>>>(
+      mp, p, c->g, yChunk, chunks, shots, g.n);
+  E3D_LAUNCH_CHECK();
   return E3D_OK;
 }
 
@@ -1094,7 +1121,7 @@ int setGraphLoop(Context* c, int on) {
 // path checks host tables the same way): every entry an updated cell.  flagDev
 // is a device word the check may overwrite; the result is read back on `st`.
 static int checkDevicePositions(const DevSignals* const* sets, int nsets, int nz, int nx, int ny, unsigned* flagDev,
-                                cudaStream_t st) {
+                                cudaStream_t st, int shots = 1) {
   bool any = false;
   for (int i = 0; i < nsets; i++) any = any || sets[i]->off[NCOMP] > 0;
   if (!any) return E3D_OK;
@@ -1103,7 +1130,7 @@ static int checkDevicePositions(const DevSignals* const* sets, int nsets, int nz
     const int n = sets[i]->off[NCOMP];
     if (n == 0) continue;
     E3D_ARG(sets[i]->pos != nullptr, "null position table");
-    kCheckPositions<<<(n + 255) / 256, 256, 0, st>>>(sets[i]->pos, n, nz, nx, ny, flagDev);
+    kCheckPositions<<<(n + 255) / 256, 256, 0, st>>>(sets[i]->pos, n, nz, nx, ny, shots, flagDev);
     E3D_LAUNCH_CHECK();
   }
   unsigned bad = 0;
@@ -1116,13 +1143,63 @@ static int checkDevicePositions(const DevSignals* const* sets, int nsets, int nz
   return E3D_OK;
 }
 
-int validateDeviceSets(Context* c, const DevSignals& a, const DevSignals& b) {
+int validateDeviceSets(Context* c, const DevSignals& a, const DevSignals& b, int shots) {
   E3D_ARG(c != nullptr, "null context");
   E3D_CUDA_TRY(cudaSetDevice(c->d.device));
   if (!c->posFlag) E3D_RET(devAlloc(c, (void**)&c->posFlag, sizeof(unsigned)));
   const DevSignals* sets[2] = {&a, &b};
   c->launches += (a.off[NCOMP] > 0) + (b.off[NCOMP] > 0);
-  return checkDevicePositions(sets, 2, c->d.nz, c->d.nx, c->d.ny, c->posFlag, c->st);
+  return checkDevicePositions(sets, 2, c->d.nz, c->d.nx, c->d.ny, c->posFlag, c->st, shots);
+}
+
+// ---------------------------------------------------------------------------
+// Batched nonlinear forward: `shots` shots of one medium advanced together.
+// Each field holds the shots stacked (shot s at offset s*n), every fine step is
+// one split-stepper launch for all shots (CTAs of one tile for consecutive
+// shots adjacent, so the medium tile comes from L2 after the first shot), one
+// injection and one recording launch over the combined tables, whose
+// positions carry the shot offset.  Loop order of propElasticFwdGpu_3D.
+// ---------------------------------------------------------------------------
+int nlForwardBatchDevice(Context* c, int shots, const DevSignals& srcSet, const DevSignals& recSet,
+                         const float* srcSig, float* recSig) {
+  E3D_ARG(c && c->haveMedium, "medium not set");
+  E3D_ARG(shots >= 1 && shots <= 1024, "shots must be in [1, 1024]");
+  E3D_ARG(c->d.nz % 4 == 0, "batched propagation needs nz % 4 == 0");
+  E3D_ARG(!c->d.freeSurface, "batched propagation has no free surface");
+  E3D_CUDA_TRY(cudaSetDevice(c->d.device));
+  const size_t bytes = (size_t)shots * c->g.n * sizeof(float);
+  if (c->batchShots != shots) {
+    for (int k = 0; k < NCOMP; k++) {
+      devFree(c, c->bw0.p[k]);
+      devFree(c, c->bw1.p[k]);
+      c->bw0.p[k] = c->bw1.p[k] = nullptr;
+    }
+    c->batchShots = 0;
+    for (int k = 0; k < NCOMP; k++) {
+      E3D_RET(devAlloc(c, (void**)&c->bw0.p[k], bytes));
+      E3D_RET(devAlloc(c, (void**)&c->bw1.p[k], bytes));
+    }
+    c->batchShots = shots;
+  }
+  for (int k = 0; k < NCOMP; k++) {
+    E3D_CUDA_TRY(cudaMemsetAsync(c->bw0.p[k], 0, bytes, c->st));
+    E3D_CUDA_TRY(cudaMemsetAsync(c->bw1.p[k], 0, bytes, c->st));
+  }
+  const int nts = c->d.nts, sub = c->d.sub;
+  E3D_CUDA_TRY(cudaMemsetAsync(recSig, 0, (size_t)std::max(recSet.off[NCOMP], 1) * nts * sizeof(float), c->st));
+  for (int its = 0; its < nts - 1; its++)
+    for (int it2 = 1; it2 <= sub; it2++) {
+      StepPtrs p = makeStep(c, c->bw0, c->bw1);
+      {
+        c->launches++;
+        TimedLaunch t(c, STEP_FWD);
+        E3D_RET(launchSplitBatch<STEP_FWD>(c, p, shots));
+      }
+      E3D_RET(launchInject(c, p, srcSet, srcSig, its, it2 - 1));
+      E3D_RET(launchRecord(c, p, recSet, recSig, its, it2));
+      swapF(c->bw0, c->bw1);
+    }
+  return E3D_OK;
 }
 
 int nlPropagateDevice(Context* c, bool adjoint, const DevSignals& srcSet, const DevSignals& recSet, float* srcSig,

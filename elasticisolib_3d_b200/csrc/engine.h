@@ -72,7 +72,12 @@ int nlPropagateDevice(Context* c, bool adjoint, const DevSignals& srcSet, const 
                       float* srcSig, float* recSig);
 // Device position tables: every entry an updated cell (E3D_ERR_BOUNDS otherwise); waits on the
 // context's stream.  The device-pointer entry points call it before any propagation.
-int validateDeviceSets(Context* c, const DevSignals& a, const DevSignals& b);
+int validateDeviceSets(Context* c, const DevSignals& a, const DevSignals& b, int shots = 1);
+// Batched nonlinear forward of `shots` shots of the context's medium (stacked per field); the
+// position tables index the stacked grids (shot s at offset s*nz*nx*ny), signals time-major over
+// the combined tables.
+int nlForwardBatchDevice(Context* c, int shots, const DevSignals& srcSet, const DevSignals& recSet,
+                         const float* srcSig, float* recSig);
 // 1 (default): nonlinear propagation replays captured coarse blocks as CUDA graphs.
 int setGraphLoop(Context* c, int on);
 // Irregular receivers as linear combinations of the regular acquisition

@@ -470,6 +470,16 @@ __device__ __forceinline__ void tmaLoad3d(float* dst, const CUtensorMap* map, in
       : "memory");
 }
 
+// 4D form: a (z, x, y, shot) map over the fields of several shots stacked per field.
+__device__ __forceinline__ void tmaLoad4d(float* dst, const CUtensorMap* map, int c0, int c1, int c2, int c3,
+                                          unsigned long long* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], "
+      "[%6];\n" ::"r"(smemAddr(dst)),
+      "l"(reinterpret_cast<unsigned long long>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smemAddr(bar))
+      : "memory");
+}
+
 template <int TX>
 __device__ __forceinline__ void tmaIssuePlane(const TmaMaps& mp, float* st, unsigned long long* bar, int y, int z0,
                                               int x0) {
@@ -686,31 +696,47 @@ struct SplitRole {
   }
 };
 
-template <bool ROLE_S>
+// BATCH: the field maps are (z, x, y, shot) maps over stacked shots and `shot`
+// selects the shot; the medium maps stay 3D (one medium for every shot).
+template <bool ROLE_S, bool BATCH>
 __device__ __forceinline__ void splitIssuePlane(const CUtensorMap* mp, float* st, unsigned long long* bar, int y,
-                                                int z0, int x0) {
+                                                int z0, int x0, int shot) {
   using R = SplitRole<ROLE_S>;
   mbarExpectTx(bar, (unsigned)SPL_STAGE_F * 4u);
 #pragma unroll
-  for (int t = 0; t < R::NH; t++) tmaLoad3d(st + t * SPL_HALO_F, &mp[t], z0 - HALO, x0 - HALO, y, bar);
+  for (int t = 0; t < R::NH; t++) {
+    if (BATCH) tmaLoad4d(st + t * SPL_HALO_F, &mp[t], z0 - HALO, x0 - HALO, y, shot, bar);
+    else tmaLoad3d(st + t * SPL_HALO_F, &mp[t], z0 - HALO, x0 - HALO, y, bar);
+  }
 #pragma unroll
-  for (int q = 0; q < 3; q++)
-    tmaLoad3d(st + R::LEAD_OFF + q * SPL_INT_F, &mp[R::NH + q], z0, x0, y + R::base(q) + 7, bar);
+  for (int q = 0; q < 3; q++) {
+    if (BATCH) tmaLoad4d(st + R::LEAD_OFF + q * SPL_INT_F, &mp[R::NH + q], z0, x0, y + R::base(q) + 7, shot, bar);
+    else tmaLoad3d(st + R::LEAD_OFF + q * SPL_INT_F, &mp[R::NH + q], z0, x0, y + R::base(q) + 7, bar);
+  }
 #pragma unroll
-  for (int k = 0; k < R::NO; k++) tmaLoad3d(st + R::OLD_OFF + k * SPL_INT_F, &mp[R::NH + 3 + k], z0, x0, y, bar);
+  for (int k = 0; k < R::NO; k++) {
+    if (BATCH) tmaLoad4d(st + R::OLD_OFF + k * SPL_INT_F, &mp[R::NH + 3 + k], z0, x0, y, shot, bar);
+    else tmaLoad3d(st + R::OLD_OFF + k * SPL_INT_F, &mp[R::NH + 3 + k], z0, x0, y, bar);
+  }
 #pragma unroll
   for (int k = 0; k < R::NM; k++)
     tmaLoad3d(st + R::MED_OFF + k * SPL_INT_F, &mp[R::NH + 3 + R::NO + k], z0, x0, y, bar);
 }
 
-template <int MODE, bool ROLE_S, int STAGES>
+template <int MODE, bool ROLE_S, int STAGES, bool BATCH>
 __device__ __forceinline__ void splitRole(const CUtensorMap* mp, const StepPtrs& p, const GridConst& g, int yChunk,
-                                          int chunk, float* smem, unsigned long long* bars) {
+                                          int chunk, float* smem, unsigned long long* bars, int nshots,
+                                          long long shotStride) {
   using R = SplitRole<ROLE_S>;
   constexpr int TXS = 8;
   const int tz = threadIdx.x, tx = threadIdx.y;
   const int tid = tx * TZ + tz;
-  const int z0 = FAT + blockIdx.x * TZ, x0 = FAT + blockIdx.y * TXS;
+  // stacked shots: consecutive CTAs take one tile for consecutive shots, so a
+  // medium tile fetched for one shot is in L2 for the others
+  const int shot = BATCH ? (int)(blockIdx.x % nshots) : 0;
+  const int tileZ = BATCH ? (int)(blockIdx.x / nshots) : (int)blockIdx.x;
+  const long long soff = BATCH ? (long long)shot * shotStride : 0;
+  const int z0 = FAT + tileZ * TZ, x0 = FAT + blockIdx.y * TXS;
   const int iz = z0 + tz, ix = x0 + tx;
   const bool active = (iz < g.nz - FAT) && (ix < g.nx - FAT);
   const int yBeg = FAT + chunk * yChunk;
@@ -724,14 +750,16 @@ __device__ __forceinline__ void splitRole(const CUtensorMap* mp, const StepPtrs&
   __syncthreads();
   if (tid == 0) {
     for (int s = 0; s < STAGES - 1; s++)
-      if (yBeg + s < yEnd) splitIssuePlane<ROLE_S>(mp, smem + s * SPL_STAGE_F, &bars[s], yBeg + s, z0, x0);
+      if (yBeg + s < yEnd)
+        splitIssuePlane<ROLE_S, BATCH>(mp, smem + s * SPL_STAGE_F, &bars[s], yBeg + s, z0, x0, shot);
   }
   float w[3][8];
   if (active) {
 #pragma unroll
     for (int q = 0; q < 3; q++)
 #pragma unroll
-      for (int k = 0; k < 7; k++) w[q][k] = __ldg(p.c[R::lead(q)] + (long long)(yBeg + R::base(q) + k) * ys + col);
+      for (int k = 0; k < 7; k++)
+        w[q][k] = __ldg(p.c[R::lead(q)] + soff + (long long)(yBeg + R::base(q) + k) * ys + col);
   }
   const int dzx = min(min(topDistance(g, iz), ix - FAT), min(g.nz - iz - 1 - FAT, g.nx - ix - 1 - FAT));
   const float Gzx = (active && dzx < g.minPad) ? __ldg(g.taper + dzx) : 1.0f;
@@ -757,11 +785,12 @@ __device__ __forceinline__ void splitRole(const CUtensorMap* mp, const StepPtrs&
       const int yn = y + STAGES - 1;
       int ns = slot + STAGES - 1;
       if (ns >= STAGES) ns -= STAGES;
-      if (yn < yEnd) splitIssuePlane<ROLE_S>(mp, smem + ns * SPL_STAGE_F, &bars[ns], yn, z0, x0);
+      if (yn < yEnd) splitIssuePlane<ROLE_S, BATCH>(mp, smem + ns * SPL_STAGE_F, &bars[ns], yn, z0, x0, shot);
     }
     const float* st = smem + slot * SPL_STAGE_F;
     if (active) {
       const long long ic = (long long)y * ys + col;
+      const long long icf = ic + soff;  // this shot's cell in the stacked fields
 #pragma unroll
       for (int q = 0; q < 3; q++) w[q][7] = st[R::LEAD_OFF + q * SPL_INT_F + li];
       const float* cz = g.cz;
@@ -792,11 +821,11 @@ __device__ __forceinline__ void splitRole(const CUtensorMap* mp, const StepPtrs&
 #pragma unroll
         for (int k = 0; k < 3; k++) nv[k] = G * (G * ov[k * SPL_INT_F] + up[k]);
 #pragma unroll
-        for (int k = 0; k < 3; k++) dst[VX + k][ic] = nv[k];
+        for (int k = 0; k < 3; k++) dst[VX + k][icf] = nv[k];
         if (MODE == STEP_ADJ_EXACT && p.oP[0]) {
-          p.oP[VX][ic] = nv[0] * rhox;
-          p.oP[VY][ic] = nv[1] * rhoy;
-          p.oP[VZ][ic] = nv[2] * rhoz;
+          p.oP[VX][icf] = nv[0] * rhox;
+          p.oP[VY][icf] = nv[1] * rhoy;
+          p.oP[VZ][icf] = nv[2] * rhoz;
         }
       } else {
         const float* tVX = st;
@@ -826,14 +855,14 @@ __device__ __forceinline__ void splitRole(const CUtensorMap* mp, const StepPtrs&
 #pragma unroll
         for (int k = 0; k < 6; k++) nv[k] = G * (G * ov[k * SPL_INT_F] + up[k]);
 #pragma unroll
-        for (int k = 0; k < 6; k++) dst[SXX + k][ic] = nv[k];
+        for (int k = 0; k < 6; k++) dst[SXX + k][icf] = nv[k];
         if (MODE == STEP_ADJ_EXACT && p.oP[0]) {
-          p.oP[SXX][ic] = nv[0] * l2m + (nv[1] + nv[2]) * lam;
-          p.oP[SYY][ic] = nv[1] * l2m + (nv[0] + nv[2]) * lam;
-          p.oP[SZZ][ic] = nv[2] * l2m + (nv[0] + nv[1]) * lam;
-          p.oP[SXZ][ic] = nv[3] * muxz;
-          p.oP[SXY][ic] = nv[4] * muxy;
-          p.oP[SYZ][ic] = nv[5] * muyz;
+          p.oP[SXX][icf] = nv[0] * l2m + (nv[1] + nv[2]) * lam;
+          p.oP[SYY][icf] = nv[1] * l2m + (nv[0] + nv[2]) * lam;
+          p.oP[SZZ][icf] = nv[2] * l2m + (nv[0] + nv[1]) * lam;
+          p.oP[SXZ][icf] = nv[3] * muxz;
+          p.oP[SXY][icf] = nv[4] * muxy;
+          p.oP[SYZ][icf] = nv[5] * muyz;
         }
       }
 #pragma unroll
@@ -845,13 +874,18 @@ __device__ __forceinline__ void splitRole(const CUtensorMap* mp, const StepPtrs&
   }
 }
 
-template <int MODE, int STAGES, int MINB>
+// BATCH: nshots shots stacked per field (shot s at offset s * shotStride), field
+// maps 4D, blockIdx.x = tile * nshots + shot; forward and time-reversed modes only.
+template <int MODE, int STAGES, int MINB, bool BATCH = false>
 __global__ void __launch_bounds__(TZ * 8, MINB) kStepSplit(const __grid_constant__ SplitMaps mp, StepPtrs p,
-                                                            GridConst g, int yChunk, int chunksV) {
+                                                            GridConst g, int yChunk, int chunksV, int nshots,
+                                                            long long shotStride) {
   extern __shared__ __align__(1024) float smem[];
   __shared__ __align__(8) unsigned long long bars[STAGES];
-  if ((int)blockIdx.z < chunksV) splitRole<MODE, false, STAGES>(mp.v, p, g, yChunk, blockIdx.z, smem, bars);
-  else splitRole<MODE, true, STAGES>(mp.s, p, g, yChunk, blockIdx.z - chunksV, smem, bars);
+  if ((int)blockIdx.z < chunksV)
+    splitRole<MODE, false, STAGES, BATCH>(mp.v, p, g, yChunk, blockIdx.z, smem, bars, nshots, shotStride);
+  else
+    splitRole<MODE, true, STAGES, BATCH>(mp.s, p, g, yChunk, blockIdx.z - chunksV, smem, bars, nshots, shotStride);
 }
 
 // Recompute the premultiplied level at injected points (dual-state mode 2):
@@ -1219,7 +1253,7 @@ __device__ __forceinline__ void injectAt(const StepPtrs& p, const GridConst& g, 
   const float v = sigL[j] * wl + sigR[j] * wr;
   const int iz = (int)(pos % g.nz);
   const int ix = (int)((pos / g.nz) % g.nx);
-  const int iy = (int)(pos / g.yStride);
+  const int iy = (int)((pos / g.yStride) % g.ny);  // positions of stacked shots carry shot * n
   const float add = taperAt(g, iz, ix, iy) * v;
   p.o[k][pos] += add;
   // keep a decimation that the stepper fused in consistent with the injected value
@@ -1232,15 +1266,16 @@ __device__ __forceinline__ void injectAt(const StepPtrs& p, const GridConst& g, 
 // Check of a device position table before any injection or recording: every
 // entry must be an updated cell (not in the FAT ring, not outside the grid), as
 // the host path requires of host tables.  Reads the table only; a bad entry
-// sets *bad, which the host reads back.
-__global__ void kCheckPositions(const long long* pos, int n, int nz, int nx, int ny, unsigned* bad) {
+// sets *bad, which the host reads back.  With shots > 1 the table indexes that
+// many grids stacked one after another (shot s at offset s * nz*nx*ny).
+__global__ void kCheckPositions(const long long* pos, int n, int nz, int nx, int ny, int shots, unsigned* bad) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= n) return;
   const long long p = pos[j];
   const long long ys = (long long)nz * nx;
-  bool ok = p >= 0 && p < ys * ny;
+  bool ok = p >= 0 && p < ys * ny * shots;
   if (ok) {
-    const long long iz = p % nz, ix = (p / nz) % nx, iy = p / ys;
+    const long long iz = p % nz, ix = (p / nz) % nx, iy = (p / ys) % ny;
     ok = iz >= FAT && iz < nz - FAT && ix >= FAT && ix < nx - FAT && iy >= FAT && iy < ny - FAT;
   }
   if (!ok) atomicOr(bad, 1u);
@@ -1349,7 +1384,7 @@ __global__ void kExtractSource(StepPtrs p, GridConst g, SparseSet s, float* outL
   const long long pos = s.pos[j];
   const int iz = (int)(pos % g.nz);
   const int ix = (int)((pos / g.nz) % g.nx);
-  const int iy = (int)(pos / g.yStride);
+  const int iy = (int)((pos / g.yStride) % g.ny);  // positions of stacked shots carry shot * n
   const float v = taperAt(g, iz, ix, iy) * p.o[k][pos];
   outL[j] += v * wl;
   outR[j] += v * wr;

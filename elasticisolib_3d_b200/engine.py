@@ -55,6 +55,24 @@ def checkpoint_plan(n_cells, ny, nts, budget_bytes, ckpt="auto", velocity="auto"
     return ("fp32", "fp16", "bf16")[ck.value], ("fp32", "fp16")[vt.value], L.value, b.value
 
 
+class BatchTables:
+    """Stacked device tables of a batched forward (see Propagator.batch_tables)."""
+
+    def __init__(self, shots, src_pos, src_off, rec_pos, rec_off, src_sig, rec_sig):
+        self.shots, self.src_pos, self.src_off = shots, src_pos, list(src_off)
+        self.rec_pos, self.rec_off, self.src_sig, self.rec_sig = rec_pos, list(rec_off), src_sig, rec_sig
+
+    def split(self, out):
+        """Per-shot nine receiver blocks (n_k, nts) of a receiver-major array out (total, nts)."""
+        data = [[None] * 9 for _ in range(self.shots)]
+        for k in range(9):
+            nk = (self.rec_off[k + 1] - self.rec_off[k]) // self.shots
+            for s in range(self.shots):
+                a = self.rec_off[k] + s * nk
+                data[s][k] = np.ascontiguousarray(out[a:a + nk])
+        return data
+
+
 class Propagator:
     def __init__(self, nz, nx, ny, nts, sub, minPad, dz, dx, dy, dts, alphaCos=0.99, device=0, fix_q1=0,
                  q2compat=1, q3compat=1, free_surface=0):
@@ -66,6 +84,7 @@ class Propagator:
         self._h = ctypes.c_void_p()
         N.call("e3d_context_create", ctypes.byref(d), ctypes.byref(self._h))
         self.device = int(device)
+        self.q2compat = int(q2compat)
 
     def close(self):
         if getattr(self, "_h", None) and self._h.value:
@@ -144,6 +163,48 @@ class Propagator:
         RP, RN, k2 = _geom(rec_pos7)
         N.call("e3d_nl_forward", self._h, N.ptr_array(model), N.ptr_array(data), SP, SN, RP, RN)
         return data
+
+    def batch_tables(self, models, src_pos7s, rec_pos7):
+        """Device tables of a batched forward: models[s] = nine regular source blocks (n_k, nts) of
+        shot s on its tables src_pos7s[s]; the receivers rec_pos7 are shared.  Shot s owns cells
+        [s n, (s+1) n) of each stacked field, so its positions carry the offset s n; component k's
+        entries are the shots' tables in shot order.  Returns a BatchTables on this device."""
+        import torch
+        S = len(models)
+        n = self.nz * self.nx * self.ny
+        dev = torch.device("cuda", self.device)
+        rtab = [np.asarray(rec_pos7[g], dtype=np.int64) for g in range(7)]
+        src_pos, src_off, rec_pos, rec_off, sig = [], [0], [], [0], []
+        for k in range(9):
+            for s in range(S):
+                tab = np.asarray(src_pos7s[s][COMP_GRID[k]], dtype=np.int64)
+                src_pos.append(tab + s * n)
+                sig.append(np.asarray(models[s][k], dtype=np.float32).reshape(len(tab), self.nts))
+            src_off.append(src_off[-1] + sum(len(src_pos7s[s][COMP_GRID[k]]) for s in range(S)))
+            # the reference's sxz receivers read the first n_xz entries of the z-grid table (quirk Q2)
+            rk = rtab[3][:len(rtab[4])] if (self.q2compat and k == 6) else rtab[COMP_GRID[k]]
+            for s in range(S):
+                rec_pos.append(rk + s * n)
+            rec_off.append(rec_off[-1] + S * len(rk))
+        return BatchTables(S, torch.from_numpy(np.concatenate(src_pos)).to(dev), src_off,
+                           torch.from_numpy(np.concatenate(rec_pos)).to(dev), rec_off,
+                           torch.from_numpy(np.ascontiguousarray(np.concatenate(sig, axis=0).T)).to(dev),
+                           torch.empty((self.nts, rec_off[-1]), dtype=torch.float32, device=dev))
+
+    def nl_forward_batch_device(self, bt):
+        """Launch the batched forward of BatchTables bt on the context's stream (asynchronous); the
+        traces land in bt.rec_sig (nts, total receivers), time-major."""
+        N.call("e3d_nl_forward_batch_device", self._h, bt.shots, bt.src_pos.data_ptr(),
+               (ctypes.c_int * 10)(*bt.src_off), bt.rec_pos.data_ptr(), (ctypes.c_int * 10)(*bt.rec_off),
+               bt.src_sig.data_ptr(), bt.rec_sig.data_ptr())
+
+    def nl_forward_batch(self, models, src_pos7s, rec_pos7):
+        """Batched nonlinear forward of several shots in one medium: one list of nine receiver
+        blocks per shot, as nl_forward returns for each shot alone."""
+        bt = self.batch_tables(models, src_pos7s, rec_pos7)
+        self.nl_forward_batch_device(bt)
+        N.call("e3d_synchronize", self._h)
+        return bt.split(bt.rec_sig.cpu().numpy().T)
 
     def nl_adjoint(self, data9, src_pos7, rec_pos7):
         data = [N.as_f32(d) for d in data9]

@@ -341,6 +341,18 @@ int e3d_born_adjoint(e3d_context* ctx, const float* const* src9, const float* co
 int e3d_nl_propagate_device(e3d_context* ctx, int adjoint, const long long* src_pos_dev, const int* src_off10,
                             const long long* rec_pos_dev, const int* rec_off10, float* src_sig_dev,
                             float* rec_sig_dev);
+/* Batched nonlinear forward: `shots` shots in the context's medium advanced
+ * together, one stepper launch per fine step for all of them (the reference
+ * runs one propElasticFwdGpu_3D per shot from an OpenMP loop over GPUs,
+ * nonlinearPropElasticShotsGpu_3D.cpp:177-216).  The position tables and
+ * signals are the concatenation over shots, component-major: component k's
+ * range off10[k]..off10[k+1] holds the entries of every shot, and an entry of
+ * shot s carries s*nz*nx*ny added to its grid position.  Signals are
+ * time-major over the combined tables.  The shots' wavefields take
+ * 18*shots*nz*nx*ny floats; nz % 4 == 0; no free surface. */
+int e3d_nl_forward_batch_device(e3d_context* ctx, int shots, const long long* src_pos_dev, const int* src_off10,
+                                const long long* rec_pos_dev, const int* rec_off10, const float* src_sig_dev,
+                                float* rec_sig_dev);
 /* Irregular receivers as linear combinations of the regular receiver points
  * (spaceInterpGpu_3D::forward/adjoint, spaceInterpGpu_3D.cpp:140-175), all
  * arrays on the device.  Receiver row r = k*n_irreg + i for component k.
