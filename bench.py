@@ -62,7 +62,7 @@ UNIT = "shots/s"
 KIND_NAMES = {0: "forward stepper (kStepSplit<0,3,3>: velocity and stress CTA roles)",
               1: "exact-adjoint stepper on premultiplied levels (kStepSplit<1,3,3>, the time-reversed update on P)",
               2: "dual-state exact-adjoint stepper (kStepTma<2,8,2>)",
-              6: "block imaging from the adjoint ring (kImagingTma)", 7: "source-velocity decimation (kDecimateVelocity)",
+              6: "block imaging from the adjoint ring (kImagingLev: levels staged by TMA)", 7: "source-velocity decimation (kDecimateVelocity)",
               3: "forward stepper + 3-field decimation accumulators", 5: "dual adjoint stepper + 9-field accumulators"}
 PROFILE = {0: "profiles/kStepSplit_forward_392x392x104.txt", 2: "profiles/kStepTma_adjoint_dual_392x392x104.txt",
            1: "profiles/kStepSplit_adjoint_premultiplied_392x392x104.txt",
@@ -94,6 +94,8 @@ def parse():
     ap.add_argument("--decimation", default="ring", choices=["ring", "acc"],
                     help="gradient passes: decimate from a ring of fine levels once per coarse block (ring) "
                          "or through accumulators fused into every fine step (acc)")
+    ap.add_argument("--imaging", default="auto", choices=["auto", "cells", "tma", "tma-levels"],
+                    help="block imaging kernel of the decimation ring (Propagator.set_imaging_variant)")
     ap.add_argument("--adjoint-state", default="auto", choices=["auto", "dual"],
                     help="gradient adjoint pass: premultiplied levels only where the medium allows (auto) or "
                          "the dual raw + premultiplied state everywhere")
@@ -172,6 +174,7 @@ def build_problem(args, device):
                "auto": "auto"}[args.variant]
     prob = F.FwiProblem(fd, device=device, ckpt=args.ckpt, variant=variant, velocity=args.velocity,
                         decimation_ring=args.decimation == "ring", premultiplied=args.adjoint_state == "auto")
+    prob.prop.set_imaging_variant(args.imaging)
     rank = int(os.environ.get("RANK", "0"))
     shot_id = rank % len(sv.src_xyz)
     src = H.build_devices(*sv.src_xyz[shot_id], ax7, fd.nts, sv.par)

@@ -69,6 +69,7 @@ SIGNATURES = {
     "e3d_velocity_storage": ([P], I),
     "e3d_set_decimation_ring": ([P, I], I),
     "e3d_set_imaging_chunks": ([P, I], I),
+    "e3d_set_imaging_variant": ([P, I], I),
     "e3d_set_premultiplied_adjoint": ([P, I], I),
     "e3d_nl_forward_batch_device": ([P, I, P, P, P, P, P, P], I),
     "e3d_checkpoint_type": ([P], I),

@@ -486,6 +486,11 @@ int e3d_set_imaging_chunks(e3d_context* ctx, int chunks) {
   return setImagingChunks(ctx->c, chunks);
 }
 
+int e3d_set_imaging_variant(e3d_context* ctx, int variant) {
+  CTX_OR_FAIL(ctx);
+  return setImagingVariant(ctx->c, variant);
+}
+
 int e3d_set_decimation_ring(e3d_context* ctx, int on) {
   CTX_OR_FAIL(ctx);
   return setDecimationRing(ctx->c, on);

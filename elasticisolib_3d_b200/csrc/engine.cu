@@ -102,6 +102,7 @@ struct Context {
   std::vector<Fields9> srcRing, adjRing;
   int ringMode = 1;          // 1: decimate from rings when sub allows it
   int imgChunks = 0;         // y chunks of the y-marching imaging launch (0: automatic)
+  int imgVariant = 0;        // block imaging kernel: 0 automatic, 1 kImagingBlock, 2 kImagingTma, 3 kImagingLev
   // exact adjoint state of the ring passes: 1 premultiplied-only where the medium's premultiplication
   // is well conditioned (premCond <= kPremCondMax), 0 always the dual raw + premultiplied state
   int premMode = 1;
@@ -313,6 +314,13 @@ int setStepperVariant(Context* c, int tx, int stages, int loader) {
 int setImagingChunks(Context* c, int chunks) {
   E3D_ARG(c && chunks >= 0, "bad chunk count");
   c->imgChunks = chunks;
+  return E3D_OK;
+}
+
+int setImagingVariant(Context* c, int variant) {
+  E3D_ARG(c != nullptr, "null context");
+  E3D_ARG(variant >= 0 && variant <= 3, "imaging variant must be 0 (automatic), 1, 2 or 3");
+  c->imgVariant = variant;
   return E3D_OK;
 }
 
@@ -1493,6 +1501,47 @@ static int launchDecimate(Context* c, long long mEnd, float* vLeft, int leftMode
 
 // Adjoint imaging of block its from the adjoint ring; the block's last fine
 // level (it2 = 0) is mEnd, so level it2 is mEnd - it2.  v[0..3] = V(its-1..its+2).
+// Halo and lead maps of the source velocities at the two coarse times a block images
+// (time 0 absent without a left image: any valid field stands in, it is not loaded).
+static int imagingVelocityMaps(Context* c, const ImagingBlockPtrs& q, CUtensorMap halo[2][3], CUtensorMap lead[2][3]) {
+  const CUtensorMap* m = nullptr;
+  for (int t = 0; t < 2; t++)
+    for (int k = 0; k < 3; k++) {
+      const float* src = q.v[t + 1][k] ? q.v[t + 1][k] : q.v[2][k];
+      E3D_RET(tensorMap(c, src, SZ, IMG_TX + 2 * HALO, &m));
+      halo[t][k] = *m;
+      E3D_RET(tensorMap(c, src, TZ, IMG_TX, &m));
+      lead[t][k] = *m;
+    }
+  return E3D_OK;
+}
+
+// Block imaging with the levels and the medium staged by TMA (kImagingLev): one CTA per SM.
+template <int NLEV>
+static int launchImagingLev(Context* c, const ImagingBlockPtrs& q, int tiz, int tix, int nyi) {
+  constexpr int STAGES = imgLevStages(NLEV);
+  constexpr size_t smem = (size_t)STAGES * imgLevStageF(NLEV) * sizeof(float);
+  static std::atomic<unsigned long long> configured{0};
+  E3D_RET(ensureSmemAttr((const void*)kImagingLev<NLEV, STAGES>, smem, configured));
+  ImagingLevMaps<NLEV> mp;
+  E3D_RET(imagingVelocityMaps(c, q, mp.halo, mp.lead));
+  const CUtensorMap* m = nullptr;
+  for (int j = 0; j < NLEV; j++)
+    for (int k = 0; k < NCOMP; k++) {
+      E3D_RET(tensorMap(c, q.lev[j][k], TZ, IMG_TX, &m));
+      mp.lev[j][k] = *m;
+    }
+  for (int k = 0; k < NMED; k++) {
+    E3D_RET(tensorMap(c, q.med[k], TZ, IMG_TX, &m));
+    mp.med[k] = *m;
+  }
+  const int chunks0 = c->imgChunks > 0 ? std::min(c->imgChunks, nyi) : chooseChunks(c, (long long)tiz * tix, nyi, 1);
+  const int yChunk = (nyi + chunks0 - 1) / chunks0;
+  const int chunks = (nyi + yChunk - 1) / yChunk;
+  kImagingLev<NLEV, STAGES><<<dim3(tiz, tix, chunks), dim3(TZ, IMG_TX), smem, c->st>>>(mp, q, c->g, yChunk);
+  return E3D_OK;
+}
+
 static int launchImagingBlock(Context* c, long long mEnd, float* const v[4], bool carryIn, bool leftImage,
                               Fields9& carry, bool prem) {
   ImagingBlockPtrs q{};
@@ -1519,24 +1568,31 @@ static int launchImagingBlock(Context* c, long long mEnd, float* const v[4], boo
   q.q3compat = c->d.q3compat;
   c->launches++;
   TimedLaunch tl(c, 6);
-  if (c->d.nz % 4 == 0 && c->loader >= 2) {
+  const bool tma = c->d.nz % 4 == 0 && c->loader >= 2;
+  int variant = c->imgVariant;
+  if (variant == 0) variant = tma ? 3 : 1;
+  if (variant >= 2 && c->d.nz % 4 != 0) variant = 1;  // the TMA forms need 16-byte rows
+  const int tiz = (c->g.nz - 2 * FAT + TZ - 1) / TZ;
+  const int tix = (c->g.nx - 2 * FAT + IMG_TX - 1) / IMG_TX;
+  const int nyi = c->g.ny - 2 * FAT;
+  if (variant == 3) {
+    switch (sub) {
+      case 1: E3D_RET(launchImagingLev<1>(c, q, tiz, tix, nyi)); break;
+      case 2: E3D_RET(launchImagingLev<2>(c, q, tiz, tix, nyi)); break;
+      case 3: E3D_RET(launchImagingLev<3>(c, q, tiz, tix, nyi)); break;
+      case 4: E3D_RET(launchImagingLev<4>(c, q, tiz, tix, nyi)); break;
+      case 5: E3D_RET(launchImagingLev<5>(c, q, tiz, tix, nyi)); break;
+      case 6: E3D_RET(launchImagingLev<6>(c, q, tiz, tix, nyi)); break;
+      case 7: E3D_RET(launchImagingLev<7>(c, q, tiz, tix, nyi)); break;
+      default: E3D_RET(launchImagingLev<8>(c, q, tiz, tix, nyi)); break;
+    }
+  } else if (variant == 2) {
     // y-marching TMA form: tensor maps of the velocity fields (cached per pointer)
     ImagingMaps mp;
-    const CUtensorMap* m = nullptr;
-    for (int t = 0; t < 2; t++)
-      for (int k = 0; k < 3; k++) {
-        const float* src = q.v[t + 1][k] ? q.v[t + 1][k] : q.v[2][k];  // time 0 absent: any valid field
-        E3D_RET(tensorMap(c, src, SZ, IMG_TX + 2 * HALO, &m));
-        mp.halo[t][k] = *m;
-        E3D_RET(tensorMap(c, src, TZ, IMG_TX, &m));
-        mp.lead[t][k] = *m;
-      }
+    E3D_RET(imagingVelocityMaps(c, q, mp.halo, mp.lead));
     constexpr size_t smem = (size_t)2 * IMG_STAGE_F * sizeof(float);
     static std::atomic<unsigned long long> configured{0};
     E3D_RET(ensureSmemAttr((const void*)kImagingTma, smem, configured));
-    const int tiz = (c->g.nz - 2 * FAT + TZ - 1) / TZ;
-    const int tix = (c->g.nx - 2 * FAT + IMG_TX - 1) / IMG_TX;
-    const int nyi = c->g.ny - 2 * FAT;
     const int chunks0 = c->imgChunks > 0 ? std::min(c->imgChunks, nyi) : chooseChunks(c, (long long)tiz * tix, nyi);
     const int yChunk = (nyi + chunks0 - 1) / chunks0;
     const int chunks = (nyi + yChunk - 1) / yChunk;

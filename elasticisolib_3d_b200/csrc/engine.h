@@ -114,6 +114,7 @@ int checkpointType(const Context* c);
 int setDecimationRing(Context* c, int on);
 // y chunks of the y-marching block imaging launch (0: automatic).
 int setImagingChunks(Context* c, int chunks);
+int setImagingVariant(Context* c, int variant);
 // Exact adjoint of the ring passes: 1 (default) the premultiplied-only state where the
 // medium allows it, 0 always the dual raw + premultiplied state.
 int setPremultipliedAdjoint(Context* c, int on);

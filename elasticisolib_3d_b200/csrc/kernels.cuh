@@ -1626,6 +1626,32 @@ struct ImagingBlockPtrs {
   const float* med[NMED];  // medium planes (prem)
 };
 
+// Both decimated sums of premultiplied levels back to raw values: the inverse of premultiply.
+// The normal stresses invert the block [[a,b,b],[b,a,b],[b,b,a]] (a = lambda+2mu, b = lambda,
+// scaled), whose inverse is [[a+b,-b,-b],[-b,a+b,-b],[-b,-b,a+b]] / ((a-b)(a+2b)); the other
+// components divide by their own plane.  The reciprocals are taken once for both sums.
+__device__ __forceinline__ void premSumsToRaw(const float* md, float* L, float* R) {
+  const float r[6] = {__frcp_rn(md[RHOX]), __frcp_rn(md[RHOY]), __frcp_rn(md[RHOZ]),
+                      __frcp_rn(md[MUXZ]), __frcp_rn(md[MUXY]), __frcp_rn(md[MUYZ])};
+  const float det = __frcp_rn((md[L2M] - md[LAM]) * (md[L2M] + 2.0f * md[LAM]));
+  const float apb = md[L2M] + md[LAM], lam = md[LAM];
+  float* const sums[2] = {L, R};
+#pragma unroll
+  for (int s = 0; s < 2; s++) {
+    float* v = sums[s];
+    const float xx = v[SXX], yy = v[SYY], zz = v[SZZ];
+    v[VX] *= r[0];
+    v[VY] *= r[1];
+    v[VZ] *= r[2];
+    v[SXX] = (apb * xx - lam * (yy + zz)) * det;
+    v[SYY] = (apb * yy - lam * (xx + zz)) * det;
+    v[SZZ] = (apb * zz - lam * (xx + yy)) * det;
+    v[SXZ] *= r[3];
+    v[SXY] *= r[4];
+    v[SYZ] *= r[5];
+  }
+}
+
 // Decimated sums of one block from its levels: L (coarse sample its) and R (its+1), raw values,
 // R including the carried left part of the block after it when carryIn.
 __device__ __forceinline__ void blockSums(const ImagingBlockPtrs& q, long long ic, float* L, float* R) {
@@ -1644,32 +1670,10 @@ __device__ __forceinline__ void blockSums(const ImagingBlockPtrs& q, long long i
     }
   }
   if (q.prem) {
-    // both sums back to raw values: the inverse of premultiply.  The normal stresses invert the
-    // block [[a,b,b],[b,a,b],[b,b,a]] (a = lambda+2mu, b = lambda, scaled), whose inverse is
-    // [[a+b,-b,-b],[-b,a+b,-b],[-b,-b,a+b]] / ((a-b)(a+2b)); the other components divide by their
-    // own plane.  The reciprocals are taken once for both sums.
     float md[NMED];
 #pragma unroll
     for (int k = 0; k < NMED; k++) md[k] = __ldg(q.med[k] + ic);
-    const float r[6] = {__frcp_rn(md[RHOX]), __frcp_rn(md[RHOY]), __frcp_rn(md[RHOZ]),
-                        __frcp_rn(md[MUXZ]), __frcp_rn(md[MUXY]), __frcp_rn(md[MUYZ])};
-    const float det = __frcp_rn((md[L2M] - md[LAM]) * (md[L2M] + 2.0f * md[LAM]));
-    const float apb = md[L2M] + md[LAM], lam = md[LAM];
-    float* const sums[2] = {L, R};
-#pragma unroll
-    for (int s = 0; s < 2; s++) {
-      float* v = sums[s];
-      const float xx = v[SXX], yy = v[SYY], zz = v[SZZ];
-      v[VX] *= r[0];
-      v[VY] *= r[1];
-      v[VZ] *= r[2];
-      v[SXX] = (apb * xx - lam * (yy + zz)) * det;
-      v[SYY] = (apb * yy - lam * (xx + zz)) * det;
-      v[SZZ] = (apb * zz - lam * (xx + yy)) * det;
-      v[SXZ] *= r[3];
-      v[SXY] *= r[4];
-      v[SYZ] *= r[5];
-    }
+    premSumsToRaw(md, L, R);
   }
   if (q.carryIn) {
 #pragma unroll
@@ -1867,6 +1871,200 @@ __global__ void __launch_bounds__(TZ * IMG_TX) kImagingTma(const __grid_constant
           for (int k = 0; k < 7; k++) w[t][f][k] = w[t][f][k + 1];
     }
     slot ^= 1;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// kImagingTma with every per-cell operand of the block sums staged by TMA as
+// well: per plane the elected thread also issues one interior box per level
+// component (NLEV levels x 9) and, for premultiplied levels, per medium plane,
+// so the sums read shared memory instead of waiting on NLEV rounds of
+// dependent global loads.  The image planes, the carried part and the
+// time-derivative neighbours stay coalesced loads issued before the wait.
+// STAGES-deep pipeline; one CTA per SM (the stages take most of its shared
+// memory).  Same arithmetic, in the same order, as kImagingTma.
+// ---------------------------------------------------------------------------
+template <int NLEV>
+struct ImagingLevMaps {
+  CUtensorMap halo[2][3];
+  CUtensorMap lead[2][3];
+  CUtensorMap lev[NLEV][NCOMP];
+  CUtensorMap med[NMED];
+};
+constexpr int IMG_LEV_OFF = 6 * IMG_HALO_F + 6 * IMG_INT_F;  // first level box of a stage
+__host__ __device__ constexpr int imgLevStageF(int nlev) { return IMG_LEV_OFF + (nlev * NCOMP + NMED) * IMG_INT_F; }
+// three stages where they fit in 227 KB of shared memory, else two
+__host__ __device__ constexpr int imgLevStages(int nlev) { return 3 * imgLevStageF(nlev) * 4 <= 227 * 1024 ? 3 : 2; }
+
+template <int NLEV>
+__device__ __forceinline__ void imgLevIssuePlane(const ImagingLevMaps<NLEV>& mp, float* st, unsigned long long* bar,
+                                                 int y, int z0, int x0, int ntimes, bool prem) {
+  const unsigned floats = (unsigned)(ntimes * 3 * (IMG_HALO_F + IMG_INT_F) + (NLEV * NCOMP + (prem ? NMED : 0)) * IMG_INT_F);
+  mbarExpectTx(bar, floats * 4u);
+  for (int t = 2 - ntimes; t < 2; t++)
+#pragma unroll
+    for (int f = 0; f < 3; f++) {
+      tmaLoad3d(st + (t * 3 + f) * IMG_HALO_F, &mp.halo[t][f], z0 - HALO, x0 - HALO, y, bar);
+      tmaLoad3d(st + 6 * IMG_HALO_F + (t * 3 + f) * IMG_INT_F, &mp.lead[t][f], z0, x0, y + imgBase(f) + 7, bar);
+    }
+#pragma unroll
+  for (int j = 0; j < NLEV; j++)
+#pragma unroll
+    for (int k = 0; k < NCOMP; k++)
+      tmaLoad3d(st + IMG_LEV_OFF + (j * NCOMP + k) * IMG_INT_F, &mp.lev[j][k], z0, x0, y, bar);
+  if (prem)
+#pragma unroll
+    for (int k = 0; k < NMED; k++)
+      tmaLoad3d(st + IMG_LEV_OFF + (NLEV * NCOMP + k) * IMG_INT_F, &mp.med[k], z0, x0, y, bar);
+}
+
+template <int NLEV, int STAGES>
+__global__ void __launch_bounds__(TZ * IMG_TX, 1) kImagingLev(const __grid_constant__ ImagingLevMaps<NLEV> mp,
+                                                              ImagingBlockPtrs q, GridConst g, int yChunk) {
+  constexpr int SF = imgLevStageF(NLEV);
+  extern __shared__ __align__(1024) float smem[];
+  __shared__ __align__(8) unsigned long long bars[STAGES];
+  const int tz = threadIdx.x, tx = threadIdx.y;
+  const int tid = tx * TZ + tz;
+  const int z0 = FAT + blockIdx.x * TZ, x0 = FAT + blockIdx.y * IMG_TX;
+  const int iz = z0 + tz, ix = x0 + tx;
+  const bool active = (iz < g.nz - FAT) && (ix < g.nx - FAT);
+  const int yBeg = FAT + blockIdx.z * yChunk;
+  const int yEnd = min(yBeg + yChunk, g.ny - FAT);
+  const long long ys = g.yStride;
+  const long long col = (long long)ix * g.nz + iz;
+  const int ntimes = q.leftImage ? 2 : 1;
+  const int t0 = 2 - ntimes;
+  const bool prem = q.prem != 0;
+
+  if (tid == 0) {
+    for (int s = 0; s < STAGES; s++) mbarInit(&bars[s], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  __syncthreads();
+  if (tid == 0)
+    for (int s = 0; s < STAGES - 1; s++)
+      if (yBeg + s < yEnd) imgLevIssuePlane<NLEV>(mp, smem + s * SF, &bars[s], yBeg + s, z0, x0, ntimes, prem);
+  float w[2][3][8];
+  if (active) {
+#pragma unroll
+    for (int t = 0; t < 2; t++)
+#pragma unroll
+      for (int f = 0; f < 3; f++)
+#pragma unroll
+        for (int k = 0; k < 7; k++)
+          w[t][f][k] = (t >= t0) ? __ldg(q.v[t + 1][f] + (long long)(yBeg + imgBase(f) + k) * ys + col) : 0.f;
+  }
+  const int lc = (tx + HALO) * SZ + (tz + HALO);
+  const int li = tx * TZ + tz;
+  int slot = 0;
+  unsigned parity = 0;
+  for (int y = yBeg; y < yEnd; y++) {
+    const long long ic = (long long)y * ys + col;
+    float pv[NMED], nxt[3], prv[3], cur0[3], cin[NCOMP];
+    if (active) {
+#pragma unroll
+      for (int k = 0; k < 3; k++) {
+        nxt[k] = q.v[3][k] ? __ldg(q.v[3][k] + ic) : 0.f;                   // V(its+2)
+        prv[k] = (q.leftImage && q.v[0][k]) ? __ldg(q.v[0][k] + ic) : 0.f;  // V(its-1)
+        cur0[k] = q.leftImage ? 0.f : __ldg(q.v[1][k] + ic);                // V(its) without its tile
+      }
+#pragma unroll
+      for (int k = 0; k < NCOMP; k++) cin[k] = q.carryIn ? q.carry[k][ic] : 0.f;
+#pragma unroll
+      for (int k = 0; k < NMED; k++) pv[k] = q.pert[k][ic];
+    }
+    const bool ok = mbarWaitBounded(&bars[slot], (parity >> slot) & 1u);
+    if (__syncthreads_or(!ok)) {
+      if (tid == 0) {
+        atomicExch(&g_e3dPipeError, 1u);
+        for (int s = 0; s < STAGES; s++) mbarWaitBounded(&bars[s], (parity >> s) & 1u);
+      }
+      __syncthreads();
+      return;
+    }
+    parity ^= 1u << slot;
+    if (tid == 0) {
+      const int yn = y + STAGES - 1;
+      int ns = slot + STAGES - 1;
+      if (ns >= STAGES) ns -= STAGES;
+      if (yn < yEnd) imgLevIssuePlane<NLEV>(mp, smem + ns * SF, &bars[ns], yn, z0, x0, ntimes, prem);
+    }
+    const float* st = smem + slot * SF;
+    if (active) {
+      // block sums from the staged levels, in blockSums' order
+      float L[NCOMP], R[NCOMP];
+#pragma unroll
+      for (int k = 0; k < NCOMP; k++) {
+        L[k] = 0.f;
+        R[k] = 0.f;
+      }
+#pragma unroll
+      for (int j = 0; j < NLEV; j++) {
+        const float wl = q.wl[j], wr = q.wr[j];
+#pragma unroll
+        for (int k = 0; k < NCOMP; k++) {
+          const float a = st[IMG_LEV_OFF + (j * NCOMP + k) * IMG_INT_F + li];
+          L[k] = fmaf(a, wl, L[k]);
+          R[k] = fmaf(a, wr, R[k]);
+        }
+      }
+      if (prem) {
+        float md[NMED];
+#pragma unroll
+        for (int k = 0; k < NMED; k++) md[k] = st[IMG_LEV_OFF + (NLEV * NCOMP + k) * IMG_INT_F + li];
+        premSumsToRaw(md, L, R);
+      }
+      if (q.carryIn) {
+#pragma unroll
+        for (int k = 0; k < NCOMP; k++) R[k] += cin[k];
+      }
+#pragma unroll
+      for (int t = 0; t < 2; t++)
+#pragma unroll
+        for (int f = 0; f < 3; f++)
+          if (t >= t0) w[t][f][7] = st[6 * IMG_HALO_F + (t * 3 + f) * IMG_INT_F + li];
+      const float* h1x = st + 3 * IMG_HALO_F;
+      const float* h1y = st + 4 * IMG_HALO_F;
+      const float* h1z = st + 5 * IMG_HALO_F;
+      float prevR[3];
+      if (q.leftImage) {
+        prevR[0] = st[0 * IMG_HALO_F + lc];
+        prevR[1] = st[1 * IMG_HALO_F + lc];
+        prevR[2] = st[2 * IMG_HALO_F + lc];
+      } else {
+        prevR[0] = cur0[0];
+        prevR[1] = cur0[1];
+        prevR[2] = cur0[2];
+      }
+      float acc[NMED];
+      {
+        const VelTerms t1 = tileVelTerms(h1x, h1y, h1z, w[1][0], w[1][1], w[1][2], lc, g, prevR, nxt, q.dtsInv,
+                                         q.q3compat);
+        imagingTerms(t1, R, acc);
+      }
+      if (q.leftImage) {
+        float nextL[3] = {h1x[lc], h1y[lc], h1z[lc]};
+        const VelTerms tl = tileVelTerms(st, st + IMG_HALO_F, st + 2 * IMG_HALO_F, w[0][0], w[0][1], w[0][2], lc,
+                                         g, prv, nextL, q.dtsInv, q.q3compat);
+        float accL[NMED];
+        imagingTerms(tl, L, accL);
+#pragma unroll
+        for (int k = 0; k < NMED; k++) acc[k] += accL[k];
+      } else {
+#pragma unroll
+        for (int k = 0; k < NCOMP; k++) q.carry[k][ic] = L[k];
+      }
+#pragma unroll
+      for (int k = 0; k < NMED; k++) q.pert[k][ic] = pv[k] + acc[k];
+#pragma unroll
+      for (int t = 0; t < 2; t++)
+#pragma unroll
+        for (int f = 0; f < 3; f++)
+#pragma unroll
+          for (int k = 0; k < 7; k++) w[t][f][k] = w[t][f][k + 1];
+    }
+    slot = (slot + 1 == STAGES) ? 0 : slot + 1;
   }
 }
 

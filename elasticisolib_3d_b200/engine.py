@@ -310,3 +310,10 @@ class Propagator:
     def set_imaging_chunks(self, chunks=0):
         """y chunks of the block imaging launch (0 = automatic)."""
         N.call("e3d_set_imaging_chunks", self._h, int(chunks))
+
+    IMAGING = {"auto": 0, "cells": 1, "tma": 2, "tma-levels": 3}
+
+    def set_imaging_variant(self, variant="auto"):
+        """Block imaging kernel: auto, cells (one thread per cell, global loads), tma (velocity tiles
+        staged by TMA) or tma-levels (velocity tiles, adjoint levels and medium staged by TMA)."""
+        N.call("e3d_set_imaging_variant", self._h, self.IMAGING[variant])

@@ -17,7 +17,6 @@ import json
 import numpy as np
 import torch
 
-from . import _native as N
 from . import hostprep as H
 from . import operators as OP
 from . import synthetic as S
@@ -78,7 +77,6 @@ def main(argv=None):
                       "speedup": res["sequential"] / res["batched"],
                       "batched_gcells_per_s": cells / res["batched"] / 1e9,
                       "last_shot_max_abs_diff": diff, "last_shot_max_abs": scale}), flush=True)
-    del N
     pr.close()
 
 

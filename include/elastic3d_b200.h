@@ -281,6 +281,14 @@ int e3d_set_decimation_ring(e3d_context* ctx, int on);
 /* y chunks of the block imaging launch of the decimation ring (0 = automatic:
  * the rule of the stepper grids).  A tuning knob; no counterpart in the reference. */
 int e3d_set_imaging_chunks(e3d_context* ctx, int chunks);
+/* Kernel of that block imaging: 0 = automatic (3 where the TMA forms apply:
+ * nz % 4 == 0 and a TMA stepper loader, else 1), 1 = one thread per cell
+ * reading every operand from global memory, 2 = y-march with the velocity
+ * tiles staged by TMA and the adjoint levels read per cell, 3 = y-march with
+ * the velocity tiles, the adjoint levels and the medium staged by TMA.  The
+ * same sums in the same order; a tuning knob with no counterpart in the
+ * reference. */
+int e3d_set_imaging_variant(e3d_context* ctx, int variant);
 /* State of the exact adjoint (the transpose of stepFwdGpu_3D's update, as
  * stepAdjGpuBorn_3D, kernelsElaGpu_3D.cu:825-1177) in the checkpointed passes
  * with a decimation ring.  on = 1 (default): where the medium allows it -- all
@@ -349,7 +357,8 @@ int e3d_nl_propagate_device(e3d_context* ctx, int adjoint, const long long* src_
  * range off10[k]..off10[k+1] holds the entries of every shot, and an entry of
  * shot s carries s*nz*nx*ny added to its grid position.  Signals are
  * time-major over the combined tables.  The shots' wavefields take
- * 18*shots*nz*nx*ny floats; nz % 4 == 0; no free surface. */
+ * 18*shots*nz*nx*ny floats; nz % 4 == 0; no free surface.  The tables are
+ * checked on the device first, as above, against the stacked grids. */
 int e3d_nl_forward_batch_device(e3d_context* ctx, int shots, const long long* src_pos_dev, const int* src_off10,
                                 const long long* rec_pos_dev, const int* rec_off10, const float* src_sig_dev,
                                 float* rec_sig_dev);
