@@ -59,19 +59,54 @@ UNIT = "shots/s"
 #     V[b] (12 B), write V[b] and V[b+1] (24 B) = 84 B at sub = 4
 #   with --decimation acc: 3 = forward + 3-field accumulators (188 B), 5 = dual adjoint + 9-field
 #     accumulators (320 B)
-KIND_NAMES = {0: "forward stepper (kStepSplit<0,3,3>: velocity and stress CTA roles)",
-              1: "exact-adjoint stepper on premultiplied levels (kStepSplit<1,3,3>, the time-reversed update on P)",
-              2: "dual-state exact-adjoint stepper (kStepTma<2,8,2>)",
-              6: "block imaging from the adjoint ring (kImagingLev: levels staged by TMA)", 7: "source-velocity decimation (kDecimateVelocity)",
-              3: "forward stepper + 3-field decimation accumulators", 5: "dual adjoint stepper + 9-field accumulators"}
+KIND_NAMES = {0: "forward stepper", 1: "exact-adjoint stepper on premultiplied levels",
+              2: "dual-state exact-adjoint stepper", 6: "block imaging from the adjoint ring",
+              7: "source-velocity decimation", 3: "forward stepper + 3-field decimation accumulators",
+              5: "dual adjoint stepper + 9-field accumulators"}
 PROFILE = {0: "profiles/kStepSplit_forward_392x392x104.txt", 2: "profiles/kStepTma_adjoint_dual_392x392x104.txt",
            1: "profiles/kStepSplit_adjoint_premultiplied_392x392x104.txt",
-           6: "profiles/kImagingTma_392x392x104.txt"}
+           6: "profiles/kImagingTma_280x280x280.txt"}
 
 
-def kind_bytes(kind, sub, prem=False):
-    return {0: 140.0, 1: 140.0, 2: 176.0, 6: sub * 36.0 + 48.0 + 64.0 + (32.0 if prem else 0.0), 7: sub * 12.0 + 36.0,
-            3: 188.0, 5: 320.0}[kind]
+def kind_names(args):
+    """The kernel each timed kind runs with this command's stepper and imaging choices."""
+    fwd = {"split": "kStepSplit<0,3,3>: velocity and stress CTA roles", "tma": "kStepTma<0,8,2>",
+           "plain": "kStep<0,8>: plain loads", "auto": "autotuned stepper"}[args.variant]
+    rev = {"split": "kStepSplit<1,3,3>", "tma": "kStepTma<1,8,2>", "plain": "kStep<1,8>: plain loads",
+           "auto": "autotuned stepper"}[args.variant]
+    img = {"auto": "kImagingBlock" if args.variant == "plain" else "kImagingTma", "tma": "kImagingTma",
+           "tma-levels": "kImagingLev: levels staged by TMA",
+           "cells": "kImagingBlock"}[args.imaging]
+    plain = args.variant == "plain"
+    acc = "kStep<0,8>: plain loads" if plain else "kStepTma<0,8>"
+    # without a TMA loader the exact adjoint keeps one raw state and premultiplies its neighbours
+    adj = "kStep<2,8>: plain loads, neighbours premultiplied on the fly" if plain else "kStepTma<2,8,2>"
+    return {0: f"forward stepper ({fwd})",
+            1: f"exact-adjoint stepper on premultiplied levels ({rev}, the time-reversed update on P)",
+            2: f"exact-adjoint stepper ({adj})" if plain else "dual-state exact-adjoint stepper (kStepTma<2,8,2>)",
+            6: f"block imaging from the adjoint ring ({img})",
+            7: "source-velocity decimation (kDecimateVelocity)",
+            3: f"forward stepper + 3-field decimation accumulators ({acc})",
+            5: f"exact-adjoint stepper + 9-field accumulators ({adj})"}
+
+
+def profiled(kind, args):
+    """The ncu summary whose DRAM bytes per cell stand for this kind's launches, where it profiled
+    the same kernel."""
+    if args.variant != "split" or kind not in PROFILE:
+        return None
+    if kind == 6 and args.imaging not in ("auto", "tma"):
+        return None
+    return os.path.join(ROOT, PROFILE[kind])
+
+
+def kind_bytes(kind, sub, prem=False, dual=True):
+    """Algorithmic bytes per updated cell of a timed kind; dual=False: the exact adjoint keeps one
+    raw state (the plain-load stepper premultiplies its neighbours on the fly), 140 B and 284 B
+    with the 9-field accumulators."""
+    adj, adj_acc = (176.0, 320.0) if dual else (140.0, 284.0)
+    return {0: 140.0, 1: 140.0, 2: adj, 6: sub * 36.0 + 48.0 + 64.0 + (32.0 if prem else 0.0), 7: sub * 12.0 + 36.0,
+            3: 188.0, 5: adj_acc}[kind]
 
 
 def parse():
@@ -409,14 +444,14 @@ def run_ours(args):
             if cnt == 0 or kind not in per_step:
                 continue
             traffic_per_cell = None
-            prof = os.path.join(ROOT, PROFILE[kind]) if kind in PROFILE and args.variant == "split" else None
+            prof = profiled(kind, args)
             if prof and os.path.exists(prof):
                 for line in open(prof):
                     if line.startswith("dram_bytes_per_cell:"):
                         traffic_per_cell = float(line.split(":")[1])
-            nbytes = kind_bytes(kind, fd.sub, prem)
+            nbytes = kind_bytes(kind, fd.sub, prem, dual=args.variant != "plain")
             ach = nbytes * cells / (avg / 1e3) / 1e9 if avg > 0 else None
-            kernels[kind] = {"kernel": KIND_NAMES[kind], "bound": "hbm", "achieved": ach, "peak": peak,
+            kernels[kind] = {"kernel": kind_names(args)[kind], "bound": "hbm", "achieved": ach, "peak": peak,
                              "peak_source": peak_src, "unit": "GB/s", "frac": (ach / peak) if ach else None,
                              "traffic": traffic_per_cell * cells if traffic_per_cell else None,
                              "algorithmic_bytes_per_cell": nbytes, "cells_per_launch": cells,

@@ -1570,7 +1570,9 @@ static int launchImagingBlock(Context* c, long long mEnd, float* const v[4], boo
   TimedLaunch tl(c, 6);
   const bool tma = c->d.nz % 4 == 0 && c->loader >= 2;
   int variant = c->imgVariant;
-  if (variant == 0) variant = tma ? 3 : 1;
+  // automatic: the y-march with velocity tiles staged by TMA.  Measured on B200 in the 288^3
+  // gradient: 1.46 ms per block against 1.88 ms with the levels staged too (one CTA per SM)
+  if (variant == 0) variant = tma ? 2 : 1;
   if (variant >= 2 && c->d.nz % 4 != 0) variant = 1;  // the TMA forms need 16-byte rows
   const int tiz = (c->g.nz - 2 * FAT + TZ - 1) / TZ;
   const int tix = (c->g.nx - 2 * FAT + IMG_TX - 1) / IMG_TX;

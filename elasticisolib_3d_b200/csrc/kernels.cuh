@@ -1660,6 +1660,8 @@ __device__ __forceinline__ void blockSums(const ImagingBlockPtrs& q, long long i
     L[k] = 0.f;
     R[k] = 0.f;
   }
+  // a runtime loop over the levels: measured faster on B200 than the loads unrolled for a
+  // compile-time level count (1.51 against 1.71 ms per block in the 288^3 gradient)
   for (int j = 0; j < q.nlev; j++) {
     const float wl = q.wl[j], wr = q.wr[j];
 #pragma unroll

@@ -281,13 +281,13 @@ int e3d_set_decimation_ring(e3d_context* ctx, int on);
 /* y chunks of the block imaging launch of the decimation ring (0 = automatic:
  * the rule of the stepper grids).  A tuning knob; no counterpart in the reference. */
 int e3d_set_imaging_chunks(e3d_context* ctx, int chunks);
-/* Kernel of that block imaging: 0 = automatic (3 where the TMA forms apply:
+/* Kernel of that block imaging: 0 = automatic (2 where the TMA forms apply:
  * nz % 4 == 0 and a TMA stepper loader, else 1), 1 = one thread per cell
  * reading every operand from global memory, 2 = y-march with the velocity
  * tiles staged by TMA and the adjoint levels read per cell, 3 = y-march with
- * the velocity tiles, the adjoint levels and the medium staged by TMA.  The
- * same sums in the same order; a tuning knob with no counterpart in the
- * reference. */
+ * the velocity tiles, the adjoint levels and the medium staged by TMA (one
+ * CTA per SM; measured slower than 2 on B200 at sub = 4).  The same sums in
+ * the same order; a tuning knob with no counterpart in the reference. */
 int e3d_set_imaging_variant(e3d_context* ctx, int variant);
 /* State of the exact adjoint (the transpose of stepFwdGpu_3D's update, as
  * stepAdjGpuBorn_3D, kernelsElaGpu_3D.cu:825-1177) in the checkpointed passes

@@ -117,15 +117,16 @@ def test_premultiplied_only_adjoint_matches_dual_state(ckpt, segment, velocity):
 
 @pytest.mark.parametrize("prem,segment", [(True, 0), (True, 3), (False, 3)])
 def test_imaging_variants_agree(prem, segment):
-    """The three block-imaging kernels of the decimation ring (per-cell global loads, velocity tiles
-    staged by TMA, velocity tiles + adjoint levels + medium staged by TMA) compute the same sums in
-    the same order: the gradients agree to FP32 rounding (relative 1e-6), on premultiplied levels
-    and on the dual state, with segments that carry a block's left part to the next."""
+    """The block-imaging kernels of the decimation ring (per-cell global loads; velocity tiles staged
+    by TMA; velocity tiles + adjoint levels + medium staged by TMA) compute the same sums in the same order: the gradients agree to FP32 rounding
+    (relative 1e-6), on premultiplied levels and on the dual state, with segments that carry a
+    block's left part to the next."""
     sv, true = survey()
     orc = OracleFwi(sv)
     d_obs, _ = orc.data(true)
     grads = []
-    for variant in ("cells", "tma", "tma-levels"):
+    variants = ("cells", "tma", "tma-levels")
+    for variant in variants:
         prob, src, rec = _problem(sv, "fp32", segment, (8, 3, "split-fwd"), "fp32", True, prem)
         prob.prop.set_imaging_variant(variant)
         prob.shots.append(F.make_shot(src, rec, explosive(sv.par.getInt("nts"), sv.wavelet),
@@ -133,10 +134,10 @@ def test_imaging_variants_agree(prem, segment):
         m = [torch.tensor(sv.elastic[k], device="cuda", requires_grad=True) for k in range(3)]
         F.ElasticFwiMisfit.apply(m[0], m[1], m[2], prob).backward()
         grads.append(np.stack([x.grad.double().cpu().numpy() for x in m]))
-    for i in (1, 2):
+    for i in range(1, len(variants)):
         for k in range(3):
             err = float(np.linalg.norm(grads[i][k] - grads[0][k]) / np.linalg.norm(grads[0][k]))
-            print(f"imaging variant {i} vs per-cell (premultiplied {prem}, segment {segment}): component {k} {err:.2e}")
+            print(f"imaging variant {variants[i]} vs per-cell (premultiplied {prem}, segment {segment}): component {k} {err:.2e}")
             assert err < 1e-6, (i, k, err)
 
 
