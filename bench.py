@@ -63,17 +63,23 @@ KIND_NAMES = {0: "forward stepper", 1: "exact-adjoint stepper on premultiplied l
               2: "dual-state exact-adjoint stepper", 6: "block imaging from the adjoint ring",
               7: "source-velocity decimation", 3: "forward stepper + 3-field decimation accumulators",
               5: "dual adjoint stepper + 9-field accumulators"}
-PROFILE = {0: "profiles/kStepSplit_forward_392x392x104.txt", 2: "profiles/kStepTma_adjoint_dual_392x392x104.txt",
-           1: "profiles/kStepSplit_adjoint_premultiplied_392x392x104.txt",
-           6: "profiles/kImagingTma_280x280x280.txt"}
+# ncu summaries (DRAM bytes per updated cell) of the kernels each stepper choice runs
+PROFILES = {
+    "split": {0: "profiles/kStepSplit_forward_392x392x104.txt",
+              1: "profiles/kStepSplit_adjoint_premultiplied_392x392x104.txt"},
+    "split-pair": {0: "profiles/kStepSplitPair_forward_392x392x104.txt",
+                   1: "profiles/kStepSplitPair_time_reversed_392x392x104.txt"},
+}
+PROFILE_COMMON = {2: "profiles/kStepTma_adjoint_dual_392x392x104.txt", 6: "profiles/kImagingTma_280x280x280.txt"}
 
 
 def kind_names(args):
     """The kernel each timed kind runs with this command's stepper and imaging choices."""
-    fwd = {"split": "kStepSplit<0,3,3>: velocity and stress CTA roles", "tma": "kStepTma<0,8,2>",
-           "plain": "kStep<0,8>: plain loads", "auto": "autotuned stepper"}[args.variant]
-    rev = {"split": "kStepSplit<1,3,3>", "tma": "kStepTma<1,8,2>", "plain": "kStep<1,8>: plain loads",
-           "auto": "autotuned stepper"}[args.variant]
+    fwd = {"split": "kStepSplit<0,3,3>: velocity and stress CTA roles",
+           "split-pair": "kStepSplitPair<0,3,3>: velocity and stress CTA roles, two z cells per thread",
+           "tma": "kStepTma<0,8,2>", "plain": "kStep<0,8>: plain loads", "auto": "autotuned stepper"}[args.variant]
+    rev = {"split": "kStepSplit<1,3,3>", "split-pair": "kStepSplitPair<1,3,3>", "tma": "kStepTma<1,8,2>",
+           "plain": "kStep<1,8>: plain loads", "auto": "autotuned stepper"}[args.variant]
     img = {"auto": "kImagingBlock" if args.variant == "plain" else "kImagingTma", "tma": "kImagingTma",
            "tma-levels": "kImagingLev: levels staged by TMA",
            "cells": "kImagingBlock"}[args.imaging]
@@ -93,11 +99,12 @@ def kind_names(args):
 def profiled(kind, args):
     """The ncu summary whose DRAM bytes per cell stand for this kind's launches, where it profiled
     the same kernel."""
-    if args.variant != "split" or kind not in PROFILE:
+    table = dict(PROFILE_COMMON, **PROFILES.get(args.variant, {})) if args.variant in PROFILES else {}
+    if kind not in table:
         return None
     if kind == 6 and args.imaging not in ("auto", "tma"):
         return None
-    return os.path.join(ROOT, PROFILE[kind])
+    return os.path.join(ROOT, table[kind])
 
 
 def kind_bytes(kind, sub, prem=False, dual=True):
@@ -117,11 +124,12 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--nts", type=int, default=2500)
     ap.add_argument("--interior", type=int, default=300)
-    ap.add_argument("--variant", default="split", choices=["split", "tma", "plain", "auto"],
-                    help="stepper: split (default: velocity and stress updates as two CTA roles with 3-stage TMA "
-                         "pipelines for the forward-type steps, the 2-stage TMA stepper for the dual-state "
-                         "adjoint), tma (2-stage TMA stepper for every step), plain (plain loads, no dual-state "
-                         "adjoint), auto (autotuned)")
+    ap.add_argument("--variant", default="split-pair", choices=["split", "split-pair", "tma", "plain", "auto"],
+                    help="stepper: split-pair (default: velocity and stress updates as two CTA roles with 3-stage "
+                         "TMA pipelines and two z cells per thread for the forward-type steps, the 2-stage TMA "
+                         "stepper for the dual-state adjoint), split (the same with one cell per thread), tma "
+                         "(2-stage TMA stepper for every step), plain (plain loads, no dual-state adjoint), auto "
+                         "(autotuned)")
     ap.add_argument("--ckpt", default="auto", choices=["auto", "fp32", "fp16", "bf16"])
     ap.add_argument("--velocity", default="auto", choices=["auto", "fp32", "fp16"],
                     help="storage of the decimated source velocity slots (fp32 with --ckpt fp32: the "
@@ -205,7 +213,8 @@ def build_problem(args, device):
     sv, true_el = S.fwi_gradient_survey(nzi=n, nxi=n, nyi=n, nts=args.nts, with_true=True)
     fd = H.FdParam(sv.elastic, sv.axes, sv.par)
     ax7 = H.grid_axes(*(a.n for a in sv.axes), *(a.o for a in sv.axes), *(a.d for a in sv.axes))
-    variant = {"split": (8, 3, "split-fwd"), "tma": (8, 2, "tma"), "plain": (8, 2, "plain"),
+    variant = {"split": (8, 3, "split-fwd"), "split-pair": (8, 3, "split-pair"), "tma": (8, 2, "tma"),
+               "plain": (8, 2, "plain"),
                "auto": "auto"}[args.variant]
     prob = F.FwiProblem(fd, device=device, ckpt=args.ckpt, variant=variant, velocity=args.velocity,
                         decimation_ring=args.decimation == "ring", premultiplied=args.adjoint_state == "auto")

@@ -37,6 +37,8 @@ SIGNATURES = {
     "deallocateNonlinearElasticGpu_3D": ([I, I], I),
     "propElasticFwdGpu_3D": (_SEAM_SIG, I),
     "propElasticAdjGpu_3D": (_SEAM_SIG, I),
+    "propElasticFwdGpudomDec_3D": (_SEAM_SIG[:-2] + [P, I, P, I], I),
+    "propElasticAdjGpudomDec_3D": (_SEAM_SIG[:-2] + [P, I, P, I], I),
     "initBornElasticGpu_3D": ([F, F, F, I, I, I, I, F, I, I, I, F, I, I, I], I),
     "allocateBornElasticGpu_3D": ([P] * 8 + [I] * 5, I),
     "deallocateBornElasticGpu_3D": ([I, I], I),

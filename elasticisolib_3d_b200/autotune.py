@@ -12,9 +12,10 @@ import torch
 
 from .engine import Propagator
 
-CANDIDATES = [(8, 3, "split-fwd"), (8, 3, "split"), (8, 2, "split"), (8, 2, "tma"), (16, 2, "tma"), (8, 3, "tma"),
+CANDIDATES = [(8, 3, "split-fwd"), (8, 3, "split-pair"), (8, 2, "split-pair"), (8, 3, "split"), (8, 2, "split"),
+              (8, 2, "tma"), (16, 2, "tma"), (8, 3, "tma"),
               (8, 2, "cpasync"), (16, 2, "cpasync"), (8, 2, "plain"), (8, 2, "tma-ring"), (8, 2, "tma-ring-ldg")]
-TMA_LOADERS = ("tma", "split", "split-fwd")
+TMA_LOADERS = ("tma", "split", "split-fwd", "split-pair")
 
 
 def autotune(prop: Propagator, mode: int = 0, steps: int = 6, warmup: int = 2, candidates=None):

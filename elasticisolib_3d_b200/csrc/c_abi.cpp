@@ -4,6 +4,7 @@
 
 #include <algorithm>
 #include <mutex>
+#include <vector>
 
 #include "../../include/elastic3d_b200.h"
 #include "engine.h"
@@ -24,6 +25,8 @@ struct Slot {
   bool inited = false;
   ContextDesc desc;
   Context* ctx = nullptr;
+  int ny = 0;      // planes of the allocated context (a y-slab's when below desc.ny)
+  int device = 0;  // its device
 };
 
 std::mutex g_mutex;
@@ -58,12 +61,16 @@ int allocSlot(Slot* table, const float* const* planes, int nx, int ny, int nz, i
   if (iGpu < 0 || iGpu >= N_SLOTS) return fail(E3D_ERR_ARG, "iGpu out of range");
   Slot& s = table[iGpu];
   if (!s.inited) return fail(E3D_ERR_STATE, "allocate before init");
-  if (s.desc.nx != nx || s.desc.ny != ny || s.desc.nz != nz) return fail(E3D_ERR_ARG, "grid differs from init");
+  // ny below the init's ny: a y-slab of a decomposed grid (the reference allocates ny_domDec[iGpu]
+  // planes of the shifted medium, nonlinearPropElasticGpu_3D.cpp:37-48)
+  if (s.desc.nx != nx || ny > s.desc.ny || (ny < s.desc.ny && ny < 3 * FAT) || s.desc.nz != nz)
+    return fail(E3D_ERR_ARG, "grid differs from init");
   if (s.ctx) {
     destroyContext(s.ctx);
     s.ctx = nullptr;
   }
   ContextDesc d = s.desc;
+  d.ny = ny;
   d.device = iGpuId;
   Context* c = nullptr;
   int st = createContext(d, &c);
@@ -74,6 +81,8 @@ int allocSlot(Slot* table, const float* const* planes, int nx, int ny, int nz, i
     return st;
   }
   s.ctx = c;
+  s.ny = ny;
+  s.device = iGpuId;
   return E3D_OK;
 }
 
@@ -87,8 +96,25 @@ int freeSlot(Slot* table, int iGpu) {
 Context* slotCtx(Slot* table, int iGpu, int nx, int ny, int nz) {
   if (iGpu < 0 || iGpu >= N_SLOTS || !table[iGpu].ctx) return nullptr;
   const ContextDesc& d = table[iGpu].desc;
-  if (d.nx != nx || d.ny != ny || d.nz != nz) return nullptr;
+  if (d.nx != nx || d.ny != ny || d.nz != nz || table[iGpu].ny != ny) return nullptr;
   return table[iGpu].ctx;
+}
+
+// The slab contexts of a decomposed propagation: slots 0..n-1 allocated with ny_domDec[i] planes
+// on gpuList[i], the init's ny the whole grid's.
+int slabCtxs(Slot* table, int nx, int ny, int nz, const int* nyDomDec, int nDomDec, const int* gpuList, int nGpu,
+             std::vector<Context*>& out) {
+  if (!nyDomDec || !gpuList || nDomDec < 2 || nDomDec != nGpu || nDomDec > N_SLOTS)
+    return fail(E3D_ERR_ARG, "domain decomposition needs one ny_domDec entry per GPU and at least two");
+  out.clear();
+  for (int i = 0; i < nDomDec; i++) {
+    const Slot& s = table[i];
+    if (!s.ctx || s.desc.nx != nx || s.desc.ny != ny || s.desc.nz != nz || s.ny != nyDomDec[i] ||
+        s.device != gpuList[i])
+      return fail(E3D_ERR_STATE, "slab slot not allocated with ny_domDec[iGpu] planes on gpuList[iGpu]");
+    out.push_back(s.ctx);
+  }
+  return E3D_OK;
 }
 
 HostGeom geom14(long long* p0, long long n0, long long* p1, long long n1, long long* p2, long long n2,
@@ -192,6 +218,30 @@ int propElasticAdjGpu_3D(E3D_SEAM_SIGNALS, int nx, int ny, int nz, int iGpu, int
   float* data[9] = {d0, d1, d2, d3, d4, d5, d6, d7, d8};
   return nlPropagateHost(c, true, model, data, geom14(s0, ns0, s1, ns1, s2, ns2, s3, ns3, s4, ns4, s5, ns5, s6, ns6),
                          geom14(r0, nr0, r1, nr1, r2, nr2, r3, nr3, r4, nr4, r5, nr5, r6, nr6));
+}
+
+int propElasticFwdGpudomDec_3D(E3D_SEAM_SIGNALS, int nx, int ny, int nz, const int* ny_domDec, int nDomDec,
+                               const int* gpuList, int nGpu) {
+  std::vector<Context*> slabs;
+  int st = slabCtxs(g_nl, nx, ny, nz, ny_domDec, nDomDec, gpuList, nGpu, slabs);
+  if (st != E3D_OK) return st;
+  float* model[9] = {m0, m1, m2, m3, m4, m5, m6, m7, m8};
+  float* data[9] = {d0, d1, d2, d3, d4, d5, d6, d7, d8};
+  return nlPropagateSlabsHost(slabs.data(), (int)slabs.size(), ny, false, model, data,
+                              geom14(s0, ns0, s1, ns1, s2, ns2, s3, ns3, s4, ns4, s5, ns5, s6, ns6),
+                              geom14(r0, nr0, r1, nr1, r2, nr2, r3, nr3, r4, nr4, r5, nr5, r6, nr6));
+}
+
+int propElasticAdjGpudomDec_3D(E3D_SEAM_SIGNALS, int nx, int ny, int nz, const int* ny_domDec, int nDomDec,
+                               const int* gpuList, int nGpu) {
+  std::vector<Context*> slabs;
+  int st = slabCtxs(g_nl, nx, ny, nz, ny_domDec, nDomDec, gpuList, nGpu, slabs);
+  if (st != E3D_OK) return st;
+  float* model[9] = {m0, m1, m2, m3, m4, m5, m6, m7, m8};
+  float* data[9] = {d0, d1, d2, d3, d4, d5, d6, d7, d8};
+  return nlPropagateSlabsHost(slabs.data(), (int)slabs.size(), ny, true, model, data,
+                              geom14(s0, ns0, s1, ns1, s2, ns2, s3, ns3, s4, ns4, s5, ns5, s6, ns6),
+                              geom14(r0, nr0, r1, nr1, r2, nr2, r3, nr3, r4, nr4, r5, nr5, r6, nr6));
 }
 
 int initBornElasticGpu_3D(float dz, float dx, float dy, int nz, int nx, int ny, int nts, float dts, int sub,

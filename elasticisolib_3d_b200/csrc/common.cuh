@@ -47,6 +47,9 @@ struct GridConst {
   float cz[4], cx[4], cy[4];
   const float* taper;  // device, minPad entries
   int freeSurface;     // 1: free surface at z = FAT, whose face is not tapered (0: the reference's sponge)
+  // y-slab of a decomposed grid: local plane y is global plane y + yOff of a grid of nyTaper
+  // planes, whose y faces carry the sponge (a whole grid: yOff = 0, nyTaper = ny)
+  int yOff, nyTaper;
 };
 
 #ifdef __CUDACC__
@@ -56,9 +59,14 @@ struct GridConst {
 __device__ __forceinline__ int topDistance(const GridConst& g, int iz) {
   return g.freeSurface ? (1 << 30) : iz - FAT;
 }
+// Distance of local plane y to the closest tapered y face of the (possibly decomposed) grid.
+__device__ __forceinline__ int yDistance(const GridConst& g, int y) {
+  const int yg = y + g.yOff;
+  return min(yg - FAT, g.nyTaper - yg - 1 - FAT);
+}
 __device__ __forceinline__ float taperAt(const GridConst& g, int iz, int ix, int iy) {
   int d = min(min(topDistance(g, iz), ix - FAT), min(g.nz - iz - 1 - FAT, g.nx - ix - 1 - FAT));
-  d = min(d, min(iy - FAT, g.ny - iy - 1 - FAT));
+  d = min(d, yDistance(g, iy));
   return d < g.minPad ? __ldg(g.taper + d) : 1.0f;
 }
 #endif

@@ -70,9 +70,10 @@ struct Context {
   int tx = 8;
   int stages = 3;            // shared-memory pipeline depth of the stepper
   // 0: plain loads, 1: cp.async, 2: TMA bulk tensor copies, 3-5: TMA forms with a rotating
-  // y-window, 6: split velocity/stress roles for every mode, 7 (default): split roles for the
-  // forward and time-reversed steps, loader 2's two-stage stepper for the exact adjoint
-  int loader = 7;
+  // y-window, 6: split velocity/stress roles for every mode, 7: split roles for the forward and
+  // time-reversed steps, loader 2's two-stage stepper for the exact adjoint, 8 (default): 7 with
+  // two z cells per thread (measured on B200 in the 288^3 gradient: steppers 3.5-4 % faster)
+  int loader = 8;
   int yChunks = 0;           // y chunks per (z, x) tile column of the stepper grid (0: automatic)
   int numSMs = 148;          // multiprocessors of the device
   int graphLoop = 1;         // 1: replay coarse blocks of the nonlinear loop as a CUDA graph
@@ -201,6 +202,7 @@ int createContext(const ContextDesc& d, Context** out) {
   }
   GridConst& g = c->g;
   g.nz = d.nz; g.nx = d.nx; g.ny = d.ny; g.minPad = d.minPad;
+  g.yOff = 0; g.nyTaper = d.ny;
   g.freeSurface = d.freeSurface ? 1 : 0;
   g.yStride = (long long)d.nz * d.nx;
   g.n = g.yStride * d.ny;
@@ -300,7 +302,7 @@ int setMedium(Context* c, const float* const* planes, bool onDevice) {
 
 int setStepperVariant(Context* c, int tx, int stages, int loader) {
   E3D_ARG(c && (tx == 8 || tx == 16), "tile width must be 8 or 16");
-  E3D_ARG(loader >= 0 && loader <= 7, "loader must be 0 (plain), 1 (cp.async), 2-5 (TMA forms), 6-7 (split TMA)");
+  E3D_ARG(loader >= 0 && loader <= 8, "loader must be 0 (plain), 1 (cp.async), 2-5 (TMA forms), 6-8 (split TMA)");
   E3D_ARG(stages == 2 || stages == 3 || (loader >= 6 && stages == 4),
           "pipeline depth must be 2 or 3 (4 with the split stepper)");
   E3D_ARG(!(tx == 16 && stages == 3), "16-wide tiles fit two stages at most");
@@ -549,6 +551,30 @@ static int launchSplitBatch(Context* c, const StepPtrs& p, int shots) {
   return E3D_OK;
 }
 
+// Paired split stepper (two z cells per thread, blockDim TZ/2 x 8): the y runs of launchSplit.
+template <int MODE, int STAGES, int MINB>
+static int launchSplitPair(Context* c, const StepPtrs& p, int tiz, int tix, int nyi) {
+  constexpr size_t smem = (size_t)STAGES * SPL_STAGE_F * sizeof(float);
+  static std::atomic<unsigned long long> configured{0};
+  E3D_RET(ensureSmemAttr((const void*)kStepSplitPair<MODE, STAGES, MINB>, smem, configured));
+  SplitMaps mp;
+  E3D_RET(buildSplitMaps(c, p, mp));
+  int chunks = c->yChunks > 0 ? std::min(c->yChunks, nyi) : (nyi + 31) / 32;
+  chunks = std::max(chunks, 1);
+  const int yChunk = (nyi + chunks - 1) / chunks;
+  chunks = (nyi + yChunk - 1) / yChunk;
+  kStepSplitPair<MODE, STAGES, MINB><<<dim3(tiz, tix, 2 * chunks), dim3(TZ / 2, 8), smem, c->st>>>(mp, p, c->g,
+                                                                                                   yChunk, chunks);
+  return E3D_OK;
+}
+
+template <int MODE>
+static int launchSplitPairVariant(Context* c, const StepPtrs& p, int tiz, int tix, int nyi) {
+  if (c->stages == 4) return launchSplitPair<MODE, 4, 2>(c, p, tiz, tix, nyi);
+  if (c->stages == 2) return launchSplitPair<MODE, 2, 4>(c, p, tiz, tix, nyi);
+  return launchSplitPair<MODE, 3, 3>(c, p, tiz, tix, nyi);
+}
+
 template <int MODE>
 static int launchSplitVariant(Context* c, const StepPtrs& p, int tiz, int tix, int nyi) {
   if (c->stages == 4) return launchSplit<MODE, 4, 2>(c, p, tiz, tix, nyi);
@@ -718,8 +744,16 @@ static int launchStepRaw(Context* c, int mode, const StepPtrs& p) {
   // it keeps the long runs.
   int chunks = chooseChunks(c, tiles, nyi);
   const bool dual = mode == STEP_ADJ_EXACT && p.oP[0] != nullptr;
-  // the split stepper (loader 6; loader 7: all but the exact adjoint, which keeps kStepTma) takes
-  // every step without a fused decimation or secondary source
+  // the split stepper (loader 6; loader 7: all but the exact adjoint, which keeps kStepTma; loader
+  // 8: loader 7 with two z cells per thread) takes every step without a fused decimation or
+  // secondary source
+  if (c->loader == 8 && mode != STEP_ADJ_EXACT && g.nz % 4 == 0 && p.accL[0] == nullptr && p.ssL[0] == nullptr) {
+    const int tixS = (g.nx - 2 * FAT + 7) / 8;
+    if (mode == STEP_FWD) E3D_RET(launchSplitPairVariant<STEP_FWD>(c, p, tiz, tixS, nyi));
+    else E3D_RET(launchSplitPairVariant<STEP_ADJ_REVERSED>(c, p, tiz, tixS, nyi));
+    E3D_LAUNCH_CHECK();
+    return E3D_OK;
+  }
   if ((c->loader == 6 || (c->loader == 7 && mode != STEP_ADJ_EXACT)) && g.nz % 4 == 0 && p.accL[0] == nullptr &&
       p.ssL[0] == nullptr) {
     const int tixS = (g.nx - 2 * FAT + 7) / 8;
@@ -1055,25 +1089,31 @@ static int launchRecordIdx(Context* c, const StepPtrs& p, const DevSignals& s, f
 // record (k=it2) -> swap.  Time-reversed (propElasticAdjGpu_3D, quirk Q7):
 // it2 = sub-1..0  step -> inject data (k=it2+1) -> [free surface] -> record
 // source (k=it2) -> swap.  With idx the coarse index is read on the device.
-static int nlBlock(Context* c, bool adjoint, const DevSignals& srcSet, const DevSignals& recSet, float* srcSig,
-                   float* recSig, int its, const int* idx) {
+// Fine step s of coarse block its (the reference's loop order): step, inject, free surface,
+// record; the new level ends in c->w1.
+static int nlSubStep(Context* c, bool adjoint, const DevSignals& srcSet, const DevSignals& recSet, float* srcSig,
+                     float* recSig, int its, int s, const int* idx) {
   const int sub = c->d.sub;
   const DevSignals& inSet = adjoint ? recSet : srcSet;
   const DevSignals& outSet = adjoint ? srcSet : recSet;
   float* inSig = adjoint ? recSig : srcSig;
   float* outSig = adjoint ? srcSig : recSig;
-  for (int s = 0; s < sub; s++) {
-    const int it2 = adjoint ? sub - 1 - s : s + 1;
-    const int kIn = adjoint ? it2 + 1 : it2 - 1;
-    StepPtrs p = makeStep(c, c->w0, c->w1);
-    E3D_RET(launchStep(c, adjoint ? STEP_ADJ_REVERSED : STEP_FWD, p));
-    if (idx) E3D_RET(launchInjectIdx(c, p, inSet, inSig, idx, kIn));
-    else E3D_RET(launchInject(c, p, inSet, inSig, its, kIn));
-    E3D_RET(launchFreeSurface(c, p, adjoint ? -1.f : 1.f));
-    if (idx) E3D_RET(launchRecordIdx(c, p, outSet, outSig, idx, it2));
-    else E3D_RET(launchRecord(c, p, outSet, outSig, its, it2));
-    swapF(c->w0, c->w1);
-  }
+  const int it2 = adjoint ? sub - 1 - s : s + 1;
+  const int kIn = adjoint ? it2 + 1 : it2 - 1;
+  StepPtrs p = makeStep(c, c->w0, c->w1);
+  E3D_RET(launchStep(c, adjoint ? STEP_ADJ_REVERSED : STEP_FWD, p));
+  if (idx) E3D_RET(launchInjectIdx(c, p, inSet, inSig, idx, kIn));
+  else E3D_RET(launchInject(c, p, inSet, inSig, its, kIn));
+  E3D_RET(launchFreeSurface(c, p, adjoint ? -1.f : 1.f));
+  if (idx) E3D_RET(launchRecordIdx(c, p, outSet, outSig, idx, it2));
+  else E3D_RET(launchRecord(c, p, outSet, outSig, its, it2));
+  swapF(c->w0, c->w1);
+  return E3D_OK;
+}
+
+static int nlBlock(Context* c, bool adjoint, const DevSignals& srcSet, const DevSignals& recSet, float* srcSig,
+                   float* recSig, int its, const int* idx) {
+  for (int s = 0; s < c->d.sub; s++) E3D_RET(nlSubStep(c, adjoint, srcSet, recSet, srcSig, recSig, its, s, idx));
   return E3D_OK;
 }
 
@@ -1276,6 +1316,247 @@ int nlPropagateHost(Context* c, bool adjoint, float* const* model, float* const*
   }
   releaseStaged(c, S);
   releaseStaged(c, R);
+  return st;
+}
+
+// ---------------------------------------------------------------------------
+// y-slab domain decomposition of the nonlinear propagation
+// (propElasticFwdGpudomDec_3D / propElasticAdjGpudomDec_3D,
+// nonlinearPropElasticGpuFunctions_3D.cu:976-1297, 1396-1719; slab sizes as
+// nonlinearPropElasticShotsGpu_3D.cpp:48-76).  Slab s is a context over the
+// global planes [Y_s, Y_s + ny_s), Y_0 = 0 and Y_{s+1} = Y_s + ny_s - 2 FAT, so
+// neighbours overlap by 2 FAT planes: each updates its own planes
+// [FAT, ny_s - FAT) and keeps its neighbours' boundary planes in its FAT
+// planes.  After every fine step and its injection the new level's boundary
+// planes (FAT planes of the nine fields) are copied into the neighbours' ghost
+// planes; events order the copies between the slabs' streams, so no kernel waits
+// on another.  Every acquisition point goes to the slab that updates it, and
+// every cell is updated with the arithmetic of the undivided grid (the taper
+// reads global y), so the result is the undivided propagation's.
+// ---------------------------------------------------------------------------
+namespace {
+struct SlabRun {
+  Context* c = nullptr;
+  long long y0 = 0;  // global plane of local plane 0
+  Staged S, R;
+  std::vector<long long> pos[2][NCOMP], rows[2][NCOMP];  // [0] sources, [1] receivers
+  std::vector<float> sig[2][NCOMP];
+  cudaEvent_t stepped = nullptr, copied = nullptr;
+};
+
+// Component tables of one side (sources or receivers) in component order, with the sxz receiver
+// rule (quirk Q2) applied, as stageGeom builds them.
+int componentTable(const Context* c, const HostGeom& g, bool receivers, int k, const long long** tab, long long* n) {
+  const int gi = gridOfComp(k);
+  E3D_ARG(g.n[gi] >= 0 && g.n[gi] < (1LL << 30), "bad device count");
+  const long long* src = g.pos[gi];
+  if (receivers && k == SXZ && c->d.q2compat) {
+    E3D_ARG(g.n[GXZ] <= g.n[GZ], "sxz receivers read past the z-grid table (reference quirk Q2)");
+    src = g.pos[GZ];
+  }
+  E3D_ARG(g.n[gi] == 0 || src != nullptr, "null position table");
+  *tab = src;
+  *n = g.n[gi];
+  return E3D_OK;
+}
+
+int stageSlabTables(Context* c, const std::vector<long long>* pos, Staged& s) {
+  long long tot = 0;
+  for (int k = 0; k < NCOMP; k++) {
+    s.set.off[k] = (int)tot;
+    tot += (long long)pos[k].size();
+  }
+  s.set.off[NCOMP] = (int)tot;
+  s.ntot = (int)tot;
+  std::vector<long long> h(std::max<long long>(tot, 1));
+  for (int k = 0; k < NCOMP; k++) std::copy(pos[k].begin(), pos[k].end(), h.begin() + s.set.off[k]);
+  E3D_RET(devAlloc(c, (void**)&s.pos, h.size() * sizeof(long long)));
+  E3D_CUDA_TRY(cudaMemcpyAsync(s.pos, h.data(), h.size() * sizeof(long long), cudaMemcpyHostToDevice, c->st));
+  E3D_CUDA_TRY(cudaStreamSynchronize(c->st));  // h is a local buffer
+  s.set.pos = s.pos;
+  return E3D_OK;
+}
+
+// Copy planes [from, from + FAT) of the nine fields of `src` into planes [to, to + FAT) of `dst`
+// on dst's stream (peer copies between devices through unified addressing).
+int copyGhostPlanes(const SlabRun& dst, long long to, const SlabRun& src, long long from) {
+  const long long ys = dst.c->g.yStride;
+  const size_t bytes = (size_t)FAT * ys * sizeof(float);
+  for (int k = 0; k < NCOMP; k++)
+    E3D_CUDA_TRY(cudaMemcpyAsync(dst.c->w1.p[k] + to * ys, src.c->w1.p[k] + from * ys, bytes, cudaMemcpyDefault,
+                                 dst.c->st));
+  return E3D_OK;
+}
+}  // namespace
+
+int nlPropagateSlabsHost(Context* const* slabs, int nSlabs, int nyGlobal, bool adjoint, float* const* model,
+                         float* const* data, const HostGeom& src, const HostGeom& rec) {
+  E3D_ARG(slabs && nSlabs >= 1 && nSlabs <= 64 && model && data, "bad slab arguments");
+  std::vector<SlabRun> sl(nSlabs);
+  const Context* c0 = slabs[0];
+  E3D_ARG(c0 && c0->haveMedium, "slab 0 has no medium");
+  long long y = 0;
+  for (int i = 0; i < nSlabs; i++) {
+    Context* c = slabs[i];
+    E3D_ARG(c && c->haveMedium, "a slab has no medium");
+    const ContextDesc &d = c->d, &d0 = c0->d;
+    E3D_ARG(d.nz == d0.nz && d.nx == d0.nx && d.nts == d0.nts && d.sub == d0.sub && d.minPad == d0.minPad &&
+                d.dz == d0.dz && d.dx == d0.dx && d.dy == d0.dy && d.dts == d0.dts && d.alphaCos == d0.alphaCos &&
+                d.fixQ1 == d0.fixQ1 && d.q2compat == d0.q2compat && d.freeSurface == d0.freeSurface,
+            "slabs of one grid must share every parameter but ny");
+    // each slab sends FAT of its own planes to each neighbour
+    E3D_ARG(d.ny >= 3 * FAT, "a slab needs at least FAT planes of its own (ny_domDec >= 3*FAT)");
+    for (int j = 0; j < i; j++) E3D_ARG(slabs[j] != c, "a context appears twice among the slabs");
+    sl[i].c = c;
+    sl[i].y0 = y;
+    y += d.ny - 2 * FAT;
+  }
+  E3D_ARG(y + 2 * FAT == nyGlobal, "slab sizes do not add up to ny (sum of ny_domDec - 2*FAT*(n-1) != ny)");
+  const long long ys = c0->g.yStride;
+  const long long nG = ys * nyGlobal;
+
+  // deal the acquisition points to the slabs that update them
+  for (int side = 0; side < 2; side++) {
+    const HostGeom& g = side ? rec : src;
+    for (int k = 0; k < NCOMP; k++) {
+      const long long* tab = nullptr;
+      long long n = 0;
+      E3D_RET(componentTable(c0, g, side == 1, k, &tab, &n));
+      for (long long i = 0; i < n; i++) {
+        const long long p = tab[i];
+        E3D_ARG(p >= 0 && p < nG, "acquisition point outside the grid");
+        const long long iy = p / ys;
+        int owner = -1;
+        for (int t = 0; t < nSlabs && owner < 0; t++)
+          if (iy >= sl[t].y0 + FAT && iy < sl[t].y0 + sl[t].c->d.ny - FAT) owner = t;
+        if (owner < 0) {
+          setLastError("acquisition point inside the FAT ring", __FILE__, __LINE__);
+          return E3D_ERR_BOUNDS;
+        }
+        sl[owner].pos[side][k].push_back(p - sl[owner].y0 * ys);
+        sl[owner].rows[side][k].push_back(i);
+      }
+    }
+  }
+  const int nts = c0->d.nts, sub = c0->d.sub;
+  const int inSide = adjoint ? 1 : 0;
+  float* const* inHost = adjoint ? data : model;
+  float* const* outHost = adjoint ? model : data;
+  int st = E3D_OK;
+  // a failed CUDA call of the slab orchestration: its message and E3D_ERR_CUDA
+  auto cu = [&](cudaError_t e) {
+    if (e != cudaSuccess && st == E3D_OK) {
+      setLastError(cudaGetErrorString(e), __FILE__, __LINE__);
+      st = E3D_ERR_CUDA;
+    }
+    return st == E3D_OK;
+  };
+  for (int i = 0; i < nSlabs && st == E3D_OK; i++) {
+    SlabRun& r = sl[i];
+    Context* c = r.c;
+    cu(cudaSetDevice(c->d.device));
+    if (st == E3D_OK) {
+      c->g.yOff = (int)r.y0;
+      c->g.nyTaper = nyGlobal;
+    }
+    // input rows gathered into slab-local blocks, [n_k][nts] as the host layout
+    const float* in[NCOMP];
+    for (int k = 0; k < NCOMP && st == E3D_OK; k++) {
+      const auto& rows = r.rows[inSide][k];
+      r.sig[inSide][k].resize(std::max<size_t>(rows.size(), 1) * nts);
+      for (size_t j = 0; j < rows.size(); j++) {
+        if (!inHost[k]) {
+          setLastError("null signal block", __FILE__, __LINE__);
+          st = E3D_ERR_ARG;
+          break;
+        }
+        std::copy(inHost[k] + rows[j] * nts, inHost[k] + (rows[j] + 1) * nts, r.sig[inSide][k].begin() + j * nts);
+      }
+      in[k] = r.sig[inSide][k].data();
+    }
+    if (st == E3D_OK) st = stageSlabTables(c, r.pos[0], r.S);
+    if (st == E3D_OK) st = stageSlabTables(c, r.pos[1], r.R);
+    if (st == E3D_OK) st = adjoint ? stageSignalsZero(c, r.S) : stageSignalsIn(c, r.S, in);
+    if (st == E3D_OK) st = adjoint ? stageSignalsIn(c, r.R, in) : stageSignalsZero(c, r.R);
+    if (st == E3D_OK) st = allocFields(c, c->w0, true);
+    if (st == E3D_OK) st = allocFields(c, c->w1, true);
+    if (st == E3D_OK) cu(cudaEventCreateWithFlags(&r.stepped, cudaEventDisableTiming));
+    if (st == E3D_OK) cu(cudaEventCreateWithFlags(&r.copied, cudaEventDisableTiming));
+  }
+  // the time loop: every slab steps, then every slab fetches its ghost planes
+  for (int b = 0; b < nts - 1 && st == E3D_OK; b++) {
+    const int its = adjoint ? nts - 2 - b : b;
+    for (int s = 0; s < sub && st == E3D_OK; s++) {
+      const bool first = b == 0 && s == 0;
+      for (int i = 0; i < nSlabs && st == E3D_OK; i++) {
+        SlabRun& r = sl[i];
+        Context* c = r.c;
+        if (!cu(cudaSetDevice(c->d.device))) break;
+        // the neighbours have read this slab's previous level before it is overwritten
+        if (!first) {
+          if (i > 0) cu(cudaStreamWaitEvent(c->st, sl[i - 1].copied, 0));
+          if (i + 1 < nSlabs) cu(cudaStreamWaitEvent(c->st, sl[i + 1].copied, 0));
+        }
+        if (st == E3D_OK) st = nlSubStep(c, adjoint, r.S.set, r.R.set, r.S.sig, r.R.sig, its, s, nullptr);
+        if (st == E3D_OK) cu(cudaEventRecord(r.stepped, c->st));
+      }
+      for (int i = 0; i < nSlabs && st == E3D_OK; i++) {
+        SlabRun& r = sl[i];
+        Context* c = r.c;
+        if (!cu(cudaSetDevice(c->d.device))) break;
+        const long long ny = c->d.ny;
+        if (i > 0) {
+          const SlabRun& lo = sl[i - 1];
+          cu(cudaStreamWaitEvent(c->st, lo.stepped, 0));
+          // the lower neighbour's top own planes into this slab's bottom ghost planes
+          if (st == E3D_OK) st = copyGhostPlanes(r, 0, lo, lo.c->d.ny - 2 * FAT);
+        }
+        if (i + 1 < nSlabs && st == E3D_OK) {
+          const SlabRun& hi = sl[i + 1];
+          cu(cudaStreamWaitEvent(c->st, hi.stepped, 0));
+          // the upper neighbour's bottom own planes into this slab's top ghost planes
+          if (st == E3D_OK) st = copyGhostPlanes(r, ny - FAT, hi, FAT);
+        }
+        if (st == E3D_OK) cu(cudaEventRecord(r.copied, c->st));
+      }
+    }
+  }
+  // outputs back to the host rows they came from
+  for (int i = 0; i < nSlabs; i++) {
+    SlabRun& r = sl[i];
+    Context* c = r.c;
+    cudaSetDevice(c->d.device);
+    const int outSide = 1 - inSide;
+    float* out[NCOMP];
+    for (int k = 0; k < NCOMP; k++) {
+      r.sig[outSide][k].assign(std::max<size_t>(r.rows[outSide][k].size(), 1) * nts, 0.f);
+      out[k] = r.sig[outSide][k].data();
+    }
+    if (st == E3D_OK) st = stageSignalsOut(c, adjoint ? r.S : r.R, out);
+    if (st == E3D_OK) st = checkPipeError(c);  // synchronizes the slab's stream
+    if (st == E3D_OK)
+      for (int k = 0; k < NCOMP && st == E3D_OK; k++) {
+        const auto& rows = r.rows[outSide][k];
+        if (!rows.empty() && !outHost[k]) {
+          setLastError("null output block", __FILE__, __LINE__);
+          st = E3D_ERR_ARG;
+        }
+        for (size_t j = 0; j < rows.size() && st == E3D_OK; j++)
+          std::copy(out[k] + j * nts, out[k] + (j + 1) * nts, outHost[k] + rows[j] * nts);
+      }
+  }
+  for (int i = 0; i < nSlabs; i++) {
+    SlabRun& r = sl[i];
+    Context* c = r.c;
+    cudaSetDevice(c->d.device);
+    cudaStreamSynchronize(c->st);
+    releaseStaged(c, r.S);
+    releaseStaged(c, r.R);
+    if (r.stepped) cudaEventDestroy(r.stepped);
+    if (r.copied) cudaEventDestroy(r.copied);
+    c->g.yOff = 0;
+    c->g.nyTaper = c->d.ny;
+  }
   return st;
 }
 
@@ -2566,6 +2847,7 @@ int nlPropagateStatic(const ContextDesc& d, const float* const* planes, bool adj
   // grid constants as in createContext
   GridConst g{};
   g.nz = d.nz; g.nx = d.nx; g.ny = d.ny; g.minPad = d.minPad;
+  g.yOff = 0; g.nyTaper = d.ny;
   g.yStride = (long long)d.nz * d.nx;
   g.n = n;
   const double kc[4] = {1.196289062541883, -0.079752604188901, 0.009570312506634, -6.975446437140719e-04};

@@ -68,6 +68,11 @@ struct DevSignals {
   const long long* pos;
   int off[NCOMP + 1];
 };
+// y-slab domain decomposition: `slabs` are contexts over consecutive y-slabs of one grid of
+// nyGlobal planes (slab s over ny_s planes, neighbours overlapping by 2*FAT), each with its slab
+// of the medium; host geometry in global positions, host signals as nlPropagateHost.
+int nlPropagateSlabsHost(Context* const* slabs, int nSlabs, int nyGlobal, bool adjoint, float* const* model,
+                         float* const* data, const HostGeom& src, const HostGeom& rec);
 int nlPropagateDevice(Context* c, bool adjoint, const DevSignals& srcSet, const DevSignals& recSet,
                       float* srcSig, float* recSig);
 // Device position tables: every entry an updated cell (E3D_ERR_BOUNDS otherwise); waits on the

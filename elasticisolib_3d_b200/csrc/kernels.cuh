@@ -540,7 +540,7 @@ __global__ void __launch_bounds__(TZ * TX) kStepTma(const __grid_constant__ TmaM
   int slot = 0;
   unsigned parity = 0;  // bit s: parity of the next completion of stage s
   for (int y = yBeg; y < yEnd; y++) {
-    const int dyy = min(y - FAT, g.ny - y - 1 - FAT);
+    const int dyy = yDistance(g, y);
     const float Gy = dyy < g.minPad ? __ldg(g.taper + dyy) : 1.0f;
     const bool ok = mbarWaitBounded(&bars[slot], (parity >> slot) & 1u);
     // barrier: every thread is past plane y-1, so its stage can be refilled;
@@ -769,7 +769,7 @@ __device__ __forceinline__ void splitRole(const CUtensorMap* mp, const StepPtrs&
   int slot = 0;
   unsigned parity = 0;
   for (int y = yBeg; y < yEnd; y++) {
-    const int dyy = min(y - FAT, g.ny - y - 1 - FAT);
+    const int dyy = yDistance(g, y);
     const float Gy = dyy < g.minPad ? __ldg(g.taper + dyy) : 1.0f;
     const bool ok = mbarWaitBounded(&bars[slot], (parity >> slot) & 1u);
     if (__syncthreads_or(!ok)) {
@@ -872,6 +872,218 @@ __device__ __forceinline__ void splitRole(const CUtensorMap* mp, const StepPtrs&
     }
     slot = (slot + 1 == STAGES) ? 0 : slot + 1;
   }
+}
+
+// ---------------------------------------------------------------------------
+// Paired split stepper: the same tiles, TMA boxes, stages and barriers as
+// kStepSplit, with each thread updating two consecutive z cells (iz, iz+1,
+// iz even) of its column.  The two cells' stencil operands are read from shared
+// memory as 8-byte pairs: a z derivative of both cells takes 5 paired loads
+// instead of 16 single ones, an x derivative 8 instead of 16, and the old level,
+// medium and y-window planes one paired load per field; the new level is
+// stored as float2.  Each cell's arithmetic is kStepSplit's, term by term.
+// blockDim (TZ/2, 8); forward and time-reversed modes.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float2 lds2(const float* t, int i) { return *reinterpret_cast<const float2*>(t + i); }
+
+// z derivatives of cells i and i+1 (i even) of a shared tile row: forward (+) and backward (-)
+__device__ __forceinline__ void dPlusZ2(const float* t, int i, const float* c, float& r0, float& r1) {
+  const float2 a = lds2(t, i - 4), b = lds2(t, i - 2), m = lds2(t, i), d = lds2(t, i + 2), e = lds2(t, i + 4);
+  r0 = c[0] * (m.y - m.x) + c[1] * (d.x - b.y) + c[2] * (d.y - b.x) + c[3] * (e.x - a.y);
+  r1 = c[0] * (d.x - m.y) + c[1] * (d.y - m.x) + c[2] * (e.x - b.y) + c[3] * (e.y - b.x);
+}
+__device__ __forceinline__ void dMinusZ2(const float* t, int i, const float* c, float& r0, float& r1) {
+  const float2 a = lds2(t, i - 4), b = lds2(t, i - 2), m = lds2(t, i), d = lds2(t, i + 2), e = lds2(t, i + 4);
+  r0 = c[0] * (m.x - b.y) + c[1] * (m.y - b.x) + c[2] * (d.x - a.y) + c[3] * (d.y - a.x);
+  r1 = c[0] * (m.y - m.x) + c[1] * (d.x - b.y) + c[2] * (d.y - b.x) + c[3] * (e.x - a.y);
+}
+// derivatives of cells i and i+1 along the tile's x axis (stride s, even)
+__device__ __forceinline__ void dPlusX2(const float* t, int i, int s, const float* c, float& r0, float& r1) {
+  const float2 m3 = lds2(t, i - 3 * s), m2 = lds2(t, i - 2 * s), m1 = lds2(t, i - s), p0 = lds2(t, i);
+  const float2 p1 = lds2(t, i + s), p2 = lds2(t, i + 2 * s), p3 = lds2(t, i + 3 * s), p4 = lds2(t, i + 4 * s);
+  r0 = c[0] * (p1.x - p0.x) + c[1] * (p2.x - m1.x) + c[2] * (p3.x - m2.x) + c[3] * (p4.x - m3.x);
+  r1 = c[0] * (p1.y - p0.y) + c[1] * (p2.y - m1.y) + c[2] * (p3.y - m2.y) + c[3] * (p4.y - m3.y);
+}
+__device__ __forceinline__ void dMinusX2(const float* t, int i, int s, const float* c, float& r0, float& r1) {
+  const float2 m4 = lds2(t, i - 4 * s), m3 = lds2(t, i - 3 * s), m2 = lds2(t, i - 2 * s), m1 = lds2(t, i - s);
+  const float2 p0 = lds2(t, i), p1 = lds2(t, i + s), p2 = lds2(t, i + 2 * s), p3 = lds2(t, i + 3 * s);
+  r0 = c[0] * (p0.x - m1.x) + c[1] * (p1.x - m2.x) + c[2] * (p2.x - m3.x) + c[3] * (p3.x - m4.x);
+  r1 = c[0] * (p0.y - m1.y) + c[1] * (p1.y - m2.y) + c[2] * (p2.y - m3.y) + c[3] * (p3.y - m4.y);
+}
+
+template <int MODE, bool ROLE_S, int STAGES>
+__device__ __forceinline__ void splitRolePair(const CUtensorMap* mp, const StepPtrs& p, const GridConst& g,
+                                              int yChunk, int chunk, float* smem, unsigned long long* bars) {
+  static_assert(MODE != STEP_ADJ_EXACT, "the paired split stepper takes the forward and time-reversed modes");
+  using R = SplitRole<ROLE_S>;
+  constexpr int TXS = 8;
+  const int tz2 = threadIdx.x, tx = threadIdx.y;
+  const int tid = tx * (TZ / 2) + tz2;
+  const int z0 = FAT + blockIdx.x * TZ, x0 = FAT + blockIdx.y * TXS;
+  const int iz = z0 + 2 * tz2, ix = x0 + tx;  // cells iz and iz+1
+  // nz - FAT is even (nz % 4 == 0) and iz is even, so both cells are inside or both outside
+  const bool active = (iz < g.nz - FAT) && (ix < g.nx - FAT);
+  const int yBeg = FAT + chunk * yChunk;
+  const int yEnd = min(yBeg + yChunk, g.ny - FAT);
+  const long long ys = g.yStride;
+  const long long col = (long long)ix * g.nz + iz;
+  if (tid == 0) {
+    for (int s = 0; s < STAGES; s++) mbarInit(&bars[s], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  __syncthreads();
+  if (tid == 0) {
+    for (int s = 0; s < STAGES - 1; s++)
+      if (yBeg + s < yEnd) splitIssuePlane<ROLE_S, false>(mp, smem + s * SPL_STAGE_F, &bars[s], yBeg + s, z0, x0, 0);
+  }
+  float w0[3][8], w1[3][8];  // y-windows of cells iz and iz+1
+  if (active) {
+#pragma unroll
+    for (int q = 0; q < 3; q++)
+#pragma unroll
+      for (int k = 0; k < 7; k++) {
+        const float2 v = __ldg(reinterpret_cast<const float2*>(p.c[R::lead(q)] + (long long)(yBeg + R::base(q) + k) * ys + col));
+        w0[q][k] = v.x;
+        w1[q][k] = v.y;
+      }
+  }
+  int dzx[2];
+  float Gzx[2];
+#pragma unroll
+  for (int h = 0; h < 2; h++) {
+    dzx[h] = min(min(topDistance(g, iz + h), ix - FAT), min(g.nz - iz - h - 1 - FAT, g.nx - ix - 1 - FAT));
+    Gzx[h] = (active && dzx[h] < g.minPad) ? __ldg(g.taper + dzx[h]) : 1.0f;
+  }
+  const int lc = (tx + HALO) * SZ + (2 * tz2 + HALO);
+  const int li = tx * TZ + 2 * tz2;
+  float* const* dst = p.nw[0] ? p.nw : p.o;
+  int slot = 0;
+  unsigned parity = 0;
+  for (int y = yBeg; y < yEnd; y++) {
+    const int dyy = yDistance(g, y);
+    const float Gy = dyy < g.minPad ? __ldg(g.taper + dyy) : 1.0f;
+    const bool ok = mbarWaitBounded(&bars[slot], (parity >> slot) & 1u);
+    if (__syncthreads_or(!ok)) {
+      if (tid == 0) {
+        atomicExch(&g_e3dPipeError, 1u);
+        for (int s = 0; s < STAGES; s++) mbarWaitBounded(&bars[s], (parity >> s) & 1u);
+      }
+      __syncthreads();
+      return;
+    }
+    parity ^= 1u << slot;
+    if (tid == 0) {
+      const int yn = y + STAGES - 1;
+      int ns = slot + STAGES - 1;
+      if (ns >= STAGES) ns -= STAGES;
+      if (yn < yEnd) splitIssuePlane<ROLE_S, false>(mp, smem + ns * SPL_STAGE_F, &bars[ns], yn, z0, x0, 0);
+    }
+    const float* st = smem + slot * SPL_STAGE_F;
+    if (active) {
+      const long long ic = (long long)y * ys + col;
+#pragma unroll
+      for (int q = 0; q < 3; q++) {
+        const float2 v = lds2(st, R::LEAD_OFF + q * SPL_INT_F + li);
+        w0[q][7] = v.x;
+        w1[q][7] = v.y;
+      }
+      const float* cz = g.cz;
+      const float* cx = g.cx;
+      const float* cy = g.cy;
+      const float G[2] = {dyy < dzx[0] ? Gy : Gzx[0], dyy < dzx[1] ? Gy : Gzx[1]};
+      const float sgn = (MODE == STEP_FWD) ? 1.0f : -1.0f;
+      if (!ROLE_S) {
+        const float* tSXX = st;
+        const float* tSXY = st + SPL_HALO_F;
+        const float* tSXZ = st + 2 * SPL_HALO_F;
+        const float* tSYZ = st + 3 * SPL_HALO_F;
+        const float* tSZZ = st + 4 * SPL_HALO_F;
+        float a0, a1, b0, b1, e0, e1;
+        float fv[3][2];
+        dMinusX2(tSXX, lc, SZ, cx, a0, a1);
+        dPlusZ2(tSXZ, lc, cz, b0, b1);
+        fv[0][0] = a0 + dWin(w0[0], cy) + b0;
+        fv[0][1] = a1 + dWin(w1[0], cy) + b1;
+        dPlusX2(tSXY, lc, SZ, cx, a0, a1);
+        dPlusZ2(tSYZ, lc, cz, b0, b1);
+        fv[1][0] = a0 + dWin(w0[1], cy) + b0;
+        fv[1][1] = a1 + dWin(w1[1], cy) + b1;
+        dPlusX2(tSXZ, lc, SZ, cx, a0, a1);
+        dMinusZ2(tSZZ, lc, cz, e0, e1);
+        fv[2][0] = a0 + dWin(w0[2], cy) + e0;
+        fv[2][1] = a1 + dWin(w1[2], cy) + e1;
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+          const float2 rho = lds2(st, R::MED_OFF + k * SPL_INT_F + li);
+          const float2 ov = lds2(st, R::OLD_OFF + k * SPL_INT_F + li);
+          float2 nv;
+          nv.x = G[0] * (G[0] * ov.x + sgn * (rho.x * fv[k][0]));
+          nv.y = G[1] * (G[1] * ov.y + sgn * (rho.y * fv[k][1]));
+          *reinterpret_cast<float2*>(dst[VX + k] + ic) = nv;
+        }
+      } else {
+        const float* tVX = st;
+        const float* tVY = st + SPL_HALO_F;
+        const float* tVZ = st + 2 * SPL_HALO_F;
+        float dxx[2], dyy_[2], dzz[2], fxy[2], fxz[2], fyz[2], a0, a1, b0, b1;
+        dPlusX2(tVX, lc, SZ, cx, dxx[0], dxx[1]);
+        dyy_[0] = dWin(w0[1], cy);
+        dyy_[1] = dWin(w1[1], cy);
+        dPlusZ2(tVZ, lc, cz, dzz[0], dzz[1]);
+        dMinusX2(tVY, lc, SZ, cx, a0, a1);
+        fxy[0] = dWin(w0[0], cy) + a0;
+        fxy[1] = dWin(w1[0], cy) + a1;
+        dMinusZ2(tVX, lc, cz, a0, a1);
+        dMinusX2(tVZ, lc, SZ, cx, b0, b1);
+        fxz[0] = a0 + b0;
+        fxz[1] = a1 + b1;
+        dMinusZ2(tVY, lc, cz, a0, a1);
+        fyz[0] = dWin(w0[2], cy) + a0;
+        fyz[1] = dWin(w1[2], cy) + a1;
+        const float2 l2m = lds2(st, R::MED_OFF + li), lam = lds2(st, R::MED_OFF + SPL_INT_F + li);
+        const float2 muxz = lds2(st, R::MED_OFF + 2 * SPL_INT_F + li);
+        const float2 muxy = lds2(st, R::MED_OFF + 3 * SPL_INT_F + li);
+        const float2 muyz = lds2(st, R::MED_OFF + 4 * SPL_INT_F + li);
+        const float L2M_[2] = {l2m.x, l2m.y}, LAM_[2] = {lam.x, lam.y};
+        const float MXZ[2] = {muxz.x, muxz.y}, MXY[2] = {muxy.x, muxy.y}, MYZ[2] = {muyz.x, muyz.y};
+        float up[6][2];
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+          up[0][h] = sgn * (L2M_[h] * dxx[h] + LAM_[h] * (dyy_[h] + dzz[h]));
+          up[1][h] = sgn * (L2M_[h] * dyy_[h] + LAM_[h] * (dxx[h] + dzz[h]));
+          up[2][h] = sgn * (L2M_[h] * dzz[h] + LAM_[h] * (dxx[h] + dyy_[h]));
+          up[3][h] = sgn * (MXZ[h] * fxz[h]);
+          up[4][h] = sgn * (MXY[h] * fxy[h]);
+          up[5][h] = sgn * (MYZ[h] * fyz[h]);
+        }
+#pragma unroll
+        for (int k = 0; k < 6; k++) {
+          const float2 ov = lds2(st, R::OLD_OFF + k * SPL_INT_F + li);
+          float2 nv;
+          nv.x = G[0] * (G[0] * ov.x + up[k][0]);
+          nv.y = G[1] * (G[1] * ov.y + up[k][1]);
+          *reinterpret_cast<float2*>(dst[SXX + k] + ic) = nv;
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < 3; q++)
+#pragma unroll
+        for (int k = 0; k < 7; k++) {
+          w0[q][k] = w0[q][k + 1];
+          w1[q][k] = w1[q][k + 1];
+        }
+    }
+    slot = (slot + 1 == STAGES) ? 0 : slot + 1;
+  }
+}
+
+template <int MODE, int STAGES, int MINB>
+__global__ void __launch_bounds__(TZ / 2 * 8, MINB) kStepSplitPair(const __grid_constant__ SplitMaps mp, StepPtrs p,
+                                                                   GridConst g, int yChunk, int chunksV) {
+  extern __shared__ __align__(1024) float smem[];
+  __shared__ __align__(8) unsigned long long bars[STAGES];
+  if ((int)blockIdx.z < chunksV) splitRolePair<MODE, false, STAGES>(mp.v, p, g, yChunk, blockIdx.z, smem, bars);
+  else splitRolePair<MODE, true, STAGES>(mp.s, p, g, yChunk, blockIdx.z - chunksV, smem, bars);
 }
 
 // BATCH: nshots shots stacked per field (shot s at offset s * shotStride), field
@@ -1146,7 +1358,7 @@ __device__ __forceinline__ bool tma2Plane(Tma2State<MODE, TX, STAGES, OM_SMEM>& 
     up[SXZ] = sgn * (mvr[MUXZ] * fxz);
     up[SXY] = sgn * (mvr[MUXY] * fxy);
     up[SYZ] = sgn * (mvr[MUYZ] * fyz);
-    const int d = min(S.dzx, min(y - FAT, g.ny - y - 1 - FAT));
+    const int d = min(S.dzx, yDistance(g, y));
     const float G = d < g.minPad ? __ldg(g.taper + d) : 1.0f;
     const bool hasSS = p.ssL[0] != nullptr;
     const bool hasAcc = p.accL[0] != nullptr;

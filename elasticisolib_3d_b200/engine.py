@@ -26,6 +26,20 @@ def _geom(pos7):
     return P, C, pos
 
 
+def domain_decomposition(ny, n_gpu, fat=4, min_pad=0):
+    """y-slab sizes (ny_domDec) of a grid of ny planes over n_gpu GPUs, by the reference's rule
+    (nonlinearPropElasticShotsGpu_3D.cpp:48-76): slab 0 takes ny//n_gpu + fat planes, middle slabs
+    ny//n_gpu + 2*fat, the last the rest + fat; neighbours overlap by 2*fat planes.  Raises
+    ValueError where the reference refuses the split (one GPU, or too few planes per slab)."""
+    if n_gpu < 2:
+        raise ValueError("domain decomposition needs at least two GPUs")
+    chunk = ny // n_gpu
+    if (chunk <= 3 * fat and n_gpu > 2) or (chunk <= 2 * fat and n_gpu == 2) or chunk - 2 * fat <= min_pad:
+        raise ValueError("decomposition not feasible with this ny; use fewer GPUs")
+    sizes = [chunk + fat] + [chunk + 2 * fat] * (n_gpu - 2) + [ny - chunk * (n_gpu - 1) + fat]
+    return sizes
+
+
 def checkpoint_schedule(blocks, segment_len):
     """Checkpoint schedule of a record of `blocks` coarse blocks (nts - 1) with segments of
     `segment_len` blocks, as the engine runs it: (first block of each segment followed by
@@ -112,9 +126,9 @@ class Propagator:
             N.call("e3d_set_medium", self._h, N.ptr_array(planes), 0)
 
     LOADERS = {"plain": 0, "cpasync": 1, "tma": 2, "tma-ring": 3, "tma-ring-ldg": 4, "tma-ring-ldg2": 5, "split": 6,
-               "split-fwd": 7}
+               "split-fwd": 7, "split-pair": 8}
 
-    def set_stepper_variant(self, tx=8, stages=3, loader="split-fwd"):
+    def set_stepper_variant(self, tx=8, stages=3, loader="split-pair"):
         """Stepper variant: x tile width (8/16), shared-memory stages (2/3) and plane loader."""
         N.call("e3d_set_stepper_variant", self._h, int(tx), int(stages), self.LOADERS[loader])
 

@@ -257,7 +257,7 @@ def _half_sum_sq(x, rows_per_chunk=64):
 class FwiProblem:
     """One propagation grid, its context and shots; shared by forward modelling and gradients."""
 
-    def __init__(self, fd: H.FdParam, device="cuda", ckpt="auto", segment=0, variant=(8, 3, "split-fwd"),
+    def __init__(self, fd: H.FdParam, device="cuda", ckpt="auto", segment=0, variant=(8, 3, "split-pair"),
                  velocity="auto", q3compat=1, source_term=False, decimation_ring=True, premultiplied=True):
         """q3compat=1 keeps the reference's Born yz shear term (the xz derivative pair, quirk Q3);
         0 uses the yz pair, the linearisation of the propagator's own yz stress update.

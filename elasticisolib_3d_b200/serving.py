@@ -80,7 +80,7 @@ class GradientServer:
         shape = (fd.nz, fd.nx, fd.ny)
         with self._lock:
             tuned = self.variants.get(shape)
-        variant = tuned if tuned is not None else ("auto" if self.autotune else (8, 3, "split-fwd"))
+        variant = tuned if tuned is not None else ("auto" if self.autotune else (8, 3, "split-pair"))
         prob = F.FwiProblem(fd, device=f"cuda:{dev}", ckpt=self.ckpt, variant=variant)
         probs[key] = prob
         return prob

@@ -122,6 +122,64 @@ int propElasticAdjGpu_3D(float* modelRegDts_vx, float* modelRegDts_vy, float* mo
                          long long* receiversPositionRegYZGrid, long long nReceiversRegYZGrid, int nx, int ny,
                          int nz, int iGpu, int iGpuId);
 
+/* Replaces propElasticFwdGpudomDec_3D (nonlinearPropElasticGpuFunctions_3D.h:15, driver
+ * nonlinearPropElasticGpuFunctions_3D.cu:976-1297): the forward over y-slabs of one grid.  Slot
+ * iGpu (0..nGpu-1) holds slab iGpu, allocated by allocateNonlinearElasticGpu_3D with
+ * ny_domDec[iGpu] planes of the medium shifted by the planes of the slabs before it less 2*FAT
+ * each (neighbours overlap by 2*FAT), on gpuList[iGpu]; init takes the whole grid's ny.
+ * The slab sizes follow nonlinearPropElasticShotsGpu_3D.cpp:48-76: slab 0 ny/nGpu + FAT, middle
+ * slabs ny/nGpu + 2*FAT, the last the rest + FAT; every slab needs at least 3*FAT planes.
+ * Positions are global.  Each slab updates its own planes; after every fine step and its
+ * injection the nine fields' FAT boundary planes go to the neighbours (peer copies between
+ * GPUs).  The result equals propElasticFwdGpu_3D on the whole grid.  The reference's
+ * std::vector arguments become a pointer and a count. */
+int propElasticFwdGpudomDec_3D(float* modelRegDts_vx, float* modelRegDts_vy, float* modelRegDts_vz,
+                               float* modelRegDts_sigmaxx, float* modelRegDts_sigmayy, float* modelRegDts_sigmazz,
+                               float* modelRegDts_sigmaxz, float* modelRegDts_sigmaxy, float* modelRegDts_sigmayz,
+                               float* dataRegDts_vx, float* dataRegDts_vy, float* dataRegDts_vz,
+                               float* dataRegDts_sigmaxx, float* dataRegDts_sigmayy, float* dataRegDts_sigmazz,
+                               float* dataRegDts_sigmaxz, float* dataRegDts_sigmaxy, float* dataRegDts_sigmayz,
+                               long long* sourcesPositionRegCenterGrid, long long nSourcesRegCenterGrid,
+                               long long* sourcesPositionRegXGrid, long long nSourcesRegXGrid,
+                               long long* sourcesPositionRegYGrid, long long nSourcesRegYGrid,
+                               long long* sourcesPositionRegZGrid, long long nSourcesRegZGrid,
+                               long long* sourcesPositionRegXZGrid, long long nSourcesRegXZGrid,
+                               long long* sourcesPositionRegXYGrid, long long nSourcesRegXYGrid,
+                               long long* sourcesPositionRegYZGrid, long long nSourcesRegYZGrid,
+                               long long* receiversPositionRegCenterGrid, long long nReceiversRegCenterGrid,
+                               long long* receiversPositionRegXGrid, long long nReceiversRegXGrid,
+                               long long* receiversPositionRegYGrid, long long nReceiversRegYGrid,
+                               long long* receiversPositionRegZGrid, long long nReceiversRegZGrid,
+                               long long* receiversPositionRegXZGrid, long long nReceiversRegXZGrid,
+                               long long* receiversPositionRegXYGrid, long long nReceiversRegXYGrid,
+                               long long* receiversPositionRegYZGrid, long long nReceiversRegYZGrid, int nx,
+                               int ny, int nz, const int* ny_domDec, int nDomDec, const int* gpuList, int nGpu);
+
+/* Replaces propElasticAdjGpudomDec_3D (nonlinearPropElasticGpuFunctions_3D.h:19, driver
+ * nonlinearPropElasticGpuFunctions_3D.cu:1396-1719): the time-reversed adjoint over the same
+ * slabs; equals propElasticAdjGpu_3D on the whole grid. */
+int propElasticAdjGpudomDec_3D(float* modelRegDts_vx, float* modelRegDts_vy, float* modelRegDts_vz,
+                               float* modelRegDts_sigmaxx, float* modelRegDts_sigmayy, float* modelRegDts_sigmazz,
+                               float* modelRegDts_sigmaxz, float* modelRegDts_sigmaxy, float* modelRegDts_sigmayz,
+                               float* dataRegDts_vx, float* dataRegDts_vy, float* dataRegDts_vz,
+                               float* dataRegDts_sigmaxx, float* dataRegDts_sigmayy, float* dataRegDts_sigmazz,
+                               float* dataRegDts_sigmaxz, float* dataRegDts_sigmaxy, float* dataRegDts_sigmayz,
+                               long long* sourcesPositionRegCenterGrid, long long nSourcesRegCenterGrid,
+                               long long* sourcesPositionRegXGrid, long long nSourcesRegXGrid,
+                               long long* sourcesPositionRegYGrid, long long nSourcesRegYGrid,
+                               long long* sourcesPositionRegZGrid, long long nSourcesRegZGrid,
+                               long long* sourcesPositionRegXZGrid, long long nSourcesRegXZGrid,
+                               long long* sourcesPositionRegXYGrid, long long nSourcesRegXYGrid,
+                               long long* sourcesPositionRegYZGrid, long long nSourcesRegYZGrid,
+                               long long* receiversPositionRegCenterGrid, long long nReceiversRegCenterGrid,
+                               long long* receiversPositionRegXGrid, long long nReceiversRegXGrid,
+                               long long* receiversPositionRegYGrid, long long nReceiversRegYGrid,
+                               long long* receiversPositionRegZGrid, long long nReceiversRegZGrid,
+                               long long* receiversPositionRegXZGrid, long long nReceiversRegXZGrid,
+                               long long* receiversPositionRegXYGrid, long long nReceiversRegXYGrid,
+                               long long* receiversPositionRegYZGrid, long long nReceiversRegYZGrid, int nx,
+                               int ny, int nz, const int* ny_domDec, int nDomDec, const int* gpuList, int nGpu);
+
 /* ------------------------------------------------------------------------
  * 1b. Drop-in seam -- Born propagator
  * ---------------------------------------------------------------------- */
@@ -221,11 +279,12 @@ int e3d_context_destroy(e3d_context* ctx);
 /* Eight medium planes (see allocateNonlinearElasticGpu_3D); on_device != 0 for device pointers. */
 int e3d_set_medium(e3d_context* ctx, const float* const* planes8, int on_device);
 /* Stepper variant (autotuner hook): tile width along x (8 or 16), shared-memory
- * pipeline depth (2 or 3 stages; 2 to 4 with loader 6) and plane loader (0 plain
+ * pipeline depth (2 or 3 stages; 2 to 4 with loaders 6 to 8) and plane loader (0 plain
  * loads, 1 cp.async, 2 TMA bulk tensor copies, 3-5 TMA with a rotating y-window,
  * 6 TMA with the velocity and stress updates of a step as two CTA roles of one
  * launch, 8-wide tiles, 7 the same for the forward and time-reversed steps with
- * the exact adjoint on loader 2's stepper; 1 to 7 need nz % 4 == 0). */
+ * the exact adjoint on loader 2's stepper, 8 as 7 with each thread updating two
+ * consecutive z cells from paired shared-memory loads; 1 to 8 need nz % 4 == 0). */
 int e3d_set_stepper_variant(e3d_context* ctx, int tx, int stages, int loader);
 /* Nonlinear propagation (e3d_nl_* and the seam's propElastic*Gpu_3D): on = 1
  * (default) captures one coarse block as a CUDA graph after running the first

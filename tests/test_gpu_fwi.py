@@ -33,6 +33,7 @@ def _problem(sv, ckpt="fp32", segment=0, variant=(8, 2, "tma"), velocity="auto",
     ("fp32", 1, (8, 2, "tma"), "fp16", 1e-3, True),
     ("bf16", 4, (8, 2, "tma"), "fp16", 3e-3, True),
     ("fp32", 3, (8, 2, "tma"), "fp32", 1e-3, False),
+    ("fp16", 3, (8, 3, "split-pair"), "fp16", 1e-3, True),
     ("fp16", 4, (8, 2, "tma"), "fp16", 1e-3, False),
     ("fp32", 0, (8, 3, "split"), "fp32", 1e-3, True),
     ("fp16", 3, (8, 3, "split"), "fp16", 1e-3, True),
@@ -67,6 +68,7 @@ def test_fwi_gradient_matches_fp64_oracle(ckpt, segment, variant, velocity, tol,
     ("fp32", 2, (8, 2, "plain"), "fp32"),
     ("fp32", 5, (8, 2, "cpasync"), "fp16"),
     ("fp32", 3, (8, 3, "split"), "fp32"),
+    ("fp32", 3, (8, 3, "split-pair"), "fp32"),
 ])
 def test_ring_decimation_matches_fused_accumulators(ckpt, segment, variant, velocity):
     """The gradient with the fine levels of each block decimated from a ring (one launch per block,

@@ -23,7 +23,8 @@ def _prop(p, **kw):
 VARIANTS = [(8, 2, "plain"), (16, 2, "plain"), (8, 2, "cpasync"), (8, 3, "cpasync"), (16, 2, "cpasync"),
             (8, 2, "tma"), (8, 3, "tma"), (16, 2, "tma"), (8, 2, "tma-ring"), (16, 2, "tma-ring"),
             (8, 2, "tma-ring-ldg"), (8, 3, "tma-ring-ldg"), (8, 2, "tma-ring-ldg2"),
-            (8, 2, "split"), (8, 3, "split"), (8, 4, "split")]
+            (8, 2, "split"), (8, 3, "split"), (8, 4, "split"),
+            (8, 2, "split-pair"), (8, 3, "split-pair"), (8, 4, "split-pair")]
 
 
 @pytest.mark.parametrize("tx,stages,loader", VARIANTS)
@@ -43,7 +44,7 @@ def test_nl_forward_matches_oracle(tx, stages, loader):
     assert rel_l2(got, ref64) < 1e-5
 
 
-@pytest.mark.parametrize("loader", ["plain", "tma", "split"])
+@pytest.mark.parametrize("loader", ["plain", "tma", "split", "split-pair"])
 def test_nl_adjoint_matches_oracle(loader):
     sv, p, med, src, rec, dtw = prepared(seed=2)
     rng = np.random.default_rng(6)
@@ -51,7 +52,7 @@ def test_nl_adjoint_matches_oracle(loader):
     rpos = [d.unique for d in rec]
     dat = random_signals(rpos, p.nts, rng)
     pr = _prop(p)
-    pr.set_stepper_variant(8, 3 if loader == "split" else 2, loader)
+    pr.set_stepper_variant(8, 3 if loader.startswith("split") else 2, loader)
     pr.set_medium(med)
     got = pr.nl_adjoint(dat, spos, rpos)
     ref = O.nl_adjoint_reg(p, med, dat, spos, rpos, np.float32)
@@ -84,7 +85,7 @@ def test_born_adjoint_matches_oracle(segment, loader):
     pr = _prop(p)
     pr.set_medium(med)
     pr.set_checkpoint_policy("fp32", segment)
-    pr.set_stepper_variant(8, 3 if loader == "split" else 2, loader)
+    pr.set_stepper_variant(8, 3 if loader.startswith("split") else 2, loader)
     got = pr.born_adjoint(sig, dat, spos, rpos)
     ref = O.born_adjoint_reg(p, med, sig, dat, spos, rpos, None, np.float32)
     assert rel_l2(got, ref) < 1e-5
