@@ -58,6 +58,7 @@ SIGNATURES = {
     "e3d_checkpoint_segment": ([P], I),
     "e3d_nl_forward": ([P] * 7, I),
     "e3d_nl_adjoint": ([P] * 7, I),
+    "e3d_nl_propagate_slabs": ([P, I, I, I] + [P] * 6, I),
     "e3d_born_forward": ([P] * 8, I),
     "e3d_born_adjoint": ([P] * 8, I),
     "e3d_nl_propagate_device": ([P, I, P, P, P, P, P, P], I),

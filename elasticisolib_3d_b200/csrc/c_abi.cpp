@@ -415,6 +415,20 @@ int e3d_nl_adjoint(e3d_context* ctx, float* const* model9, const float* const* d
                          geomArrays(rec_pos, n_rec));
 }
 
+int e3d_nl_propagate_slabs(e3d_context* const* slabs, int n_slabs, int ny_global, int adjoint, float* const* model9,
+                           float* const* data9, const long long* const* src_pos, const long long* n_src,
+                           const long long* const* rec_pos, const long long* n_rec) {
+  if (!slabs || n_slabs < 1 || n_slabs > 64) return fail(E3D_ERR_ARG, "bad slab list");
+  if (!src_pos || !n_src || !rec_pos || !n_rec) return fail(E3D_ERR_ARG, "null geometry");
+  std::vector<Context*> cs;
+  for (int i = 0; i < n_slabs; i++) {
+    if (!slabs[i] || !slabs[i]->c) return fail(E3D_ERR_ARG, "null slab context");
+    cs.push_back(slabs[i]->c);
+  }
+  return nlPropagateSlabsHost(cs.data(), n_slabs, ny_global, adjoint != 0, model9, data9,
+                              geomArrays(src_pos, n_src), geomArrays(rec_pos, n_rec));
+}
+
 int e3d_born_forward(e3d_context* ctx, const float* const* src9, float* const* data9, const long long* const* src_pos,
                      const long long* n_src, const long long* const* rec_pos, const long long* n_rec,
                      const float* const* pert8) {

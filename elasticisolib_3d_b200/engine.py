@@ -69,6 +69,54 @@ def checkpoint_plan(n_cells, ny, nts, budget_bytes, ckpt="auto", velocity="auto"
     return ("fp32", "fp16", "bf16")[ck.value], ("fp32", "fp16")[vt.value], L.value, b.value
 
 
+class SlabPropagator:
+    """One grid decomposed into y-slabs (the reference's domain decomposition): a Propagator per
+    slab, each over ny_domdec[s] planes of the medium, slab s starting at global plane
+    sum(ny_domdec[:s]) - 2*FAT*s; nl_forward / nl_adjoint take and return what Propagator's do on
+    the whole grid (global positions) and give the same traces (e3d_nl_propagate_slabs).  The
+    slabs may share a device."""
+
+    def __init__(self, nz, nx, ny, nts, sub, minPad, dz, dx, dy, dts, alphaCos=0.99, devices=(0, 1),
+                 ny_domdec=None, **kw):
+        self.ny, self.nts = int(ny), int(nts)
+        self.sizes = list(ny_domdec) if ny_domdec is not None else domain_decomposition(ny, len(devices), 4, minPad)
+        if len(self.sizes) != len(devices):
+            raise ValueError("one slab size per device")
+        self.y0 = [0]
+        for sz in self.sizes[:-1]:
+            self.y0.append(self.y0[-1] + sz - 8)
+        self.slabs = [Propagator(nz, nx, sz, nts, sub, minPad, dz, dx, dy, dts, alphaCos, device=d, **kw)
+                      for sz, d in zip(self.sizes, devices)]
+
+    def set_medium(self, planes8):
+        """Eight scaled medium planes of the whole grid, numpy (8, ny, nx, nz)."""
+        for pr, y0, sz in zip(self.slabs, self.y0, self.sizes):
+            pr.set_medium(np.ascontiguousarray(np.asarray(planes8)[:, y0:y0 + sz]))
+
+    def _run(self, adjoint, model, data, src_pos7, rec_pos7):
+        SP, SN, k1 = _geom(src_pos7)
+        RP, RN, k2 = _geom(rec_pos7)
+        hs = (ctypes.c_void_p * len(self.slabs))(*[pr.handle.value for pr in self.slabs])
+        N.call("e3d_nl_propagate_slabs", hs, len(self.slabs), self.ny, int(adjoint), N.ptr_array(model),
+               N.ptr_array(data), SP, SN, RP, RN)
+
+    def nl_forward(self, model9, src_pos7, rec_pos7):
+        model = [N.as_f32(m) for m in model9]
+        data = [np.zeros((len(rec_pos7[COMP_GRID[k]]), self.nts), dtype=np.float32) for k in range(9)]
+        self._run(False, model, data, src_pos7, rec_pos7)
+        return data
+
+    def nl_adjoint(self, data9, src_pos7, rec_pos7):
+        data = [N.as_f32(d) for d in data9]
+        model = [np.zeros((len(src_pos7[COMP_GRID[k]]), self.nts), dtype=np.float32) for k in range(9)]
+        self._run(True, model, data, src_pos7, rec_pos7)
+        return model
+
+    def close(self):
+        for pr in self.slabs:
+            pr.close()
+
+
 class BatchTables:
     """Stacked device tables of a batched forward (see Propagator.batch_tables)."""
 

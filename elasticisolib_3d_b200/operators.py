@@ -41,7 +41,7 @@ from concurrent.futures import ThreadPoolExecutor
 import numpy as np
 
 from . import hostprep as H
-from .engine import COMP_GRID, Propagator
+from .engine import COMP_GRID, Propagator, SlabPropagator, domain_decomposition
 
 
 def _nd(v):
@@ -194,6 +194,8 @@ def born_planes_to_model(planes8, scaling3, dtw):
 class _ShotOperatorBase:
     """Shared set-up: finite-difference parameters, per-GPU contexts and acquisition lists."""
 
+    _slab_capable = False  # the operator can run a shot over y-slabs (domDec=1)
+
     def __init__(self, domain, range, elasticParam, paramP, devices14):
         self.setDomainRange(domain, range)
         self.par = paramP
@@ -209,22 +211,35 @@ class _ShotOperatorBase:
         self.constantRecGeom = len(self.rec[0]) == 1
         if not self.constantRecGeom and any(len(r) != self.nExp for r in self.rec):
             raise ValueError("receiver acquisition lists must have one entry or one per shot")
+        # domDec=1: every shot runs over y-slabs of the grid, one per listed GPU
+        # (nonlinearPropElasticShotsGpu_3D.cpp:43-77); the slabs may share a device
+        self.domDec = paramP.getInt("domDec", 0) == 1
+        if self.domDec and not self._slab_capable:
+            raise ValueError("domain decomposition is built for the nonlinear operators only")
         gpus = str(paramP.getString("iGpu", "-1"))
         ids = [int(t) for t in gpus.split(",") if t.strip() != ""]
         if ids and ids[0] >= 0:
-            if len(set(ids)) != len(ids):
+            if len(set(ids)) != len(ids) and not self.domDec:
                 raise ValueError("duplicate GPU ids in iGpu")
-            self.gpus = sorted(ids)
+            self.gpus = ids if self.domDec else sorted(ids)
         else:
             self.gpus = list(builtins.range(paramP.getInt("nGpu", 1)))
-        if len(self.gpus) > self.nExp:
+        if len(self.gpus) > self.nExp and not self.domDec:
             raise ValueError("more GPUs than shots to model")
         fd = self.fd
         # freeSurface=1 in the parameters runs the free surface (nonlinear operators only: the
         # engine refuses it on the Born path, which has no exact adjoint of it)
-        self.props = [Propagator(fd.nz, fd.nx, fd.ny, fd.nts, fd.sub, fd.minPad, float(fd.dz), float(fd.dx),
-                                 float(fd.dy), float(fd.dts), float(fd.alphaCos), device=g,
-                                 free_surface=int(fd.freeSurface)) for g in self.gpus]
+        if self.domDec:
+            if len(self.gpus) < 2:
+                raise ValueError("cannot use domain decomposition on a single card")
+            self.props = [SlabPropagator(fd.nz, fd.nx, fd.ny, fd.nts, fd.sub, fd.minPad, float(fd.dz), float(fd.dx),
+                                         float(fd.dy), float(fd.dts), float(fd.alphaCos), devices=self.gpus,
+                                         ny_domdec=domain_decomposition(fd.ny, len(self.gpus), 4, fd.minPad),
+                                         free_surface=int(fd.freeSurface))]
+        else:
+            self.props = [Propagator(fd.nz, fd.nx, fd.ny, fd.nts, fd.sub, fd.minPad, float(fd.dz), float(fd.dx),
+                                     float(fd.dy), float(fd.dts), float(fd.alphaCos), device=g,
+                                     free_surface=int(fd.freeSurface)) for g in self.gpus]
         for pr in self.props:
             pr.set_medium(fd.planes)
         self._lock = threading.Lock()
@@ -305,6 +320,8 @@ class nonlinearPropElasticShotsGpu_3D(_ShotOperatorBase):
     slice uses the same signals for every shot.  adjoint: data -> model, with the reference's
     time-reversed stepper (its quirk Q7: not the exact transpose in heterogeneous media).
     """
+
+    _slab_capable = True
 
     def __init__(self, domain, range, elasticParam, paramP, *devices14):
         super().__init__(domain, range, elasticParam, paramP, devices14)

@@ -9,7 +9,7 @@
  *    Every function returns an int status (0 = success) instead of void;
  *    the reference printed and called exit(-1) on CUDA errors
  *    (elastic_iso_float/src/cudaErrors_3D.cu:4-27).  Host arrays are owned
- *    by the caller; outputs are overwritten, as in the reference.  The two
+ *    by the caller; outputs are overwritten, as in the reference.  The
  *    functions that took std::vector take a pointer and a count.
  *
  * 2. An explicit-context API (e3d_*) for new callers: several grids per
@@ -389,6 +389,16 @@ int e3d_nl_forward(e3d_context* ctx, const float* const* model9, float* const* d
 int e3d_nl_adjoint(e3d_context* ctx, float* const* model9, const float* const* data9,
                    const long long* const* src_pos, const long long* n_src, const long long* const* rec_pos,
                    const long long* n_rec);
+/* One shot over y-slab contexts (the explicit-context form of
+ * propElasticFwdGpudomDec_3D / propElasticAdjGpudomDec_3D): slabs[s] are
+ * contexts of the same parameters created with ny_domDec[s] planes and their
+ * slab of the medium (planes shifted by the planes of the slabs before it less
+ * 2*FAT each); ny_global is the whole grid's ny.  Positions are global and the
+ * signals are as e3d_nl_forward (adjoint = 0) or e3d_nl_adjoint (adjoint = 1).
+ * The contexts may share a device. */
+int e3d_nl_propagate_slabs(e3d_context* const* slabs, int n_slabs, int ny_global, int adjoint, float* const* model9,
+                           float* const* data9, const long long* const* src_pos, const long long* n_src,
+                           const long long* const* rec_pos, const long long* n_rec);
 int e3d_born_forward(e3d_context* ctx, const float* const* src9, float* const* data9,
                      const long long* const* src_pos, const long long* n_src, const long long* const* rec_pos,
                      const long long* n_rec, const float* const* pert8);

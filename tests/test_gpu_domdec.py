@@ -109,3 +109,33 @@ def test_decomposition_refuses_sizes_that_do_not_cover_the_grid():
     del keep
     for s in range(2):
         assert lib.deallocateNonlinearElasticGpu_3D(s, 0) == 0
+
+
+def test_operator_with_domdec_equals_the_undivided_operator():
+    """The drop-in operator with domDec=1 (every shot over y-slabs, here two slabs sharing device 0
+    through iGpu=0,0) models and back-propagates as the undivided operator does."""
+    from operator_case import OperatorCase
+    from elasticisolib_3d_b200 import hostprep as H
+    from elasticisolib_3d_b200 import operators as OP
+    c = OperatorCase()
+    rng = np.random.default_rng(11)
+    model = rng.standard_normal((2, 9, c.n_sim, c.nts)).astype(np.float32)
+    data = np.zeros((2, 9, c.n_rec, c.nts), np.float32)
+    par_dd = H.ParamObj(c.par)
+    par_dd["domDec"] = 1
+    par_dd["iGpu"] = "0,0"
+    whole = OP.nonlinearPropElasticShotsGpu_3D(model, data, c.sv.elastic, c.par, *c.devices14)
+    split = OP.nonlinearPropElasticShotsGpu_3D(model, data, c.sv.elastic, par_dd, *c.devices14)
+    assert split.domDec and len(split.props[0].slabs) == 2
+    d_whole, d_split = np.zeros_like(data), np.zeros_like(data)
+    whole.forward(False, model, d_whole)
+    split.forward(False, model, d_split)
+    e = _rel([d_split], [d_whole])
+    print(f"operator forward, domDec=1 vs undivided: {e:.2e}")
+    assert np.abs(d_whole).max() > 0 and e < 1e-7
+    m_whole, m_split = np.zeros_like(model), np.zeros_like(model)
+    whole.adjoint(False, m_whole, d_whole)
+    split.adjoint(False, m_split, d_whole)
+    e = _rel([m_split], [m_whole])
+    print(f"operator adjoint, domDec=1 vs undivided: {e:.2e}")
+    assert e < 1e-7
