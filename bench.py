@@ -82,6 +82,7 @@ def kind_names(args):
            "plain": "kStep<1,8>: plain loads", "auto": "autotuned stepper"}[args.variant]
     img = {"auto": "kImagingBlock" if args.variant == "plain" else "kImagingTma", "tma": "kImagingTma",
            "tma-levels": "kImagingLev: levels staged by TMA",
+           "tma-levels-4": "kImagingLev, 4-wide tiles: levels staged by TMA",
            "cells": "kImagingBlock"}[args.imaging]
     plain = args.variant == "plain"
     acc = "kStep<0,8>: plain loads" if plain else "kStepTma<0,8>"
@@ -137,7 +138,7 @@ def parse():
     ap.add_argument("--decimation", default="ring", choices=["ring", "acc"],
                     help="gradient passes: decimate from a ring of fine levels once per coarse block (ring) "
                          "or through accumulators fused into every fine step (acc)")
-    ap.add_argument("--imaging", default="auto", choices=["auto", "cells", "tma", "tma-levels"],
+    ap.add_argument("--imaging", default="auto", choices=["auto", "cells", "tma", "tma-levels", "tma-levels-4"],
                     help="block imaging kernel of the decimation ring (Propagator.set_imaging_variant)")
     ap.add_argument("--adjoint-state", default="auto", choices=["auto", "dual"],
                     help="gradient adjoint pass: premultiplied levels only where the medium allows (auto) or "

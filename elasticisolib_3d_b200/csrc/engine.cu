@@ -103,7 +103,7 @@ struct Context {
   std::vector<Fields9> srcRing, adjRing;
   int ringMode = 1;          // 1: decimate from rings when sub allows it
   int imgChunks = 0;         // y chunks of the y-marching imaging launch (0: automatic)
-  int imgVariant = 0;        // block imaging kernel: 0 automatic, 1 kImagingBlock, 2 kImagingTma, 3 kImagingLev
+  int imgVariant = 0;        // block imaging kernel: 0 automatic, 1 kImagingBlock, 2 kImagingTma, 3/4 kImagingLev 8/4 wide
   // exact adjoint state of the ring passes: 1 premultiplied-only where the medium's premultiplication
   // is well conditioned (premCond <= kPremCondMax), 0 always the dual raw + premultiplied state
   int premMode = 1;
@@ -321,7 +321,7 @@ int setImagingChunks(Context* c, int chunks) {
 
 int setImagingVariant(Context* c, int variant) {
   E3D_ARG(c != nullptr, "null context");
-  E3D_ARG(variant >= 0 && variant <= 3, "imaging variant must be 0 (automatic), 1, 2 or 3");
+  E3D_ARG(variant >= 0 && variant <= 4, "imaging variant must be 0 (automatic), 1, 2, 3 or 4");
   c->imgVariant = variant;
   return E3D_OK;
 }
@@ -1784,43 +1784,62 @@ static int launchDecimate(Context* c, long long mEnd, float* vLeft, int leftMode
 // level (it2 = 0) is mEnd, so level it2 is mEnd - it2.  v[0..3] = V(its-1..its+2).
 // Halo and lead maps of the source velocities at the two coarse times a block images
 // (time 0 absent without a left image: any valid field stands in, it is not loaded).
-static int imagingVelocityMaps(Context* c, const ImagingBlockPtrs& q, CUtensorMap halo[2][3], CUtensorMap lead[2][3]) {
+static int imagingVelocityMaps(Context* c, const ImagingBlockPtrs& q, CUtensorMap halo[2][3], CUtensorMap lead[2][3],
+                               int itx = IMG_TX) {
   const CUtensorMap* m = nullptr;
   for (int t = 0; t < 2; t++)
     for (int k = 0; k < 3; k++) {
       const float* src = q.v[t + 1][k] ? q.v[t + 1][k] : q.v[2][k];
-      E3D_RET(tensorMap(c, src, SZ, IMG_TX + 2 * HALO, &m));
+      E3D_RET(tensorMap(c, src, SZ, itx + 2 * HALO, &m));
       halo[t][k] = *m;
-      E3D_RET(tensorMap(c, src, TZ, IMG_TX, &m));
+      E3D_RET(tensorMap(c, src, TZ, itx, &m));
       lead[t][k] = *m;
     }
   return E3D_OK;
 }
 
-// Block imaging with the levels and the medium staged by TMA (kImagingLev): one CTA per SM.
-template <int NLEV>
-static int launchImagingLev(Context* c, const ImagingBlockPtrs& q, int tiz, int tix, int nyi) {
-  constexpr int STAGES = imgLevStages(NLEV);
-  constexpr size_t smem = (size_t)STAGES * imgLevStageF(NLEV) * sizeof(float);
+// Block imaging with the levels and the medium staged by TMA (kImagingLev): ITX = 8, one CTA
+// per SM; ITX = 4, three.
+template <int NLEV, int ITX>
+static int launchImagingLev(Context* c, const ImagingBlockPtrs& q, int tiz, int nyi) {
+  constexpr int STAGES = imgLevStages(NLEV, ITX);
+  constexpr size_t smem = (size_t)STAGES * imgLevStageF(NLEV, ITX) * sizeof(float);
   static std::atomic<unsigned long long> configured{0};
-  E3D_RET(ensureSmemAttr((const void*)kImagingLev<NLEV, STAGES>, smem, configured));
+  E3D_RET(ensureSmemAttr((const void*)kImagingLev<NLEV, STAGES, ITX>, smem, configured));
   ImagingLevMaps<NLEV> mp;
-  E3D_RET(imagingVelocityMaps(c, q, mp.halo, mp.lead));
+  E3D_RET(imagingVelocityMaps(c, q, mp.halo, mp.lead, ITX));
   const CUtensorMap* m = nullptr;
   for (int j = 0; j < NLEV; j++)
     for (int k = 0; k < NCOMP; k++) {
-      E3D_RET(tensorMap(c, q.lev[j][k], TZ, IMG_TX, &m));
+      E3D_RET(tensorMap(c, q.lev[j][k], TZ, ITX, &m));
       mp.lev[j][k] = *m;
     }
   for (int k = 0; k < NMED; k++) {
-    E3D_RET(tensorMap(c, q.med[k], TZ, IMG_TX, &m));
+    E3D_RET(tensorMap(c, q.med[k], TZ, ITX, &m));
     mp.med[k] = *m;
   }
-  const int chunks0 = c->imgChunks > 0 ? std::min(c->imgChunks, nyi) : chooseChunks(c, (long long)tiz * tix, nyi, 1);
+  const int tix = (c->g.nx - 2 * FAT + ITX - 1) / ITX;
+  const int perSM = ITX == 4 ? 3 : 1;
+  const int chunks0 =
+      c->imgChunks > 0 ? std::min(c->imgChunks, nyi) : chooseChunks(c, (long long)tiz * tix, nyi, perSM);
   const int yChunk = (nyi + chunks0 - 1) / chunks0;
   const int chunks = (nyi + yChunk - 1) / yChunk;
-  kImagingLev<NLEV, STAGES><<<dim3(tiz, tix, chunks), dim3(TZ, IMG_TX), smem, c->st>>>(mp, q, c->g, yChunk);
+  kImagingLev<NLEV, STAGES, ITX><<<dim3(tiz, tix, chunks), dim3(TZ, ITX), smem, c->st>>>(mp, q, c->g, yChunk);
   return E3D_OK;
+}
+
+template <int ITX>
+static int launchImagingLevSub(Context* c, const ImagingBlockPtrs& q, int tiz, int nyi, int sub) {
+  switch (sub) {
+    case 1: return launchImagingLev<1, ITX>(c, q, tiz, nyi);
+    case 2: return launchImagingLev<2, ITX>(c, q, tiz, nyi);
+    case 3: return launchImagingLev<3, ITX>(c, q, tiz, nyi);
+    case 4: return launchImagingLev<4, ITX>(c, q, tiz, nyi);
+    case 5: return launchImagingLev<5, ITX>(c, q, tiz, nyi);
+    case 6: return launchImagingLev<6, ITX>(c, q, tiz, nyi);
+    case 7: return launchImagingLev<7, ITX>(c, q, tiz, nyi);
+    default: return launchImagingLev<8, ITX>(c, q, tiz, nyi);
+  }
 }
 
 static int launchImagingBlock(Context* c, long long mEnd, float* const v[4], bool carryIn, bool leftImage,
@@ -1859,16 +1878,9 @@ static int launchImagingBlock(Context* c, long long mEnd, float* const v[4], boo
   const int tix = (c->g.nx - 2 * FAT + IMG_TX - 1) / IMG_TX;
   const int nyi = c->g.ny - 2 * FAT;
   if (variant == 3) {
-    switch (sub) {
-      case 1: E3D_RET(launchImagingLev<1>(c, q, tiz, tix, nyi)); break;
-      case 2: E3D_RET(launchImagingLev<2>(c, q, tiz, tix, nyi)); break;
-      case 3: E3D_RET(launchImagingLev<3>(c, q, tiz, tix, nyi)); break;
-      case 4: E3D_RET(launchImagingLev<4>(c, q, tiz, tix, nyi)); break;
-      case 5: E3D_RET(launchImagingLev<5>(c, q, tiz, tix, nyi)); break;
-      case 6: E3D_RET(launchImagingLev<6>(c, q, tiz, tix, nyi)); break;
-      case 7: E3D_RET(launchImagingLev<7>(c, q, tiz, tix, nyi)); break;
-      default: E3D_RET(launchImagingLev<8>(c, q, tiz, tix, nyi)); break;
-    }
+    E3D_RET(launchImagingLevSub<8>(c, q, tiz, nyi, sub));
+  } else if (variant == 4) {
+    E3D_RET(launchImagingLevSub<4>(c, q, tiz, nyi, sub));
   } else if (variant == 2) {
     // y-marching TMA form: tensor maps of the velocity fields (cached per pointer)
     ImagingMaps mp;

@@ -2105,14 +2105,22 @@ struct ImagingLevMaps {
   CUtensorMap lev[NLEV][NCOMP];
   CUtensorMap med[NMED];
 };
-constexpr int IMG_LEV_OFF = 6 * IMG_HALO_F + 6 * IMG_INT_F;  // first level box of a stage
-__host__ __device__ constexpr int imgLevStageF(int nlev) { return IMG_LEV_OFF + (nlev * NCOMP + NMED) * IMG_INT_F; }
-// three stages where they fit in 227 KB of shared memory, else two
-__host__ __device__ constexpr int imgLevStages(int nlev) { return 3 * imgLevStageF(nlev) * 4 <= 227 * 1024 ? 3 : 2; }
+// ITX-wide tiles (8: one CTA per SM; 4: three CTAs per SM with two stages)
+__host__ __device__ constexpr int imgHaloF(int itx) { return SZ * (itx + 2 * HALO); }
+__host__ __device__ constexpr int imgIntF(int itx) { return TZ * itx; }
+__host__ __device__ constexpr int imgLevOff(int itx) { return 6 * imgHaloF(itx) + 6 * imgIntF(itx); }  // first level box
+__host__ __device__ constexpr int imgLevStageF(int nlev, int itx) {
+  return imgLevOff(itx) + (nlev * NCOMP + NMED) * imgIntF(itx);
+}
+// 8-wide tiles: three stages where they fit in 227 KB of shared memory, else two; 4-wide: two
+__host__ __device__ constexpr int imgLevStages(int nlev, int itx) {
+  return itx == 8 && 3 * imgLevStageF(nlev, itx) * 4 <= 227 * 1024 ? 3 : 2;
+}
 
-template <int NLEV>
+template <int NLEV, int ITX>
 __device__ __forceinline__ void imgLevIssuePlane(const ImagingLevMaps<NLEV>& mp, float* st, unsigned long long* bar,
                                                  int y, int z0, int x0, int ntimes, bool prem) {
+  constexpr int IMG_HALO_F = imgHaloF(ITX), IMG_INT_F = imgIntF(ITX), IMG_LEV_OFF = imgLevOff(ITX);
   const unsigned floats = (unsigned)(ntimes * 3 * (IMG_HALO_F + IMG_INT_F) + (NLEV * NCOMP + (prem ? NMED : 0)) * IMG_INT_F);
   mbarExpectTx(bar, floats * 4u);
   for (int t = 2 - ntimes; t < 2; t++)
@@ -2132,10 +2140,11 @@ __device__ __forceinline__ void imgLevIssuePlane(const ImagingLevMaps<NLEV>& mp,
       tmaLoad3d(st + IMG_LEV_OFF + (NLEV * NCOMP + k) * IMG_INT_F, &mp.med[k], z0, x0, y, bar);
 }
 
-template <int NLEV, int STAGES>
-__global__ void __launch_bounds__(TZ * IMG_TX, 1) kImagingLev(const __grid_constant__ ImagingLevMaps<NLEV> mp,
-                                                              ImagingBlockPtrs q, GridConst g, int yChunk) {
-  constexpr int SF = imgLevStageF(NLEV);
+template <int NLEV, int STAGES, int ITX>
+__global__ void __launch_bounds__(TZ * ITX, ITX == 4 ? 3 : 1) kImagingLev(const __grid_constant__ ImagingLevMaps<NLEV> mp,
+                                                                          ImagingBlockPtrs q, GridConst g, int yChunk) {
+  constexpr int SF = imgLevStageF(NLEV, ITX);
+  constexpr int IMG_TX = ITX, IMG_HALO_F = imgHaloF(ITX), IMG_INT_F = imgIntF(ITX), IMG_LEV_OFF = imgLevOff(ITX);
   extern __shared__ __align__(1024) float smem[];
   __shared__ __align__(8) unsigned long long bars[STAGES];
   const int tz = threadIdx.x, tx = threadIdx.y;
@@ -2158,7 +2167,7 @@ __global__ void __launch_bounds__(TZ * IMG_TX, 1) kImagingLev(const __grid_const
   __syncthreads();
   if (tid == 0)
     for (int s = 0; s < STAGES - 1; s++)
-      if (yBeg + s < yEnd) imgLevIssuePlane<NLEV>(mp, smem + s * SF, &bars[s], yBeg + s, z0, x0, ntimes, prem);
+      if (yBeg + s < yEnd) imgLevIssuePlane<NLEV, ITX>(mp, smem + s * SF, &bars[s], yBeg + s, z0, x0, ntimes, prem);
   float w[2][3][8];
   if (active) {
 #pragma unroll
@@ -2202,7 +2211,7 @@ __global__ void __launch_bounds__(TZ * IMG_TX, 1) kImagingLev(const __grid_const
       const int yn = y + STAGES - 1;
       int ns = slot + STAGES - 1;
       if (ns >= STAGES) ns -= STAGES;
-      if (yn < yEnd) imgLevIssuePlane<NLEV>(mp, smem + ns * SF, &bars[ns], yn, z0, x0, ntimes, prem);
+      if (yn < yEnd) imgLevIssuePlane<NLEV, ITX>(mp, smem + ns * SF, &bars[ns], yn, z0, x0, ntimes, prem);
     }
     const float* st = smem + slot * SF;
     if (active) {

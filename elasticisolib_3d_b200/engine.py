@@ -373,7 +373,7 @@ class Propagator:
         """y chunks of the block imaging launch (0 = automatic)."""
         N.call("e3d_set_imaging_chunks", self._h, int(chunks))
 
-    IMAGING = {"auto": 0, "cells": 1, "tma": 2, "tma-levels": 3}
+    IMAGING = {"auto": 0, "cells": 1, "tma": 2, "tma-levels": 3, "tma-levels-4": 4}
 
     def set_imaging_variant(self, variant="auto"):
         """Block imaging kernel: auto, cells (one thread per cell, global loads), tma (velocity tiles

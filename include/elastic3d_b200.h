@@ -345,8 +345,9 @@ int e3d_set_imaging_chunks(e3d_context* ctx, int chunks);
  * reading every operand from global memory, 2 = y-march with the velocity
  * tiles staged by TMA and the adjoint levels read per cell, 3 = y-march with
  * the velocity tiles, the adjoint levels and the medium staged by TMA (one
- * CTA per SM; measured slower than 2 on B200 at sub = 4).  The same sums in
- * the same order; a tuning knob with no counterpart in the reference. */
+ * CTA per SM; measured slower than 2 on B200 at sub = 4), 4 = 3 on 4-wide
+ * tiles (three CTAs per SM).  The same sums in the same order; a tuning knob
+ * with no counterpart in the reference. */
 int e3d_set_imaging_variant(e3d_context* ctx, int variant);
 /* State of the exact adjoint (the transpose of stepFwdGpu_3D's update, as
  * stepAdjGpuBorn_3D, kernelsElaGpu_3D.cu:825-1177) in the checkpointed passes

@@ -127,7 +127,7 @@ def test_imaging_variants_agree(prem, segment):
     orc = OracleFwi(sv)
     d_obs, _ = orc.data(true)
     grads = []
-    variants = ("cells", "tma", "tma-levels")
+    variants = ("cells", "tma", "tma-levels", "tma-levels-4")
     for variant in variants:
         prob, src, rec = _problem(sv, "fp32", segment, (8, 3, "split-fwd"), "fp32", True, prem)
         prob.prop.set_imaging_variant(variant)
