@@ -1117,18 +1117,18 @@ static int nlBlock(Context* c, bool adjoint, const DevSignals& srcSet, const Dev
   return E3D_OK;
 }
 
-// Capture one coarse block (device-indexed, then the index advanced by `delta`)
-// into an executable graph.  Counted launches of the capture are returned in
-// *perBlock and taken back out of the context's count.
-static int captureBlock(Context* c, bool adjoint, const DevSignals& srcSet, const DevSignals& recSet,
-                        float* srcSig, float* recSig, cudaGraphExec_t* exec, long long* perBlock) {
+// Capture one coarse block (block(idx) with the device-resident coarse index,
+// then the index advanced by `delta`) into an executable graph.  Counted launches
+// of the capture are returned in *perBlock and taken back out of the context's count.
+template <class Block>
+static int captureBlockWith(Context* c, Block block, int delta, cudaGraphExec_t* exec, long long* perBlock) {
   const long long before = c->launches;
   cudaGraph_t graph = nullptr;
   E3D_CUDA_TRY(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
   c->inCapture = true;
-  int st = nlBlock(c, adjoint, srcSet, recSet, srcSig, recSig, 0, c->blockIndex);
+  int st = block(c->blockIndex);
   if (st == E3D_OK) {
-    kAdvanceIndex<<<1, 32, 0, c->st>>>(c->blockIndex, adjoint ? -1 : 1);
+    kAdvanceIndex<<<1, 32, 0, c->st>>>(c->blockIndex, delta);
     c->launches++;
     if (cudaGetLastError() != cudaSuccess) {
       setLastError("index advance launch failed", __FILE__, __LINE__);
@@ -1151,6 +1151,41 @@ static int captureBlock(Context* c, bool adjoint, const DevSignals& srcSet, cons
     }
   }
   if (graph) cudaGraphDestroy(graph);
+  return st;
+}
+
+// Replay of coarse blocks 1..blocks-1 after block 0 ran eagerly: one captured block (two when
+// sub is odd, for the two pointer parities of the leapfrog levels lv0/lv1), the coarse index on
+// the device starting at `next` and moving by `delta`.
+template <class Block>
+static int replayBlocks(Context* c, Block block, int blocks, int next, int delta, Fields9& lv0, Fields9& lv1) {
+  if (!c->blockIndex) E3D_RET(devAlloc(c, (void**)&c->blockIndex, sizeof(int)));
+  kSetIndex<<<1, 32, 0, c->st>>>(c->blockIndex, next);
+  c->launches++;
+  E3D_LAUNCH_CHECK();
+  const int sub = c->d.sub;
+  const int ng = (sub % 2) ? 2 : 1;
+  cudaGraphExec_t exec[2] = {nullptr, nullptr};
+  long long perBlock[2] = {0, 0};
+  int st = E3D_OK;
+  for (int i = 0; i < ng && st == E3D_OK; i++) st = captureBlockWith(c, block, delta, &exec[i], &perBlock[i]);
+  for (int b = 1; b < blocks && st == E3D_OK; b++) {
+    const int i = (b - 1) % ng;
+    const cudaError_t e = cudaGraphLaunch(exec[i], c->st);
+    if (e != cudaSuccess) {
+      setLastError(cudaGetErrorString(e), __FILE__, __LINE__);
+      st = E3D_ERR_CUDA;
+    }
+    c->launches += perBlock[i];
+  }
+  // the host-side level pointers follow the replayed blocks: each capture swapped them sub
+  // times, and capture ng - 1 more blocks' worth than ran
+  if (st == E3D_OK) {
+    const long long swapsCaptured = (long long)ng * sub, swapsRun = (long long)(blocks - 1) * sub;
+    if ((swapsCaptured + swapsRun) % 2) swapF(lv0, lv1);
+  }
+  for (int i = 0; i < ng; i++)
+    if (exec[i]) cudaGraphExecDestroy(exec[i]);
   return st;
 }
 
@@ -1235,7 +1270,8 @@ int nlForwardBatchDevice(Context* c, int shots, const DevSignals& srcSet, const 
   }
   const int nts = c->d.nts, sub = c->d.sub;
   E3D_CUDA_TRY(cudaMemsetAsync(recSig, 0, (size_t)std::max(recSet.off[NCOMP], 1) * nts * sizeof(float), c->st));
-  for (int its = 0; its < nts - 1; its++)
+  // one coarse block (its, or the device index idx) of all shots
+  auto block = [&](int its, const int* idx) -> int {
     for (int it2 = 1; it2 <= sub; it2++) {
       StepPtrs p = makeStep(c, c->bw0, c->bw1);
       {
@@ -1243,11 +1279,23 @@ int nlForwardBatchDevice(Context* c, int shots, const DevSignals& srcSet, const 
         TimedLaunch t(c, STEP_FWD);
         E3D_RET(launchSplitBatch<STEP_FWD>(c, p, shots));
       }
-      E3D_RET(launchInject(c, p, srcSet, srcSig, its, it2 - 1));
-      E3D_RET(launchRecord(c, p, recSet, recSig, its, it2));
+      if (idx) E3D_RET(launchInjectIdx(c, p, srcSet, srcSig, idx, it2 - 1));
+      else E3D_RET(launchInject(c, p, srcSet, srcSig, its, it2 - 1));
+      if (idx) E3D_RET(launchRecordIdx(c, p, recSet, recSig, idx, it2));
+      else E3D_RET(launchRecord(c, p, recSet, recSig, its, it2));
       swapF(c->bw0, c->bw1);
     }
-  return E3D_OK;
+    return E3D_OK;
+  };
+  const int blocks = nts - 1;
+  const bool graph = c->graphLoop && c->st != nullptr && c->timingEvery == 0 && blocks >= 4;
+  if (!graph) {
+    for (int its = 0; its < blocks; its++) E3D_RET(block(its, nullptr));
+    return E3D_OK;
+  }
+  // the time loop as replays of one captured coarse block, as nlPropagateDevice
+  E3D_RET(block(0, nullptr));
+  return replayBlocks(c, [&](const int* idx) { return block(0, idx); }, blocks, 1, 1, c->bw0, c->bw1);
 }
 
 int nlPropagateDevice(Context* c, bool adjoint, const DevSignals& srcSet, const DevSignals& recSet, float* srcSig,
@@ -1269,30 +1317,9 @@ int nlPropagateDevice(Context* c, bool adjoint, const DevSignals& srcSet, const 
     return E3D_OK;
   }
   E3D_RET(nlBlock(c, adjoint, srcSet, recSet, srcSig, recSig, first, nullptr));
-  if (!c->blockIndex) E3D_RET(devAlloc(c, (void**)&c->blockIndex, sizeof(int)));
-  kSetIndex<<<1, 32, 0, c->st>>>(c->blockIndex, first + dir);
-  c->launches++;
-  E3D_LAUNCH_CHECK();
-  const int ng = (sub % 2) ? 2 : 1;
-  cudaGraphExec_t exec[2] = {nullptr, nullptr};
-  long long perBlock[2] = {0, 0};
-  int st = E3D_OK;
-  for (int i = 0; i < ng && st == E3D_OK; i++)
-    st = captureBlock(c, adjoint, srcSet, recSet, srcSig, recSig, &exec[i], &perBlock[i]);
-  for (int b = 1; b < blocks && st == E3D_OK; b++) {
-    const int i = (b - 1) % ng;
-    const cudaError_t e = cudaGraphLaunch(exec[i], c->st);
-    if (e != cudaSuccess) {
-      setLastError(cudaGetErrorString(e), __FILE__, __LINE__);
-      st = E3D_ERR_CUDA;
-    }
-    c->launches += perBlock[i];
-  }
-  // the host-side level pointers follow the replayed blocks
-  if (st == E3D_OK && ((long long)(blocks - 1) * sub) % 2) swapF(c->w0, c->w1);
-  for (int i = 0; i < ng; i++)
-    if (exec[i]) cudaGraphExecDestroy(exec[i]);
-  return st;
+  return replayBlocks(
+      c, [&](const int* idx) { return nlBlock(c, adjoint, srcSet, recSet, srcSig, recSig, 0, idx); }, blocks,
+      first + dir, dir, c->w0, c->w1);
 }
 
 int nlPropagateHost(Context* c, bool adjoint, float* const* model, float* const* data, const HostGeom& src,

@@ -120,18 +120,20 @@ class SlabPropagator:
 class BatchTables:
     """Stacked device tables of a batched forward (see Propagator.batch_tables)."""
 
-    def __init__(self, shots, src_pos, src_off, rec_pos, rec_off, src_sig, rec_sig):
+    def __init__(self, shots, src_pos, src_off, rec_pos, rec_off, src_sig, rec_sig, lengths=None):
         self.shots, self.src_pos, self.src_off = shots, src_pos, list(src_off)
         self.rec_pos, self.rec_off, self.src_sig, self.rec_sig = rec_pos, list(rec_off), src_sig, rec_sig
+        self.lengths = list(lengths) if lengths is not None else [src_sig.shape[0]] * shots
 
     def split(self, out):
-        """Per-shot nine receiver blocks (n_k, nts) of a receiver-major array out (total, nts)."""
+        """Per-shot nine receiver blocks (n_k, nts_s) of a receiver-major array out (total, nts),
+        each shot's traces cut to its own record length."""
         data = [[None] * 9 for _ in range(self.shots)]
         for k in range(9):
             nk = (self.rec_off[k + 1] - self.rec_off[k]) // self.shots
             for s in range(self.shots):
                 a = self.rec_off[k] + s * nk
-                data[s][k] = np.ascontiguousarray(out[a:a + nk])
+                data[s][k] = np.ascontiguousarray(out[a:a + nk, :self.lengths[s]])
         return data
 
 
@@ -241,17 +243,26 @@ class Propagator:
             for s in range(S):
                 tab = np.asarray(src_pos7s[s][COMP_GRID[k]], dtype=np.int64)
                 src_pos.append(tab + s * n)
-                sig.append(np.asarray(models[s][k], dtype=np.float32).reshape(len(tab), self.nts))
+                blk = np.asarray(models[s][k], dtype=np.float32).reshape(len(tab), -1)
+                # a shorter record is the same shot propagated to the longest one and cut
+                sig.append(np.pad(blk, ((0, 0), (0, self.nts - blk.shape[1]))) if blk.shape[1] < self.nts else blk)
             src_off.append(src_off[-1] + sum(len(src_pos7s[s][COMP_GRID[k]]) for s in range(S)))
             # the reference's sxz receivers read the first n_xz entries of the z-grid table (quirk Q2)
             rk = rtab[3][:len(rtab[4])] if (self.q2compat and k == 6) else rtab[COMP_GRID[k]]
             for s in range(S):
                 rec_pos.append(rk + s * n)
             rec_off.append(rec_off[-1] + S * len(rk))
+        lengths = []
+        for s in range(S):
+            ks = [k for k in range(9) if len(src_pos7s[s][COMP_GRID[k]])]
+            lengths.append(int(np.asarray(models[s][ks[0]]).reshape(len(src_pos7s[s][COMP_GRID[ks[0]]]), -1).shape[1])
+                           if ks else self.nts)
+            if lengths[-1] > self.nts:
+                raise ValueError("a shot's record is longer than the propagator's nts")
         return BatchTables(S, torch.from_numpy(np.concatenate(src_pos)).to(dev), src_off,
                            torch.from_numpy(np.concatenate(rec_pos)).to(dev), rec_off,
                            torch.from_numpy(np.ascontiguousarray(np.concatenate(sig, axis=0).T)).to(dev),
-                           torch.empty((self.nts, rec_off[-1]), dtype=torch.float32, device=dev))
+                           torch.empty((self.nts, rec_off[-1]), dtype=torch.float32, device=dev), lengths)
 
     def nl_forward_batch_device(self, bt):
         """Launch the batched forward of BatchTables bt on the context's stream (asynchronous); the
@@ -262,7 +273,9 @@ class Propagator:
 
     def nl_forward_batch(self, models, src_pos7s, rec_pos7):
         """Batched nonlinear forward of several shots in one medium: one list of nine receiver
-        blocks per shot, as nl_forward returns for each shot alone."""
+        blocks per shot, as nl_forward returns for each shot alone.  Shots may have different
+        record lengths (the widths of their source blocks, at most nts): a shorter shot is
+        propagated to nts with zero sources and its traces cut to its own length."""
         bt = self.batch_tables(models, src_pos7s, rec_pos7)
         self.nl_forward_batch_device(bt)
         N.call("e3d_synchronize", self._h)

@@ -74,3 +74,24 @@ def test_batched_forward_rejects_a_position_outside_its_shot():
     assert rel_l2(got[1], pr.nl_forward(models[1], spos[1], rpos)) < 1e-6
     del torch
     pr.close()
+
+
+def test_batched_forward_with_different_record_lengths():
+    """Shots of one batch may have different record lengths (the widths of their source blocks):
+    a shorter shot's traces are the first samples of the same shot propagated on the context's
+    time axis with zero sources after its end."""
+    p, med, spos, rpos = _shots(3, seed=12)
+    rng = np.random.default_rng(13)
+    lengths = [p.nts, p.nts - 5, p.nts - 9]
+    models = [[m[:, :L].copy() for m in random_signals(sp, p.nts, rng)] for sp, L in zip(spos, lengths)]
+    pr = Propagator(p.nz, p.nx, p.ny, p.nts, p.sub, p.minPad, p.dz, p.dx, p.dy, p.dts, p.alphaCos, q2compat=0)
+    pr.set_medium(med)
+    batched = pr.nl_forward_batch(models, spos, rpos)
+    for s, L in enumerate(lengths):
+        padded = [np.pad(m, ((0, 0), (0, p.nts - L))) for m in models[s]]
+        single = pr.nl_forward(padded, spos[s], rpos)
+        assert all(b.shape[1] == L for b in batched[s])
+        e = rel_l2(batched[s], [x[:, :L] for x in single])
+        print(f"record length {L} of {p.nts}: batched vs single {e:.2e}")
+        assert e < 1e-6
+    pr.close()
