@@ -100,7 +100,7 @@ def kind_names(args):
 def profiled(kind, args):
     """The ncu summary whose DRAM bytes per cell stand for this kind's launches, where it profiled
     the same kernel."""
-    table = dict(PROFILE_COMMON, **PROFILES.get(args.variant, {})) if args.variant in PROFILES else {}
+    table = {**PROFILE_COMMON, **PROFILES[args.variant]} if args.variant in PROFILES else {}
     if kind not in table:
         return None
     if kind == 6 and args.imaging not in ("auto", "tma"):
@@ -117,7 +117,7 @@ def kind_bytes(kind, sub, prem=False, dual=True):
             3: 188.0, 5: adj_acc}[kind]
 
 
-def parse():
+def parse(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=1)
@@ -146,7 +146,7 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--breakdown", action="store_true",
                     help="after the measurement, print the device time per kernel of one more gradient")
-    return ap.parse_args()
+    return ap.parse_args(argv)
 
 
 class ClockSampler:
