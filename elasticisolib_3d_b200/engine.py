@@ -13,6 +13,7 @@ import ctypes
 import numpy as np
 
 from . import _native as N
+from .hostprep import FAT
 
 # grid of each wavefield component: vx->x, vy->y, vz->z, sxx/syy/szz->center, sxz->xz, sxy->xy, syz->yz
 COMP_GRID = (1, 2, 3, 0, 0, 0, 4, 5, 6)
@@ -26,11 +27,12 @@ def _geom(pos7):
     return P, C, pos
 
 
-def domain_decomposition(ny, n_gpu, fat=4, min_pad=0):
+def domain_decomposition(ny, n_gpu, fat=None, min_pad=0):
     """y-slab sizes (ny_domDec) of a grid of ny planes over n_gpu GPUs, by the reference's rule
     (nonlinearPropElasticShotsGpu_3D.cpp:48-76): slab 0 takes ny//n_gpu + fat planes, middle slabs
     ny//n_gpu + 2*fat, the last the rest + fat; neighbours overlap by 2*fat planes.  Raises
     ValueError where the reference refuses the split (one GPU, or too few planes per slab)."""
+    fat = FAT if fat is None else fat
     if n_gpu < 2:
         raise ValueError("domain decomposition needs at least two GPUs")
     chunk = ny // n_gpu
@@ -79,12 +81,13 @@ class SlabPropagator:
     def __init__(self, nz, nx, ny, nts, sub, minPad, dz, dx, dy, dts, alphaCos=0.99, devices=(0, 1),
                  ny_domdec=None, **kw):
         self.ny, self.nts = int(ny), int(nts)
-        self.sizes = list(ny_domdec) if ny_domdec is not None else domain_decomposition(ny, len(devices), 4, minPad)
+        self.sizes = list(ny_domdec) if ny_domdec is not None else domain_decomposition(ny, len(devices), FAT,
+                                                                                           minPad)
         if len(self.sizes) != len(devices):
             raise ValueError("one slab size per device")
         self.y0 = [0]
         for sz in self.sizes[:-1]:
-            self.y0.append(self.y0[-1] + sz - 8)
+            self.y0.append(self.y0[-1] + sz - 2 * FAT)  # neighbours overlap by 2*FAT planes
         self.slabs = [Propagator(nz, nx, sz, nts, sub, minPad, dz, dx, dy, dts, alphaCos, device=d, **kw)
                       for sz, d in zip(self.sizes, devices)]
 
