@@ -42,6 +42,30 @@ def domain_decomposition(ny, n_gpu, fat=None, min_pad=0):
     return sizes
 
 
+def forward_batch_plan(n_shots, n_cells, nts, src_points, rec_points, free_bytes, margin=0.9):
+    """Shots per batched forward launch admitted by device memory: each shot of a batch holds both
+    leapfrog levels of the nine fields (18 * n_cells floats), its time-major source and receiver
+    signals (nts * (src_points + rec_points) floats) and its position tables (8 B per point);
+    at most `margin` of `free_bytes` is used.  Returns the batches as lists of shot indices, as
+    even in size as the budget allows.  ValueError when not even one shot fits."""
+    if n_shots < 1:
+        return []
+    per_shot = 18 * int(n_cells) * 4 + int(nts) * (int(src_points) + int(rec_points)) * 4 + \
+        8 * (int(src_points) + int(rec_points))
+    k = int(margin * float(free_bytes)) // per_shot
+    if k < 1:
+        raise ValueError(f"one shot needs {per_shot / 1e9:.2f} GB of device memory, "
+                         f"{margin * float(free_bytes) / 1e9:.2f} GB are available")
+    n_batches = -(-n_shots // min(k, n_shots))
+    base, extra = divmod(n_shots, n_batches)
+    out, start = [], 0
+    for b in range(n_batches):
+        size = base + (1 if b < extra else 0)
+        out.append(list(range(start, start + size)))
+        start += size
+    return out
+
+
 def checkpoint_schedule(blocks, segment_len):
     """Checkpoint schedule of a record of `blocks` coarse blocks (nts - 1) with segments of
     `segment_len` blocks, as the engine runs it: (first block of each segment followed by
@@ -283,6 +307,22 @@ class Propagator:
         self.nl_forward_batch_device(bt)
         N.call("e3d_synchronize", self._h)
         return bt.split(bt.rec_sig.cpu().numpy().T)
+
+    def nl_forward_shots(self, models, src_pos7s, rec_pos7, free_bytes=None, margin=0.9):
+        """Forward modelling of any number of shots: the shots are admitted into batched launches
+        (nl_forward_batch) by the device memory free now (or `free_bytes`), as forward_batch_plan
+        deals them.  Returns one list of nine receiver blocks per shot, in shot order."""
+        import torch
+        if free_bytes is None:
+            free_bytes, _ = torch.cuda.mem_get_info(torch.device("cuda", self.device))
+        src_points = max(sum(len(sp[COMP_GRID[k]]) for k in range(9)) for sp in src_pos7s) if src_pos7s else 0
+        rec_points = sum(len(rec_pos7[COMP_GRID[k]]) for k in range(9))
+        plan = forward_batch_plan(len(models), self.nz * self.nx * self.ny, self.nts, src_points, rec_points,
+                                  free_bytes, margin)
+        out = []
+        for batch in plan:
+            out.extend(self.nl_forward_batch([models[i] for i in batch], [src_pos7s[i] for i in batch], rec_pos7))
+        return out
 
     def nl_adjoint(self, data9, src_pos7, rec_pos7):
         data = [N.as_f32(d) for d in data9]

@@ -54,3 +54,27 @@ def test_seam_refuses_bad_decompositions_before_any_gpu_work(name):
     assert _call(name, [64], [0]) == E3D_ERR_ARG
     assert _call(name, [36, 36], [0]) == E3D_ERR_ARG
     assert _call(name, [36, 36], [0, 0]) == E3D_ERR_STATE
+
+
+# ---- admission of shots into batched forward launches (host arithmetic) ----------------------
+from elasticisolib_3d_b200.engine import forward_batch_plan  # noqa: E402
+
+
+def test_batches_fit_the_budget_and_keep_every_shot_once():
+    n_cells, nts, sp, rp = 392 * 488 * 488, 2000, 27, 9 * 40000
+    per_shot = 18 * n_cells * 4 + nts * (sp + rp) * 4 + 8 * (sp + rp)
+    for n_shots in (1, 3, 16, 17):
+        for free in (1.2 * per_shot, 3.3 * per_shot, 180e9):
+            plan = forward_batch_plan(n_shots, n_cells, nts, sp, rp, free)
+            assert sorted(i for b in plan for i in b) == list(range(n_shots))
+            assert all(len(b) * per_shot <= 0.9 * free for b in plan)
+            sizes = [len(b) for b in plan]
+            assert max(sizes) - min(sizes) <= 1          # as even as the budget allows
+    # 180 GB: 16 shots of the 93 M-cell grid (2000 samples, 200 x 200 receivers) per launch
+    assert len(forward_batch_plan(16, n_cells, nts, sp, rp, 180e9)) == 1
+    assert forward_batch_plan(0, n_cells, nts, sp, rp, 180e9) == []
+
+
+def test_a_shot_that_does_not_fit_is_refused():
+    with pytest.raises(ValueError):
+        forward_batch_plan(4, 392 * 488 * 488, 2000, 27, 360000, 1e9)

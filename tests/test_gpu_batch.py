@@ -95,3 +95,26 @@ def test_batched_forward_with_different_record_lengths():
         print(f"record length {L} of {p.nts}: batched vs single {e:.2e}")
         assert e < 1e-6
     pr.close()
+
+
+def test_shots_admitted_by_memory_budget_equal_one_batch():
+    """nl_forward_shots deals the shots into batched launches by a memory budget; with a budget
+    that admits two shots per launch, three shots run as two launches and give the traces of one
+    batch of three."""
+    from elasticisolib_3d_b200.engine import forward_batch_plan
+    p, med, spos, rpos = _shots(3, seed=14)
+    rng = np.random.default_rng(15)
+    models = [random_signals(sp, p.nts, rng) for sp in spos]
+    pr = Propagator(p.nz, p.nx, p.ny, p.nts, p.sub, p.minPad, p.dz, p.dx, p.dy, p.dts, p.alphaCos, q2compat=0)
+    pr.set_medium(med)
+    n = p.nz * p.nx * p.ny
+    sp = max(sum(len(s[O.COMP_GRID[k]]) for k in range(9)) for s in spos)
+    rp = sum(len(rpos[O.COMP_GRID[k]]) for k in range(9))
+    per_shot = 18 * n * 4 + p.nts * (sp + rp) * 4 + 8 * (sp + rp)
+    budget = 2.5 * per_shot / 0.9
+    assert [len(b) for b in forward_batch_plan(3, n, p.nts, sp, rp, budget)] == [2, 1]
+    dealt = pr.nl_forward_shots(models, spos, rpos, free_bytes=budget)
+    whole = pr.nl_forward_batch(models, spos, rpos)
+    for s in range(3):
+        assert rel_l2(dealt[s], whole[s]) < 1e-6
+    pr.close()
