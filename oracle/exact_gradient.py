@@ -171,3 +171,74 @@ def scale_signals_t(reg9, src_pos7, planes, dx, dy, dz):
 def interp_matrix(dev):
     """The regular -> irregular map of an oracle.SpaceInterp as a dense (n_irreg, n_reg) matrix."""
     return torch.as_tensor(dev.forward(np.eye(dev.n_reg, dtype=np.float64)))
+
+
+# ---- the same gradient by a hand-written adjoint recursion ---------------------------------------
+def exact_gradient_by_adjoint(p: O.PropParams, med, src9, src_pos7, rec_pos7, drec9):
+    """Exact gradient of a functional of the recorded traces with respect to the eight medium
+    planes, by the adjoint recursion a GPU mode would run (FP64 numpy, the oracle's own steppers).
+
+    drec9: nine (n_rec_k, nts) blocks, the derivative of the functional by the recorded traces.
+    With (X_j, Y_j) the two levels at the start of fine step j, the forward step is
+    X_{j+1} = G Y_j, Y_{j+1} = G (X_j + M D(Y_j) + S_j), and step j records Y_{j+1}.  Backwards,
+    with (xi, eta) the derivatives by (X_{j+1}, Y_{j+1}):
+      eta~ = eta + the recording weights of step j applied to drec9 (at the receiver positions)
+      grad_M += (G eta~) * D(Y_j), term by term (the imaging of every fine step)
+      xi, eta <- G eta~, G xi + T(G eta~)
+    where T(q) = -D(M q) is the reference's exact-transpose stepper (stepAdjGpuBorn_3D,
+    kernelsElaGpu_3D.cu:825-1177) applied to q from zero.  The sources are held fixed."""
+    tf = TorchForward(p, src_pos7, rec_pos7)
+    shape = (p.ny, p.nx, p.nz)
+    f, h = tf.filt, tf.h
+    G = tf.G.numpy()
+    src_idx = [s.numpy() for s in tf.src]
+    rec_idx = [r.numpy() for r in tf.rec]
+    steps = [(its, it2) for its in range(p.nts - 1) for it2 in range(1, p.sub + 1)]
+    X = [np.zeros(shape) for _ in range(9)]
+    Y = [np.zeros(shape) for _ in range(9)]
+    ys = []
+    for its, it2 in steps:
+        ys.append([y.copy() for y in Y])
+        Xn, _ = O.step_once(p, X, Y, med, 0, 0, np.float64)
+        for c in range(9):
+            if len(src_idx[c]):
+                v = src9[c][:, its] * f[it2 - 1] + src9[c][:, its + 1] * f[h + it2 - 1]
+                np.add.at(Xn[c].reshape(-1), src_idx[c], v)
+        X, Y = [G * y for y in Y], [G * x for x in Xn]
+    inner = (slice(FAT, -FAT),) * 3
+    cz, cx, cy = tf.cz, tf.cx, tf.cy
+
+    def D(a, axis, plus, c):
+        return (tf._dplus if plus else tf._dminus)(torch.as_tensor(a), axis, c).numpy()
+
+    grad = np.zeros((8,) + shape)
+    xi = [np.zeros(shape) for _ in range(9)]
+    eta = [np.zeros(shape) for _ in range(9)]
+    for j in range(len(steps) - 1, -1, -1):
+        its, it2 = steps[j]
+        et = [e.copy() for e in eta]
+        for c in range(9):
+            if len(rec_idx[c]):
+                v = np.asarray(drec9[c])[:, its] * f[it2] + np.asarray(drec9[c])[:, its + 1] * f[h + it2]
+                np.add.at(et[c].reshape(-1), rec_idx[c], v)
+        ge = [G * e for e in et]
+        y = ys[j]
+        dvx_dx, dvy_dy, dvz_dz = D(y[VX], 1, True, cx), D(y[VY], 0, True, cy), D(y[VZ], 2, True, cz)
+        fvx = D(y[SXX], 1, False, cx) + D(y[SXY], 0, True, cy) + D(y[SXZ], 2, True, cz)
+        fvy = D(y[SXY], 1, True, cx) + D(y[SYY], 0, False, cy) + D(y[SYZ], 2, True, cz)
+        fvz = D(y[SXZ], 1, True, cx) + D(y[SYZ], 0, True, cy) + D(y[SZZ], 2, False, cz)
+        fxy = D(y[VX], 0, False, cy) + D(y[VY], 1, False, cx)
+        fxz = D(y[VX], 2, False, cz) + D(y[VZ], 1, False, cx)
+        fyz = D(y[VZ], 0, False, cy) + D(y[VY], 2, False, cz)
+        e = [x[inner] for x in ge]
+        grad[RHOX][inner] += e[VX] * fvx
+        grad[RHOY][inner] += e[VY] * fvy
+        grad[RHOZ][inner] += e[VZ] * fvz
+        grad[L2M][inner] += e[SXX] * dvx_dx + e[SYY] * dvy_dy + e[SZZ] * dvz_dz
+        grad[LAM][inner] += e[SXX] * (dvy_dy + dvz_dz) + e[SYY] * (dvx_dx + dvz_dz) + e[SZZ] * (dvx_dx + dvy_dy)
+        grad[MUXZ][inner] += e[SXZ] * fxz
+        grad[MUXY][inner] += e[SXY] * fxy
+        grad[MUYZ][inner] += e[SYZ] * fyz
+        t, _ = O.step_once(p, [np.zeros(shape) for _ in range(9)], ge, med, 2, 0, np.float64)
+        xi, eta = ge, [G * a + b for a, b in zip(xi, t)]
+    return grad

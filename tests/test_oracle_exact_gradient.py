@@ -100,3 +100,23 @@ def test_born_gradient_against_the_exact_one(case):
                   f"{corr[0]:+.3f} {corr[1]:+.3f} {corr[2]:+.3f}, relative error {rel[0]:.3f} {rel[1]:.3f} {rel[2]:.3f}")
     assert min(stats[(0, "fixed sources")]) > 0.98
     assert stats[(1, "with source term")][1] < 0.5   # the source term dominates lambda
+
+
+def test_adjoint_recursion_equals_autograd():
+    """The hand-written adjoint recursion (per-fine-step imaging against the adjoint state, the
+    oracle's exact-transpose stepper for the transpose) gives autograd's gradient to rounding."""
+    from oracle.exact_gradient import exact_gradient_by_adjoint
+    sv, _ = survey(nts=10)
+    orc = OracleFwi(sv)
+    med = O.medium_planes(np.asarray(sv.elastic, np.float64), orc.dtw, np.float64)
+    src = orc.src_reg(med)
+    tf = TorchForward(orc.p, orc.spos, orc.rpos)
+    rng = np.random.default_rng(0)
+    w = [rng.standard_normal((len(r), orc.p.nts)) for r in tf.rec]
+    pl = torch.tensor(np.stack(med)).requires_grad_(True)
+    d = tf.forward(pl, [torch.tensor(s) for s in src])
+    sum((torch.tensor(a) * b).sum() for a, b in zip(w, d)).backward()
+    g = exact_gradient_by_adjoint(orc.p, med, src, orc.spos, orc.rpos, w)
+    e = float(np.linalg.norm(g - pl.grad.numpy()) / np.linalg.norm(pl.grad.numpy()))
+    print(f"adjoint recursion vs autograd: {e:.2e}")
+    assert e < 1e-12
